@@ -1,0 +1,109 @@
+/*
+ * Build-time knobs for compiling the reference sources as the oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This header takes the place of the reference's
+ * g2parameters.h (same names, same meaning; reference g2parameters.h:19-100)
+ * when oracle/Makefile compiles the unmodified reference .cpp files with
+ * `-Ioracle/ref_cfg -I<reference> -I-`, so every configuration is a
+ * recompile with different -D values instead of an edited copy.
+ *
+ *   GABE_N        lattice points per side             (reference :57)
+ *   GABE_L        box side in program units           (reference :58)
+ *   GABE_DT       time step                           (reference :61)
+ *   GABE_GWS      0/1 tensor perturbations            (reference :55)
+ *   GABE_MODEL    0 = shipped m^2 phi^2 + g^2 phi^2 chi^2 model
+ *                     (reference g2model.cpp, constants :44-48, B = mphi)
+ *                 1 = lambda phi^4 + g^2 phi^2 chi^2 in the reference's
+ *                     rescaling convention (oracle/ref_cfg/g2model_lphi4.cpp)
+ *   GABE_PARALLEL 0 -> one thread, deterministic rand() order (reference :53,97-100)
+ *   GABE_SEED     randseed                            (reference :56)
+ *
+ * tot_num_thrds becomes a run-time value (env GABE_REF_THREADS) so one
+ * binary can be timed with every host core.
+ */
+#include <math.h>
+
+#define fftw_flag 0
+#define gNum double
+
+#ifndef GABE_N
+#define GABE_N 64
+#endif
+#ifndef GABE_L
+#define GABE_L 20.
+#endif
+#ifndef GABE_DT
+#define GABE_DT 0.01
+#endif
+#ifndef GABE_GWS
+#define GABE_GWS 0
+#endif
+#ifndef GABE_MODEL
+#define GABE_MODEL 1
+#endif
+#ifndef GABE_PARALLEL
+#define GABE_PARALLEL 0
+#endif
+#ifndef GABE_SEED
+#define GABE_SEED 44463132
+#endif
+
+#define num_flds 2
+
+#if GABE_MODEL == 0
+/* shipped model: V = m^2 phi^2/2 + g^2 phi^2 chi^2/2, program units B = m */
+const gNum mphi = 1.e-6;
+const gNum phi0 = 0.193;
+const gNum gsq = 2.5e-7;
+const gNum f0[2] = {phi0, 0.};
+const gNum df0[2] = {-0.142231, 0.};
+const gNum rescale_B = mphi;
+#else
+/* lambda phi^4 + g^2 phi^2 chi^2, program units B = sqrt(lambda) phi0:
+ * V_pr = lam_pr phi^4/4 + gsq_pr phi^2 chi^2/2 with lam_pr = 1/phi0^2,
+ * gsq_pr = (g^2/lambda)/phi0^2. */
+const gNum lambda_phys = 9.e-14;
+const gNum g2_over_lambda = 100.;
+const gNum phi0 = 0.342;
+const gNum lam_pr = 1. / (phi0 * phi0);
+const gNum gsq_pr = g2_over_lambda / (phi0 * phi0);
+const gNum f0[2] = {phi0, 0.};
+const gNum df0[2] = {0., 0.};
+const gNum rescale_B = sqrt(lambda_phys) * phi0;
+/* names the shipped g2model.cpp would expect; unused by the lphi4 model */
+const gNum mphi = rescale_B;
+const gNum gsq = g2_over_lambda * lambda_phys;
+#endif
+
+#define parallelize GABE_PARALLEL
+int gabe_ref_threads(void);
+#define tot_num_thrds (gabe_ref_threads())
+#define calc_gws GABE_GWS
+const int randseed = GABE_SEED;
+const int N = GABE_N;
+const gNum L = GABE_L;
+const gNum starttime = 0.;
+const gNum endtime = 1.e9; /* the harness fixes the step count itself */
+const gNum dt = GABE_DT;
+#define expansion_type 1
+
+#define rand_init 1
+#define field_full_rand 1
+
+const gNum screentime = 0;
+const int slicewait = 1;
+const int slicenumber = 1;
+const int field_sliceskip = 2;
+const int specnumber = 1;
+#define field_outdim 0
+#define spec_output 1
+#define var_output 0
+
+const int nflds = num_flds;
+const gNum dx = L / ((gNum)N);
+const gNum gridsize = N * N * N;
+
+#if parallelize != 1
+#undef tot_num_thrds
+#define tot_num_thrds 1
+#endif

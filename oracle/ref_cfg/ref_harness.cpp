@@ -1,0 +1,193 @@
+/*
+ * Harness main for the reference build (replaces g2main.cpp).
+ *
+ * TEST INFRASTRUCTURE ONLY.  It owns the globals that g2main.cpp:24-40
+ * defines, allocates them as g2main.cpp:49-99 does, and then either runs the
+ * reference's own initialisation sequence (g2main.cpp:111-118: initfields,
+ * initexpansion, initfields) or loads an initial state from a dump file, and
+ * calls the reference step() a fixed number of times.  It writes binary
+ * state dumps (format in oracle/gabe_dump.h) and spectra files through the
+ * reference's own specOut(), and can time step() for the CPU baseline.
+ *
+ * Usage:
+ *   ref_<cfg> [--steps K] [--ic FILE] [--dump-prefix P] [--dump-at a,b,c]
+ *             [--spectra-at a,b,c] [--time] [--cheap-ic]
+ * Dumps go to P<step>.bin; spectra to ./slices/slices_spectra_<n>.dat.
+ * GABE_REF_THREADS sets the OpenMP thread count (default: all cores).
+ */
+#include "g2header.h"
+#include "gabe_dump.h"
+
+#include <omp.h>
+#include <string.h>
+#include <vector>
+#include <string>
+
+gNum t = starttime;
+gNum (*field)[nflds][N][N][N];
+gNum (*dfield)[nflds][N][N][N];
+gNum a[2];
+gNum adot[2];
+gNum edpot[2];
+gNum edkin[2];
+gNum edgrad[2];
+gNum edrho[2];
+#if calc_gws == 1
+gNum (*h)[12][N][N][N / 2 + 1];
+gNum (*l)[12][N][N][N / 2 + 1];
+gNum (*T_gw)[12][N][N][N / 2 + 1];
+fftw_plan plan_fft_gw;
+#endif
+
+int gabe_ref_threads(void)
+{
+    static int n = 0;
+    if (n == 0) {
+        const char *e = getenv("GABE_REF_THREADS");
+        n = e ? atoi(e) : omp_get_num_procs();
+        if (n < 1) n = 1;
+    }
+    return n;
+}
+
+static std::vector<long> parse_list(const char *s)
+{
+    std::vector<long> v;
+    while (s && *s) {
+        v.push_back(strtol(s, (char **)&s, 10));
+        if (*s == ',') s++;
+    }
+    return v;
+}
+
+static bool contains(const std::vector<long> &v, long x)
+{
+    for (long y : v) if (y == x) return true;
+    return false;
+}
+
+static void fill_header(gabe_dump_header *hd, long step)
+{
+    gabe_dump_header_init(hd, N, nflds, calc_gws, 8, GABE_MODEL);
+    hd->step = step;
+    hd->t = t;
+    hd->L = L;
+    hd->dt = dt;
+    for (int s = 0; s < 2; s++) {
+        hd->a[s] = a[s]; hd->adot[s] = adot[s];
+        hd->edkin[s] = edkin[s]; hd->edpot[s] = edpot[s];
+        hd->edgrad[s] = edgrad[s]; hd->edrho[s] = edrho[s];
+    }
+}
+
+static int write_dump(const std::string &path, long step)
+{
+    gabe_dump_header hd;
+    fill_header(&hd, step);
+    const double *arrs[4] = {&field[0][0][0][0][0], &dfield[0][0][0][0][0], NULL, NULL};
+#if calc_gws == 1
+    arrs[2] = &h[0][0][0][0][0];
+    arrs[3] = &l[0][0][0][0][0];
+#endif
+    return gabe_dump_write(path.c_str(), &hd, arrs);
+}
+
+static int read_dump(const char *path)
+{
+    gabe_dump_header hd;
+    double *arrs[4] = {&field[0][0][0][0][0], &dfield[0][0][0][0][0], NULL, NULL};
+#if calc_gws == 1
+    arrs[2] = &h[0][0][0][0][0];
+    arrs[3] = &l[0][0][0][0][0];
+#endif
+    if (gabe_dump_read(path, &hd, arrs, N, nflds, calc_gws) != 0) return 1;
+    t = hd.t;
+    for (int s = 0; s < 2; s++) {
+        a[s] = hd.a[s]; adot[s] = hd.adot[s];
+        edkin[s] = hd.edkin[s]; edpot[s] = hd.edpot[s];
+        edgrad[s] = hd.edgrad[s]; edrho[s] = hd.edrho[s];
+    }
+    return 0;
+}
+
+/* Deterministic smooth perturbation, used only to time step() at sizes where
+ * the reference's rand()-based initialisation would dominate the run. */
+static void cheap_ic(void)
+{
+    DECLARE_INDEX
+    fldLOOP {
+        double ph = 2. * M_PI * (i + 2 * j + 3 * k + 7 * fld) / (double)N;
+        field[0][fld][i][j][k] = f0[fld] + 1e-6 * sin(ph);
+        dfield[0][fld][i][j][k] = df0[fld] + 1e-6 * cos(ph);
+    }
+    a[0] = 1.;
+    calcEnergy(0);
+    adot[0] = adf(0);
+}
+
+int main(int argc, char **argv)
+{
+    long steps = 0;
+    const char *ic = NULL;
+    std::string prefix = "state_";
+    std::vector<long> dump_at, spec_at;
+    bool timing = false, cheap = false;
+    for (int i = 1; i < argc; i++) {
+        if (!strcmp(argv[i], "--steps") && i + 1 < argc) steps = atol(argv[++i]);
+        else if (!strcmp(argv[i], "--ic") && i + 1 < argc) ic = argv[++i];
+        else if (!strcmp(argv[i], "--dump-prefix") && i + 1 < argc) prefix = argv[++i];
+        else if (!strcmp(argv[i], "--dump-at") && i + 1 < argc) dump_at = parse_list(argv[++i]);
+        else if (!strcmp(argv[i], "--spectra-at") && i + 1 < argc) spec_at = parse_list(argv[++i]);
+        else if (!strcmp(argv[i], "--time")) timing = true;
+        else if (!strcmp(argv[i], "--cheap-ic")) cheap = true;
+        else { fprintf(stderr, "unknown argument %s\n", argv[i]); return 2; }
+    }
+
+    double t_alloc0 = omp_get_wtime();
+    field = (gNum(*)[nflds][N][N][N])malloc(sizeof(gNum) * nflds * 2 * (size_t)N * N * N);
+    dfield = (gNum(*)[nflds][N][N][N])malloc(sizeof(gNum) * nflds * 2 * (size_t)N * N * N);
+    if (!field || !dfield) { fprintf(stderr, "allocation failed\n"); return 3; }
+#if calc_gws == 1
+    size_t hsz = sizeof(gNum) * 2 * (size_t)(N / 2 + 1) * N * N * 12;
+    h = (gNum(*)[12][N][N][N / 2 + 1])malloc(hsz);
+    l = (gNum(*)[12][N][N][N / 2 + 1])malloc(hsz);
+    T_gw = (gNum(*)[12][N][N][N / 2 + 1])malloc(hsz);
+    if (!h || !l || !T_gw) { fprintf(stderr, "allocation failed\n"); return 3; }
+    memset(h, 0, hsz);
+    memset(l, 0, hsz);
+#endif
+    double t_init0 = omp_get_wtime();
+
+    if (ic) {
+        if (read_dump(ic) != 0) { fprintf(stderr, "cannot read %s\n", ic); return 4; }
+    } else if (cheap) {
+        cheap_ic();
+    } else {
+        initfields();
+        initexpansion();
+        initfields();
+    }
+    double t_init1 = omp_get_wtime();
+
+    int nspec = 0;
+    if (contains(dump_at, 0)) write_dump(prefix + "0.bin", 0);
+    if (contains(spec_at, 0)) specOut(nspec++);
+
+    std::vector<double> st;
+    for (long n = 1; n <= steps; n++) {
+        double s0 = omp_get_wtime();
+        step();
+        double s1 = omp_get_wtime();
+        t += dt;
+        st.push_back(s1 - s0);
+        if (contains(dump_at, n)) write_dump(prefix + std::to_string(n) + ".bin", n);
+        if (contains(spec_at, n)) specOut(nspec++);
+    }
+    if (timing) {
+        printf("{\"N\": %d, \"gws\": %d, \"threads\": %d, \"alloc_s\": %.6f, \"init_s\": %.6f, \"step_s\": [",
+               N, calc_gws, tot_num_thrds, t_init0 - t_alloc0, t_init1 - t_init0);
+        for (size_t i = 0; i < st.size(); i++) printf("%s%.6f", i ? ", " : "", st[i]);
+        printf("], \"a\": %.17g, \"adot\": %.17g, \"edrho\": %.17g}\n", a[0], adot[0], edrho[0]);
+    }
+    return 0;
+}
