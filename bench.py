@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of GABE's RK2 lattice step on B200: site-updates/s at 512^3
+with GWs on, FP32 storage (headline) next to the FP64 path.
+
+One JSON line on rank 0.  A step is one RK2 step of the full path (field
+stencil sweeps, GW sources, 12 R2C transforms, TT projection + h/l update,
+Friedmann scalars).  Each rank evolves its own lattice (independent
+replicas of the workload, weak scaling); no collective touches the data
+path, only the timing max over ranks.
+
+  value   device-resident: state uploaded before the timed region, K steps
+          bracketed by CUDA events on the library's stream.
+  e2e     the drop-in driver's use of the C ABI: upload the FP64 initial
+          state from pinned host memory, then per step gabe_step +
+          gabe_energies (the scalars slices_time.dat records), then one
+          specOut and a download of field[0]/dfield[0] -- all inside the
+          timed region.
+  --impl reference  times the reference's own CPU step() (compiled from the
+          reference sources under oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "site-updates/s FP32-storage vs FP64 RK2 at 512³+GW, ≤1e-4 energy err; HBM %"
+UNIT = "site-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--N", type=int, default=512)
+    ap.add_argument("--gws", type=int, default=1)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-N", type=int, default=256, help="lattice of the CPU reference sample")
+    ap.add_argument("--profile-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(N: int, w: int, gws: bool) -> dict:
+    """Bytes each phase must move per step (one launch each)."""
+    n3 = N ** 3
+    M = N * N * (N // 2 + 1)
+    b = {"stage1": (4 + (12 if gws else 0)) * n3 * w, "stage2": 8 * n3 * w}
+    if gws:
+        b["fft"] = 12 * (n3 + 2 * M) * w
+        b["kspace"] = 72 * M * w
+    return b
+
+
+def traffic_scaled(kernel: str, precision: str, N: int):
+    """ncu-measured DRAM bytes per launch from profiles/traffic.json, scaled
+    from the captured lattice to N by the sites processed."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as fh:
+        d = json.load(fh)
+    e = d.get(precision, {}).get(kernel)
+    if not e:
+        return None
+    return e["bytes"] * (N / e["N"]) ** 3
+
+
+def cpu_reference_sample(N: int, steps: int, warm: int = 1):
+    """Time the reference's own step() (oracle/_ref binary) with all host
+    threads on an N^3 GW-on lattice; returns (site-updates/s, info)."""
+    from oracle import pyoracle as po
+
+    threads = os.cpu_count() or 1
+    binary = po.ref_binary(1, N, 1, 1)
+    import tempfile
+
+    if os.path.exists(binary):
+        with tempfile.TemporaryDirectory() as d:
+            out = po.run_ref(binary, ["--steps", str(warm + steps), "--cheap-ic", "--time"], d, threads=threads,
+                             timeout=3600)
+        rec = json.loads(out.strip().splitlines()[-1])
+        st = rec["step_s"][warm:]
+        return N ** 3 * len(st) / sum(st), {"kind": "reference", "cores": threads, "step_s": st,
+                                            "sample": f"reference step() on a {N}^3 lattice, GWs on, L=20, dt=0.01, "
+                                                      f"lambda phi^4 g^2/lambda=100, {len(st)} timed steps after "
+                                                      f"{warm} warm-up, {threads} OpenMP threads, FFT via the "
+                                                      f"project's FFTW-API shim"}
+    # the oracle restatement (serial) if the reference binary was not built
+    Np = 32
+    cfg = po.Config(N=Np, gws=1)
+    stt = po.init_state(cfg)
+    po.step(stt, 1)
+    t0 = time.perf_counter()
+    po.step(stt, steps)
+    dt = time.perf_counter() - t0
+    return Np ** 3 * steps / dt, {"kind": "port", "cores": 1, "sample": f"oracle port, {Np}^3 GW on, {steps} steps"}
+
+
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    v, info = cpu_reference_sample(args.ref_N, args.steps, warm=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(info.get("step_s", [0])) / max(1, len(info.get("step_s", [1]))),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"GABE RK2 step, {args.ref_N}^3 lattice sample of the 512^3+GW workload",
+                   "N": args.ref_N, "gws": 1, "L": 20.0, "dt": 0.01, "model": "lambda phi^4, g^2/lambda=100"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                         "sample": info["sample"]},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+
+    import gabe_b200 as gb
+    from gabe_b200.ic import random_state
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as tdist
+
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist = tdist
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if not dist:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    N, K, W, gws = args.N, args.steps, args.warmup, bool(args.gws)
+    hbm_peak, peak_kind = peaks()
+    f, d, a0, adot0 = random_state(N, seed=44463132 + 1000 * rank, device="cuda")
+    hf = torch.empty(f.shape, dtype=torch.float64, pin_memory=True)
+    hd = torch.empty(d.shape, dtype=torch.float64, pin_memory=True)
+    hf.copy_(f)
+    hd.copy_(d)
+    of = torch.empty_like(hf, pin_memory=True)
+    od = torch.empty_like(hd, pin_memory=True)
+    del f, d
+    torch.cuda.empty_cache()
+
+    legs = {}
+    precisions = [("fp32", gb.FP32)] + ([] if args.no_fp64 else [("fp64", gb.FP64)])
+    clocks = None
+    for name, prec in precisions:
+        lat = gb.Lattice(N, gws=gws, precision=prec, device=local)
+        stream = torch.cuda.ExternalStream(lat.stream_ptr)
+        # ---- device-resident leg
+        lat.upload_ptrs(hf.data_ptr(), hd.data_ptr(), None, None, a0, adot0)
+        lat.step(W)
+        lat.sync()
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local)
+        with sampler:
+            time.sleep(0.3)
+            ev0.record(stream)
+            lat.step(K)
+            ev1.record(stream)
+            ev1.synchronize()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        if name == "fp32":
+            clocks = sampler.summary()
+        try:
+            en = lat.calc_energy()
+            finite = True
+        except gb.GabeError:
+            en, finite = None, False
+        phases = lat.profile_steps(args.profile_steps)
+        # ---- end-to-end leg through the C ABI with host buffers
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        lat.upload_ptrs(hf.data_ptr(), hd.data_ptr(), None, None, a0, adot0)
+        nonfinite_e2e = False
+        for _ in range(K):
+            lat.step(1)
+            try:
+                lat.calc_energy()
+            except gb.GabeError:
+                nonfinite_e2e = True
+        try:
+            lat.spec_out()
+        except gb.GabeError:
+            nonfinite_e2e = True
+        lat.download_ptrs(of.data_ptr(), od.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+        legs[name] = {"ms": ms, "ms_e2e": ms_e2e, "phases": phases, "energies": en, "finite": finite,
+                      "nonfinite_e2e": nonfinite_e2e, "device_bytes": lat.device_bytes,
+                      "launches_per_step": lat.launches_per_step}
+        lat.close()
+        torch.cuda.empty_cache()
+
+    sites = N ** 3
+    L32 = legs["fp32"]
+    value = world * sites * K / (L32["ms"] / 1e3)
+    e2e = world * sites * K / (L32["ms_e2e"] / 1e3)
+    w = 4
+    algo = algorithmic_bytes(N, w, gws)
+    kern = {}
+    for ph, b in algo.items():
+        t = L32["phases"][ph] / 1e3
+        kern[ph] = {"ms": L32["phases"][ph], "algorithmic_bytes": b, "achieved_gbs": b / t / 1e9 if t > 0 else None}
+    own = {k: v for k, v in kern.items() if k != "fft"}
+    dom = max(own, key=lambda k: own[k]["ms"])
+    ach = kern[dom]["achieved_gbs"]
+    step_bytes = sum(algo.values())
+    roofline = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                "traffic": traffic_scaled(dom, "fp32", N), "kernel": dom, "peak_kind": peak_kind,
+                "step_algorithmic_bytes": step_bytes,
+                "step_achieved_gbs": step_bytes / (L32["ms"] / K / 1e3) / 1e9,
+                "step_frac": step_bytes / (L32["ms"] / K / 1e3) / 1e9 / hbm_peak,
+                "kernels": kern}
+    extra = {}
+    if "fp64" in legs:
+        L64 = legs["fp64"]
+        v64 = world * sites * K / (L64["ms"] / 1e3)
+        extra["fp64"] = {"value": v64, "ms_per_step": L64["ms"] / K, "e2e": world * sites * K / (L64["ms_e2e"] / 1e3),
+                         "phases_ms": L64["phases"]}
+        extra["fp32_over_fp64"] = value / v64
+        if L32["energies"] and L64["energies"]:
+            extra["energy_rel_diff_fp32_vs_fp64"] = {
+                k: abs(L32["energies"][k] - L64["energies"][k]) / abs(L64["energies"][k])
+                for k in ("kin", "pot", "grad", "rho", "a", "adot")}
+    h2d = 2 * 2 * sites * 8 / K
+    d2h = (K * 48 + gb.numbins(N) * 8 * 8 + 2 * 2 * sites * 8) / K
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": L32["ms"] / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"GABE RK2 step, {N}^3 lattice, GWs on, FP32 storage / FP64 scalars",
+                   "N": N, "gws": int(gws), "L": 20.0, "dt": 0.01, "model": "lambda phi^4, g^2/lambda=100",
+                   "ic": "Gaussian random field with the reference's randInit distribution (torch generator)",
+                   "l2": "inputs larger than L2 (state alone is 2 GiB)"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_total": L32["ms_e2e"]},
+        "roofline": roofline,
+        "gpu_launches": K * L32["launches_per_step"],
+        "clocks": clocks,
+        "finite": L32["finite"],
+        "device_bytes": L32["device_bytes"],
+    }
+    line.update(extra)
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        v, info = cpu_reference_sample(args.ref_N, 2, warm=1)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                                "sample": info["sample"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,280 @@
+"""gabe_b200 -- B200 (sm_100a) implementation of GABE's lattice-evolution path.
+
+The product is the C-ABI library libgabe_b200.so (include/gabe.h).  This
+module is its host-side mirror for Python callers: `Lattice` wraps one
+handle and exposes the reference's operations on that path under their
+reference names and meanings --
+
+    Lattice.step()          step()            g2functions.cpp:201-304
+    Lattice.calc_energy()   calcEnergy(0)     g2functions.cpp:168-174
+    Lattice.adf()           adf(0)            g2functions.cpp:188-191
+    Lattice.spec_out()      specOut(first)    g2spectra.cpp:23-234
+    Lattice.meansvars()     meansvars()       g2output.cpp:70-121
+
+with host arrays in the reference layout (field/dfield [nflds][N][N][N],
+h/l [12][N][N][N/2+1], FP64).  There is no CPU fallback: without the built
+library or a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+__all__ = [
+    "GabeError", "Params", "Lattice", "library", "lib_path", "lphi4_constants",
+    "FP64", "FP32", "MODEL_QUADRATIC", "MODEL_LPHI4", "numbins",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(HERE, "libgabe_b200.so")
+
+FP64, FP32 = 0, 1
+MODEL_QUADRATIC, MODEL_LPHI4 = 0, 1
+FLAG_NO_GRAPH = 1
+
+STATUS = {
+    0: "GABE_OK", 1: "GABE_ERR_PARAM", 2: "GABE_ERR_CUDA", 3: "GABE_ERR_CUFFT", 4: "GABE_ERR_NOMEM",
+    5: "GABE_ERR_NONFINITE", 6: "GABE_ERR_TIMEOUT", 7: "GABE_ERR_STATE",
+}
+
+
+class GabeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("N", ctypes.c_int32), ("nflds", ctypes.c_int32),
+        ("calc_gws", ctypes.c_int32), ("expansion_type", ctypes.c_int32), ("model", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("gw_spec_quirk", ctypes.c_int32),
+        ("L", ctypes.c_double), ("dt", ctypes.c_double), ("model_c", ctypes.c_double * 2),
+        ("device", ctypes.c_int32), ("flags", ctypes.c_int32), ("tile_ci", ctypes.c_int32),
+        ("tile_shape", ctypes.c_int32), ("reserved", ctypes.c_int64 * 4),
+    ]
+
+
+_lib = None
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def lib_path() -> str:
+    return _LIB_PATH
+
+
+def library():
+    """Loads libgabe_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise RuntimeError(f"{_LIB_PATH} is missing; build it with `python -m gabe_b200.build`")
+    L = ctypes.CDLL(_LIB_PATH)
+    H = ctypes.c_void_p
+    L.gabe_default_params.argtypes = [ctypes.POINTER(Params), ctypes.c_int]
+    L.gabe_default_params.restype = None
+    L.gabe_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(H)]
+    L.gabe_destroy.argtypes = [H]
+    L.gabe_upload_state.argtypes = [H, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_double]
+    L.gabe_step.argtypes = [H, ctypes.c_int]
+    L.gabe_sync.argtypes = [H]
+    L.gabe_energies.argtypes = [H, _dp, _dp, _dp]
+    L.gabe_scalars.argtypes = [H, _dp]
+    L.gabe_download_state.argtypes = [H, _dp, _dp, _dp, _dp]
+    L.gabe_spectra_numbins.argtypes = [ctypes.c_int]
+    L.gabe_spectra.argtypes = [H, _dp, ctypes.c_int, ctypes.c_int]
+    L.gabe_spectra_raw.argtypes = [H, _dp, _dp, ctypes.c_int, ctypes.c_int]
+    L.gabe_last_error.argtypes = [H]
+    L.gabe_last_error.restype = ctypes.c_char_p
+    L.gabe_device_bytes.argtypes = [H]
+    L.gabe_device_bytes.restype = ctypes.c_size_t
+    L.gabe_launches_per_step.argtypes = [H]
+    L.gabe_profile_steps.argtypes = [H, ctypes.c_int, _dp]
+    L.gabe_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
+    _lib = L
+    return L
+
+
+def numbins(N: int) -> int:
+    return int(math.sqrt(3.0) * N / 2 + 1)
+
+
+def lphi4_constants(g2_over_lambda: float = 100.0, phi0: float = 0.342) -> tuple[float, float]:
+    """(lam_pr, gsq_pr) of V = lambda phi^4/4 + g^2 phi^2 chi^2/2 in program
+    units with B = sqrt(lambda) phi0 (the reference's rescaling,
+    g2model.cpp:12-18)."""
+    return 1.0 / (phi0 * phi0), g2_over_lambda / (phi0 * phi0)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if not (a.dtype == np.float64 and a.flags.c_contiguous):
+        raise ValueError("arrays must be C-contiguous float64")
+    return a.ctypes.data_as(_dp)
+
+
+class Lattice:
+    """One lattice on one GPU (a gabe_handle)."""
+
+    def __init__(self, N: int, *, L: float = 20.0, dt: float = 0.01, gws: bool = False,
+                 model: int = MODEL_LPHI4, model_c=None, precision: int = FP64, device: int = -1,
+                 gw_spec_quirk: bool = True, flags: int = 0, tile_ci: int = 0, tile_shape: int = -1):
+        lib = library()
+        p = Params()
+        lib.gabe_default_params(ctypes.byref(p), int(N))
+        p.L, p.dt, p.calc_gws, p.model, p.precision = float(L), float(dt), int(bool(gws)), int(model), int(precision)
+        if model_c is None:
+            model_c = lphi4_constants() if model == MODEL_LPHI4 else (1e-6, 2.5e-7)
+        p.model_c[0], p.model_c[1] = float(model_c[0]), float(model_c[1])
+        p.device, p.gw_spec_quirk, p.flags = int(device), int(bool(gw_spec_quirk)), int(flags)
+        p.tile_ci, p.tile_shape = int(tile_ci), int(tile_shape)
+        self.params = p
+        self.N, self.gws, self.precision = int(N), bool(gws), int(precision)
+        self.nz = self.N // 2 + 1
+        self._h = ctypes.c_void_p()
+        rc = lib.gabe_create(ctypes.byref(p), ctypes.byref(self._h))
+        if rc != 0:
+            msg = lib.gabe_last_error(None).decode()
+            self._h = None
+            raise GabeError(rc, msg)
+
+    # -- plumbing ---------------------------------------------------------
+    def _check(self, rc: int):
+        if rc != 0:
+            raise GabeError(rc, library().gabe_last_error(self._h).decode())
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            library().gabe_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        return library().gabe_device_bytes(self._h)
+
+    @property
+    def launches_per_step(self) -> int:
+        return library().gabe_launches_per_step(self._h)
+
+    # -- state ------------------------------------------------------------
+    def upload_state(self, field0, dfield0, h0=None, l0=None, *, a0: float = 1.0, adot0: float):
+        N = self.N
+        f = np.ascontiguousarray(field0, dtype=np.float64).reshape(2, N, N, N)
+        d = np.ascontiguousarray(dfield0, dtype=np.float64).reshape(2, N, N, N)
+        hh = ll = None
+        if self.gws:
+            if h0 is not None:
+                hh = np.ascontiguousarray(h0, dtype=np.float64).reshape(12, N, N, self.nz)
+            if l0 is not None:
+                ll = np.ascontiguousarray(l0, dtype=np.float64).reshape(12, N, N, self.nz)
+        self._check(library().gabe_upload_state(self._h, _ptr(f), _ptr(d), _ptr(hh), _ptr(ll), a0, adot0))
+
+    def upload_ptrs(self, field0: int, dfield0: int, h0: int | None, l0: int | None, a0: float, adot0: float):
+        """Upload from raw host addresses (e.g. pinned buffers)."""
+        c = lambda v: ctypes.cast(ctypes.c_void_p(v), _dp) if v else None
+        self._check(library().gabe_upload_state(self._h, c(field0), c(dfield0), c(h0), c(l0), a0, adot0))
+
+    def download_state(self, want_gw: bool = True):
+        N = self.N
+        f = np.empty((2, N, N, N))
+        d = np.empty((2, N, N, N))
+        hh = ll = None
+        if self.gws and want_gw:
+            hh = np.empty((12, N, N, self.nz))
+            ll = np.empty((12, N, N, self.nz))
+        self._check(library().gabe_download_state(self._h, _ptr(f), _ptr(d), _ptr(hh), _ptr(ll)))
+        return f, d, hh, ll
+
+    def download_ptrs(self, field0: int, dfield0: int, h0: int | None = None, l0: int | None = None):
+        c = lambda v: ctypes.cast(ctypes.c_void_p(v), _dp) if v else None
+        self._check(library().gabe_download_state(self._h, c(field0), c(dfield0), c(h0), c(l0)))
+
+    # -- hot path ---------------------------------------------------------
+    def step(self, n: int = 1):
+        self._check(library().gabe_step(self._h, int(n)))
+
+    def profile_steps(self, n: int) -> dict:
+        """Mean ms per step of each phase (direct launches with CUDA events)."""
+        out = (ctypes.c_double * 4)()
+        self._check(library().gabe_profile_steps(self._h, int(n), out))
+        return {"stage1": out[0], "fft": out[1], "kspace": out[2], "stage2": out[3]}
+
+    @property
+    def stream_ptr(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(library().gabe_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    def sync(self):
+        self._check(library().gabe_sync(self._h))
+
+    def calc_energy(self) -> dict:
+        e = (ctypes.c_double * 4)()
+        a = ctypes.c_double()
+        ad = ctypes.c_double()
+        self._check(library().gabe_energies(self._h, e, ctypes.byref(a), ctypes.byref(ad)))
+        return {"kin": e[0], "pot": e[1], "grad": e[2], "rho": e[3], "a": a.value, "adot": ad.value}
+
+    energies = calc_energy
+
+    def adf(self) -> float:
+        return self.calc_energy()["adot"]
+
+    def scalars(self) -> dict:
+        out = (ctypes.c_double * 12)()
+        self._check(library().gabe_scalars(self._h, out))
+        names = ("a", "adot", "edkin", "edpot", "edgrad", "edrho")
+        return {n: (out[2 * i], out[2 * i + 1]) for i, n in enumerate(names)}
+
+    # -- analysis ---------------------------------------------------------
+    def spec_out(self) -> np.ndarray:
+        nb = numbins(self.N)
+        nc = 8 if self.gws else 5
+        out = np.zeros((nb, nc))
+        self._check(library().gabe_spectra(self._h, _ptr(out), nb, nc))
+        return out
+
+    spectra = spec_out
+
+    def spectra_raw(self):
+        nb = numbins(self.N)
+        ns = 3 if self.gws else 2
+        sums = np.zeros((ns, nb))
+        cnt = np.zeros(nb)
+        self._check(library().gabe_spectra_raw(self._h, _ptr(sums), _ptr(cnt), nb, ns))
+        return sums, cnt
+
+    def meansvars(self) -> np.ndarray:
+        """Mean and variance of each field (meansvars, g2output.cpp:70-121),
+        from a downloaded state: rows (mean, var) per field.  Raises
+        GabeError(GABE_ERR_NONFINITE) where the reference would exit(1)."""
+        f, _, _, _ = self.download_state(want_gw=False)
+        out = np.zeros((2, 2))
+        for q in range(2):
+            av = f[q].mean()
+            var = (f[q] * f[q] - av * av).mean()
+            if av != 0.0 and not np.isfinite(av):
+                raise GabeError(5, f"unstable solution: field {q} not numerical")
+            out[q] = (av, var)
+        return out

@@ -1,0 +1,730 @@
+// C ABI of the B200 lattice-evolution library (include/gabe.h).
+//
+// One handle = one lattice on one GPU with one stream.  Device buffers are
+// allocated once in gabe_create; a step is captured once into a CUDA graph
+// per ping-pong parity and replayed by gabe_step.  cuFFT plans use a work
+// area this file allocates, so nothing is allocated after creation.
+#include <cufft.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gabe.h"
+#include "launch.h"
+
+using namespace gabe;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr int kBinBlocks = 296;  // 2 x 148 SMs
+
+}  // namespace
+
+struct gabe_handle {
+    gabe_params p{};
+    int dev = 0;
+    bool f32 = false;
+    int N = 0, nz = 0;
+    size_t n3 = 0, M = 0, esz = 8;
+    cudaStream_t stream = nullptr;
+    void *X[2] = {nullptr, nullptr}, *D[2] = {nullptr, nullptr};
+    void *H = nullptr, *L = nullptr;
+    void *S = nullptr;  // sources / spectra scratch / staging
+    size_t S_bytes = 0;
+    int nslots = 0;
+    double *partials = nullptr;
+    size_t npartials = 0;
+    unsigned int *counters = nullptr;
+    DevScalars *sc = nullptr;
+    double *bin_part = nullptr, *bin_sum = nullptr;
+    unsigned int *bin_cnt_part = nullptr;
+    int nbins = 0;
+    cufftHandle plan_src = 0, plan_spec = 0;
+    bool have_plan_src = false, have_plan_spec = false;
+    void *fft_work = nullptr;
+    size_t fft_work_bytes = 0;
+    LatticeConsts lc{};
+    dim3 tile;
+    int ci = 0;
+    dim3 grid;
+    size_t smem1 = 0, smem2 = 0;
+    int cur = 0;
+    bool uploaded = false;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_tried = false, graph_ok = false;
+    size_t dev_bytes = 0;
+    std::string err;
+};
+
+namespace {
+
+int set_err(gabe_handle *h, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf;
+    else g_create_error = buf;
+    return code;
+}
+
+#define CK(h, x)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (x);                                                                      \
+        if (e_ != cudaSuccess) return set_err(h, GABE_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+#define CF(h, x)                                                                                   \
+    do {                                                                                           \
+        cufftResult r_ = (x);                                                                      \
+        if (r_ != CUFFT_SUCCESS) return set_err(h, GABE_ERR_CUFFT, "%s: cufft error %d", #x, (int)r_); \
+    } while (0)
+
+int dalloc(gabe_handle *h, void **ptr, size_t bytes) {
+    if (bytes == 0) bytes = 256;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        cudaGetLastError();
+        return set_err(h, GABE_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    h->dev_bytes += bytes;
+    return GABE_OK;
+}
+
+// Constants with the operation sequence the reference's compiler folds
+// (g2parameters.h:93, g2functions.cpp:41, g2evolutionpert.cpp:53,198,486-487,
+// g2model.cpp:64,68).
+LatticeConsts make_consts(const gabe_params &p) {
+    LatticeConsts c{};
+    c.N = p.N;
+    c.model = p.model;
+    const double L = p.L, dt = p.dt;
+    const double dx = L / ((double)p.N);
+    c.dt = dt;
+    c.half_dt = .5 * dt;
+    c.inv_dx2_div = dx * dx;
+    c.dn = (double)(1 / (dx * dx));
+    c.c13 = (1. / 3.) * c.dn;
+    c.c23 = (2. / 3.) * c.dn;
+    if (p.model == GABE_MODEL_QUADRATIC) {
+        const double mphi = p.model_c[0], gsq = p.model_c[1];
+        c.mc[0] = gsq / mphi / mphi;
+        c.mc[1] = 0.5 * gsq / mphi / mphi;
+    } else {
+        const double lam = p.model_c[0], g = p.model_c[1];
+        c.mc[0] = lam;
+        c.mc[1] = g;
+        c.mc[2] = 0.25 * lam;
+        c.mc[3] = 0.5 * g;
+        c.mc[4] = 3. * lam;
+    }
+    c.gridsize = (double)((long long)p.N * p.N * p.N);
+    c.eight_pi_3 = 8. * M_PI / 3.;
+    c.k2norm_c = 4. * M_PI * M_PI / L / L;
+    c.eight_pi = 8. * M_PI;
+    c.normmm = pow(dx, 3);
+    return c;
+}
+
+void choose_tile(gabe_handle *h) {
+    const int N = h->N;
+    int TK = 32;
+    while (TK > 1 && (TK > N || N % TK)) TK /= 2;
+    int TJ = 8;
+    while (TJ > 1 && (TJ > N || N % TJ)) TJ /= 2;
+    static const int shapes[][2] = {{32, 8}, {32, 4}, {16, 16}, {16, 8}, {32, 2}, {64, 4}};
+    if (h->p.tile_shape >= 0 && h->p.tile_shape < (int)(sizeof(shapes) / sizeof(shapes[0]))) {
+        const int tk = shapes[h->p.tile_shape][0], tj = shapes[h->p.tile_shape][1];
+        if (tk <= N && tj <= N && N % tk == 0 && N % tj == 0) { TK = tk; TJ = tj; }
+    }
+    const int bxy = (N / TK) * (N / TJ);
+    int ci = h->p.tile_ci > 0 ? h->p.tile_ci : N;
+    if (h->p.tile_ci <= 0)
+        while (ci > 4 && (long long)bxy * ((N + ci - 1) / ci) < 8 * 148) ci /= 2;
+    if (ci > N) ci = N;
+    h->tile = dim3(TK, TJ, 1);
+    h->ci = ci;
+    h->grid = dim3(N / TK, N / TJ, (N + ci - 1) / ci);
+    const size_t P1 = (size_t)(TK + 2) * (TJ + 2), P2 = (size_t)(TK + 4) * (TJ + 4);
+    h->smem1 = 12 * P1 * h->esz;
+    h->smem2 = (8 * P2 + 12 * P1) * h->esz;
+}
+
+int make_plans(gabe_handle *h) {
+    const long long N = h->N, nz = h->nz;
+    long long n[3] = {N, N, N};
+    size_t ws_src = 0, ws_spec = 0;
+    const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
+    if (h->p.calc_gws) {
+        long long inem[3] = {N, N, 2 * nz}, onem[3] = {N, N, nz};
+        CF(h, cufftCreate(&h->plan_src));
+        h->have_plan_src = true;
+        CF(h, cufftSetAutoAllocation(h->plan_src, 0));
+        CF(h, cufftMakePlanMany64(h->plan_src, 3, n, inem, 1, N * N * 2 * nz, onem, 1, N * N * nz, t, 12, &ws_src));
+    }
+    {
+        long long inem[3] = {N, N, N}, onem[3] = {N, N, nz};
+        CF(h, cufftCreate(&h->plan_spec));
+        h->have_plan_spec = true;
+        CF(h, cufftSetAutoAllocation(h->plan_spec, 0));
+        CF(h, cufftMakePlanMany64(h->plan_spec, 3, n, inem, 1, N * N * N, onem, 1, N * N * nz, t, 2, &ws_spec));
+    }
+    h->fft_work_bytes = ws_src > ws_spec ? ws_src : ws_spec;
+    int rc = dalloc(h, &h->fft_work, h->fft_work_bytes);
+    if (rc) return rc;
+    if (h->have_plan_src) {
+        CF(h, cufftSetWorkArea(h->plan_src, h->fft_work));
+        CF(h, cufftSetStream(h->plan_src, h->stream));
+    }
+    CF(h, cufftSetWorkArea(h->plan_spec, h->fft_work));
+    CF(h, cufftSetStream(h->plan_spec, h->stream));
+    return GABE_OK;
+}
+
+int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
+    if (h->f32) CF(h, cufftExecR2C(plan, (cufftReal *)in, (cufftComplex *)out));
+    else CF(h, cufftExecD2Z(plan, (cufftDoubleReal *)in, (cufftDoubleComplex *)out));
+    return GABE_OK;
+}
+
+StencilArgs stencil_args(gabe_handle *h, int cur) {
+    StencilArgs a{};
+    a.X = h->X[cur];
+    a.D = h->D[cur];
+    a.Xo = h->X[1 - cur];
+    a.Do = h->D[1 - cur];
+    a.S = h->S;
+    a.partials = h->partials;
+    a.sc = h->sc;
+    a.c = h->lc;
+    a.ci = h->ci;
+    a.gws = h->p.calc_gws;
+    return a;
+}
+
+// Enqueues one step reading buffer `cur` and writing buffer 1-cur.  With
+// `ev` (5 events) the phase boundaries stage1 | FFT | kspace | stage2 are
+// recorded for gabe_profile_steps.
+int enqueue_step(gabe_handle *h, int cur, cudaEvent_t *ev = nullptr) {
+    StencilArgs a = stencil_args(h, cur);
+    a.counter = h->counters + 0;
+    Launch l1{h->grid, h->tile, h->smem1, h->stream};
+    if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
+    CK(h, h->f32 ? stage1_f32(a, l1) : stage1_f64(a, l1));
+    if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
+    if (h->p.calc_gws) {
+        int rc = fft_r2c(h, h->plan_src, h->S, h->S);
+        if (rc) return rc;
+        if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
+        KspaceArgs k{};
+        k.S = h->S;
+        k.h = h->H;
+        k.l = h->L;
+        k.sc = h->sc;
+        k.c = h->lc;
+        Launch lk{dim3(148 * 8), dim3(256), 0, h->stream};
+        CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
+    } else if (ev) {
+        CK(h, cudaEventRecord(ev[2], h->stream));
+    }
+    if (ev) CK(h, cudaEventRecord(ev[3], h->stream));
+    a.counter = h->counters + 1;
+    Launch l2{h->grid, h->tile, h->smem2, h->stream};
+    CK(h, h->f32 ? stage2_f32(a, l2) : stage2_f64(a, l2));
+    if (ev) CK(h, cudaEventRecord(ev[4], h->stream));
+    return GABE_OK;
+}
+
+int build_graphs(gabe_handle *h) {
+    h->graph_tried = true;
+    if (h->p.flags & GABE_FLAG_NO_GRAPH) return GABE_OK;
+    for (int par = 0; par < 2; par++) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return GABE_OK;
+        }
+        int rc = enqueue_step(h, par);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (rc != GABE_OK || e != cudaSuccess || !g) {
+            cudaGetLastError();
+            if (g) cudaGraphDestroy(g);
+            h->err.clear();
+            return GABE_OK;  // fall back to direct launches
+        }
+        e = cudaGraphInstantiate(&h->graph[par], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            h->graph[par] = nullptr;
+            return GABE_OK;
+        }
+    }
+    h->graph_ok = true;
+    return GABE_OK;
+}
+
+int read_scalars(gabe_handle *h, DevScalars *out) {
+    CK(h, cudaStreamSynchronize(h->stream));
+    CK(h, cudaMemcpy(out, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
+    if (out->status & ST_NONFINITE)
+        return set_err(h, GABE_ERR_NONFINITE, "non-finite energy density at step %lld", out->step);
+    return GABE_OK;
+}
+
+// Device address of fbar[f] / dfbar[f] inside the scalar block.
+double *dev_mean(gabe_handle *h, bool momentum, int f) {
+    const size_t off = momentum ? offsetof(DevScalars, dfbar) : offsetof(DevScalars, fbar);
+    return reinterpret_cast<double *>(reinterpret_cast<char *>(h->sc) + off) + f;
+}
+
+int mean_blocks(size_t n) {
+    size_t b = (n + 255) / 256;
+    return (int)(b < 592 ? (b ? b : 1) : 592);
+}
+
+}  // namespace
+
+extern "C" {
+
+void gabe_default_params(gabe_params *p, int N) {
+    std::memset(p, 0, sizeof(*p));
+    p->struct_size = (int32_t)sizeof(gabe_params);
+    p->N = N;
+    p->nflds = 2;
+    p->calc_gws = 0;
+    p->expansion_type = 1;
+    p->model = GABE_MODEL_LPHI4;
+    p->precision = GABE_FP64;
+    p->gw_spec_quirk = 1;
+    p->L = 20.;
+    p->dt = 0.01;
+    const double phi0 = 0.342;
+    p->model_c[0] = 1. / (phi0 * phi0);
+    p->model_c[1] = 100. / (phi0 * phi0);
+    p->device = -1;
+    p->flags = 0;
+    p->tile_ci = 0;
+    p->tile_shape = -1;
+}
+
+int gabe_create(const gabe_params *p, gabe_handle **out) {
+    if (!out) return set_err(nullptr, GABE_ERR_PARAM, "out is NULL");
+    *out = nullptr;
+    if (!p) return set_err(nullptr, GABE_ERR_PARAM, "params is NULL");
+    if (p->struct_size != (int32_t)sizeof(gabe_params))
+        return set_err(nullptr, GABE_ERR_PARAM, "struct_size %d != %zu", p->struct_size, sizeof(gabe_params));
+    if (p->N < 4 || p->N > 1290 || (p->N & 1))
+        return set_err(nullptr, GABE_ERR_PARAM, "N must be even and in [4, 1290], got %d", p->N);
+    if (p->nflds != 2) return set_err(nullptr, GABE_ERR_PARAM, "nflds must be 2, got %d", p->nflds);
+    if (p->expansion_type != 1)
+        return set_err(nullptr, GABE_ERR_PARAM, "only expansion_type 1 is implemented, got %d", p->expansion_type);
+    if (p->calc_gws != 0 && p->calc_gws != 1) return set_err(nullptr, GABE_ERR_PARAM, "calc_gws must be 0 or 1");
+    if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4)
+        return set_err(nullptr, GABE_ERR_PARAM, "unknown model %d", p->model);
+    if (p->precision != GABE_FP64 && p->precision != GABE_FP32)
+        return set_err(nullptr, GABE_ERR_PARAM, "unknown precision %d", p->precision);
+    if (!(p->L > 0) || !(p->dt > 0) || !std::isfinite(p->L) || !std::isfinite(p->dt))
+        return set_err(nullptr, GABE_ERR_PARAM, "L and dt must be positive and finite");
+    if (!std::isfinite(p->model_c[0]) || !std::isfinite(p->model_c[1]) ||
+        (p->model == GABE_MODEL_QUADRATIC && p->model_c[0] == 0.0))
+        return set_err(nullptr, GABE_ERR_PARAM, "invalid model constants");
+
+    gabe_handle *h = new (std::nothrow) gabe_handle();
+    if (!h) return set_err(nullptr, GABE_ERR_NOMEM, "host allocation failed");
+    h->p = *p;
+    int rc = GABE_OK;
+    auto bail = [&](int code) {
+        g_create_error = h->err;
+        gabe_destroy(h);
+        return code;
+    };
+    if (p->device >= 0) {
+        if (cudaSetDevice(p->device) != cudaSuccess) {
+            cudaGetLastError();
+            set_err(h, GABE_ERR_CUDA, "cudaSetDevice(%d) failed", p->device);
+            return bail(GABE_ERR_CUDA);
+        }
+    }
+    if (cudaGetDevice(&h->dev) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(h, GABE_ERR_CUDA, "no CUDA device");
+        return bail(GABE_ERR_CUDA);
+    }
+    h->f32 = p->precision == GABE_FP32;
+    h->esz = h->f32 ? 4 : 8;
+    h->N = p->N;
+    h->nz = p->N / 2 + 1;
+    h->n3 = (size_t)p->N * p->N * p->N;
+    h->M = (size_t)p->N * p->N * h->nz;
+    h->lc = make_consts(*p);
+    choose_tile(h);
+    h->nbins = gabe_spectra_numbins(p->N);
+
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(h, GABE_ERR_CUDA, "cudaStreamCreate failed");
+        return bail(GABE_ERR_CUDA);
+    }
+    size_t max_smem = h->smem2 > h->smem1 ? h->smem2 : h->smem1;
+    const size_t bin_smem = (size_t)h->nbins * (3 * 8 + 4);
+    if (bin_smem > max_smem) max_smem = bin_smem;
+    if ((h->f32 ? configure_f32(max_smem) : configure_f64(max_smem)) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(h, GABE_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes shared) failed", max_smem);
+        return bail(GABE_ERR_CUDA);
+    }
+    const size_t field_bytes = 2 * h->n3 * h->esz;
+    for (int b = 0; b < 2; b++) {
+        if ((rc = dalloc(h, &h->X[b], field_bytes))) return bail(rc);
+        if ((rc = dalloc(h, &h->D[b], field_bytes))) return bail(rc);
+    }
+    if (p->calc_gws) {
+        if ((rc = dalloc(h, &h->H, 12 * h->M * h->esz))) return bail(rc);
+        if ((rc = dalloc(h, &h->L, 12 * h->M * h->esz))) return bail(rc);
+    }
+    // sources need 12 padded slots; spectra need 2; the FP32 upload stages one FP64 field array
+    h->nslots = p->calc_gws ? 12 : 2;
+    h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
+    if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
+    const size_t nblk_stencil = (size_t)h->grid.x * h->grid.y * h->grid.z;
+    h->npartials = 3 * (nblk_stencil > 4096 ? nblk_stencil : 4096);
+    if ((rc = dalloc(h, (void **)&h->partials, h->npartials * sizeof(double)))) return bail(rc);
+    if ((rc = dalloc(h, (void **)&h->counters, 8 * sizeof(unsigned int)))) return bail(rc);
+    if ((rc = dalloc(h, (void **)&h->sc, sizeof(DevScalars)))) return bail(rc);
+    if ((rc = dalloc(h, (void **)&h->bin_part, (size_t)kBinBlocks * 3 * h->nbins * sizeof(double)))) return bail(rc);
+    if ((rc = dalloc(h, (void **)&h->bin_cnt_part, (size_t)kBinBlocks * h->nbins * sizeof(unsigned int))))
+        return bail(rc);
+    if ((rc = dalloc(h, (void **)&h->bin_sum, (size_t)4 * h->nbins * sizeof(double)))) return bail(rc);
+    if (cudaMemset(h->counters, 0, 8 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMemset(h->sc, 0, sizeof(DevScalars)) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(h, GABE_ERR_CUDA, "cudaMemset failed");
+        return bail(GABE_ERR_CUDA);
+    }
+    if ((rc = make_plans(h))) return bail(rc);
+    *out = h;
+    return GABE_OK;
+}
+
+int gabe_destroy(gabe_handle *h) {
+    if (!h) return GABE_OK;
+    cudaSetDevice(h->dev);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int i = 0; i < 2; i++)
+        if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
+    if (h->have_plan_src) cufftDestroy(h->plan_src);
+    if (h->have_plan_spec) cufftDestroy(h->plan_spec);
+    void *bufs[] = {h->X[0], h->X[1], h->D[0], h->D[1], h->H, h->L, h->S, h->partials, h->counters,
+                    h->sc, h->bin_part, h->bin_cnt_part, h->bin_sum, h->fft_work};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    cudaGetLastError();
+    delete h;
+    return GABE_OK;
+}
+
+int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield0, const double *h0,
+                      const double *l0, double a0, double adot0) {
+    if (!h) return GABE_ERR_PARAM;
+    if (!field0 || !dfield0) return set_err(h, GABE_ERR_PARAM, "field0/dfield0 must not be NULL");
+    if (!(a0 > 0) || !std::isfinite(a0) || !std::isfinite(adot0))
+        return set_err(h, GABE_ERR_PARAM, "a0 must be positive and finite");
+    CK(h, cudaSetDevice(h->dev));
+    h->err.clear();
+    DevScalars s{};
+    s.a[0] = a0;
+    s.adot[0] = adot0;
+    CK(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+    const size_t nf = h->n3;
+    if (!h->f32) {
+        CK(h, cudaMemcpyAsync(h->X[0], field0, 2 * nf * 8, cudaMemcpyHostToDevice, h->stream));
+        CK(h, cudaMemcpyAsync(h->D[0], dfield0, 2 * nf * 8, cudaMemcpyHostToDevice, h->stream));
+        if (h->p.calc_gws) {
+            if (h0) CK(h, cudaMemcpyAsync(h->H, h0, 12 * h->M * 8, cudaMemcpyHostToDevice, h->stream));
+            else CK(h, cudaMemsetAsync(h->H, 0, 12 * h->M * 8, h->stream));
+            if (l0) CK(h, cudaMemcpyAsync(h->L, l0, 12 * h->M * 8, cudaMemcpyHostToDevice, h->stream));
+            else CK(h, cudaMemsetAsync(h->L, 0, 12 * h->M * 8, h->stream));
+        }
+    } else {
+        // each field array: stage in S as FP64, take its mean, store float fluctuations
+        double *stage = static_cast<double *>(h->S);
+        const double *src[2] = {field0, dfield0};
+        void *dst[2] = {h->X[0], h->D[0]};
+        for (int a = 0; a < 2; a++)
+            for (int f = 0; f < 2; f++) {
+                double *mean = dev_mean(h, a != 0, f);
+                CK(h, cudaMemcpyAsync(stage, src[a] + f * nf, nf * 8, cudaMemcpyHostToDevice, h->stream));
+                CK(h, mean_f64(stage, nf, h->partials, h->counters + 3, mean, mean_blocks(nf), h->stream));
+                CK(h, to_fluct(stage, nf, mean, static_cast<float *>(dst[a]) + f * nf, h->stream));
+            }
+        if (h->p.calc_gws) {
+            const double *gsrc[2] = {h0, l0};
+            void *gdst[2] = {h->H, h->L};
+            const size_t chunk = h->S_bytes / 8;
+            for (int a = 0; a < 2; a++) {
+                if (!gsrc[a]) {
+                    CK(h, cudaMemsetAsync(gdst[a], 0, 12 * h->M * 4, h->stream));
+                    continue;
+                }
+                for (size_t off = 0; off < 12 * h->M; off += chunk) {
+                    const size_t n = (12 * h->M - off) < chunk ? (12 * h->M - off) : chunk;
+                    CK(h, cudaMemcpyAsync(stage, gsrc[a] + off, n * 8, cudaMemcpyHostToDevice, h->stream));
+                    CK(h, to_fluct(stage, n, nullptr, static_cast<float *>(gdst[a]) + off, h->stream));
+                }
+            }
+        }
+    }
+    h->cur = 0;
+    EnergyArgs e{};
+    e.X = h->X[0];
+    e.D = h->D[0];
+    e.partials = h->partials;
+    e.counter = h->counters + 2;
+    e.sc = h->sc;
+    e.c = h->lc;
+    size_t nb = (h->n3 + 255) / 256;
+    Launch le{dim3((unsigned)(nb < 4096 ? nb : 4096)), dim3(256), 0, h->stream};
+    CK(h, h->f32 ? energy0_f32(e, le) : energy0_f64(e, le));
+    DevScalars chk;
+    int rc = read_scalars(h, &chk);
+    if (rc) return rc;
+    h->uploaded = true;
+    return GABE_OK;
+}
+
+int gabe_step(gabe_handle *h, int nsteps) {
+    if (!h) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "gabe_step before gabe_upload_state");
+    if (nsteps < 0) return set_err(h, GABE_ERR_PARAM, "nsteps < 0");
+    CK(h, cudaSetDevice(h->dev));
+    if (!h->graph_tried) {
+        int rc = build_graphs(h);
+        if (rc) return rc;
+    }
+    for (int s = 0; s < nsteps; s++) {
+        if (h->graph_ok) {
+            CK(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
+        } else {
+            int rc = enqueue_step(h, h->cur);
+            if (rc) return rc;
+        }
+        h->cur ^= 1;
+    }
+    return GABE_OK;
+}
+
+int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]) {
+    if (!h || !ms_out || nsteps < 1) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "profile before upload");
+    CK(h, cudaSetDevice(h->dev));
+    std::vector<cudaEvent_t> ev((size_t)5 * nsteps);
+    for (auto &e : ev) CK(h, cudaEventCreate(&e));
+    int rc = GABE_OK;
+    for (int s = 0; s < nsteps && rc == GABE_OK; s++) {
+        rc = enqueue_step(h, h->cur, ev.data() + 5 * s);
+        h->cur ^= 1;
+    }
+    double acc[4] = {0, 0, 0, 0};
+    if (rc == GABE_OK && cudaStreamSynchronize(h->stream) == cudaSuccess) {
+        for (int s = 0; s < nsteps; s++)
+            for (int q = 0; q < 4; q++) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[5 * s + q], ev[5 * s + q + 1]);
+                acc[q] += ms;
+            }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    for (int q = 0; q < 4; q++) ms_out[q] = acc[q] / nsteps;
+    DevScalars sc;
+    return read_scalars(h, &sc);
+}
+
+int gabe_stream(gabe_handle *h, void **stream) {
+    if (!h || !stream) return GABE_ERR_PARAM;
+    *stream = (void *)h->stream;
+    return GABE_OK;
+}
+
+int gabe_sync(gabe_handle *h) {
+    if (!h) return GABE_ERR_PARAM;
+    CK(h, cudaSetDevice(h->dev));
+    DevScalars s;
+    return read_scalars(h, &s);
+}
+
+int gabe_energies(gabe_handle *h, double out4[4], double *a, double *adot) {
+    if (!h) return GABE_ERR_PARAM;
+    CK(h, cudaSetDevice(h->dev));
+    DevScalars s;
+    int rc = read_scalars(h, &s);
+    if (out4) {
+        out4[0] = s.edkin[0];
+        out4[1] = s.edpot[0];
+        out4[2] = s.edgrad[0];
+        out4[3] = s.edrho[0];
+    }
+    if (a) *a = s.a[0];
+    if (adot) *adot = s.adot[0];
+    return rc;
+}
+
+int gabe_scalars(gabe_handle *h, double out12[12]) {
+    if (!h || !out12) return GABE_ERR_PARAM;
+    CK(h, cudaSetDevice(h->dev));
+    DevScalars s;
+    int rc = read_scalars(h, &s);
+    const double *src[6] = {s.a, s.adot, s.edkin, s.edpot, s.edgrad, s.edrho};
+    for (int q = 0; q < 6; q++) {
+        out12[2 * q] = src[q][0];
+        out12[2 * q + 1] = src[q][1];
+    }
+    return rc;
+}
+
+int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double *h0, double *l0) {
+    if (!h) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "download before upload");
+    CK(h, cudaSetDevice(h->dev));
+    const size_t nf = h->n3;
+    const int c = h->cur;
+    if (!h->f32) {
+        if (field0) CK(h, cudaMemcpyAsync(field0, h->X[c], 2 * nf * 8, cudaMemcpyDeviceToHost, h->stream));
+        if (dfield0) CK(h, cudaMemcpyAsync(dfield0, h->D[c], 2 * nf * 8, cudaMemcpyDeviceToHost, h->stream));
+        if (h->p.calc_gws) {
+            if (h0) CK(h, cudaMemcpyAsync(h0, h->H, 12 * h->M * 8, cudaMemcpyDeviceToHost, h->stream));
+            if (l0) CK(h, cudaMemcpyAsync(l0, h->L, 12 * h->M * 8, cudaMemcpyDeviceToHost, h->stream));
+        }
+    } else {
+        double *stage = static_cast<double *>(h->S);
+        double *dst[2] = {field0, dfield0};
+        const void *src[2] = {h->X[c], h->D[c]};
+        for (int a = 0; a < 2; a++) {
+            if (!dst[a]) continue;
+            for (int f = 0; f < 2; f++) {
+                const double *mean = dev_mean(h, a != 0, f);
+                CK(h, from_fluct(static_cast<const float *>(src[a]) + f * nf, nf, mean, stage, h->stream));
+                CK(h, cudaMemcpyAsync(dst[a] + f * nf, stage, nf * 8, cudaMemcpyDeviceToHost, h->stream));
+            }
+        }
+        if (h->p.calc_gws) {
+            double *gdst[2] = {h0, l0};
+            const void *gsrc[2] = {h->H, h->L};
+            const size_t chunk = h->S_bytes / 8;
+            for (int a = 0; a < 2; a++) {
+                if (!gdst[a]) continue;
+                for (size_t off = 0; off < 12 * h->M; off += chunk) {
+                    const size_t n = (12 * h->M - off) < chunk ? (12 * h->M - off) : chunk;
+                    CK(h, from_fluct(static_cast<const float *>(gsrc[a]) + off, n, nullptr, stage, h->stream));
+                    CK(h, cudaMemcpyAsync(gdst[a] + off, stage, n * 8, cudaMemcpyDeviceToHost, h->stream));
+                }
+            }
+        }
+    }
+    CK(h, cudaStreamSynchronize(h->stream));
+    return GABE_OK;
+}
+
+int gabe_spectra_numbins(int N) { return ((int)(sqrt(3.) * N / 2 + 1)); }
+
+int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries) {
+    if (!h) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "spectra before upload");
+    const int ns = 2 + (h->p.calc_gws ? 1 : 0);
+    if (nbins != h->nbins || nseries != ns)
+        return set_err(h, GABE_ERR_PARAM, "spectra_raw wants nbins=%d nseries=%d", h->nbins, ns);
+    CK(h, cudaSetDevice(h->dev));
+    DevScalars s;
+    int rc = read_scalars(h, &s);
+    if (rc) return rc;
+    rc = fft_r2c(h, h->plan_spec, h->X[h->cur], h->S);
+    if (rc) return rc;
+    BinArgs b{};
+    b.F = h->S;
+    b.l = h->L;
+    b.part_sum = h->bin_part;
+    b.part_cnt = h->bin_cnt_part;
+    b.N = h->N;
+    b.nbins = h->nbins;
+    b.nseries = ns;
+    b.quirk = h->p.gw_spec_quirk;
+    b.fix_zero = h->f32 ? 1 : 0;
+    b.zero_re[0] = h->lc.gridsize * s.fbar[0];
+    b.zero_re[1] = h->lc.gridsize * s.fbar[1];
+    const size_t smem = (size_t)h->nbins * (ns * 8 + 4);
+    Launch lb{dim3(kBinBlocks), dim3(256), smem, h->stream};
+    CK(h, h->f32 ? bins_f32(b, lb) : bins_f64(b, lb));
+    double *dsum = h->bin_sum, *dcnt = h->bin_sum + 3 * h->nbins;
+    CK(h, bin_reduce(h->bin_part, h->bin_cnt_part, kBinBlocks, ns, h->nbins, dsum, dcnt, h->stream));
+    CK(h, cudaMemcpyAsync(sums, dsum, (size_t)ns * h->nbins * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaMemcpyAsync(counts, dcnt, (size_t)h->nbins * 8, cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    return GABE_OK;
+}
+
+int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols) {
+    if (!h || !out) return GABE_ERR_PARAM;
+    const int gws = h->p.calc_gws;
+    const int want = 5 + (gws ? 3 : 0);
+    if (nbins != h->nbins || ncols != want)
+        return set_err(h, GABE_ERR_PARAM, "spectra wants nbins=%d ncols=%d", h->nbins, want);
+    const int ns = 2 + gws;
+    std::vector<double> sums((size_t)ns * nbins), cnt(nbins);
+    int rc = gabe_spectra_raw(h, sums.data(), cnt.data(), nbins, ns);
+    if (rc) return rc;
+    DevScalars s;
+    rc = read_scalars(h, &s);
+    if (rc) return rc;
+    // normalisation of g2spectra.cpp:27,94-103,114-117,186-195
+    const double L = h->p.L;
+    const int N = h->N;
+    const double spec_norm = pow(L / (double)N, 6.) * pow(2. * M_PI / L, 3.);
+    const double hub = sqrt(8. * M_PI / 3.) * sqrt(s.edrho[0]);
+    const double dp = 2. * M_PI / (double)L;
+    const double norm1 = 4.e-5 / pow(100., .333) / 24. / M_PI / M_PI / pow(L, 3.) / (hub * hub);
+    for (int b = 0; b < nbins; b++) {
+        double *row = out + (size_t)b * ncols;
+        row[0] = 2. * M_PI * b / L;
+        for (int f = 0; f < 2; f++) {
+            const double pw = sums[(size_t)f * nbins + b], np = cnt[b];
+            if (np > 0) {
+                row[1 + 2 * f] = pw * spec_norm / np;
+                row[2 + 2 * f] = pow((double)b * 2. * M_PI / L, 3) * pw * spec_norm / np / 2. / M_PI / M_PI;
+            } else {
+                row[1 + 2 * f] = 0.;
+                row[2 + 2 * f] = 0.;
+            }
+        }
+        if (gws) {
+            const double pw = sums[(size_t)2 * nbins + b], np = cnt[b];
+            if (np > 0) {
+                row[5] = pw * spec_norm / np;
+                row[6] = norm1 * pow((double)b * 2 * M_PI / L, 3.) * pw / np;
+            } else {
+                row[5] = 0.;
+                row[6] = 0.;
+            }
+            row[7] = dp * (double)b;
+        }
+    }
+    return GABE_OK;
+}
+
+const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
+
+int gabe_launches_per_step(const gabe_handle *h) { return h ? (h->p.calc_gws ? 3 : 2) : 0; }
+
+}  // extern "C"

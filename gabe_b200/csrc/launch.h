@@ -1,0 +1,45 @@
+// Host-side launch entry points of the precision-specific kernel units.
+// kernels_f64.cu is compiled without FMA contraction so that the FP64 path
+// rounds every operation as the reference's x86-64 build does;
+// kernels_f32.cu is compiled with contraction on.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "energy.cuh"
+#include "kspace.cuh"
+#include "spectra.cuh"
+#include "stencil.cuh"
+
+namespace gabe {
+
+struct Launch {
+    dim3 grid, block;
+    size_t smem;
+    cudaStream_t stream;
+};
+
+cudaError_t configure_f64(size_t max_smem);
+cudaError_t configure_f32(size_t max_smem);
+
+cudaError_t stage1_f64(const StencilArgs &a, const Launch &l);
+cudaError_t stage2_f64(const StencilArgs &a, const Launch &l);
+cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l);
+cudaError_t energy0_f64(const EnergyArgs &a, const Launch &l);
+cudaError_t bins_f64(const BinArgs &a, const Launch &l);
+
+cudaError_t stage1_f32(const StencilArgs &a, const Launch &l);
+cudaError_t stage2_f32(const StencilArgs &a, const Launch &l);
+cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);
+cudaError_t energy0_f32(const EnergyArgs &a, const Launch &l);
+cudaError_t bins_f32(const BinArgs &a, const Launch &l);
+
+cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *counter, double *out, int nblocks,
+                     cudaStream_t s);
+cudaError_t to_fluct(const double *x, size_t n, const double *mean, float *out, cudaStream_t s);
+cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out, cudaStream_t s);
+
+cudaError_t bin_reduce(const double *part_sum, const unsigned int *part_cnt, int nblocks, int nseries, int nbins,
+                       double *sum, double *cnt, cudaStream_t s);
+
+}  // namespace gabe

@@ -1,0 +1,163 @@
+/*
+ * gabe.h -- C ABI of the B200 (sm_100a) lattice-evolution library.
+ *
+ * The reference (GABE) has no plugin or FFI layer: its driver calls C++
+ * functions that read and write global arrays.  This header is the boundary
+ * that replaces the bodies of those functions:
+ *
+ *   reference call (file:line)                  replaced by
+ *   ------------------------------------------  ---------------------------------
+ *   step()             g2functions.cpp:201-304  gabe_step
+ *     called from      g2main.cpp:126
+ *   calcEnergy(0)      g2functions.cpp:168-174  gabe_upload_state (computes the
+ *     called from      g2model.cpp:141,          stage-0 energies of the uploaded
+ *                      g2init.cpp:28             state), gabe_energies
+ *   adf(0)             g2functions.cpp:188-191  gabe_energies (adot)
+ *   specOut(first)     g2spectra.cpp:23-234     gabe_spectra
+ *     called from      g2output.cpp:161
+ *   evolve_perts()     g2evolutionpert.cpp:343  inside gabe_step (calc_gws)
+ *   globals field, dfield, a, adot, ed[kin,pot,  gabe_upload_state /
+ *                      grad,rho], h, l (g2header.h:52-63,171-174)   gabe_download_state / gabe_scalars
+ *
+ * Conventions: every call returns an int status (GABE_OK == 0); the library
+ * never exits the process.  Host arrays use the reference layout and FP64
+ * whatever the device precision: field/dfield [nflds][N][N][N] (k fastest,
+ * g2main.cpp:49,99), h/l [12][N][N][N/2+1] with the 12 components ordered as
+ * (re,im) of 11,12,13,22,23,33 (g2evolutionpert.cpp:216-310).  A handle is
+ * used from one host thread at a time and owns one CUDA stream; gabe_step
+ * only enqueues work, calls that return data synchronise.
+ */
+#ifndef GABE_H
+#define GABE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GABE_ABI_VERSION 1
+
+enum gabe_status {
+    GABE_OK = 0,
+    GABE_ERR_PARAM = 1,     /* invalid or unsupported parameter */
+    GABE_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    GABE_ERR_CUFFT = 3,     /* a cuFFT call failed */
+    GABE_ERR_NOMEM = 4,     /* device allocation failed */
+    GABE_ERR_NONFINITE = 5, /* NaN/Inf in the energies (the reference's meansvars abort, g2output.cpp:106-117) */
+    GABE_ERR_TIMEOUT = 6,   /* a bounded device wait gave up */
+    GABE_ERR_STATE = 7      /* call out of order (e.g. step before upload) */
+};
+
+enum gabe_precision {
+    GABE_FP64 = 0, /* reference arithmetic, operation order kept */
+    GABE_FP32 = 1  /* FP32 storage of fluctuations about an FP64 homogeneous
+                      trajectory; FP64 scalars and reductions */
+};
+
+enum gabe_model {
+    GABE_MODEL_QUADRATIC = 0, /* V = phi^2/2 + (g^2/m^2) phi^2 chi^2/2 (g2model.cpp:66-87);
+                                 model_c = {mphi, gsq} */
+    GABE_MODEL_LPHI4 = 1      /* V = lam phi^4/4 + g phi^2 chi^2/2 in program units;
+                                 model_c = {lam_pr, gsq_pr} */
+};
+
+enum gabe_flags {
+    GABE_FLAG_NO_GRAPH = 1 /* launch kernels one by one instead of replaying a CUDA graph */
+};
+
+/* Run-time form of the g2parameters.h knobs that the hot path reads. */
+typedef struct {
+    int32_t struct_size;    /* sizeof(gabe_params) */
+    int32_t N;              /* points per side (g2parameters.h:57) */
+    int32_t nflds;          /* must be 2 (g2parameters.h:43) */
+    int32_t calc_gws;       /* 0/1 (g2parameters.h:55) */
+    int32_t expansion_type; /* must be 1 (g2parameters.h:62) */
+    int32_t model;          /* enum gabe_model */
+    int32_t precision;      /* enum gabe_precision */
+    int32_t gw_spec_quirk;  /* 1: GW spectrum reads l at kz=N/2 for the kz=0 plane, as g2spectra.cpp:149-164 does */
+    double L;               /* box side (g2parameters.h:58) */
+    double dt;              /* time step (g2parameters.h:61) */
+    double model_c[2];      /* see enum gabe_model */
+    int32_t device;         /* CUDA device ordinal, -1 = current */
+    int32_t flags;          /* enum gabe_flags */
+    int32_t tile_ci;        /* planes per stencil block along i, 0 = autotuned/default */
+    int32_t tile_shape;     /* stencil tile shape id, -1 = autotuned/default */
+    int64_t reserved[4];
+} gabe_params;
+
+typedef struct gabe_handle gabe_handle;
+
+/* Fills p with the reference's defaults for an N^3 lattice (L=20, dt=0.01,
+ * lambda phi^4 model with g^2/lambda=100, phi0=0.342, FP64, GWs off). */
+void gabe_default_params(gabe_params *p, int N);
+
+/* Creates a handle and allocates every device buffer.  *out is NULL on error. */
+int gabe_create(const gabe_params *p, gabe_handle **out);
+int gabe_destroy(gabe_handle *h);
+
+/* Copies stage 0 of the state to the device: field0/dfield0 [nflds][N^3],
+ * h0/l0 [12][N][N][N/2+1] (NULL = zero; ignored without GWs).  a0/adot0 are
+ * taken as given -- after the reference's initialisation adot[0] belongs to
+ * the homogeneous state (g2init.cpp:29) -- and the stage-0 energies are
+ * recomputed on the device as calcEnergy(0) would. */
+int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield0,
+                      const double *h0, const double *l0, double a0, double adot0);
+
+/* Enqueues nsteps RK2 steps (step(), g2functions.cpp:234-271). */
+int gabe_step(gabe_handle *h, int nsteps);
+
+/* Runs nsteps steps with direct launches and CUDA events between phases and
+ * returns the mean milliseconds per step of {stage-1 sweep, source FFTs,
+ * k-space update, stage-2 sweep} (FFT and k-space are 0 without GWs).  The
+ * state advances by nsteps.  Measurement hook; no reference counterpart. */
+int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]);
+
+/* The handle's CUDA stream (a cudaStream_t), so callers can order their own
+ * work or events after queued steps.  No reference counterpart. */
+int gabe_stream(gabe_handle *h, void **stream);
+
+/* Waits for queued work; returns the first error seen on the device. */
+int gabe_sync(gabe_handle *h);
+
+/* Stage-0 energies {kin, pot, grad, rho} and a, adot (synchronises). */
+int gabe_energies(gabe_handle *h, double out4[4], double *a, double *adot);
+
+/* All per-stage scalars as the reference keeps them: a[2], adot[2],
+ * edkin[2], edpot[2], edgrad[2], edrho[2] (12 doubles, synchronises). */
+int gabe_scalars(gabe_handle *h, double out12[12]);
+
+/* Copies stage 0 back to the host; any pointer may be NULL. */
+int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double *h0, double *l0);
+
+/* Number of native |k| bins, (int)(sqrt(3) N/2 + 1) (g2spectra.cpp:31). */
+int gabe_spectra_numbins(int N);
+
+/* specOut of the current state: out is nbins x ncols, row-major, columns
+ * k, P_phi, D2_phi, P_chi, D2_chi [, P_gw, Omega_gw, p] exactly as written to
+ * slices_spectra_<n>.dat (g2spectra.cpp:208-230).  ncols must be 5, or 8 with
+ * GWs; nbins must equal gabe_spectra_numbins(N). */
+int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols);
+
+/* Per-bin sums and counts behind gabe_spectra (weighted power sums before
+ * normalisation): sums is nseries x nbins, series-major, with nseries =
+ * nflds + calc_gws (phi, chi[, GW]); counts has nbins entries.  Callers can
+ * rebin these exactly (e.g. into log-spaced |k| bins). */
+int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries);
+
+/* Message for the last error on this handle ("" if none).  NULL handle ->
+ * message of the last failed gabe_create in this thread. */
+const char *gabe_last_error(const gabe_handle *h);
+
+/* Device bytes held by the handle. */
+size_t gabe_device_bytes(const gabe_handle *h);
+
+/* Kernel launches one step enqueues (for launch accounting). */
+int gabe_launches_per_step(const gabe_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

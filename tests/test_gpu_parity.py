@@ -1,0 +1,282 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle.
+
+The oracle (oracle/gabe_oracle.c) reproduces the reference build bit for
+bit (tests/test_oracle_golden.py); here the GPU library evolves the same
+initial states and is compared with it:
+
+  FP64  fields and momenta pointwise to <= 1e-10 relative (the GPU keeps the
+        reference's operation order; only reduction order differs), h and l
+        to <= 1e-10 in norm (cuFFT vs the oracle's FFT differ at rounding
+        level), scalars to <= 1e-12, spectra to <= 1e-10 per bin.
+  FP32  energies, a(t) and spectra against the FP64 path (<= 1e-4 energy).
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import gabe_b200 as gb
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _lattice(cfg: po.Config, precision=gb.FP64, **kw):
+    c0, c1, *_ = po.model_constants(cfg.model)
+    return gb.Lattice(cfg.N, L=cfg.L, dt=cfg.dt, gws=bool(cfg.gws), model=cfg.model, model_c=(c0, c1),
+                      precision=precision, gw_spec_quirk=bool(cfg.gw_spec_quirk), **kw)
+
+
+def _upload(lat: gb.Lattice, st: po.State):
+    lat.upload_state(st.field[0], st.dfield[0], st.h[0] if st.cfg.gws else None,
+                     st.l[0] if st.cfg.gws else None, a0=st.sc.a[0], adot0=st.sc.adot[0])
+
+
+def _pointwise_rel(got, want):
+    """max over points of |got-want| / (|want| + rms(want))."""
+    scale = np.abs(want) + np.sqrt(np.mean(want * want))
+    return float(np.max(np.abs(got - want) / scale))
+
+
+def _norm_rel(got, want):
+    n = np.linalg.norm(want)
+    return float(np.linalg.norm(got - want) / n) if n > 0 else float(np.abs(got).max())
+
+
+CASES = [
+    # model, N, gws, steps
+    (po.MODEL_LPHI4, 16, 1, 50),
+    (po.MODEL_QUADRATIC, 32, 1, 20),
+    (po.MODEL_LPHI4, 32, 0, 200),
+    (po.MODEL_LPHI4, 48, 1, 10),
+    (po.MODEL_LPHI4, 8, 1, 30),
+    (po.MODEL_LPHI4, 64, 0, 200),
+]
+
+
+@pytest.mark.parametrize("model,N,gws,steps", CASES)
+def test_fp64_matches_oracle(model, N, gws, steps):
+    cfg = po.Config(N=N, model=model, gws=gws)
+    st = po.init_state(cfg)
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        e0 = lat.calc_energy()
+        for k in ("kin", "pot", "grad", "rho"):
+            want = {"kin": st.sc.edkin[0], "pot": st.sc.edpot[0], "grad": st.sc.edgrad[0], "rho": st.sc.edrho[0]}[k]
+            assert abs(e0[k] - want) <= 1e-12 * abs(want) + 1e-300, (k, e0[k], want)
+        done = 0
+        for chunk in (1, steps - 1):
+            lat.step(chunk)
+            po.step(st, chunk)
+            done += chunk
+            f, d, h, l = lat.download_state()
+            assert _pointwise_rel(f, st.field[0]) <= 1e-10, done
+            assert _pointwise_rel(d, st.dfield[0]) <= 1e-10, done
+            if gws:
+                assert _norm_rel(h, st.h[0]) <= 1e-10, done
+                assert _norm_rel(l, st.l[0]) <= 1e-10, done
+            sc = lat.scalars()
+            for k in ("a", "adot", "edkin", "edpot", "edgrad", "edrho"):
+                for s in (0, 1):
+                    want = getattr(st.sc, k)[s]
+                    assert abs(sc[k][s] - want) <= 1e-12 * abs(want), (k, s, sc[k][s], want)
+
+
+def test_fp64_from_reference_dump():
+    """Start from the state the reference itself wrote after 10 steps."""
+    d = np.load(os.path.join(HERE, "golden", "ref_m1_n16_g1_step10.npz"))
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=1)
+    st = po.State.empty(cfg)
+    st.field[0], st.dfield[0], st.h[0], st.l[0] = d["field"], d["dfield"], d["h"], d["l"]
+    for q, k in enumerate(("a", "adot", "edkin", "edpot", "edgrad", "edrho")):
+        getattr(st.sc, k)[0], getattr(st.sc, k)[1] = d["scalars"][q]
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        lat.step(40)
+        po.step(st, 40)
+        f, dd, h, l = lat.download_state()
+        assert _pointwise_rel(f, st.field[0]) <= 1e-10
+        assert _pointwise_rel(dd, st.dfield[0]) <= 1e-10
+        assert _norm_rel(l, st.l[0]) <= 1e-10
+
+
+@pytest.mark.parametrize("gws", [0, 1])
+def test_fp64_spectra_match_oracle(gws):
+    cfg = po.Config(N=32, model=po.MODEL_LPHI4, gws=gws)
+    st = po.init_state(cfg)
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        lat.step(25)
+        po.step(st, 25)
+        got = lat.spec_out()
+        want = po.spectra(cfg, st.field[0], st.l[0] if gws else None, st.sc.edrho[0])
+        assert got.shape == want.shape
+        np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-300)
+
+
+def test_gw_spectrum_quirk_switch():
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=1, gw_spec_quirk=0)
+    st = po.init_state(cfg)
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        lat.step(10)
+        po.step(st, 10)
+        got = lat.spec_out()
+        want = po.spectra(cfg, st.field[0], st.l[0], st.sc.edrho[0])
+        np.testing.assert_allclose(got, want, rtol=1e-10, atol=1e-300)
+
+
+def test_config1_64cubed_1000_steps():
+    """64^3, L=20, dt=0.01, GWs off, 1000 steps: pointwise to 200 steps, then
+    a(t), energies and binned spectra within 1%."""
+    cfg = po.Config(N=64, model=po.MODEL_LPHI4, gws=0)
+    st = po.init_state(cfg)
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        lat.step(200)
+        po.step(st, 200)
+        f, d, _, _ = lat.download_state()
+        assert _pointwise_rel(f, st.field[0]) <= 1e-10
+        lat.step(800)
+        po.step(st, 800)
+        sc = lat.scalars()
+        for k in ("a", "adot", "edkin", "edpot", "edgrad", "edrho"):
+            assert abs(sc[k][0] - getattr(st.sc, k)[0]) <= 1e-2 * abs(getattr(st.sc, k)[0]), k
+        got = lat.spec_out()
+        want = po.spectra(cfg, st.field[0], None, st.sc.edrho[0])
+        m = want[:, 1] > 0
+        assert np.max(np.abs(got[m, 1:] - want[m, 1:]) / np.abs(want[m, 1:])) <= 1e-2
+
+
+def test_graph_and_direct_launches_agree():
+    cfg = po.Config(N=32, model=po.MODEL_LPHI4, gws=1)
+    st = po.init_state(cfg)
+    out = []
+    for flags in (0, gb.FLAG_NO_GRAPH):
+        with _lattice(cfg, flags=flags) as lat:
+            _upload(lat, st)
+            lat.step(7)
+            out.append(lat.download_state())
+    for a, b in zip(out[0], out[1]):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("precision", [gb.FP64, gb.FP32])
+def test_tile_shapes_and_chunks_agree(precision):
+    cfg = po.Config(N=32, model=po.MODEL_LPHI4, gws=1)
+    st = po.init_state(cfg)
+    res = []
+    for shape, ci in ((-1, 0), (2, 3), (3, 32), (1, 5)):
+        with _lattice(cfg, precision=precision, tile_shape=shape, tile_ci=ci) as lat:
+            _upload(lat, st)
+            lat.step(5)
+            res.append(lat.download_state())
+    tol = 1e-14 if precision == gb.FP64 else 1e-6
+    for r in res[1:]:
+        for a, b in zip(res[0], r):
+            assert _norm_rel(b, a) <= tol
+
+
+def test_runs_are_deterministic():
+    cfg = po.Config(N=32, model=po.MODEL_LPHI4, gws=1)
+    st = po.init_state(cfg)
+    out = []
+    for _ in range(2):
+        with _lattice(cfg) as lat:
+            _upload(lat, st)
+            lat.step(6)
+            out.append((lat.download_state(), lat.scalars()))
+    for a, b in zip(out[0][0], out[1][0]):
+        np.testing.assert_array_equal(a, b)
+    assert out[0][1] == out[1][1]
+
+
+@pytest.mark.parametrize("gws", [0, 1])
+def test_fp32_against_fp64(gws):
+    """FP32 storage of fluctuations vs the FP64 path: energies <= 1e-4."""
+    N, steps = 32, 200
+    cfg = po.Config(N=N, model=po.MODEL_LPHI4, gws=gws)
+    st = po.init_state(cfg)
+    with _lattice(cfg, precision=gb.FP64) as l64, _lattice(cfg, precision=gb.FP32) as l32:
+        _upload(l64, st)
+        _upload(l32, st)
+        e64, e32 = l64.calc_energy(), l32.calc_energy()
+        for k in ("kin", "pot", "grad", "rho"):
+            assert abs(e32[k] - e64[k]) <= 1e-6 * abs(e64[k]), (k, e32[k], e64[k])
+        l64.step(steps)
+        l32.step(steps)
+        e64, e32 = l64.calc_energy(), l32.calc_energy()
+        for k in ("kin", "pot", "rho", "a", "adot"):
+            assert abs(e32[k] - e64[k]) <= 1e-4 * abs(e64[k]), (k, e32[k], e64[k])
+        assert abs(e32["grad"] - e64["grad"]) <= 1e-4 * abs(e64["grad"]) + 1e-6 * e64["rho"]
+        f64, d64, h64, ll64 = l64.download_state()
+        f32, d32, h32, ll32 = l32.download_state()
+        for q in range(2):
+            fl = f64[q] - f64[q].mean()
+            assert np.abs((f32[q] - f32[q].mean()) - fl).max() <= 1e-3 * np.abs(fl).max()
+        s64, s32 = l64.spec_out(), l32.spec_out()
+        m = s64[:, 1] > 0
+        assert np.max(np.abs(s32[m, 1:5] - s64[m, 1:5]) / np.abs(s64[m, 1:5])) <= 1e-3
+        if gws:
+            assert _norm_rel(ll32, ll64) <= 1e-3
+
+
+def test_upload_download_roundtrip():
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=1)
+    st = po.init_state(cfg)
+    st.l[0] = np.random.default_rng(0).standard_normal(st.l[0].shape) * 1e-9
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        f, d, h, l = lat.download_state()
+        np.testing.assert_array_equal(f, st.field[0])
+        np.testing.assert_array_equal(l, st.l[0])
+    with _lattice(cfg, precision=gb.FP32) as lat:
+        _upload(lat, st)
+        f, d, h, l = lat.download_state()
+        for q in range(2):
+            fl = st.field[0, q] - st.field[0, q].mean()
+            assert np.abs(f[q] - st.field[0, q]).max() <= 1e-6 * np.abs(fl).max() + 1e-15
+        assert np.abs(l - st.l[0]).max() <= 1e-6 * np.abs(st.l[0]).max()
+
+
+def test_nonfinite_state_is_reported():
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=0)
+    st = po.init_state(cfg)
+    st.field[0, 1, 3, 4, 5] = np.nan
+    with _lattice(cfg) as lat:
+        with pytest.raises(gb.GabeError) as ei:
+            _upload(lat, st)
+        assert ei.value.code == 5
+
+
+def test_blowup_during_steps_is_reported():
+    # an absurd time step makes the stencil diverge within a few steps
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=0, dt=5.0)
+    st = po.init_state(cfg)
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        lat.step(400)
+        with pytest.raises(gb.GabeError) as ei:
+            lat.sync()
+        assert ei.value.code == 5
+
+
+def test_step_before_upload_is_an_error():
+    cfg = po.Config(N=16)
+    with _lattice(cfg) as lat:
+        with pytest.raises(gb.GabeError) as ei:
+            lat.step(1)
+        assert ei.value.code == 7
+
+
+def test_meansvars_matches_numpy():
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=0)
+    st = po.init_state(cfg)
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        mv = lat.meansvars()
+    for q in range(2):
+        av = st.field[0, q].mean()
+        assert abs(mv[q, 0] - av) <= 1e-15 + 1e-13 * abs(av)

@@ -1,0 +1,86 @@
+"""The oracle restatement against the reference's own outputs.
+
+tests/golden was written by running the reference sources compiled as-is
+(tests/golden/make_golden.py); the oracle must reproduce them bit for bit
+(same IC from srand/rand, same step arithmetic) and match the reference's
+spectra files to their printed precision (%e, 7 significant digits)."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+CASES = ["m1_n16_g1", "m0_n32_g1", "m1_n32_g0", "m1_n64_g0", "m1_n64_g1"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference_bitwise(golden, name):
+    g = golden["cases"][name]
+    cfg = po.Config(N=g["N"], model=g["model"], gws=g["gws"])
+    st = po.init_state(cfg, seed=golden["seed"])
+    steps = sorted(int(s) for s in g["steps"])
+    prev = 0
+    for s in steps:
+        po.step(st, s - prev)
+        prev = s
+        ref = g["steps"][str(s)]
+        assert sha(st.field[0]) == ref["field"], f"field differs at step {s}"
+        assert sha(st.dfield[0]) == ref["dfield"], f"dfield differs at step {s}"
+        if cfg.gws:
+            assert sha(st.h[0]) == ref["h"], f"h differs at step {s}"
+            assert sha(st.l[0]) == ref["l"], f"l differs at step {s}"
+        for k, v in ref["scalars"].items():
+            got = [float(getattr(st.sc, k)[q]) for q in (0, 1)]
+            want = [float.fromhex(x) for x in v]
+            if s == 0:  # stage-1 slots are untouched globals before the first step
+                got, want = got[:1], want[:1]
+            assert got == want, (k, s, got, want)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_spectra_match_reference_files(golden, name):
+    g = golden["cases"][name]
+    cfg = po.Config(N=g["N"], model=g["model"], gws=g["gws"])
+    st = po.init_state(cfg, seed=golden["seed"])
+    prev = 0
+    for s in sorted(int(x) for x in g["spectra"]):
+        po.step(st, s - prev)
+        prev = s
+        ref = np.array(g["spectra"][str(s)])
+        got = po.spectra(cfg, st.field[0], st.l[0] if cfg.gws else None, st.sc.edrho[0])
+        assert got.shape == ref.shape
+        # the reference prints %e: 7 significant digits
+        np.testing.assert_allclose(got, ref, rtol=6e-7, atol=0)
+
+
+def test_full_state_fixture_roundtrip():
+    d = np.load(os.path.join(HERE, "golden", "ref_m1_n16_g1_step10.npz"))
+    cfg = po.Config(N=16, model=1, gws=1)
+    st = po.init_state(cfg)
+    po.step(st, 10)
+    np.testing.assert_array_equal(st.field[0], d["field"])
+    np.testing.assert_array_equal(st.dfield[0], d["dfield"])
+    np.testing.assert_array_equal(st.h[0], d["h"])
+    np.testing.assert_array_equal(st.l[0], d["l"])
+
+
+def test_dump_format_roundtrip(tmp_path):
+    cfg = po.Config(N=8, model=1, gws=1)
+    st = po.init_state(cfg)
+    po.step(st, 3)
+    p = tmp_path / "s.bin"
+    po.write_dump(str(p), st)
+    back = po.read_dump(str(p))
+    np.testing.assert_array_equal(back.field[0], st.field[0])
+    np.testing.assert_array_equal(back.l[0], st.l[0])
+    assert back.scalars(0) == st.scalars(0)
+    assert back.step == 3
