@@ -52,12 +52,12 @@ struct gabe_handle {
     void *fft_work = nullptr;
     size_t fft_work_bytes = 0;
     LatticeConsts lc{};
-    dim3 tile;
+    int shape = 0;
     int ci = 0;
     dim3 grid;
-    size_t smem1 = 0, smem2 = 0;
     int cur = 0;
     bool uploaded = false;
+    bool e0_stale = false;  // stage-0 energies/adot of the current state not yet reduced
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_tried = false, graph_ok = false;
     size_t dev_bytes = 0;
@@ -135,28 +135,26 @@ LatticeConsts make_consts(const gabe_params &p) {
     return c;
 }
 
+bool shape_fits(int shape, int N) {
+    const int tk = kShapes[shape][0], tj = kShapes[shape][1];
+    return tk <= N && tj <= N && N % tk == 0 && N % tj == 0;
+}
+
 void choose_tile(gabe_handle *h) {
     const int N = h->N;
-    int TK = 32;
-    while (TK > 1 && (TK > N || N % TK)) TK /= 2;
-    int TJ = 8;
-    while (TJ > 1 && (TJ > N || N % TJ)) TJ /= 2;
-    static const int shapes[][2] = {{32, 8}, {32, 4}, {16, 16}, {16, 8}, {32, 2}, {64, 4}};
-    if (h->p.tile_shape >= 0 && h->p.tile_shape < (int)(sizeof(shapes) / sizeof(shapes[0]))) {
-        const int tk = shapes[h->p.tile_shape][0], tj = shapes[h->p.tile_shape][1];
-        if (tk <= N && tj <= N && N % tk == 0 && N % tj == 0) { TK = tk; TJ = tj; }
-    }
+    int shape = -1;
+    if (h->p.tile_shape >= 0 && h->p.tile_shape < kNumShapes && shape_fits(h->p.tile_shape, N)) shape = h->p.tile_shape;
+    for (int q = 0; shape < 0 && q < kNumShapes; q++)
+        if (shape_fits(q, N)) shape = q;
+    const int TK = kShapes[shape][0], TJ = kShapes[shape][1];
     const int bxy = (N / TK) * (N / TJ);
     int ci = h->p.tile_ci > 0 ? h->p.tile_ci : N;
     if (h->p.tile_ci <= 0)
         while (ci > 4 && (long long)bxy * ((N + ci - 1) / ci) < 8 * 148) ci /= 2;
     if (ci > N) ci = N;
-    h->tile = dim3(TK, TJ, 1);
+    h->shape = shape;
     h->ci = ci;
     h->grid = dim3(N / TK, N / TJ, (N + ci - 1) / ci);
-    const size_t P1 = (size_t)(TK + 2) * (TJ + 2), P2 = (size_t)(TK + 4) * (TJ + 4);
-    h->smem1 = 12 * P1 * h->esz;
-    h->smem2 = (8 * P2 + 12 * P1) * h->esz;
 }
 
 int make_plans(gabe_handle *h) {
@@ -207,22 +205,26 @@ StencilArgs stencil_args(gabe_handle *h, int cur) {
     a.sc = h->sc;
     a.c = h->lc;
     a.ci = h->ci;
-    a.gws = h->p.calc_gws;
     return a;
 }
 
+int sweep(gabe_handle *h, int mode, int cur, int counter) {
+    StencilArgs a = stencil_args(h, cur);
+    a.counter = h->counters + counter;
+    CK(h, h->f32 ? sweep_f32(h->shape, mode, a, h->grid, h->stream) : sweep_f64(h->shape, mode, a, h->grid, h->stream));
+    return GABE_OK;
+}
+
 // Enqueues one step reading buffer `cur` and writing buffer 1-cur.  With
-// `ev` (5 events) the phase boundaries stage1 | FFT | kspace | stage2 are
+// `ev` (5 events) the phase boundaries sweep A | FFT | k-space | sweep B are
 // recorded for gabe_profile_steps.
 int enqueue_step(gabe_handle *h, int cur, cudaEvent_t *ev = nullptr) {
-    StencilArgs a = stencil_args(h, cur);
-    a.counter = h->counters + 0;
-    Launch l1{h->grid, h->tile, h->smem1, h->stream};
     if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
-    CK(h, h->f32 ? stage1_f32(a, l1) : stage1_f64(a, l1));
+    int rc = sweep(h, h->p.calc_gws ? MODE_A_GW : MODE_A, cur, 0);
+    if (rc) return rc;
     if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
     if (h->p.calc_gws) {
-        int rc = fft_r2c(h, h->plan_src, h->S, h->S);
+        rc = fft_r2c(h, h->plan_src, h->S, h->S);
         if (rc) return rc;
         if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
         KspaceArgs k{};
@@ -237,9 +239,8 @@ int enqueue_step(gabe_handle *h, int cur, cudaEvent_t *ev = nullptr) {
         CK(h, cudaEventRecord(ev[2], h->stream));
     }
     if (ev) CK(h, cudaEventRecord(ev[3], h->stream));
-    a.counter = h->counters + 1;
-    Launch l2{h->grid, h->tile, h->smem2, h->stream};
-    CK(h, h->f32 ? stage2_f32(a, l2) : stage2_f64(a, l2));
+    rc = sweep(h, MODE_B, cur, 1);
+    if (rc) return rc;
     if (ev) CK(h, cudaEventRecord(ev[4], h->stream));
     return GABE_OK;
 }
@@ -274,6 +275,11 @@ int build_graphs(gabe_handle *h) {
 }
 
 int read_scalars(gabe_handle *h, DevScalars *out) {
+    if (h->e0_stale) {
+        int rc = sweep(h, MODE_E0, h->cur, 2);
+        if (rc) return rc;
+        h->e0_stale = false;
+    }
     CK(h, cudaStreamSynchronize(h->stream));
     CK(h, cudaMemcpy(out, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
     if (out->status & ST_NONFINITE)
@@ -375,12 +381,10 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
         set_err(h, GABE_ERR_CUDA, "cudaStreamCreate failed");
         return bail(GABE_ERR_CUDA);
     }
-    size_t max_smem = h->smem2 > h->smem1 ? h->smem2 : h->smem1;
     const size_t bin_smem = (size_t)h->nbins * (3 * 8 + 4);
-    if (bin_smem > max_smem) max_smem = bin_smem;
-    if ((h->f32 ? configure_f32(max_smem) : configure_f64(max_smem)) != cudaSuccess) {
+    if (bin_smem > 48 * 1024 && configure_bins(bin_smem) != cudaSuccess) {
         cudaGetLastError();
-        set_err(h, GABE_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes shared) failed", max_smem);
+        set_err(h, GABE_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes shared) failed", bin_smem);
         return bail(GABE_ERR_CUDA);
     }
     const size_t field_bytes = 2 * h->n3 * h->esz;
@@ -397,7 +401,7 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
     const size_t nblk_stencil = (size_t)h->grid.x * h->grid.y * h->grid.z;
-    h->npartials = 3 * (nblk_stencil > 4096 ? nblk_stencil : 4096);
+    h->npartials = kNV * (nblk_stencil > 4096 ? nblk_stencil : 4096);
     if ((rc = dalloc(h, (void **)&h->partials, h->npartials * sizeof(double)))) return bail(rc);
     if ((rc = dalloc(h, (void **)&h->counters, 8 * sizeof(unsigned int)))) return bail(rc);
     if ((rc = dalloc(h, (void **)&h->sc, sizeof(DevScalars)))) return bail(rc);
@@ -445,6 +449,7 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
     DevScalars s{};
     s.a[0] = a0;
     s.adot[0] = adot0;
+    s.adot_given = 1;
     CK(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
     const size_t nf = h->n3;
     if (!h->f32) {
@@ -486,16 +491,7 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
         }
     }
     h->cur = 0;
-    EnergyArgs e{};
-    e.X = h->X[0];
-    e.D = h->D[0];
-    e.partials = h->partials;
-    e.counter = h->counters + 2;
-    e.sc = h->sc;
-    e.c = h->lc;
-    size_t nb = (h->n3 + 255) / 256;
-    Launch le{dim3((unsigned)(nb < 4096 ? nb : 4096)), dim3(256), 0, h->stream};
-    CK(h, h->f32 ? energy0_f32(e, le) : energy0_f64(e, le));
+    h->e0_stale = true;
     DevScalars chk;
     int rc = read_scalars(h, &chk);
     if (rc) return rc;
@@ -521,6 +517,7 @@ int gabe_step(gabe_handle *h, int nsteps) {
         }
         h->cur ^= 1;
     }
+    if (nsteps > 0) h->e0_stale = true;
     return GABE_OK;
 }
 
@@ -535,6 +532,7 @@ int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]) {
         rc = enqueue_step(h, h->cur, ev.data() + 5 * s);
         h->cur ^= 1;
     }
+    h->e0_stale = true;
     double acc[4] = {0, 0, 0, 0};
     if (rc == GABE_OK && cudaStreamSynchronize(h->stream) == cudaSuccess) {
         for (int s = 0; s < nsteps; s++)

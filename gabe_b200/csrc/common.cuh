@@ -31,7 +31,7 @@ struct DevScalars {
     double fbar[2], dfbar[2];
     long long step;
     unsigned int status;
-    unsigned int pad;
+    unsigned int adot_given;  // adot[0] came from the caller (after an upload), not from adf(0)
 };
 
 enum Model : int { MODEL_QUADRATIC = 0, MODEL_LPHI4 = 1 };

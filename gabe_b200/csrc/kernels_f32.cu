@@ -4,34 +4,32 @@
 
 namespace gabe {
 
-cudaError_t configure_f32(size_t max_smem) {
-    cudaError_t e = cudaSuccess;
-    int v = (int)max_smem;
-    if ((e = cudaFuncSetAttribute(stage1_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(stage1_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(stage2_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(bin_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    return e;
-}
-
-cudaError_t stage1_f32(const StencilArgs &a, const Launch &l) {
-    if (a.gws) stage1_kernel<float, true><<<l.grid, l.block, l.smem, l.stream>>>(a);
-    else stage1_kernel<float, false><<<l.grid, l.block, l.smem, l.stream>>>(a);
+template <int TK, int TJ>
+static cudaError_t sweep_shape(int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    const dim3 block(TK, TJ);
+    switch (mode) {
+        case MODE_A: sweep_kernel<float, TK, TJ, MODE_A><<<grid, block, 0, s>>>(a); break;
+        case MODE_A_GW: sweep_kernel<float, TK, TJ, MODE_A_GW><<<grid, block, 0, s>>>(a); break;
+        case MODE_E0: sweep_kernel<float, TK, TJ, MODE_E0><<<grid, block, 0, s>>>(a); break;
+        default: sweep_kernel<float, TK, TJ, MODE_B><<<grid, block, 0, s>>>(a); break;
+    }
     return cudaGetLastError();
 }
 
-cudaError_t stage2_f32(const StencilArgs &a, const Launch &l) {
-    stage2_kernel<float><<<l.grid, l.block, l.smem, l.stream>>>(a);
-    return cudaGetLastError();
+cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    switch (shape) {
+        case 0: return sweep_shape<32, 8>(mode, a, grid, s);
+        case 1: return sweep_shape<16, 16>(mode, a, grid, s);
+        case 2: return sweep_shape<32, 4>(mode, a, grid, s);
+        case 3: return sweep_shape<16, 8>(mode, a, grid, s);
+        case 4: return sweep_shape<8, 8>(mode, a, grid, s);
+        case 5: return sweep_shape<4, 4>(mode, a, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l) {
     kspace_kernel<float><<<l.grid, l.block, l.smem, l.stream>>>(a);
-    return cudaGetLastError();
-}
-
-cudaError_t energy0_f32(const EnergyArgs &a, const Launch &l) {
-    energy0_kernel<float><<<l.grid, l.block, l.smem, l.stream>>>(a);
     return cudaGetLastError();
 }
 

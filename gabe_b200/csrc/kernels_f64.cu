@@ -3,25 +3,28 @@
 
 namespace gabe {
 
-cudaError_t configure_f64(size_t max_smem) {
-    cudaError_t e = cudaSuccess;
-    int v = (int)max_smem;
-    if ((e = cudaFuncSetAttribute(stage1_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(stage1_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(stage2_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    if ((e = cudaFuncSetAttribute(bin_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, v))) return e;
-    return e;
-}
-
-cudaError_t stage1_f64(const StencilArgs &a, const Launch &l) {
-    if (a.gws) stage1_kernel<double, true><<<l.grid, l.block, l.smem, l.stream>>>(a);
-    else stage1_kernel<double, false><<<l.grid, l.block, l.smem, l.stream>>>(a);
+template <int TK, int TJ>
+static cudaError_t sweep_shape(int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    const dim3 block(TK, TJ);
+    switch (mode) {
+        case MODE_A: sweep_kernel<double, TK, TJ, MODE_A><<<grid, block, 0, s>>>(a); break;
+        case MODE_A_GW: sweep_kernel<double, TK, TJ, MODE_A_GW><<<grid, block, 0, s>>>(a); break;
+        case MODE_E0: sweep_kernel<double, TK, TJ, MODE_E0><<<grid, block, 0, s>>>(a); break;
+        default: sweep_kernel<double, TK, TJ, MODE_B><<<grid, block, 0, s>>>(a); break;
+    }
     return cudaGetLastError();
 }
 
-cudaError_t stage2_f64(const StencilArgs &a, const Launch &l) {
-    stage2_kernel<double><<<l.grid, l.block, l.smem, l.stream>>>(a);
-    return cudaGetLastError();
+cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    switch (shape) {
+        case 0: return sweep_shape<32, 8>(mode, a, grid, s);
+        case 1: return sweep_shape<16, 16>(mode, a, grid, s);
+        case 2: return sweep_shape<32, 4>(mode, a, grid, s);
+        case 3: return sweep_shape<16, 8>(mode, a, grid, s);
+        case 4: return sweep_shape<8, 8>(mode, a, grid, s);
+        case 5: return sweep_shape<4, 4>(mode, a, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l) {
@@ -29,14 +32,15 @@ cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l) {
     return cudaGetLastError();
 }
 
-cudaError_t energy0_f64(const EnergyArgs &a, const Launch &l) {
-    energy0_kernel<double><<<l.grid, l.block, l.smem, l.stream>>>(a);
-    return cudaGetLastError();
-}
-
 cudaError_t bins_f64(const BinArgs &a, const Launch &l) {
     bin_kernel<double><<<l.grid, l.block, l.smem, l.stream>>>(a);
     return cudaGetLastError();
+}
+
+cudaError_t configure_bins(size_t max_smem) {
+    cudaError_t e = cudaFuncSetAttribute(bin_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(bin_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
 }
 
 cudaError_t bin_reduce(const double *part_sum, const unsigned int *part_cnt, int nblocks, int nseries, int nbins,

@@ -6,7 +6,6 @@
 
 #include <cuda_runtime.h>
 
-#include "energy.cuh"
 #include "kspace.cuh"
 #include "spectra.cuh"
 #include "stencil.cuh"
@@ -19,20 +18,17 @@ struct Launch {
     cudaStream_t stream;
 };
 
-cudaError_t configure_f64(size_t max_smem);
-cudaError_t configure_f32(size_t max_smem);
+// Stencil tile shapes (TK x TJ), index = tile shape id of gabe_params.
+constexpr int kNumShapes = 6;
+constexpr int kShapes[kNumShapes][2] = {{32, 8}, {16, 16}, {32, 4}, {16, 8}, {8, 8}, {4, 4}};
 
-cudaError_t stage1_f64(const StencilArgs &a, const Launch &l);
-cudaError_t stage2_f64(const StencilArgs &a, const Launch &l);
+cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
+cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l);
-cudaError_t energy0_f64(const EnergyArgs &a, const Launch &l);
-cudaError_t bins_f64(const BinArgs &a, const Launch &l);
-
-cudaError_t stage1_f32(const StencilArgs &a, const Launch &l);
-cudaError_t stage2_f32(const StencilArgs &a, const Launch &l);
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);
-cudaError_t energy0_f32(const EnergyArgs &a, const Launch &l);
+cudaError_t bins_f64(const BinArgs &a, const Launch &l);
 cudaError_t bins_f32(const BinArgs &a, const Launch &l);
+cudaError_t configure_bins(size_t max_smem);
 
 cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *counter, double *out, int nblocks,
                      cudaStream_t s);

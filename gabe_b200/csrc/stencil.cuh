@@ -1,64 +1,58 @@
 // Fused RK2 stencil sweeps for the GABE step (expansion_type 1,
 // g2functions.cpp:234-271).
 //
-// The reference makes, per step, two field-update sweeps plus two
-// calcEnergy() calls of three sweeps each, and (with GWs) two source sweeps.
-// Its Friedmann update needs the full-volume energy of the stage-1 state
-// before stage 2 can start (g2functions.cpp:250-252), and the end-of-step
-// energy before the next step (:268-270).  Two sweeps per step is therefore
-// the minimum, and these two kernels are those sweeps:
+// The reference makes, per step, two field-update sweeps, two calcEnergy()
+// calls of three sweeps each and (with GWs) two source sweeps.  Its
+// Friedmann update needs the full-volume energy of the stage-1 state before
+// stage 2 (g2functions.cpp:250-252) and of the end state before the next
+// step (:268-270), so two sweeps per step is the minimum.  They are:
 //
-//   stage1: reads f0, fdot0 (7-point stencils); derives f1 = f0 + dt/2 fdot0
-//           and fdot1 (never stored); reduces the stage-1 energies
-//           (calcEnergy(1)); writes the GW sources of f0 and f1
-//           (g2evolutionpert.cpp:48-132, 165-180) when calc_gws.  Its last
-//           block forms a[1], adot[1] (adf).
-//   stage2: reads f0, fdot0 again; recomputes fdot1 on a one-point halo in
-//           shared memory (f0 staged with a two-point halo), writes
-//           f0' = f0 + dt fdot1 and fdot0' = fdot0 + dt fddot(f1), and reduces
-//           the end-of-step energies from f0', whose Laplacian needs fdot1
-//           on the halo.  Its last block forms a[0], adot[0].
+//   sweep A (mode A / A_GW): reads f0, fdot0 with 7-point neighbourhoods and
+//     reduces, in one pass,
+//       E0 = calcEnergy(0) of (f0, fdot0) -> adot0 = adf(0) (:268-270 of the
+//            previous step; skipped right after an upload, where adot0 is the
+//            caller's, g2init.cpp:29),
+//       the stage-1 energies: pot1 and grad1 depend only on
+//            f1 = f0 + dt/2 fdot0; fdot1 = P + adot0 Q is affine in adot0, so
+//            kin1 = sum P^2 + 2 adot0 sum PQ + adot0^2 sum Q^2 is formed from
+//            three sums without knowing adot0 during the sweep,
+//     and writes the GW sources of f0 and f1 (g2evolutionpert.cpp:48-132,
+//     165-180).  Its last block forms adot0, a[1], adot[1] (:250-252).
+//   sweep B: reads f0, fdot0 again, forms fdot1 and f1 at the 7 points,
+//     writes f0' = f0 + dt fdot1 and fdot0' = fdot0 + dt fddot(f1)
+//     (:254-262).  Its last block advances a[0] (:268).
+//   mode E0: sweep A's E0 part alone, for energies asked for between steps.
 //
-// Blocks march along i (slowest axis) over a chunk of `ci` planes, holding a
-// ring of planes per array in shared memory; (j,k) tiles are blockDim.y x
-// blockDim.x with k on the warp lanes for coalesced rows.  Periodic wrap is
-// applied when staging planes.  The FP64 instantiation keeps the reference's
-// operation order (compiled without FMA contraction); the FP32 one evolves
-// fluctuations about the FP64 homogeneous trajectory (see common.cuh).
+// Both sweeps are radius-1 stencils: each thread owns a (j,k) column of a
+// TJ x TK tile and marches along i over `ci` planes, keeping the i-1, i, i+1
+// values of its column in registers (plus i+2 prefetched), and the (j,k)
+// neighbours of plane i in a double-buffered shared-memory tile with a
+// one-point halo, so each value is read from HBM once per sweep and there is
+// one barrier per plane.  The FP64 instantiations keep the reference's
+// operation order (compiled without FMA contraction); the FP32 ones evolve
+// fluctuations about the FP64 homogeneous trajectory (common.cuh).
 #pragma once
 
 #include "common.cuh"
 
 namespace gabe {
 
+enum SweepMode : int { MODE_A = 0, MODE_A_GW = 1, MODE_E0 = 2, MODE_B = 3 };
+
 struct StencilArgs {
     const void *X;       // fields in  [2][N^3]
     const void *D;       // momenta in [2][N^3]
-    void *Xo;            // fields out   (stage2)
-    void *Do;            // momenta out  (stage2)
-    void *S;             // GW sources [12][N][N][N+2] (stage1, calc_gws)
-    double *partials;    // [nblocks][3]
+    void *Xo;            // fields out   (sweep B)
+    void *Do;            // momenta out  (sweep B)
+    void *S;             // GW sources [12][N][N][N+2] (sweep A with GWs)
+    double *partials;    // [nblocks][8]
     unsigned int *counter;
     DevScalars *sc;
     LatticeConsts c;
     int ci;              // planes per block along i
-    int gws;
 };
 
-// Stage one plane of `src` (one field, N^3) with halo H into dst
-// ((TJ+2H) x (TK+2H), row stride TK+2H).
-template <typename T>
-__device__ __forceinline__ void stage_plane(T *dst, const T *__restrict__ src, int N, int i, int j0, int k0, int H) {
-    const int TK = blockDim.x, TJ = blockDim.y;
-    const int C = TK + 2 * H, R = TJ + 2 * H;
-    const T *plane = src + (size_t)wrapi(i, N) * N * N;
-    for (int r = threadIdx.y; r < R; r += TJ) {
-        const T *row = plane + (size_t)wrapi(j0 - H + r, N) * N;
-        for (int c = threadIdx.x; c < C; c += TK) dst[r * C + c] = __ldg(row + wrapi(k0 - H + c, N));
-    }
-}
-
-__device__ __forceinline__ int ring(int p, int n) { int m = p % n; return m < 0 ? m + n : m; }
+constexpr int kNV = 8;  // reduced values: kin0 pot0 grad0 | pot1 grad1 PP PQ QQ
 
 // 7-point neighbourhood, reference order: centre, i+1, i-1, j+1, j-1, k+1, k-1.
 template <typename T>
@@ -66,20 +60,16 @@ struct Nb7 {
     T v[7];
 };
 
-template <typename T>
-__device__ __forceinline__ Nb7<T> gather7(const T *pm, const T *pc, const T *pp, int o, int C) {
-    Nb7<T> n;
-    n.v[0] = pc[o]; n.v[1] = pp[o]; n.v[2] = pm[o];
-    n.v[3] = pc[o + C]; n.v[4] = pc[o - C]; n.v[5] = pc[o + 1]; n.v[6] = pc[o - 1];
-    return n;
-}
-
 // laplacian() of g2functions.cpp:35-43 in its operation order.
 __device__ __forceinline__ double lap64(const Nb7<double> &f, double dx2) {
     return (f.v[1] + f.v[2] + f.v[3] + f.v[4] + f.v[5] + f.v[6] - 6. * f.v[0]) / dx2;
 }
+// FP32: sum of neighbour differences (each difference of nearby values is
+// formed exactly, so the small Laplacian of a smooth fluctuation keeps its
+// relative precision).
 __device__ __forceinline__ float lap32(const Nb7<float> &f, float inv_dx2) {
-    return (((f.v[1] + f.v[2]) + (f.v[3] + f.v[4])) + (f.v[5] + f.v[6]) - 6.f * f.v[0]) * inv_dx2;
+    const float c = f.v[0];
+    return (((f.v[1] - c) + (f.v[2] - c)) + ((f.v[3] - c) + (f.v[4] - c)) + ((f.v[5] - c) + (f.v[6] - c))) * inv_dx2;
 }
 
 // GW source components 11,12,13,22,23,33 of one field added into s
@@ -109,37 +99,19 @@ __device__ __forceinline__ void source_add32(float dn, const Nb7<float> &f, floa
     s[5] += dn * (d3 * d3 - t);
 }
 
-template <typename T>
-__device__ __forceinline__ void store_sources(T *S, int N, int i, int j, int k, const T *s0, const T *s1) {
-    const size_t slot = (size_t)N * N * (N + 2);
-    const size_t o = ((size_t)i * N + j) * (N + 2) + k;
-#pragma unroll
-    for (int q = 0; q < 6; q++) {
-        S[q * slot + o] = s0[q];
-        S[(6 + q) * slot + o] = s1[q];
-    }
-}
-
-// Homogeneous-trajectory values for the FP32 path at the three stages of a
-// step (start, midpoint, end), computed identically by every thread.
+// Homogeneous-trajectory values of the FP32 path (start and midpoint of a
+// step; the midpoint momentum is affine in adot0: dfb1 = p + adot0 q).
 struct MeanTraj {
-    double fb0[2], dfb0[2], fb1[2], dfb1[2], fbn[2], dfbn[2];
+    double fb0[2], dfb0[2], fb1[2], pbar[2], qbar[2];
 };
-__device__ __forceinline__ MeanTraj mean_traj(const LatticeConsts &c, const DevScalars *sc, bool need_end) {
+__device__ __forceinline__ MeanTraj mean_traj(const LatticeConsts &c, const DevScalars *sc) {
     MeanTraj m;
-    const double h = c.half_dt, dt = c.dt;
-    const double a0 = sc->a[0], c3H0 = (3. * sc->adot[0]) / a0;
+    const double h = c.half_dt, a0 = sc->a[0];
     for (int f = 0; f < 2; f++) { m.fb0[f] = sc->fbar[f]; m.dfb0[f] = sc->dfbar[f]; }
     for (int f = 0; f < 2; f++) {
         m.fb1[f] = m.fb0[f] + h * m.dfb0[f];
-        m.dfb1[f] = m.dfb0[f] + h * (-dv_h(c.model, c.mc, f, m.fb0[0], m.fb0[1]) - c3H0 * m.dfb0[f]);
-    }
-    if (need_end) {
-        const double a1 = sc->a[1], c3H1 = (3. * sc->adot[1]) / a1;
-        for (int f = 0; f < 2; f++) {
-            m.fbn[f] = m.fb0[f] + dt * m.dfb1[f];
-            m.dfbn[f] = m.dfb0[f] + dt * (-dv_h(c.model, c.mc, f, m.fb1[0], m.fb1[1]) - c3H1 * m.dfb1[f]);
-        }
+        m.pbar[f] = m.dfb0[f] - h * dv_h(c.model, c.mc, f, m.fb0[0], m.fb0[1]);
+        m.qbar[f] = -h * 3. * m.dfb0[f] / a0;
     }
     return m;
 }
@@ -156,304 +128,318 @@ __device__ __forceinline__ MeanF mean_f(const LatticeConsts &c, const double *fb
 }
 
 // ---------------------------------------------------------------------------
-// stage 1
+// plane march: 4 arrays (f0 phi, f0 chi, fdot0 phi, fdot0 chi)
 // ---------------------------------------------------------------------------
-template <typename T, bool GWS>
-__global__ void __launch_bounds__(256) stage1_kernel(StencilArgs args) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sred[8 * 3];
-    __shared__ int sflag;
-    T *sm = reinterpret_cast<T *>(smem_raw);
-    const LatticeConsts &c = args.c;
-    const int N = c.N;
-    const int TK = blockDim.x, TJ = blockDim.y, tx = threadIdx.x, ty = threadIdx.y;
-    const int C1 = TK + 2, P1 = C1 * (TJ + 2);
-    T *F0 = sm;           // [fld*3 + slot][P1]
-    T *D0 = sm + 6 * P1;  // [fld*3 + slot][P1]
-    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-    const int i0 = blockIdx.z * args.ci, i1 = min(i0 + args.ci, N);
-    const size_t n3 = (size_t)N * N * N;
-    const T *X = static_cast<const T *>(args.X), *D = static_cast<const T *>(args.D);
-    const DevScalars *scp = args.sc;
-    const double a0 = scp->a[0], ad0 = scp->adot[0];
-    const double h = c.half_dt;
-    const double c3H0 = (3. * ad0) / a0;
+template <typename T, int TK, int TJ>
+struct March {
+    static constexpr int C = TK + 2, R = TJ + 2, P = C * R, NA = 4;
+    static constexpr int NH = 2 * TK + 2 * TJ;  // halo points of a plane tile
+    const T *src[NA];
+    int N, j0, k0, tx, ty, tid;
+    // halo duty of this thread: (row, col) in the tile and global (j, k)
+    int hr, hc, hj, hk;
+    bool has_halo;
+    T prev[NA], cur[NA], nxt[NA], nn[NA], hal[NA];
 
-    MeanTraj mt;
-    MeanF m0, m1;
-    float ia02f = 0.f, c3H0f = 0.f, hf = 0.f, inv_dx2f = 0.f, dnf = 0.f;
+    __device__ __forceinline__ void init(const T *X, const T *D, int N_, size_t n3) {
+        src[0] = X; src[1] = X + n3; src[2] = D; src[3] = D + n3;
+        N = N_;
+        tx = threadIdx.x; ty = threadIdx.y; tid = tx + TK * ty;
+        j0 = blockIdx.y * TJ; k0 = blockIdx.x * TK;
+        has_halo = tid < NH;
+        int t = tid;
+        if (t < TK) { hr = 0; hc = t + 1; }
+        else if (t < 2 * TK) { hr = TJ + 1; hc = t - TK + 1; }
+        else if (t < 2 * TK + TJ) { hr = t - 2 * TK + 1; hc = 0; }
+        else { hr = t - 2 * TK - TJ + 1; hc = TK + 1; }
+        hj = wrapi(j0 + hr - 1, N);
+        hk = wrapi(k0 + hc - 1, N);
+    }
+    __device__ __forceinline__ size_t own(int i) const {
+        return ((size_t)wrapi(i, N) * N + (j0 + ty)) * N + (k0 + tx);
+    }
+    __device__ __forceinline__ size_t halo(int i) const { return ((size_t)wrapi(i, N) * N + hj) * N + hk; }
+    __device__ __forceinline__ void load_own(T (&dst)[NA], int i) const {
+        const size_t o = own(i);
+#pragma unroll
+        for (int a = 0; a < NA; a++) dst[a] = __ldg(src[a] + o);
+    }
+    __device__ __forceinline__ void load_halo(int i) {
+        if (has_halo) {
+            const size_t o = halo(i);
+#pragma unroll
+            for (int a = 0; a < NA; a++) hal[a] = __ldg(src[a] + o);
+        }
+    }
+    // writes plane values (own = v, halo = hal) into shared buffer sb
+    __device__ __forceinline__ void store(T *sb, const T (&v)[NA]) const {
+#pragma unroll
+        for (int a = 0; a < NA; a++) sb[a * P + (ty + 1) * C + (tx + 1)] = v[a];
+        if (has_halo)
+#pragma unroll
+            for (int a = 0; a < NA; a++) sb[a * P + hr * C + hc] = hal[a];
+    }
+    // 7-point neighbourhood of array a at plane i (sb holds plane i)
+    __device__ __forceinline__ Nb7<T> nb(const T *sb, int a) const {
+        const T *p = sb + a * P + (ty + 1) * C + (tx + 1);
+        Nb7<T> n;
+        n.v[0] = cur[a]; n.v[1] = nxt[a]; n.v[2] = prev[a];
+        n.v[3] = p[C]; n.v[4] = p[-C]; n.v[5] = p[1]; n.v[6] = p[-1];
+        return n;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ Nb7<T> axpy7(const Nb7<T> &x, T h, const Nb7<T> &y) {
+    Nb7<T> r;
+#pragma unroll
+    for (int q = 0; q < 7; q++) r.v[q] = x.v[q] + h * y.v[q];
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_sources(T *S, int N, int i, int j, int k, const T *s0, const T *s1) {
+    const size_t slot = (size_t)N * N * (N + 2);
+    const size_t o = ((size_t)i * N + j) * (N + 2) + k;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        S[q * slot + o] = s0[q];
+        S[(6 + q) * slot + o] = s1[q];
+    }
+}
+
+// Final scalars of sweep A / E0 from the block-summed values (thread 0 of
+// the last block).
+template <typename T, int MODE>
+__device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, const double *tot) {
+    const double a0 = s->a[0];
+    double ek0 = tot[0] / c.gridsize / 2.;
+    double ep0 = tot[1] / c.gridsize;
+    const double eg0 = tot[2] / c.gridsize / 2. / a0 / a0;
+    MeanTraj m{};
     if constexpr (sizeof(T) == 4) {
-        mt = mean_traj(c, scp, false);
-        m0 = mean_f(c, mt.fb0);
-        m1 = mean_f(c, mt.fb1);
-        ia02f = (float)(1.0 / (a0 * a0));
-        c3H0f = (float)c3H0;
-        hf = (float)h;
-        inv_dx2f = (float)(1.0 / c.inv_dx2_div);
-        dnf = (float)c.dn;
+        m = mean_traj(c, s);
+        ep0 += pot_h(c.model, c.mc, m.fb0[0], m.fb0[1]);
     }
-
-    double kin = 0., pot = 0., grad = 0.;
-    for (int p = i0 - 1; p <= i0; p++)
-        for (int f = 0; f < 2; f++) {
-            stage_plane(F0 + (f * 3 + ring(p, 3)) * P1, X + f * n3, N, p, j0, k0, 1);
-            stage_plane(D0 + (f * 3 + ring(p, 3)) * P1, D + f * n3, N, p, j0, k0, 1);
-        }
-    const int o = (ty + 1) * C1 + (tx + 1);
-    for (int i = i0; i < i1; i++) {
-        for (int f = 0; f < 2; f++) {
-            stage_plane(F0 + (f * 3 + ring(i + 1, 3)) * P1, X + f * n3, N, i + 1, j0, k0, 1);
-            stage_plane(D0 + (f * 3 + ring(i + 1, 3)) * P1, D + f * n3, N, i + 1, j0, k0, 1);
-        }
-        __syncthreads();
-        const int sm_ = ring(i - 1, 3), sc_ = ring(i, 3), sp_ = ring(i + 1, 3);
-        Nb7<T> f0[2], d0[2], f1[2];
-        for (int f = 0; f < 2; f++) {
-            f0[f] = gather7(F0 + (f * 3 + sm_) * P1, F0 + (f * 3 + sc_) * P1, F0 + (f * 3 + sp_) * P1, o, C1);
-            d0[f] = gather7(D0 + (f * 3 + sm_) * P1, D0 + (f * 3 + sc_) * P1, D0 + (f * 3 + sp_) * P1, o, C1);
-        }
-        T s0[6] = {0, 0, 0, 0, 0, 0}, s1[6] = {0, 0, 0, 0, 0, 0};
-        if constexpr (sizeof(T) == 8) {
-            for (int f = 0; f < 2; f++) {
-                const double lap0 = lap64(f0[f], c.inv_dx2_div);
-                const double dd0 = lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]) - c3H0 * d0[f].v[0];
-                const double d1c = d0[f].v[0] + h * dd0;
-#pragma unroll
-                for (int q = 0; q < 7; q++) f1[f].v[q] = f0[f].v[q] + h * d0[f].v[q];
-                const double lap1 = lap64(f1[f], c.inv_dx2_div);
-                kin += d1c * d1c;
-                grad -= f1[f].v[0] * lap1;
-                if constexpr (GWS) {
-                    source_add64(c, f0[f], s0);
-                    source_add64(c, f1[f], s1);
-                }
-            }
-            pot += pot64(c, f1[0].v[0], f1[1].v[0]);
-        } else {
-            for (int f = 0; f < 2; f++) {
-                const float lap0 = lap32(f0[f], inv_dx2f);
-                const float dd0 = lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]) - c3H0f * d0[f].v[0];
-                const float d1c = d0[f].v[0] + hf * dd0;
-#pragma unroll
-                for (int q = 0; q < 7; q++) f1[f].v[q] = f0[f].v[q] + hf * d0[f].v[q];
-                const float lap1 = lap32(f1[f], inv_dx2f);
-                const double dtot = mt.dfb1[f] + (double)d1c;
-                kin += dtot * dtot;
-                grad -= (double)(f1[f].v[0] * lap1);
-                if constexpr (GWS) {
-                    source_add32(dnf, f0[f], s0);
-                    source_add32(dnf, f1[f], s1);
-                }
-            }
-            pot += (double)v_diff32(m1, c.model, f1[0].v[0], f1[1].v[0]);
-        }
-        if constexpr (GWS) store_sources(static_cast<T *>(args.S), N, i, j0 + ty, k0 + tx, s0, s1);
-        __syncthreads();
-    }
-
-    double v[3] = {kin, pot, grad};
-    block_reduce<3>(v, sred);
-    const int tid = tx + TK * ty;
-    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (tid == 0)
-        for (int q = 0; q < 3; q++) args.partials[(size_t)bid * 3 + q] = v[q];
-    if (!last_block_done(args.counter, &sflag)) return;
-    double tot[3];
-    sum_partials<3>(args.partials, gridDim.x * gridDim.y * gridDim.z, tot, sred);
-    if (tid == 0) {
-        DevScalars *s = args.sc;
-        const double a1 = a0 + h * ad0; /* g2functions.cpp:250 */
-        double ek = tot[0] / c.gridsize / 2.;
-        double ep = tot[1] / c.gridsize;
-        double eg = tot[2] / c.gridsize / 2. / a1 / a1;
-        if constexpr (sizeof(T) == 4) {
-            MeanTraj m = mean_traj(c, s, false);
-            ep += pot_h(c.model, c.mc, m.fb1[0], m.fb1[1]);
-        }
-        const double rho = ek + ep + eg;
-        s->a[1] = a1;
-        s->edkin[1] = ek;
-        s->edpot[1] = ep;
-        s->edgrad[1] = eg;
-        s->edrho[1] = rho;
-        s->adot[1] = sqrt(c.eight_pi_3 * rho) * a1; /* adf(1), :252 */
-        if (!isfinite(rho)) s->status |= ST_NONFINITE;
-        *args.counter = 0u;
-    }
+    const double rho0 = ek0 + ep0 + eg0;
+    s->edkin[0] = ek0;
+    s->edpot[0] = ep0;
+    s->edgrad[0] = eg0;
+    s->edrho[0] = rho0;
+    if (!s->adot_given) s->adot[0] = sqrt(c.eight_pi_3 * rho0) * a0; /* adf(0), g2functions.cpp:270 */
+    if (!isfinite(rho0)) s->status |= ST_NONFINITE;
+    if constexpr (MODE == MODE_E0) return;
+    const double ad0 = s->adot[0];
+    const double a1 = a0 + c.half_dt * ad0; /* :250 */
+    const double ek1 = (tot[5] + 2. * ad0 * tot[6] + ad0 * ad0 * tot[7]) / c.gridsize / 2.;
+    double ep1 = tot[3] / c.gridsize;
+    const double eg1 = tot[4] / c.gridsize / 2. / a1 / a1;
+    if constexpr (sizeof(T) == 4) ep1 += pot_h(c.model, c.mc, m.fb1[0], m.fb1[1]);
+    const double rho1 = ek1 + ep1 + eg1;
+    s->a[1] = a1;
+    s->edkin[1] = ek1;
+    s->edpot[1] = ep1;
+    s->edgrad[1] = eg1;
+    s->edrho[1] = rho1;
+    s->adot[1] = sqrt(c.eight_pi_3 * rho1) * a1; /* adf(1), :252 */
+    if (!isfinite(rho1)) s->status |= ST_NONFINITE;
 }
 
 // ---------------------------------------------------------------------------
-// stage 2
+// the sweep kernel
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ void fdot1_region(const LatticeConsts &c, T *F0, T *D0, T *D1, int p, int P1, int P2,
-                                             int C1, int C2, double a0, double c3H0, const MeanF &m0, float ia02f,
-                                             float c3H0f, float hf, float inv_dx2f) {
-    // fdot1 = fdot0 + dt/2 * fddot(f0) on the (TJ+2) x (TK+2) region of plane p
-    const int TK = blockDim.x, TJ = blockDim.y;
-    const int R1 = TJ + 2;
-    const int sm4 = ring(p - 1, 4), sc4 = ring(p, 4), sp4 = ring(p + 1, 4), s3 = ring(p, 3);
-    for (int r = threadIdx.y; r < R1; r += TJ)
-        for (int cc = threadIdx.x; cc < C1; cc += TK) {
-            const int o2 = (r + 1) * C2 + (cc + 1), o1 = r * C1 + cc;
-            Nb7<T> g[2];
-            for (int f = 0; f < 2; f++)
-                g[f] = gather7(F0 + (f * 4 + sm4) * P2, F0 + (f * 4 + sc4) * P2, F0 + (f * 4 + sp4) * P2, o2, C2);
-            for (int f = 0; f < 2; f++) {
-                const T d0 = D0[(f * 3 + s3) * P1 + o1];
-                if constexpr (sizeof(T) == 8) {
-                    const double lap0 = lap64(g[f], c.inv_dx2_div);
-                    const double dd0 = lap0 / a0 / a0 - dv64(c, f, g[0].v[0], g[1].v[0]) - c3H0 * d0;
-                    D1[(f * 3 + s3) * P1 + o1] = d0 + c.half_dt * dd0;
-                } else {
-                    const float lap0 = lap32(g[f], inv_dx2f);
-                    const float dd0 = lap0 * ia02f - dv_diff32(m0, c.model, f, g[0].v[0], g[1].v[0]) - c3H0f * d0;
-                    D1[(f * 3 + s3) * P1 + o1] = d0 + hf * dd0;
-                }
-            }
-        }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(256) stage2_kernel(StencilArgs args) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ double sred[8 * 3];
+template <typename T, int TK, int TJ, int MODE>
+__global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
+    using M = March<T, TK, TJ>;
+    __shared__ __align__(16) T smem[2][M::NA * M::P];
+    __shared__ double sred[((TK * TJ + 31) / 32) * kNV];
     __shared__ int sflag;
-    T *sm = reinterpret_cast<T *>(smem_raw);
     const LatticeConsts &c = args.c;
     const int N = c.N;
-    const int TK = blockDim.x, TJ = blockDim.y, tx = threadIdx.x, ty = threadIdx.y;
-    const int C1 = TK + 2, P1 = C1 * (TJ + 2);
-    const int C2 = TK + 4, P2 = C2 * (TJ + 4);
-    T *F0 = sm;               // [fld*4 + slot][P2]   halo 2
-    T *D0 = F0 + 8 * P2;      // [fld*3 + slot][P1]   halo 1
-    T *D1 = D0 + 6 * P1;      // [fld*3 + slot][P1]   halo 1 (computed)
-    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-    const int i0 = blockIdx.z * args.ci, i1 = min(i0 + args.ci, N);
     const size_t n3 = (size_t)N * N * N;
-    const T *X = static_cast<const T *>(args.X), *D = static_cast<const T *>(args.D);
-    T *Xo = static_cast<T *>(args.Xo), *Do = static_cast<T *>(args.Do);
+    M m;
+    m.init(static_cast<const T *>(args.X), static_cast<const T *>(args.D), N, n3);
+    const int i0 = blockIdx.z * args.ci, i1 = min(i0 + args.ci, N);
     const DevScalars *scp = args.sc;
-    const double a0 = scp->a[0], ad0 = scp->adot[0], a1 = scp->a[1], ad1 = scp->adot[1];
     const double h = c.half_dt, dt = c.dt;
-    const double c3H0 = (3. * ad0) / a0, c3H1 = (3. * ad1) / a1;
+    const double a0 = scp->a[0];
 
-    MeanTraj mt;
-    MeanF m0, m1, mn;
-    float ia02f = 0.f, ia12f = 0.f, c3H0f = 0.f, c3H1f = 0.f, hf = 0.f, dtf = 0.f, inv_dx2f = 0.f;
+    // per-kernel constants
+    double ad0 = 0., a1 = 0., ad1 = 0.;
+    if constexpr (MODE == MODE_B) {
+        ad0 = scp->adot[0];
+        a1 = scp->a[1];
+        ad1 = scp->adot[1];
+    }
+    const double c3H0 = (3. * ad0) / a0, c3H1 = MODE == MODE_B ? (3. * ad1) / a1 : 0.;
+    MeanTraj mt{};
+    MeanF m0{}, m1{};
+    float ia02f = 0.f, ia12f = 0.f, c3H0f = 0.f, c3H1f = 0.f, hf = 0.f, dtf = 0.f, inv_dx2f = 0.f, dnf = 0.f,
+          q3f = 0.f;
     if constexpr (sizeof(T) == 4) {
-        mt = mean_traj(c, scp, true);
+        mt = mean_traj(c, scp);
         m0 = mean_f(c, mt.fb0);
         m1 = mean_f(c, mt.fb1);
-        mn = mean_f(c, mt.fbn);
         ia02f = (float)(1.0 / (a0 * a0));
-        ia12f = (float)(1.0 / (a1 * a1));
-        c3H0f = (float)c3H0;
-        c3H1f = (float)c3H1;
         hf = (float)h;
         dtf = (float)dt;
         inv_dx2f = (float)(1.0 / c.inv_dx2_div);
+        dnf = (float)c.dn;
+        q3f = (float)(-h * 3. / a0);
+        if constexpr (MODE == MODE_B) {
+            ia12f = (float)(1.0 / (a1 * a1));
+            c3H0f = (float)c3H0;
+            c3H1f = (float)c3H1;
+        }
     }
+    (void)ia12f; (void)c3H0f; (void)c3H1f; (void)dtf; (void)dnf; (void)q3f; (void)c3H1;
 
-    for (int p = i0 - 2; p <= i0 + 1; p++)
-        for (int f = 0; f < 2; f++) stage_plane(F0 + (f * 4 + ring(p, 4)) * P2, X + f * n3, N, p, j0, k0, 2);
-    for (int p = i0 - 1; p <= i0; p++)
-        for (int f = 0; f < 2; f++) stage_plane(D0 + (f * 3 + ring(p, 3)) * P1, D + f * n3, N, p, j0, k0, 1);
+    double acc[kNV];
+#pragma unroll
+    for (int q = 0; q < kNV; q++) acc[q] = 0.;
+
+    // prologue: registers for planes i0-1, i0, i0+1; shared tile of plane i0
+    m.load_own(m.prev, i0 - 1);
+    m.load_own(m.cur, i0);
+    m.load_own(m.nxt, i0 + 1);
+    m.load_halo(i0);
+    m.store(smem[i0 & 1], m.cur);
     __syncthreads();
-    fdot1_region<T>(c, F0, D0, D1, i0 - 1, P1, P2, C1, C2, a0, c3H0, m0, ia02f, c3H0f, hf, inv_dx2f);
-    fdot1_region<T>(c, F0, D0, D1, i0, P1, P2, C1, C2, a0, c3H0, m0, ia02f, c3H0f, hf, inv_dx2f);
 
-    double kin = 0., pot = 0., grad = 0.;
-    const int o1 = (ty + 1) * C1 + (tx + 1), o2 = (ty + 2) * C2 + (tx + 2);
-    const int j = j0 + ty, k = k0 + tx;
+    T *Xo = static_cast<T *>(args.Xo), *Do = static_cast<T *>(args.Do);
+    const int j = m.j0 + m.ty, k = m.k0 + m.tx;
     for (int i = i0; i < i1; i++) {
-        __syncthreads();
-        for (int f = 0; f < 2; f++) {
-            stage_plane(F0 + (f * 4 + ring(i + 2, 4)) * P2, X + f * n3, N, i + 2, j0, k0, 2);
-            stage_plane(D0 + (f * 3 + ring(i + 1, 3)) * P1, D + f * n3, N, i + 1, j0, k0, 1);
+        const bool more = i + 1 < i1;
+        if (more) {
+            m.load_own(m.nn, i + 2);
+            m.load_halo(i + 1);
         }
-        __syncthreads();
-        fdot1_region<T>(c, F0, D0, D1, i + 1, P1, P2, C1, C2, a0, c3H0, m0, ia02f, c3H0f, hf, inv_dx2f);
-        __syncthreads();
-
-        const int m4 = ring(i - 1, 4), c4 = ring(i, 4), p4 = ring(i + 1, 4);
-        const int m3 = ring(i - 1, 3), c3 = ring(i, 3), p3 = ring(i + 1, 3);
-        Nb7<T> f0[2], d0[2], d1[2], f1[2], fn[2];
+        const T *sb = smem[i & 1];
+        Nb7<T> f0[2], d0[2];
         for (int f = 0; f < 2; f++) {
-            f0[f] = gather7(F0 + (f * 4 + m4) * P2, F0 + (f * 4 + c4) * P2, F0 + (f * 4 + p4) * P2, o2, C2);
-            d0[f] = gather7(D0 + (f * 3 + m3) * P1, D0 + (f * 3 + c3) * P1, D0 + (f * 3 + p3) * P1, o1, C1);
-            d1[f] = gather7(D1 + (f * 3 + m3) * P1, D1 + (f * 3 + c3) * P1, D1 + (f * 3 + p3) * P1, o1, C1);
+            f0[f] = m.nb(sb, f);
+            d0[f] = m.nb(sb, 2 + f);
         }
-        const size_t gx = ((size_t)i * N + j) * N + k;
-        if constexpr (sizeof(T) == 8) {
-            for (int f = 0; f < 2; f++)
-#pragma unroll
-                for (int q = 0; q < 7; q++) {
-                    f1[f].v[q] = f0[f].v[q] + h * d0[f].v[q];
-                    fn[f].v[q] = f0[f].v[q] + dt * d1[f].v[q]; /* g2functions.cpp:259 */
+        if constexpr (MODE == MODE_B) {
+            const size_t gx = ((size_t)i * N + j) * N + k;
+            if constexpr (sizeof(T) == 8) {
+                const Nb7<double> f1[2] = {axpy7(f0[0], h, d0[0]), axpy7(f0[1], h, d0[1])};
+                for (int f = 0; f < 2; f++) {
+                    const double lap0 = lap64(f0[f], c.inv_dx2_div);
+                    const double dd0 = lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]) - c3H0 * d0[f].v[0];
+                    const double d1c = d0[f].v[0] + h * dd0;                  /* g2functions.cpp:242 */
+                    const double lap1 = lap64(f1[f], c.inv_dx2_div);
+                    const double dd1 = lap1 / a1 / a1 - dv64(c, f, f1[0].v[0], f1[1].v[0]) - c3H1 * d1c;
+                    Xo[f * n3 + gx] = f0[f].v[0] + dt * d1c;                  /* :259 */
+                    Do[f * n3 + gx] = d0[f].v[0] + dt * dd1;                  /* :260 */
                 }
-            for (int f = 0; f < 2; f++) {
-                const double lap1 = lap64(f1[f], c.inv_dx2_div);
-                const double dd1 = lap1 / a1 / a1 - dv64(c, f, f1[0].v[0], f1[1].v[0]) - c3H1 * d1[f].v[0];
-                const double dnew = d0[f].v[0] + dt * dd1; /* :260 */
-                const double lapn = lap64(fn[f], c.inv_dx2_div);
-                Xo[f * n3 + gx] = fn[f].v[0];
-                Do[f * n3 + gx] = dnew;
-                kin += dnew * dnew;
-                grad -= fn[f].v[0] * lapn;
+            } else {
+                const Nb7<float> f1[2] = {axpy7(f0[0], hf, d0[0]), axpy7(f0[1], hf, d0[1])};
+                for (int f = 0; f < 2; f++) {
+                    const float lap0 = lap32(f0[f], inv_dx2f);
+                    const float dd0 = lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]) - c3H0f * d0[f].v[0];
+                    const float d1c = d0[f].v[0] + hf * dd0;
+                    const float lap1 = lap32(f1[f], inv_dx2f);
+                    const float dd1 = lap1 * ia12f - dv_diff32(m1, c.model, f, f1[0].v[0], f1[1].v[0]) - c3H1f * d1c;
+                    Xo[f * n3 + gx] = f0[f].v[0] + dtf * d1c;
+                    Do[f * n3 + gx] = d0[f].v[0] + dtf * dd1;
+                }
             }
-            pot += pot64(c, fn[0].v[0], fn[1].v[0]);
         } else {
-            for (int f = 0; f < 2; f++)
-#pragma unroll
-                for (int q = 0; q < 7; q++) {
-                    f1[f].v[q] = f0[f].v[q] + hf * d0[f].v[q];
-                    fn[f].v[q] = f0[f].v[q] + dtf * d1[f].v[q];
+            T s0[6] = {0, 0, 0, 0, 0, 0}, s1[6] = {0, 0, 0, 0, 0, 0};
+            if constexpr (sizeof(T) == 8) {
+                for (int f = 0; f < 2; f++) {
+                    const double lap0 = lap64(f0[f], c.inv_dx2_div);
+                    acc[0] += d0[f].v[0] * d0[f].v[0];
+                    acc[2] -= f0[f].v[0] * lap0;
+                    if constexpr (MODE != MODE_E0) {
+                        const Nb7<double> f1 = axpy7(f0[f], h, d0[f]);
+                        const double P = d0[f].v[0] + h * (lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]));
+                        const double Q = -h * 3. * d0[f].v[0] / a0;
+                        acc[5] += P * P;
+                        acc[6] += P * Q;
+                        acc[7] += Q * Q;
+                        acc[4] -= f1.v[0] * lap64(f1, c.inv_dx2_div);
+                        if constexpr (MODE == MODE_A_GW) {
+                            source_add64(c, f0[f], s0);
+                            source_add64(c, f1, s1);
+                        }
+                    }
                 }
-            for (int f = 0; f < 2; f++) {
-                const float lap1 = lap32(f1[f], inv_dx2f);
-                const float dd1 = lap1 * ia12f - dv_diff32(m1, c.model, f, f1[0].v[0], f1[1].v[0]) - c3H1f * d1[f].v[0];
-                const float dnew = d0[f].v[0] + dtf * dd1;
-                const float lapn = lap32(fn[f], inv_dx2f);
-                Xo[f * n3 + gx] = fn[f].v[0];
-                Do[f * n3 + gx] = dnew;
-                const double dtot = mt.dfbn[f] + (double)dnew;
-                kin += dtot * dtot;
-                grad -= (double)(fn[f].v[0] * lapn);
+                acc[1] += pot64(c, f0[0].v[0], f0[1].v[0]);
+                if constexpr (MODE != MODE_E0)
+                    acc[3] += pot64(c, f0[0].v[0] + h * d0[0].v[0], f0[1].v[0] + h * d0[1].v[0]);
+            } else {
+                float f1c[2];
+                for (int f = 0; f < 2; f++) {
+                    const float lap0 = lap32(f0[f], inv_dx2f);
+                    const double kd = mt.dfb0[f] + (double)d0[f].v[0];
+                    acc[0] = fma(kd, kd, acc[0]);
+                    acc[2] -= (double)(f0[f].v[0] * lap0);
+                    if constexpr (MODE != MODE_E0) {
+                        const Nb7<float> f1 = axpy7(f0[f], hf, d0[f]);
+                        f1c[f] = f1.v[0];
+                        const float Pd = d0[f].v[0] + hf * (lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]));
+                        const double P = mt.pbar[f] + (double)Pd;
+                        const double Q = mt.qbar[f] + (double)(q3f * d0[f].v[0]);
+                        acc[5] = fma(P, P, acc[5]);
+                        acc[6] = fma(P, Q, acc[6]);
+                        acc[7] = fma(Q, Q, acc[7]);
+                        acc[4] -= (double)(f1.v[0] * lap32(f1, inv_dx2f));
+                        if constexpr (MODE == MODE_A_GW) {
+                            source_add32(dnf, f0[f], s0);
+                            source_add32(dnf, f1, s1);
+                        }
+                    }
+                }
+                acc[1] += (double)v_diff32(m0, c.model, f0[0].v[0], f0[1].v[0]);
+                if constexpr (MODE != MODE_E0) acc[3] += (double)v_diff32(m1, c.model, f1c[0], f1c[1]);
             }
-            pot += (double)v_diff32(mn, c.model, fn[0].v[0], fn[1].v[0]);
+            if constexpr (MODE == MODE_A_GW) store_sources(static_cast<T *>(args.S), N, i, j, k, s0, s1);
         }
+        if (more) {
+#pragma unroll
+            for (int a = 0; a < M::NA; a++) {
+                m.prev[a] = m.cur[a];
+                m.cur[a] = m.nxt[a];
+                m.nxt[a] = m.nn[a];
+            }
+            m.store(smem[(i + 1) & 1], m.cur);
+        }
+        __syncthreads();
     }
 
-    double v[3] = {kin, pot, grad};
-    block_reduce<3>(v, sred);
-    const int tid = tx + TK * ty;
+    const int tid = m.tid;
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    if (tid == 0)
-        for (int q = 0; q < 3; q++) args.partials[(size_t)bid * 3 + q] = v[q];
+    if constexpr (MODE != MODE_B) {
+        block_reduce<kNV>(acc, sred);
+        if (tid == 0)
+            for (int q = 0; q < kNV; q++) args.partials[(size_t)bid * kNV + q] = acc[q];
+    }
     if (!last_block_done(args.counter, &sflag)) return;
-    double tot[3];
-    sum_partials<3>(args.partials, gridDim.x * gridDim.y * gridDim.z, tot, sred);
-    if (tid == 0) {
-        DevScalars *s = args.sc;
-        const double an = a0 + dt * ad1; /* g2functions.cpp:268 */
-        double ek = tot[0] / c.gridsize / 2.;
-        double ep = tot[1] / c.gridsize;
-        double eg = tot[2] / c.gridsize / 2. / an / an;
-        if constexpr (sizeof(T) == 4) {
-            MeanTraj m = mean_traj(c, s, true);
-            ep += pot_h(c.model, c.mc, m.fbn[0], m.fbn[1]);
-            for (int f = 0; f < 2; f++) { s->fbar[f] = m.fbn[f]; s->dfbar[f] = m.dfbn[f]; }
+    if constexpr (MODE != MODE_B) {
+        double tot[kNV];
+        sum_partials<kNV>(args.partials, gridDim.x * gridDim.y * gridDim.z, tot, sred);
+        if (tid == 0) {
+            finish_a<T, MODE>(c, args.sc, tot);
+            *args.counter = 0u;
         }
-        const double rho = ek + ep + eg;
-        s->a[0] = an;
-        s->edkin[0] = ek;
-        s->edpot[0] = ep;
-        s->edgrad[0] = eg;
-        s->edrho[0] = rho;
-        s->adot[0] = sqrt(c.eight_pi_3 * rho) * an; /* adf(0), :270 */
+    } else if (tid == 0) {
+        DevScalars *s = args.sc;
+        if constexpr (sizeof(T) == 4) {
+            // homogeneous trajectory to the end of the step, same RK2 scheme
+            MeanTraj q = mean_traj(c, s);
+            for (int f = 0; f < 2; f++) {
+                const double dfb1 = q.pbar[f] + ad0 * q.qbar[f];
+                const double fbn = q.fb0[f] + dt * dfb1;
+                const double dfbn = q.dfb0[f] + dt * (-dv_h(c.model, c.mc, f, q.fb1[0], q.fb1[1]) - c3H1 * dfb1);
+                s->fbar[f] = fbn;
+                s->dfbar[f] = dfbn;
+            }
+        }
+        s->a[0] = a0 + dt * ad1; /* g2functions.cpp:268 */
+        s->adot_given = 0;
         s->step += 1;
-        if (!isfinite(rho)) s->status |= ST_NONFINITE;
         *args.counter = 0u;
     }
 }
