@@ -117,14 +117,29 @@ class ClockSampler:
 
 
 def algorithmic_bytes(N: int, w: int, gws: bool) -> dict:
-    """Bytes each phase must move per step (one launch each)."""
+    """Bytes each phase must move per step (one launch each), w = bytes per
+    stored real:
+      stage1  sweep A: read f0, fdot0 (2 fields); write 2 x 5 traceless GW
+              source components (11,12,13,22,23 of both RK2 stages)
+      fft     10 real-to-complex transforms: read N^3, write N^2(N/2+1) complex each
+      kspace  read 10 transformed source components and the 4 TT amplitudes
+              (h+, hx, l+, lx), write the 4 amplitudes: 36 reals per k-point
+      stage2  sweep B: read f0, fdot0; write f0', fdot0'"""
     n3 = N ** 3
     M = N * N * (N // 2 + 1)
-    b = {"stage1": (4 + (12 if gws else 0)) * n3 * w, "stage2": 8 * n3 * w}
+    b = {"stage1": (4 + (10 if gws else 0)) * n3 * w, "stage2": 8 * n3 * w}
     if gws:
-        b["fft"] = 12 * (n3 + 2 * M) * w
-        b["kspace"] = 72 * M * w
+        b["fft"] = 10 * (n3 + 2 * M) * w
+        b["kspace"] = 36 * M * w
     return b
+
+
+def reference_formulation_bytes(w: int, gws: bool) -> int:
+    """Bytes per site-update the reference's own formulation needs at the
+    minimum (two state sweeps + one write of 2 fields: 12 words; with GWs
+    12 source words, 24 FFT words, 36 k-space words for 6 components of h
+    and l): 96/672 B in FP64, 48/336 B in FP32."""
+    return (12 + (72 if gws else 0)) * w
 
 
 def traffic_scaled(kernel: str, precision: str, N: int):
@@ -306,11 +321,16 @@ def main():
     dom = max(own, key=lambda k: own[k]["ms"])
     ach = kern[dom]["achieved_gbs"]
     step_bytes = sum(algo.values())
+    step_s = L32["ms"] / K / 1e3
+    ref_bytes = reference_formulation_bytes(w, gws) * sites
     roofline = {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
                 "traffic": traffic_scaled(dom, "fp32", N), "kernel": dom, "peak_kind": peak_kind,
                 "step_algorithmic_bytes": step_bytes,
-                "step_achieved_gbs": step_bytes / (L32["ms"] / K / 1e3) / 1e9,
-                "step_frac": step_bytes / (L32["ms"] / K / 1e3) / 1e9 / hbm_peak,
+                "step_achieved_gbs": step_bytes / step_s / 1e9,
+                "step_frac": step_bytes / step_s / 1e9 / hbm_peak,
+                "reference_formulation_bytes_per_site": reference_formulation_bytes(w, gws),
+                "reference_formulation_gbs": ref_bytes / step_s / 1e9,
+                "reference_formulation_frac": ref_bytes / step_s / 1e9 / hbm_peak,
                 "kernels": kern}
     extra = {}
     if "fp64" in legs:

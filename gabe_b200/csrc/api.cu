@@ -36,7 +36,8 @@ struct gabe_handle {
     size_t n3 = 0, M = 0, esz = 8;
     cudaStream_t stream = nullptr;
     void *X[2] = {nullptr, nullptr}, *D[2] = {nullptr, nullptr};
-    void *H = nullptr, *L = nullptr;
+    void *G = nullptr;  // GW amplitudes h+, hx, l+, lx [4][M] complex
+    double *gwnorm = nullptr;  // upload check: |h|^2, |h - TT(h)|^2, |l|^2, |l - TT(l)|^2
     void *S = nullptr;  // sources / spectra scratch / staging
     size_t S_bytes = 0;
     int nslots = 0;
@@ -167,7 +168,8 @@ int make_plans(gabe_handle *h) {
         CF(h, cufftCreate(&h->plan_src));
         h->have_plan_src = true;
         CF(h, cufftSetAutoAllocation(h->plan_src, 0));
-        CF(h, cufftMakePlanMany64(h->plan_src, 3, n, inem, 1, N * N * 2 * nz, onem, 1, N * N * nz, t, 12, &ws_src));
+        CF(h, cufftMakePlanMany64(h->plan_src, 3, n, inem, 1, N * N * 2 * nz, onem, 1, N * N * nz, t, 2 * kSrc,
+                                  &ws_src));
     }
     {
         long long inem[3] = {N, N, N}, onem[3] = {N, N, nz};
@@ -229,8 +231,7 @@ int enqueue_step(gabe_handle *h, int cur, cudaEvent_t *ev = nullptr) {
         if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
         KspaceArgs k{};
         k.S = h->S;
-        k.h = h->H;
-        k.l = h->L;
+        k.G = h->G;
         k.sc = h->sc;
         k.c = h->lc;
         Launch lk{dim3(148 * 8), dim3(256), 0, h->stream};
@@ -291,6 +292,63 @@ int read_scalars(gabe_handle *h, DevScalars *out) {
 double *dev_mean(gabe_handle *h, bool momentum, int f) {
     const size_t off = momentum ? offsetof(DevScalars, dfbar) : offsetof(DevScalars, fbar);
     return reinterpret_cast<double *>(reinterpret_cast<char *>(h->sc) + off) + f;
+}
+
+// k-points per staging chunk for the 12-component FP64 GW layout
+size_t gw_chunk(gabe_handle *h) {
+    size_t c = h->S_bytes / (12 * sizeof(double));
+    return c < h->M ? c : h->M;
+}
+
+// h0/l0 in the reference layout -> amplitudes, rejecting non-TT input.
+int upload_gw(gabe_handle *h, const double *h0, const double *l0) {
+    double *stage = static_cast<double *>(h->S);
+    const size_t chunk = gw_chunk(h), M = h->M;
+    CK(h, cudaMemsetAsync(h->gwnorm, 0, 4 * sizeof(double), h->stream));
+    const double *src[2] = {h0, l0};
+    for (int w = 0; w < 2; w++) {
+        if (!src[w]) {
+            CK(h, cudaMemsetAsync(static_cast<char *>(h->G) + (size_t)2 * w * M * 2 * h->esz, 0, 2 * M * 2 * h->esz,
+                                  h->stream));
+            continue;
+        }
+        for (size_t m0 = 0; m0 < M; m0 += chunk) {
+            const size_t cnt = (M - m0) < chunk ? (M - m0) : chunk;
+            for (int q = 0; q < 12; q++)
+                CK(h, cudaMemcpyAsync(stage + (size_t)q * cnt, src[w] + (size_t)q * M + m0, cnt * 8,
+                                      cudaMemcpyHostToDevice, h->stream));
+            CK(h, h->f32 ? gw_pack_f32(stage, cnt, m0, h->N, M, h->G, w, h->gwnorm + 2 * w, h->stream)
+                         : gw_pack_f64(stage, cnt, m0, h->N, M, h->G, w, h->gwnorm + 2 * w, h->stream));
+        }
+    }
+    double nr[4];
+    CK(h, cudaMemcpyAsync(nr, h->gwnorm, sizeof(nr), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (int w = 0; w < 2; w++)
+        if (!(nr[2 * w + 1] <= 1e-20 * nr[2 * w]))
+            return set_err(h, GABE_ERR_PARAM,
+                           "%s0 is not transverse-traceless (relative non-TT norm %.3g); the evolution keeps h and l "
+                           "TT, so only TT data (e.g. from a previous run) can be uploaded",
+                           w ? "l" : "h", nr[2 * w] > 0 ? sqrt(nr[2 * w + 1] / nr[2 * w]) : 0.0);
+    return GABE_OK;
+}
+
+int download_gw(gabe_handle *h, double *h0, double *l0) {
+    double *stage = static_cast<double *>(h->S);
+    const size_t chunk = gw_chunk(h), M = h->M;
+    double *dst[2] = {h0, l0};
+    for (int w = 0; w < 2; w++) {
+        if (!dst[w]) continue;
+        for (size_t m0 = 0; m0 < M; m0 += chunk) {
+            const size_t cnt = (M - m0) < chunk ? (M - m0) : chunk;
+            CK(h, h->f32 ? gw_unpack_f32(h->G, cnt, m0, h->N, M, w, stage, h->stream)
+                         : gw_unpack_f64(h->G, cnt, m0, h->N, M, w, stage, h->stream));
+            for (int q = 0; q < 12; q++)
+                CK(h, cudaMemcpyAsync(dst[w] + (size_t)q * M + m0, stage + (size_t)q * cnt, cnt * 8,
+                                      cudaMemcpyDeviceToHost, h->stream));
+        }
+    }
+    return GABE_OK;
 }
 
 int mean_blocks(size_t n) {
@@ -393,11 +451,11 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
         if ((rc = dalloc(h, &h->D[b], field_bytes))) return bail(rc);
     }
     if (p->calc_gws) {
-        if ((rc = dalloc(h, &h->H, 12 * h->M * h->esz))) return bail(rc);
-        if ((rc = dalloc(h, &h->L, 12 * h->M * h->esz))) return bail(rc);
+        if ((rc = dalloc(h, &h->G, 8 * h->M * h->esz))) return bail(rc);
+        if ((rc = dalloc(h, (void **)&h->gwnorm, 4 * sizeof(double)))) return bail(rc);
     }
-    // sources need 12 padded slots; spectra need 2; the FP32 upload stages one FP64 field array
-    h->nslots = p->calc_gws ? 12 : 2;
+    // sources need 10 padded slots; spectra need 2; uploads stage one FP64 field array
+    h->nslots = p->calc_gws ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
     const size_t nblk_stencil = (size_t)h->grid.x * h->grid.y * h->grid.z;
@@ -428,7 +486,7 @@ int gabe_destroy(gabe_handle *h) {
         if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
     if (h->have_plan_src) cufftDestroy(h->plan_src);
     if (h->have_plan_spec) cufftDestroy(h->plan_spec);
-    void *bufs[] = {h->X[0], h->X[1], h->D[0], h->D[1], h->H, h->L, h->S, h->partials, h->counters,
+    void *bufs[] = {h->X[0], h->X[1], h->D[0], h->D[1], h->G, h->gwnorm, h->S, h->partials, h->counters,
                     h->sc, h->bin_part, h->bin_cnt_part, h->bin_sum, h->fft_work};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -455,12 +513,6 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
     if (!h->f32) {
         CK(h, cudaMemcpyAsync(h->X[0], field0, 2 * nf * 8, cudaMemcpyHostToDevice, h->stream));
         CK(h, cudaMemcpyAsync(h->D[0], dfield0, 2 * nf * 8, cudaMemcpyHostToDevice, h->stream));
-        if (h->p.calc_gws) {
-            if (h0) CK(h, cudaMemcpyAsync(h->H, h0, 12 * h->M * 8, cudaMemcpyHostToDevice, h->stream));
-            else CK(h, cudaMemsetAsync(h->H, 0, 12 * h->M * 8, h->stream));
-            if (l0) CK(h, cudaMemcpyAsync(h->L, l0, 12 * h->M * 8, cudaMemcpyHostToDevice, h->stream));
-            else CK(h, cudaMemsetAsync(h->L, 0, 12 * h->M * 8, h->stream));
-        }
     } else {
         // each field array: stage in S as FP64, take its mean, store float fluctuations
         double *stage = static_cast<double *>(h->S);
@@ -473,22 +525,10 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
                 CK(h, mean_f64(stage, nf, h->partials, h->counters + 3, mean, mean_blocks(nf), h->stream));
                 CK(h, to_fluct(stage, nf, mean, static_cast<float *>(dst[a]) + f * nf, h->stream));
             }
-        if (h->p.calc_gws) {
-            const double *gsrc[2] = {h0, l0};
-            void *gdst[2] = {h->H, h->L};
-            const size_t chunk = h->S_bytes / 8;
-            for (int a = 0; a < 2; a++) {
-                if (!gsrc[a]) {
-                    CK(h, cudaMemsetAsync(gdst[a], 0, 12 * h->M * 4, h->stream));
-                    continue;
-                }
-                for (size_t off = 0; off < 12 * h->M; off += chunk) {
-                    const size_t n = (12 * h->M - off) < chunk ? (12 * h->M - off) : chunk;
-                    CK(h, cudaMemcpyAsync(stage, gsrc[a] + off, n * 8, cudaMemcpyHostToDevice, h->stream));
-                    CK(h, to_fluct(stage, n, nullptr, static_cast<float *>(gdst[a]) + off, h->stream));
-                }
-            }
-        }
+    }
+    if (h->p.calc_gws) {
+        int rc = upload_gw(h, h0, l0);
+        if (rc) return rc;
     }
     h->cur = 0;
     h->e0_stale = true;
@@ -600,10 +640,6 @@ int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double 
     if (!h->f32) {
         if (field0) CK(h, cudaMemcpyAsync(field0, h->X[c], 2 * nf * 8, cudaMemcpyDeviceToHost, h->stream));
         if (dfield0) CK(h, cudaMemcpyAsync(dfield0, h->D[c], 2 * nf * 8, cudaMemcpyDeviceToHost, h->stream));
-        if (h->p.calc_gws) {
-            if (h0) CK(h, cudaMemcpyAsync(h0, h->H, 12 * h->M * 8, cudaMemcpyDeviceToHost, h->stream));
-            if (l0) CK(h, cudaMemcpyAsync(l0, h->L, 12 * h->M * 8, cudaMemcpyDeviceToHost, h->stream));
-        }
     } else {
         double *stage = static_cast<double *>(h->S);
         double *dst[2] = {field0, dfield0};
@@ -616,19 +652,10 @@ int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double 
                 CK(h, cudaMemcpyAsync(dst[a] + f * nf, stage, nf * 8, cudaMemcpyDeviceToHost, h->stream));
             }
         }
-        if (h->p.calc_gws) {
-            double *gdst[2] = {h0, l0};
-            const void *gsrc[2] = {h->H, h->L};
-            const size_t chunk = h->S_bytes / 8;
-            for (int a = 0; a < 2; a++) {
-                if (!gdst[a]) continue;
-                for (size_t off = 0; off < 12 * h->M; off += chunk) {
-                    const size_t n = (12 * h->M - off) < chunk ? (12 * h->M - off) : chunk;
-                    CK(h, from_fluct(static_cast<const float *>(gsrc[a]) + off, n, nullptr, stage, h->stream));
-                    CK(h, cudaMemcpyAsync(gdst[a] + off, stage, n * 8, cudaMemcpyDeviceToHost, h->stream));
-                }
-            }
-        }
+    }
+    if (h->p.calc_gws) {
+        int rc = download_gw(h, h0, l0);
+        if (rc) return rc;
     }
     CK(h, cudaStreamSynchronize(h->stream));
     return GABE_OK;
@@ -650,7 +677,7 @@ int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, in
     if (rc) return rc;
     BinArgs b{};
     b.F = h->S;
-    b.l = h->L;
+    b.G = h->G;
     b.part_sum = h->bin_part;
     b.part_cnt = h->bin_cnt_part;
     b.N = h->N;

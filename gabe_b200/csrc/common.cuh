@@ -81,19 +81,21 @@ struct MeanF {
     float pb, cb;      // homogeneous values as float
     float q0, q1;      // model constants as float
     float q2, q3;
+    float pb2, cb2;    // 2 pb, 2 cb
+    float pbsq, pb3sq; // pb^2, 3 pb^2
 };
 
 __device__ __forceinline__ float dv_diff32(const MeanF &m, int model, int fld, float a, float b) {
-    const float pb = m.pb, cb = m.cb;
-    const float C = cb + b;
+    const float pb = m.pb;
+    const float C = m.cb + b;
     if (model == MODEL_QUADRATIC) {
         // V' = phi + C1 chi^2 phi ; V'_chi = C1 phi^2 chi
-        if (fld == 0) return a + m.q0 * (pb * b * (2.f * cb + b) + a * C * C);
-        return m.q0 * (a * (2.f * pb + a) * C + pb * pb * b);
+        if (fld == 0) return a + m.q0 * (pb * b * (m.cb2 + b) + a * C * C);
+        return m.q0 * (a * (m.pb2 + a) * C + m.pbsq * b);
     }
     // V' = lam phi^3 + g chi^2 phi ; V'_chi = g phi^2 chi
-    if (fld == 0) return m.q0 * a * (3.f * pb * pb + a * (3.f * pb + a)) + m.q1 * (pb * b * (2.f * cb + b) + a * C * C);
-    return m.q1 * (a * (2.f * pb + a) * C + pb * pb * b);
+    if (fld == 0) return m.q0 * a * (m.pb3sq + a * (3.f * pb + a)) + m.q1 * (pb * b * (m.cb2 + b) + a * C * C);
+    return m.q1 * (a * (m.pb2 + a) * C + m.pbsq * b);
 }
 
 __device__ __forceinline__ float v_diff32(const MeanF &m, int model, float a, float b) {

@@ -32,6 +32,17 @@ cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l) {
     return cudaGetLastError();
 }
 
+cudaError_t gw_pack_f64(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
+                      cudaStream_t s) {
+    gw_pack_kernel<double><<<4 * 148, 256, 0, s>>>(src, cnt, m0, N, M, static_cast<Cplx<double> *>(G), which, norms);
+    return cudaGetLastError();
+}
+
+cudaError_t gw_unpack_f64(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s) {
+    gw_unpack_kernel<double><<<4 * 148, 256, 0, s>>>(static_cast<const Cplx<double> *>(G), cnt, m0, N, M, which, dst);
+    return cudaGetLastError();
+}
+
 cudaError_t bins_f64(const BinArgs &a, const Launch &l) {
     bin_kernel<double><<<l.grid, l.block, l.smem, l.stream>>>(a);
     return cudaGetLastError();

@@ -2,50 +2,69 @@
 //
 // The reference, per step, calls evolve_perts twice (g2evolutionpert.cpp:
 // 343-455): each call projects the transformed source onto its
-// transverse-traceless part into T_gw[s] (fft_stresstensor, :203-321) and
-// takes one RK2 stage of  hdot = l,  ldot = -k^2/a^2 h - 3 (adot/a) l
-// + 2 (8 pi/a^2) T  (derivs, :459-516) with the continuum k^2 = |n|^2
-// (2 pi/L)^2.  Both stages touch only their own k-point, so this kernel
-// reads h0, l0 and the two transformed sources once, forms both projections
-// in registers, takes both stages, and writes h0, l0 back: T_gw, h[1] and
-// l[1] never exist in memory.
+// transverse-traceless part T = dx^3 Lambda(k^) S (fft_stresstensor,
+// :203-321) and takes one RK2 stage of  hdot = l,  ldot = -k^2/a^2 h
+// - 3 (adot/a) l + 2 (8 pi/a^2) T  (derivs, :459-516) for all six
+// components of h and l, with k^2 = |n|^2 (2 pi/L)^2.
 //
-// Projection: T = dx^3 Lambda(k^) S with Lambda S = P S P - 1/2 P tr(P S),
-// P = 1 - k^ k^T, evaluated as S - k u^T - u k^T + s k k^T
-// - 1/2 (tr S - s) P with u = S k^, s = k^.u; for a traceless S this equals
-// the reference's explicit formulas term by term (checked against them in
-// the tests).  The k = 0 mode is set to zero as :319-321 does.
+// Storage.  h and l start at zero (g2main.cpp:58-95) and are driven only by
+// T, which is transverse-traceless, through an equation whose coefficients
+// depend on |k| alone -- so h_ij and l_ij stay TT and are fixed by two
+// polarization amplitudes per k-point:  X_ij = sum_p eps^p_ij X_p  with
+// eps^+ = e1 e1 - e2 e2, eps^x = e1 e2 + e2 e1 ({e1, e2, k^} orthonormal)
+// and X_p = eps^p : X / 2.  The device keeps (h+, hx, l+, lx) -- 8 reals per
+// k-point instead of 24 -- and converts to the reference's 12-component
+// layout only at upload/download.  The source needs only five transformed
+// components per stage (11, 12, 13, 22, 23): it is traceless in real space
+// and eps^p is traceless, so S33 = -S11 - S22 gives eps^p : S exactly.
+//
+// Per k-point this kernel reads both stages' transformed sources and the
+// four amplitudes once, forms T_p = dx^3 eps^p : S / 2 for both stages in
+// registers, takes both RK2 stages and writes the amplitudes back; T_gw,
+// h[1] and l[1] never exist in memory.  k = 0 carries no TT part (the
+// reference zeroes T there, :319-321) and stays zero.
 #pragma once
 
 #include "common.cuh"
 
 namespace gabe {
 
+template <typename T>
+struct Cplx {
+    T re, im;
+};
+
 struct KspaceArgs {
-    const void *S;   // complex half-spectra [12][N][N][N/2+1]
-    void *h, *l;     // [12][N][N][N/2+1]
+    const void *S;   // complex half-spectra [10][N][N][N/2+1]: stage-0 11,12,13,22,23 then stage-1
+    void *G;         // complex amplitudes [4][N][N][N/2+1]: h+, hx, l+, lx
     const DevScalars *sc;
     LatticeConsts c;
 };
 
-template <typename T>
-struct Cplx { T re, im; };
+// Polarization tensors of the integer wave vector n (n != 0): the six
+// components 11,12,13,22,23,33 of eps^+ and eps^x.
+__host__ __device__ inline void pol_tensors(int px, int py, int pz, double ep[6], double ex[6]) {
+    const double m = sqrt((double)px * px + (double)py * py + (double)pz * pz);
+    const double kx = px / m, ky = py / m, kz = pz / m;
+    // reference axis: the one least aligned with k
+    const double ax = fabs(kx), ay = fabs(ky), az = fabs(kz);
+    const int r = (ax <= ay && ax <= az) ? 0 : (ay <= az ? 1 : 2);
+    const double kr = r == 0 ? kx : (r == 1 ? ky : kz);
+    double e1x = (r == 0 ? 1.0 : 0.0) - kr * kx, e1y = (r == 1 ? 1.0 : 0.0) - kr * ky,
+           e1z = (r == 2 ? 1.0 : 0.0) - kr * kz;
+    const double n1 = 1.0 / sqrt(e1x * e1x + e1y * e1y + e1z * e1z);
+    e1x *= n1; e1y *= n1; e1z *= n1;
+    const double e2x = ky * e1z - kz * e1y, e2y = kz * e1x - kx * e1z, e2z = kx * e1y - ky * e1x;
+    ep[0] = e1x * e1x - e2x * e2x; ep[1] = e1x * e1y - e2x * e2y; ep[2] = e1x * e1z - e2x * e2z;
+    ep[3] = e1y * e1y - e2y * e2y; ep[4] = e1y * e1z - e2y * e2z; ep[5] = e1z * e1z - e2z * e2z;
+    ex[0] = 2. * e1x * e2x; ex[1] = e1x * e2y + e2x * e1y; ex[2] = e1x * e2z + e2x * e1z;
+    ex[3] = 2. * e1y * e2y; ex[4] = e1y * e2z + e2y * e1z; ex[5] = 2. * e1z * e2z;
+}
 
+// eps : S / 2 for a symmetric traceless S given by (S11, S12, S13, S22, S23).
 template <typename T>
-__device__ __forceinline__ void tt_project(T kx, T ky, T kz, const T *S, T nm, T *out) {
-    // S, out: 6 symmetric components 11,12,13,22,23,33 (one of re/im)
-    const T S11 = S[0], S12 = S[1], S13 = S[2], S22 = S[3], S23 = S[4], S33 = S[5];
-    const T u1 = S11 * kx + S12 * ky + S13 * kz;
-    const T u2 = S12 * kx + S22 * ky + S23 * kz;
-    const T u3 = S13 * kx + S23 * ky + S33 * kz;
-    const T s = kx * u1 + ky * u2 + kz * u3;
-    const T g = T(0.5) * ((S11 + S22 + S33) - s);
-    out[0] = nm * (S11 - T(2) * kx * u1 + s * kx * kx - g * (T(1) - kx * kx));
-    out[1] = nm * (S12 - kx * u2 - u1 * ky + (s + g) * kx * ky);
-    out[2] = nm * (S13 - kx * u3 - u1 * kz + (s + g) * kx * kz);
-    out[3] = nm * (S22 - T(2) * ky * u2 + s * ky * ky - g * (T(1) - ky * ky));
-    out[4] = nm * (S23 - ky * u3 - u2 * kz + (s + g) * ky * kz);
-    out[5] = nm * (S33 - T(2) * kz * u3 + s * kz * kz - g * (T(1) - kz * kz));
+__device__ __forceinline__ T pol_contract(const T *w, const T *S) {
+    return w[0] * S[0] + w[1] * S[1] + w[2] * S[2] + w[3] * S[3] + w[4] * S[4];
 }
 
 template <typename T>
@@ -59,53 +78,142 @@ __global__ void __launch_bounds__(256) kspace_kernel(KspaceArgs args) {
     const double norm0 = c.k2norm_c / a0 / a0, norm1 = c.k2norm_c / a1 / a1;
     const double om0 = c.eight_pi / a0 / a0, om1 = c.eight_pi / a1 / a1;
     const T c3H0 = (T)(3. * ad0 / a0), c3H1 = (T)(3. * ad1 / a1);
-    const T two_om0 = (T)(2. * om0), two_om1 = (T)(2. * om1);
-    const T hdt = (T)c.half_dt, dt = (T)c.dt, nm = (T)c.normmm;
+    const T src0 = (T)(2. * om0 * c.normmm), src1 = (T)(2. * om1 * c.normmm);
+    const T hdt = (T)c.half_dt, dt = (T)c.dt;
     const Cplx<T> *Sc = static_cast<const Cplx<T> *>(args.S);
-    T *H = static_cast<T *>(args.h), *Lh = static_cast<T *>(args.l);
+    Cplx<T> *G = static_cast<Cplx<T> *>(args.G);
 
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < M; idx += (size_t)gridDim.x * blockDim.x) {
+        Cplx<T> s[10], g[4];
+#pragma unroll
+        for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
+#pragma unroll
+        for (int q = 0; q < 4; q++) g[q] = G[(size_t)q * M + idx];
         const int kzi = (int)(idx % nz);
         const size_t t = idx / nz;
         const int j = (int)(t % N), i = (int)(t / N);
         const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
         const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
+        if (m2 == 0.0) continue;  // no TT mode at k = 0; its amplitudes stay zero
+        double ep[6], ex[6];
+        pol_tensors(px, py, kzi, ep, ex);
+        // weights of (S11, S12, S13, S22, S23) in eps:S/2 with S33 = -S11-S22
+        const T wp[5] = {(T)(0.5 * (ep[0] - ep[5])), (T)ep[1], (T)ep[2], (T)(0.5 * (ep[3] - ep[5])), (T)ep[4]};
+        const T wx[5] = {(T)(0.5 * (ex[0] - ex[5])), (T)ex[1], (T)ex[2], (T)(0.5 * (ex[3] - ex[5])), (T)ex[4]};
         const T kk0 = (T)(m2 * norm0), kk1 = (T)(m2 * norm1);
-        T T0[12], T1[12];
-        if (m2 == 0.0) {
+        T Tp[2][2][2];  // [stage][pol][re/im], already times 2 (8 pi/a^2) dx^3
 #pragma unroll
-            for (int q = 0; q < 12; q++) { T0[q] = T(0); T1[q] = T(0); }
-        } else {
-            const double inv = 1.0 / sqrt(m2);
-            const T kx = (T)(px * inv), ky = (T)(py * inv), kz = (T)(kzi * inv);
-            T sr[6], si[6], tr[6], ti[6];
+        for (int st = 0; st < 2; st++) {
+            T sr[5], si[5];
 #pragma unroll
-            for (int st = 0; st < 2; st++) {
-#pragma unroll
-                for (int q = 0; q < 6; q++) {
-                    const Cplx<T> v = Sc[(size_t)(6 * st + q) * M + idx];
-                    sr[q] = v.re;
-                    si[q] = v.im;
-                }
-                tt_project(kx, ky, kz, sr, nm, tr);
-                tt_project(kx, ky, kz, si, nm, ti);
-                T *dst = st == 0 ? T0 : T1;
-#pragma unroll
-                for (int q = 0; q < 6; q++) { dst[2 * q] = tr[q]; dst[2 * q + 1] = ti[q]; }
-            }
+            for (int q = 0; q < 5; q++) { sr[q] = s[5 * st + q].re; si[q] = s[5 * st + q].im; }
+            const T f = st == 0 ? src0 : src1;
+            Tp[st][0][0] = f * pol_contract(wp, sr);
+            Tp[st][0][1] = f * pol_contract(wp, si);
+            Tp[st][1][0] = f * pol_contract(wx, sr);
+            Tp[st][1][1] = f * pol_contract(wx, si);
         }
 #pragma unroll
-        for (int q = 0; q < 12; q++) {
-            const size_t g = (size_t)q * M + idx;
-            const T h0 = H[g], l0 = Lh[g];
-            // stage 1: evolve_perts(0, 1, dt/2)
-            const T ld0 = -kk0 * h0 - c3H0 * l0 + two_om0 * T0[q];
-            const T h1 = h0 + hdt * l0;
-            const T l1 = l0 + hdt * ld0;
-            // stage 2: evolve_perts(1, 0, dt)
-            const T ld1 = -kk1 * h1 - c3H1 * l1 + two_om1 * T1[q];
-            H[g] = h0 + dt * l1;
-            Lh[g] = l0 + dt * ld1;
+        for (int p = 0; p < 2; p++) {
+            Cplx<T> hn, ln;
+#pragma unroll
+            for (int ri = 0; ri < 2; ri++) {
+                const T h0 = ri ? g[p].im : g[p].re, l0 = ri ? g[2 + p].im : g[2 + p].re;
+                // stage 1: evolve_perts(0, 1, dt/2)
+                const T ld0 = -kk0 * h0 - c3H0 * l0 + Tp[0][p][ri];
+                const T h1 = h0 + hdt * l0;
+                const T l1 = l0 + hdt * ld0;
+                // stage 2: evolve_perts(1, 0, dt)
+                const T ld1 = -kk1 * h1 - c3H1 * l1 + Tp[1][p][ri];
+                (ri ? hn.im : hn.re) = h0 + dt * l1;
+                (ri ? ln.im : ln.re) = l0 + dt * ld1;
+            }
+            G[(size_t)p * M + idx] = hn;
+            G[(size_t)(2 + p) * M + idx] = ln;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// conversions between the reference's 12-component layout (FP64 host data,
+// staged in device memory as [12][cnt]) and the amplitudes, for k-points
+// m0 .. m0+cnt-1 of the half spectrum.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void gw_pack_kernel(const double *src, size_t cnt, size_t m0, int N, size_t M, Cplx<T> *G, int which,
+                               double *norms /* [2]: |X|^2, |X - TT(X)|^2 */) {
+    const int nz = N / 2 + 1;
+    double nrm = 0., res = 0.;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t idx = m0 + q;
+        const int kzi = (int)(idx % nz);
+        const size_t t = idx / nz;
+        const int j = (int)(t % N), i = (int)(t / N);
+        const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
+        double X[2][6];  // [re/im][component]
+#pragma unroll
+        for (int c6 = 0; c6 < 6; c6++) {
+            X[0][c6] = src[(size_t)(2 * c6) * cnt + q];
+            X[1][c6] = src[(size_t)(2 * c6 + 1) * cnt + q];
+        }
+        Cplx<T> ap = {0, 0}, ax = {0, 0};
+        double ep[6] = {0, 0, 0, 0, 0, 0}, ex[6] = {0, 0, 0, 0, 0, 0};
+        double A[2][2] = {{0, 0}, {0, 0}};  // [pol][re/im]
+        if (px || py || kzi) {
+            pol_tensors(px, py, kzi, ep, ex);
+            const double w[6] = {1, 2, 2, 1, 2, 1};  // eps:X over all 9 entries
+#pragma unroll
+            for (int ri = 0; ri < 2; ri++) {
+                double sp = 0., sx = 0.;
+#pragma unroll
+                for (int c6 = 0; c6 < 6; c6++) {
+                    sp += w[c6] * ep[c6] * X[ri][c6];
+                    sx += w[c6] * ex[c6] * X[ri][c6];
+                }
+                A[0][ri] = 0.5 * sp;
+                A[1][ri] = 0.5 * sx;
+            }
+            ap = {(T)A[0][0], (T)A[0][1]};
+            ax = {(T)A[1][0], (T)A[1][1]};
+        }
+        const double w9[6] = {1, 2, 2, 1, 2, 1};
+#pragma unroll
+        for (int ri = 0; ri < 2; ri++)
+#pragma unroll
+            for (int c6 = 0; c6 < 6; c6++) {
+                const double r = X[ri][c6] - (ep[c6] * A[0][ri] + ex[c6] * A[1][ri]);
+                nrm += w9[c6] * X[ri][c6] * X[ri][c6];
+                res += w9[c6] * r * r;
+            }
+        G[(size_t)(2 * which) * M + idx] = ap;
+        G[(size_t)(2 * which + 1) * M + idx] = ax;
+    }
+    // block sums then one atomic pair per block (a check, order is irrelevant)
+    __shared__ double sred[8 * 2];
+    double v[2] = {nrm, res};
+    block_reduce<2>(v, sred);
+    if (threadIdx.x == 0) {
+        atomicAdd(norms, v[0]);
+        atomicAdd(norms + 1, v[1]);
+    }
+}
+
+template <typename T>
+__global__ void gw_unpack_kernel(const Cplx<T> *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst) {
+    const int nz = N / 2 + 1;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t idx = m0 + q;
+        const int kzi = (int)(idx % nz);
+        const size_t t = idx / nz;
+        const int j = (int)(t % N), i = (int)(t / N);
+        const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
+        double ep[6] = {0, 0, 0, 0, 0, 0}, ex[6] = {0, 0, 0, 0, 0, 0};
+        if (px || py || kzi) pol_tensors(px, py, kzi, ep, ex);
+        const Cplx<T> ap = G[(size_t)(2 * which) * M + idx], ax = G[(size_t)(2 * which + 1) * M + idx];
+#pragma unroll
+        for (int c6 = 0; c6 < 6; c6++) {
+            dst[(size_t)(2 * c6) * cnt + q] = ep[c6] * (double)ap.re + ex[c6] * (double)ax.re;
+            dst[(size_t)(2 * c6 + 1) * cnt + q] = ep[c6] * (double)ap.im + ex[c6] * (double)ax.im;
         }
     }
 }

@@ -29,6 +29,12 @@ cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);
 cudaError_t bins_f64(const BinArgs &a, const Launch &l);
 cudaError_t bins_f32(const BinArgs &a, const Launch &l);
 cudaError_t configure_bins(size_t max_smem);
+cudaError_t gw_pack_f64(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
+                        cudaStream_t s);
+cudaError_t gw_pack_f32(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
+                        cudaStream_t s);
+cudaError_t gw_unpack_f64(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s);
+cudaError_t gw_unpack_f32(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s);
 
 cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *counter, double *out, int nblocks,
                      cudaStream_t s);

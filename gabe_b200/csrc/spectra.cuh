@@ -16,7 +16,7 @@ namespace gabe {
 
 struct BinArgs {
     const void *F;          // complex field spectra, 2 slots [2][N][N][N/2+1]
-    const void *l;          // GW momenta [12][N][N][N/2+1] or null
+    const void *G;          // GW amplitudes [4][N][N][N/2+1] complex (h+, hx, l+, lx) or null
     double *part_sum;       // [nblocks][nseries][nbins]
     unsigned int *part_cnt; // [nblocks][nbins]
     int N, nbins, nseries, quirk;
@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(256) bin_kernel(BinArgs a) {
     for (int q = threadIdx.x; q < nb; q += blockDim.x) hc[q] = 0u;
     __syncthreads();
     const T *F = static_cast<const T *>(a.F);
-    const T *L = static_cast<const T *>(a.l);
+    const T *G = static_cast<const T *>(a.G);
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < M; idx += (size_t)gridDim.x * blockDim.x) {
         const int kz = (int)(idx % nz);
         const size_t t = idx / nz;
@@ -51,13 +51,12 @@ __global__ void __launch_bounds__(256) bin_kernel(BinArgs a) {
             atomicAdd(&hs[f * nb + b], w * (re * re + im * im));
         }
         if (ns > 2) {
+            // sum_ij |l_ij|^2 with the reference's weights (diagonal 1,
+            // off-diagonal 2) = 2 (|l+|^2 + |lx|^2) for a TT tensor
             const size_t src = (a.quirk && kz == 0) ? idx + (size_t)(N / 2) : idx;
-            double v[12];
-#pragma unroll
-            for (int q = 0; q < 12; q++) v[q] = (double)L[(size_t)q * M + src];
-            const double p = v[0] * v[0] + v[1] * v[1] + 2. * v[2] * v[2] + 2. * v[3] * v[3] + 2. * v[4] * v[4] +
-                             2. * v[5] * v[5] + v[6] * v[6] + v[7] * v[7] + 2. * v[8] * v[8] + 2. * v[9] * v[9] +
-                             v[10] * v[10] + v[11] * v[11];
+            const double pr = (double)G[2 * (2 * M + src)], pi = (double)G[2 * (2 * M + src) + 1];
+            const double xr = (double)G[2 * (3 * M + src)], xi = (double)G[2 * (3 * M + src) + 1];
+            const double p = 2. * ((pr * pr + pi * pi) + (xr * xr + xi * xi));
             atomicAdd(&hs[2 * nb + b], w * p);
         }
     }

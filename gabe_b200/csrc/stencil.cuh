@@ -44,7 +44,7 @@ struct StencilArgs {
     const void *D;       // momenta in [2][N^3]
     void *Xo;            // fields out   (sweep B)
     void *Do;            // momenta out  (sweep B)
-    void *S;             // GW sources [12][N][N][N+2] (sweep A with GWs)
+    void *S;             // GW sources [10][N][N][N+2] (sweep A with GWs)
     double *partials;    // [nblocks][8]
     unsigned int *counter;
     DevScalars *sc;
@@ -64,16 +64,15 @@ struct Nb7 {
 __device__ __forceinline__ double lap64(const Nb7<double> &f, double dx2) {
     return (f.v[1] + f.v[2] + f.v[3] + f.v[4] + f.v[5] + f.v[6] - 6. * f.v[0]) / dx2;
 }
-// FP32: sum of neighbour differences (each difference of nearby values is
-// formed exactly, so the small Laplacian of a smooth fluctuation keeps its
-// relative precision).
 __device__ __forceinline__ float lap32(const Nb7<float> &f, float inv_dx2) {
-    const float c = f.v[0];
-    return (((f.v[1] - c) + (f.v[2] - c)) + ((f.v[3] - c) + (f.v[4] - c)) + ((f.v[5] - c) + (f.v[6] - c))) * inv_dx2;
+    return fmaf(-6.f, f.v[0], ((f.v[1] + f.v[2]) + (f.v[3] + f.v[4])) + (f.v[5] + f.v[6])) * inv_dx2;
 }
 
-// GW source components 11,12,13,22,23,33 of one field added into s
-// (jtg_stresstensor, g2evolutionpert.cpp:48-132, operation order kept).
+// GW source components 11,12,13,22,23 of one field added into s
+// (jtg_stresstensor, g2evolutionpert.cpp:48-132, operation order kept).  The
+// source is traceless, so component 33 (= -11 - 22) is never stored: the
+// k-space update needs only the five (kspace.cuh).
+constexpr int kSrc = 5;
 __device__ __forceinline__ void source_add64(const LatticeConsts &c, const Nb7<double> &f, double *s) {
     const double d1 = (f.v[1] - f.v[2]) / 2;
     const double d2 = (f.v[3] - f.v[4]) / 2;
@@ -84,7 +83,6 @@ __device__ __forceinline__ void source_add64(const LatticeConsts &c, const Nb7<d
     s[2] += (dn * d1 * d3);
     s[3] += -c13 * d1 * d1 + c23 * d2 * d2 - c13 * d3 * d3;
     s[4] += (dn * d2 * d3);
-    s[5] += -c13 * d1 * d1 - c13 * d2 * d2 + c23 * d3 * d3;
 }
 __device__ __forceinline__ void source_add32(float dn, const Nb7<float> &f, float *s) {
     const float d1 = 0.5f * (f.v[1] - f.v[2]);
@@ -96,7 +94,6 @@ __device__ __forceinline__ void source_add32(float dn, const Nb7<float> &f, floa
     s[2] += dn * d1 * d3;
     s[3] += dn * (d2 * d2 - t);
     s[4] += dn * d2 * d3;
-    s[5] += dn * (d3 * d3 - t);
 }
 
 // Homogeneous-trajectory values of the FP32 path (start and midpoint of a
@@ -124,6 +121,10 @@ __device__ __forceinline__ MeanF mean_f(const LatticeConsts &c, const double *fb
     m.q1 = (float)c.mc[1];
     m.q2 = (float)c.mc[2];
     m.q3 = (float)c.mc[3];
+    m.pb2 = (float)(2. * fb[0]);
+    m.cb2 = (float)(2. * fb[1]);
+    m.pbsq = (float)(fb[0] * fb[0]);
+    m.pb3sq = (float)(3. * fb[0] * fb[0]);
     return m;
 }
 
@@ -202,9 +203,9 @@ __device__ __forceinline__ void store_sources(T *S, int N, int i, int j, int k, 
     const size_t slot = (size_t)N * N * (N + 2);
     const size_t o = ((size_t)i * N + j) * (N + 2) + k;
 #pragma unroll
-    for (int q = 0; q < 6; q++) {
+    for (int q = 0; q < kSrc; q++) {
         S[q * slot + o] = s0[q];
-        S[(6 + q) * slot + o] = s1[q];
+        S[(kSrc + q) * slot + o] = s1[q];
     }
 }
 
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
                 }
             }
         } else {
-            T s0[6] = {0, 0, 0, 0, 0, 0}, s1[6] = {0, 0, 0, 0, 0, 0};
+            T s0[kSrc] = {0, 0, 0, 0, 0}, s1[kSrc] = {0, 0, 0, 0, 0};
             if constexpr (sizeof(T) == 8) {
                 for (int f = 0; f < 2; f++) {
                     const double lap0 = lap64(f0[f], c.inv_dx2_div);

@@ -27,3 +27,18 @@ def tt_project(k, S):
 def sym(S):
     S11, S12, S13, S22, S23, S33 = S
     return np.array([[S11, S12, S13], [S12, S22, S23], [S13, S23, S33]])
+
+
+def pol_tensors(n):
+    """numpy restatement of pol_tensors() in gabe_b200/csrc/kspace.cuh."""
+    k = np.asarray(n, dtype=float) / np.linalg.norm(n)
+    r = int(np.argmin(np.abs(k))) if len(set(np.abs(k))) == 3 else (
+        0 if abs(k[0]) <= abs(k[1]) and abs(k[0]) <= abs(k[2]) else (1 if abs(k[1]) <= abs(k[2]) else 2))
+    a = np.zeros(3)
+    a[r] = 1.0
+    e1 = a - k[r] * k
+    e1 /= np.linalg.norm(e1)
+    e2 = np.cross(k, e1)
+    ep = np.outer(e1, e1) - np.outer(e2, e2)
+    ex = np.outer(e1, e2) + np.outer(e2, e1)
+    return ep, ex

@@ -65,9 +65,15 @@ def _scalar_tol(name, want, rho):
 
 
 def _spectra_close(got, want):
-    np.testing.assert_allclose(got[:, :5], want[:, :5], rtol=1e-8, atol=1e-300)
-    if want.shape[1] > 5:
-        np.testing.assert_allclose(got[:, 5:], want[:, 5:], rtol=1e-6, atol=1e-300)
+    """Per bin rtol, plus a floor set by the largest value of each column
+    (FFT rounding is relative to the largest mode, so nearly empty bins such
+    as chi's k=0 bin carry absolute, not relative, noise)."""
+    for cols, rtol, floor in ((slice(0, 5), 1e-8, 1e-12), (slice(5, None), 1e-6, 1e-10)):
+        g, w = got[:, cols], want[:, cols]
+        if w.size == 0:
+            continue
+        tol = rtol * np.abs(w) + floor * np.abs(w).max(axis=0, keepdims=True)
+        assert np.all(np.abs(g - w) <= tol), np.max(np.abs(g - w) / np.maximum(tol, 1e-300))
 
 
 CASES = [
@@ -253,21 +259,29 @@ def test_fp32_against_fp64(gws):
 
 
 def test_upload_download_roundtrip():
+    """h and l are kept as two TT polarization amplitudes; TT data (any state
+    the evolution produced) round-trips, non-TT data is refused."""
     cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=1)
     st = po.init_state(cfg)
-    st.l[0] = np.random.default_rng(0).standard_normal(st.l[0].shape) * 1e-9
+    po.step(st, 6)
+    for prec, tol in ((gb.FP64, 1e-14), (gb.FP32, 1e-6)):
+        with _lattice(cfg, precision=prec) as lat:
+            _upload(lat, st)
+            f, d, h, l = lat.download_state()
+            if prec == gb.FP64:
+                np.testing.assert_array_equal(f, st.field[0])
+                np.testing.assert_array_equal(d, st.dfield[0])
+            else:
+                for q in range(2):
+                    fl = st.field[0, q] - st.field[0, q].mean()
+                    assert np.abs(f[q] - st.field[0, q]).max() <= 1e-6 * np.abs(fl).max() + 1e-15
+            assert _norm_rel(h, st.h[0]) <= tol and _norm_rel(l, st.l[0]) <= tol
+    bad = st.copy()
+    bad.l[0] = np.random.default_rng(0).standard_normal(bad.l[0].shape) * 1e-9
     with _lattice(cfg) as lat:
-        _upload(lat, st)
-        f, d, h, l = lat.download_state()
-        np.testing.assert_array_equal(f, st.field[0])
-        np.testing.assert_array_equal(l, st.l[0])
-    with _lattice(cfg, precision=gb.FP32) as lat:
-        _upload(lat, st)
-        f, d, h, l = lat.download_state()
-        for q in range(2):
-            fl = st.field[0, q] - st.field[0, q].mean()
-            assert np.abs(f[q] - st.field[0, q]).max() <= 1e-6 * np.abs(fl).max() + 1e-15
-        assert np.abs(l - st.l[0]).max() <= 1e-6 * np.abs(st.l[0]).max()
+        with pytest.raises(gb.GabeError) as ei:
+            _upload(lat, bad)
+        assert ei.value.code == 1
 
 
 def test_nonfinite_state_is_reported():

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
-from tests.kspace_ref import sym, tt_project
+from tests.kspace_ref import pol_tensors, sym, tt_project
 
 
 def test_laplacian_plane_wave_eigenvalue():
@@ -118,3 +118,26 @@ def test_spectra_parseval_and_bins():
         tot = (sp[:, 1 + 2 * f] * cnt / spec_norm).sum()
         want = N ** 3 * (st.field[0, f] ** 2).sum()
         assert abs(tot - want) <= 1e-10 * want
+
+
+@pytest.mark.parametrize("n", [(1, 0, 0), (0, 0, 3), (0, 2, 0), (1, 1, 0), (3, -2, 5), (-4, 4, 4), (2, -7, 1)])
+def test_polarization_basis_spans_the_tt_projector(n):
+    """sum_p eps^p (x) eps^p / 2 equals Lambda, so evolving the two
+    amplitudes X_p = eps^p:X/2 reproduces the six-component TT evolution;
+    and with S33 = -S11 - S22 the traceless source gives the same eps^p:S."""
+    ep, ex = pol_tensors(n)
+    k = np.asarray(n, float) / np.linalg.norm(n)
+    P = np.eye(3) - np.outer(k, k)
+    lam = np.einsum("il,jm->ijlm", P, P) - 0.5 * np.einsum("ij,lm->ijlm", P, P)
+    got = 0.5 * (np.einsum("ij,lm->ijlm", ep, ep) + np.einsum("ij,lm->ijlm", ex, ex))
+    # Lambda acting on symmetric tensors: symmetrise over (l, m)
+    lam_s = 0.5 * (lam + lam.transpose(0, 1, 3, 2))
+    np.testing.assert_allclose(got, lam_s, atol=1e-14)
+    for e in (ep, ex):
+        assert abs(np.trace(e)) < 1e-14 and np.abs(e @ k).max() < 1e-14
+        assert abs(np.sum(e * e) - 2.0) < 1e-14
+    rng = np.random.default_rng(3)
+    S = rng.standard_normal((3, 3)); S = S + S.T; S -= np.trace(S) / 3 * np.eye(3)
+    T = np.einsum("ijlm,lm->ij", lam, S)
+    recon = 0.5 * (np.sum(ep * S) * ep + np.sum(ex * S) * ex)
+    np.testing.assert_allclose(recon, T, atol=1e-13)
