@@ -252,8 +252,11 @@ def test_fp32_against_fp64(gws):
             fl = f64[q] - f64[q].mean()
             assert np.abs((f32[q] - f32[q].mean()) - fl).max() <= 1e-3 * np.abs(fl).max()
         s64, s32 = l64.spec_out(), l32.spec_out()
-        nz = s64[:, 1:5] != 0
-        assert np.max(np.abs(s32[:, 1:5][nz] - s64[:, 1:5][nz]) / np.abs(s64[:, 1:5][nz])) <= 1e-3
+        # per-bin spectrum error <= 1e-4 relative, above the FFT noise floor
+        # of each column (chi's k=0 bin holds only rounding noise)
+        w, g = s64[:, 1:5], s32[:, 1:5]
+        floor = 1e-9 * np.abs(w).max(axis=0, keepdims=True)
+        assert np.all(np.abs(g - w) <= 1e-4 * np.abs(w) + floor)
         if gws:
             assert _norm_rel(ll32, ll64) <= 1e-3
 
