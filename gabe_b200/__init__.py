@@ -50,7 +50,7 @@ class GabeError(RuntimeError):
 class Params(ctypes.Structure):
     _fields_ = [
         ("struct_size", ctypes.c_int32), ("N", ctypes.c_int32), ("nflds", ctypes.c_int32),
-        ("calc_gws", ctypes.c_int32), ("expansion_type", ctypes.c_int32), ("model", ctypes.c_int32),
+        ("gws_on", ctypes.c_int32), ("expansion", ctypes.c_int32), ("model", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("gw_spec_quirk", ctypes.c_int32),
         ("L", ctypes.c_double), ("dt", ctypes.c_double), ("model_c", ctypes.c_double * 2),
         ("device", ctypes.c_int32), ("flags", ctypes.c_int32), ("tile_ci", ctypes.c_int32),
@@ -127,7 +127,7 @@ class Lattice:
         lib = library()
         p = Params()
         lib.gabe_default_params(ctypes.byref(p), int(N))
-        p.L, p.dt, p.calc_gws, p.model, p.precision = float(L), float(dt), int(bool(gws)), int(model), int(precision)
+        p.L, p.dt, p.gws_on, p.model, p.precision = float(L), float(dt), int(bool(gws)), int(model), int(precision)
         if model_c is None:
             model_c = lphi4_constants() if model == MODEL_LPHI4 else (1e-6, 2.5e-7)
         p.model_c[0], p.model_c[1] = float(model_c[0]), float(model_c[1])

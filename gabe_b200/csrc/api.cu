@@ -101,61 +101,11 @@ int dalloc(gabe_handle *h, void **ptr, size_t bytes) {
     return GABE_OK;
 }
 
-// Constants with the operation sequence the reference's compiler folds
-// (g2parameters.h:93, g2functions.cpp:41, g2evolutionpert.cpp:53,198,486-487,
-// g2model.cpp:64,68).
-LatticeConsts make_consts(const gabe_params &p) {
-    LatticeConsts c{};
-    c.N = p.N;
-    c.model = p.model;
-    const double L = p.L, dt = p.dt;
-    const double dx = L / ((double)p.N);
-    c.dt = dt;
-    c.half_dt = .5 * dt;
-    c.inv_dx2_div = dx * dx;
-    c.dn = (double)(1 / (dx * dx));
-    c.c13 = (1. / 3.) * c.dn;
-    c.c23 = (2. / 3.) * c.dn;
-    if (p.model == GABE_MODEL_QUADRATIC) {
-        const double mphi = p.model_c[0], gsq = p.model_c[1];
-        c.mc[0] = gsq / mphi / mphi;
-        c.mc[1] = 0.5 * gsq / mphi / mphi;
-    } else {
-        const double lam = p.model_c[0], g = p.model_c[1];
-        c.mc[0] = lam;
-        c.mc[1] = g;
-        c.mc[2] = 0.25 * lam;
-        c.mc[3] = 0.5 * g;
-        c.mc[4] = 3. * lam;
-    }
-    c.gridsize = (double)((long long)p.N * p.N * p.N);
-    c.eight_pi_3 = 8. * M_PI / 3.;
-    c.k2norm_c = 4. * M_PI * M_PI / L / L;
-    c.eight_pi = 8. * M_PI;
-    c.normmm = pow(dx, 3);
-    return c;
-}
-
-bool shape_fits(int shape, int N) {
-    const int tk = kShapes[shape][0], tj = kShapes[shape][1];
-    return tk <= N && tj <= N && N % tk == 0 && N % tj == 0;
-}
-
 void choose_tile(gabe_handle *h) {
-    const int N = h->N;
-    int shape = -1;
-    if (h->p.tile_shape >= 0 && h->p.tile_shape < kNumShapes && shape_fits(h->p.tile_shape, N)) shape = h->p.tile_shape;
-    for (int q = 0; shape < 0 && q < kNumShapes; q++)
-        if (shape_fits(q, N)) shape = q;
-    const int TK = kShapes[shape][0], TJ = kShapes[shape][1];
-    const int bxy = (N / TK) * (N / TJ);
-    int ci = h->p.tile_ci > 0 ? h->p.tile_ci : N;
-    if (h->p.tile_ci <= 0)
-        while (ci > 4 && (long long)bxy * ((N + ci - 1) / ci) < 8 * 148) ci /= 2;
-    if (ci > N) ci = N;
-    h->shape = shape;
-    h->ci = ci;
-    h->grid = dim3(N / TK, N / TJ, (N + ci - 1) / ci);
+    GridPlan g = plan_grid(h->N, h->p.tile_shape, h->p.tile_ci);
+    h->shape = g.shape;
+    h->ci = g.ci;
+    h->grid = g.grid;
 }
 
 int make_plans(gabe_handle *h) {
@@ -163,7 +113,7 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    if (h->p.calc_gws) {
+    if (h->p.gws_on) {
         long long inem[3] = {N, N, 2 * nz}, onem[3] = {N, N, nz};
         CF(h, cufftCreate(&h->plan_src));
         h->have_plan_src = true;
@@ -222,10 +172,10 @@ int sweep(gabe_handle *h, int mode, int cur, int counter) {
 // recorded for gabe_profile_steps.
 int enqueue_step(gabe_handle *h, int cur, cudaEvent_t *ev = nullptr) {
     if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
-    int rc = sweep(h, h->p.calc_gws ? MODE_A_GW : MODE_A, cur, 0);
+    int rc = sweep(h, h->p.gws_on ? MODE_A_GW : MODE_A, cur, 0);
     if (rc) return rc;
     if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
-    if (h->p.calc_gws) {
+    if (h->p.gws_on) {
         rc = fft_r2c(h, h->plan_src, h->S, h->S);
         if (rc) return rc;
         if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
@@ -365,8 +315,8 @@ void gabe_default_params(gabe_params *p, int N) {
     p->struct_size = (int32_t)sizeof(gabe_params);
     p->N = N;
     p->nflds = 2;
-    p->calc_gws = 0;
-    p->expansion_type = 1;
+    p->gws_on = 0;
+    p->expansion = 1;
     p->model = GABE_MODEL_LPHI4;
     p->precision = GABE_FP64;
     p->gw_spec_quirk = 1;
@@ -390,9 +340,9 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     if (p->N < 4 || p->N > 1290 || (p->N & 1))
         return set_err(nullptr, GABE_ERR_PARAM, "N must be even and in [4, 1290], got %d", p->N);
     if (p->nflds != 2) return set_err(nullptr, GABE_ERR_PARAM, "nflds must be 2, got %d", p->nflds);
-    if (p->expansion_type != 1)
-        return set_err(nullptr, GABE_ERR_PARAM, "only expansion_type 1 is implemented, got %d", p->expansion_type);
-    if (p->calc_gws != 0 && p->calc_gws != 1) return set_err(nullptr, GABE_ERR_PARAM, "calc_gws must be 0 or 1");
+    if (p->expansion != 1)
+        return set_err(nullptr, GABE_ERR_PARAM, "only expansion_type 1 is implemented, got %d", p->expansion);
+    if (p->gws_on != 0 && p->gws_on != 1) return set_err(nullptr, GABE_ERR_PARAM, "calc_gws must be 0 or 1");
     if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4)
         return set_err(nullptr, GABE_ERR_PARAM, "unknown model %d", p->model);
     if (p->precision != GABE_FP64 && p->precision != GABE_FP32)
@@ -430,7 +380,7 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     h->nz = p->N / 2 + 1;
     h->n3 = (size_t)p->N * p->N * p->N;
     h->M = (size_t)p->N * p->N * h->nz;
-    h->lc = make_consts(*p);
+    h->lc = make_lattice_consts(*p);
     choose_tile(h);
     h->nbins = gabe_spectra_numbins(p->N);
 
@@ -450,12 +400,12 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
         if ((rc = dalloc(h, &h->X[b], field_bytes))) return bail(rc);
         if ((rc = dalloc(h, &h->D[b], field_bytes))) return bail(rc);
     }
-    if (p->calc_gws) {
+    if (p->gws_on) {
         if ((rc = dalloc(h, &h->G, 8 * h->M * h->esz))) return bail(rc);
         if ((rc = dalloc(h, (void **)&h->gwnorm, 4 * sizeof(double)))) return bail(rc);
     }
     // sources need 10 padded slots; spectra need 2; uploads stage one FP64 field array
-    h->nslots = p->calc_gws ? 2 * kSrc : 2;
+    h->nslots = p->gws_on ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
     const size_t nblk_stencil = (size_t)h->grid.x * h->grid.y * h->grid.z;
@@ -526,7 +476,7 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
                 CK(h, to_fluct(stage, nf, mean, static_cast<float *>(dst[a]) + f * nf, h->stream));
             }
     }
-    if (h->p.calc_gws) {
+    if (h->p.gws_on) {
         int rc = upload_gw(h, h0, l0);
         if (rc) return rc;
     }
@@ -653,7 +603,7 @@ int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double 
             }
         }
     }
-    if (h->p.calc_gws) {
+    if (h->p.gws_on) {
         int rc = download_gw(h, h0, l0);
         if (rc) return rc;
     }
@@ -666,7 +616,7 @@ int gabe_spectra_numbins(int N) { return ((int)(sqrt(3.) * N / 2 + 1)); }
 int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries) {
     if (!h) return GABE_ERR_PARAM;
     if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "spectra before upload");
-    const int ns = 2 + (h->p.calc_gws ? 1 : 0);
+    const int ns = 2 + (h->p.gws_on ? 1 : 0);
     if (nbins != h->nbins || nseries != ns)
         return set_err(h, GABE_ERR_PARAM, "spectra_raw wants nbins=%d nseries=%d", h->nbins, ns);
     CK(h, cudaSetDevice(h->dev));
@@ -700,7 +650,7 @@ int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, in
 
 int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols) {
     if (!h || !out) return GABE_ERR_PARAM;
-    const int gws = h->p.calc_gws;
+    const int gws = h->p.gws_on;
     const int want = 5 + (gws ? 3 : 0);
     if (nbins != h->nbins || ncols != want)
         return set_err(h, GABE_ERR_PARAM, "spectra wants nbins=%d ncols=%d", h->nbins, want);
@@ -750,6 +700,6 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
-int gabe_launches_per_step(const gabe_handle *h) { return h ? (h->p.calc_gws ? 3 : 2) : 0; }
+int gabe_launches_per_step(const gabe_handle *h) { return h ? (h->p.gws_on ? 3 : 2) : 0; }
 
 }  // extern "C"

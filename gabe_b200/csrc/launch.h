@@ -6,6 +6,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
+
+#include "../../include/gabe.h"
 #include "kspace.cuh"
 #include "spectra.cuh"
 #include "stencil.cuh"
@@ -21,6 +24,65 @@ struct Launch {
 // Stencil tile shapes (TK x TJ), index = tile shape id of gabe_params.
 constexpr int kNumShapes = 6;
 constexpr int kShapes[kNumShapes][2] = {{32, 8}, {16, 16}, {32, 4}, {16, 8}, {8, 8}, {4, 4}};
+
+// Constants with the operation sequence the reference's compiler folds
+// (g2parameters.h:93, g2functions.cpp:41, g2evolutionpert.cpp:53,198,486-487,
+// g2model.cpp:64,68).
+inline LatticeConsts make_lattice_consts(const gabe_params &p) {
+    LatticeConsts c{};
+    c.N = p.N;
+    c.model = p.model;
+    const double L = p.L, dt = p.dt;
+    const double dx = L / ((double)p.N);
+    c.dt = dt;
+    c.half_dt = .5 * dt;
+    c.inv_dx2_div = dx * dx;
+    c.dn = (double)(1 / (dx * dx));
+    c.c13 = (1. / 3.) * c.dn;
+    c.c23 = (2. / 3.) * c.dn;
+    if (p.model == GABE_MODEL_QUADRATIC) {
+        const double mphi = p.model_c[0], gsq = p.model_c[1];
+        c.mc[0] = gsq / mphi / mphi;
+        c.mc[1] = 0.5 * gsq / mphi / mphi;
+    } else {
+        const double lam = p.model_c[0], g = p.model_c[1];
+        c.mc[0] = lam;
+        c.mc[1] = g;
+        c.mc[2] = 0.25 * lam;
+        c.mc[3] = 0.5 * g;
+        c.mc[4] = 3. * lam;
+    }
+    c.gridsize = (double)((long long)p.N * p.N * p.N);
+    c.eight_pi_3 = 8. * M_PI / 3.;
+    c.k2norm_c = 4. * M_PI * M_PI / L / L;
+    c.eight_pi = 8. * M_PI;
+    c.normmm = pow(dx, 3);
+    return c;
+}
+
+// Stencil grid: tile shape (the requested one if it divides N, else the first
+// in kShapes that does) and planes per block, shrunk until the grid has at
+// least 8 blocks per SM of a 148-SM B200.
+struct GridPlan {
+    int shape, ci;
+    dim3 grid;
+};
+inline GridPlan plan_grid(int N, int want_shape, int want_ci) {
+    auto fits = [N](int s) {
+        const int tk = kShapes[s][0], tj = kShapes[s][1];
+        return tk <= N && tj <= N && N % tk == 0 && N % tj == 0;
+    };
+    int shape = (want_shape >= 0 && want_shape < kNumShapes && fits(want_shape)) ? want_shape : -1;
+    for (int q = 0; shape < 0 && q < kNumShapes; q++)
+        if (fits(q)) shape = q;
+    const int TK = kShapes[shape][0], TJ = kShapes[shape][1];
+    const int bxy = (N / TK) * (N / TJ);
+    int ci = want_ci > 0 ? want_ci : N;
+    if (want_ci <= 0)
+        while (ci > 4 && (long long)bxy * ((N + ci - 1) / ci) < 8 * 148) ci /= 2;
+    if (ci > N) ci = N;
+    return GridPlan{shape, ci, dim3(N / TK, N / TJ, (N + ci - 1) / ci)};
+}
 
 cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);

@@ -67,13 +67,16 @@ enum gabe_flags {
     GABE_FLAG_NO_GRAPH = 1 /* launch kernels one by one instead of replaying a CUDA graph */
 };
 
-/* Run-time form of the g2parameters.h knobs that the hot path reads. */
+/* Run-time form of the g2parameters.h knobs that the hot path reads.  Two
+ * fields are named differently from their knobs (gws_on, expansion) because
+ * GABE defines calc_gws and expansion_type as macros, and a drop-in source
+ * file includes both headers. */
 typedef struct {
     int32_t struct_size;    /* sizeof(gabe_params) */
     int32_t N;              /* points per side (g2parameters.h:57) */
     int32_t nflds;          /* must be 2 (g2parameters.h:43) */
-    int32_t calc_gws;       /* 0/1 (g2parameters.h:55) */
-    int32_t expansion_type; /* must be 1 (g2parameters.h:62) */
+    int32_t gws_on;         /* calc_gws: 0/1 (g2parameters.h:55) */
+    int32_t expansion;      /* expansion_type: must be 1 (g2parameters.h:62) */
     int32_t model;          /* enum gabe_model */
     int32_t precision;      /* enum gabe_precision */
     int32_t gw_spec_quirk;  /* 1: GW spectrum reads l at kz=N/2 for the kz=0 plane, as g2spectra.cpp:149-164 does */

@@ -17,6 +17,9 @@
  *                     rescaling convention (oracle/ref_cfg/g2model_lphi4.cpp)
  *   GABE_PARALLEL 0 -> one thread, deterministic rand() order (reference :53,97-100)
  *   GABE_SEED     randseed                            (reference :56)
+ *   GABE_ENDTIME, GABE_SLICEWAIT, GABE_FIELD_OUTDIM, GABE_VAR_OUTPUT
+ *                 run length and output knobs (reference :60,80,84,86) for
+ *                 builds that use the reference's own g2main.cpp/g2output.cpp
  *
  * tot_num_thrds becomes a run-time value (env GABE_REF_THREADS) so one
  * binary can be timed with every host core.
@@ -46,6 +49,18 @@
 #endif
 #ifndef GABE_SEED
 #define GABE_SEED 44463132
+#endif
+#ifndef GABE_ENDTIME
+#define GABE_ENDTIME 1.e9 /* the harness fixes the step count itself */
+#endif
+#ifndef GABE_SLICEWAIT
+#define GABE_SLICEWAIT 1
+#endif
+#ifndef GABE_FIELD_OUTDIM
+#define GABE_FIELD_OUTDIM 0
+#endif
+#ifndef GABE_VAR_OUTPUT
+#define GABE_VAR_OUTPUT 0
 #endif
 
 #define num_flds 2
@@ -83,7 +98,7 @@ const int randseed = GABE_SEED;
 const int N = GABE_N;
 const gNum L = GABE_L;
 const gNum starttime = 0.;
-const gNum endtime = 1.e9; /* the harness fixes the step count itself */
+const gNum endtime = GABE_ENDTIME;
 const gNum dt = GABE_DT;
 #define expansion_type 1
 
@@ -91,13 +106,13 @@ const gNum dt = GABE_DT;
 #define field_full_rand 1
 
 const gNum screentime = 0;
-const int slicewait = 1;
+const int slicewait = GABE_SLICEWAIT;
 const int slicenumber = 1;
 const int field_sliceskip = 2;
 const int specnumber = 1;
-#define field_outdim 0
+#define field_outdim GABE_FIELD_OUTDIM
 #define spec_output 1
-#define var_output 0
+#define var_output GABE_VAR_OUTPUT
 
 const int nflds = num_flds;
 const gNum dx = L / ((gNum)N);

@@ -42,13 +42,13 @@ def test_params_struct_matches_header():
     p = gb.Params()
     lib.gabe_default_params(ctypes.byref(p), 64)
     assert p.struct_size == ctypes.sizeof(gb.Params)
-    assert p.N == 64 and p.nflds == 2 and p.expansion_type == 1
+    assert p.N == 64 and p.nflds == 2 and p.expansion == 1
     assert gb.numbins(64) == lib.gabe_spectra_numbins(64) == 56
     assert gb.numbins(256) == 222 and gb.numbins(512) == 444 and gb.numbins(1024) == 887
 
 
-@pytest.mark.parametrize("field,value", [("N", 63), ("N", 2), ("nflds", 3), ("expansion_type", 0),
-                                         ("model", 7), ("precision", 5), ("dt", -1.0), ("calc_gws", 2)])
+@pytest.mark.parametrize("field,value", [("N", 63), ("N", 2), ("nflds", 3), ("expansion", 0),
+                                         ("model", 7), ("precision", 5), ("dt", -1.0), ("gws_on", 2)])
 def test_create_rejects_bad_params(field, value):
     lib = gb.library()
     p = gb.Params()
