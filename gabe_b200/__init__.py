@@ -95,6 +95,8 @@ def library():
     L.gabe_launches_per_step.argtypes = [H]
     L.gabe_profile_steps.argtypes = [H, ctypes.c_int, _dp]
     L.gabe_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
+    L.gabe_energy_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
+                                      ctypes.c_void_p, ctypes.c_void_p]
     _lib = L
     return L
 

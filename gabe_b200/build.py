@@ -25,6 +25,7 @@ UNITS = [
     ("api.cu", []),
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", []),
+    ("noalloc.cu", ["-fmad=false"]),
 ]
 
 

@@ -149,6 +149,23 @@ int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols);
  * rebin these exactly (e.g. into log-spaced |k| bins). */
 int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries);
 
+/* Stage-0 energies {kin, pot, grad, rho} (calcEnergy(0)) of a state the
+ * caller already holds in device memory, without allocating anything: for
+ * callers that cannot allocate device memory at that point (a framework
+ * whose pool allocator owns all free device memory, or code that must not
+ * let cudaMalloc synchronise the device).  field0/dfield0 are device arrays
+ * [nflds][N^3] of FP64, out4 a device array of 4 doubles, stream a
+ * cudaStream_t (NULL = default stream); the call only enqueues work.  Uses
+ * p's N, L, model and tile fields; FP64 reference arithmetic, equal to
+ * gabe_energies for the same state.  Scratch is a fixed device array of
+ * 32768 blocks' partial sums (about 2 MiB), held by each device that loads
+ * the library until exit; a lattice needing more blocks returns
+ * GABE_ERR_PARAM.  The first call on a device looks up that array's device
+ * address (make it before any stream capture); calls that overlap on the
+ * GPU share the array and race.  No counterpart in the reference. */
+int gabe_energy_noalloc(const gabe_params *p, const double *field0, const double *dfield0, double a0,
+                        double *out4, void *stream);
+
 /* Message for the last error on this handle ("" if none).  NULL handle ->
  * message of the last failed gabe_create in this thread. */
 const char *gabe_last_error(const gabe_handle *h);
