@@ -153,7 +153,9 @@ def traffic_scaled(kernel: str, precision: str, N: int):
     e = d.get(precision, {}).get(kernel)
     if not e:
         return None
-    return e["bytes"] * (N / e["N"]) ** 3
+    # DRAM bytes grow with the sites (sweeps) or k-points (k-space) processed
+    scale = (N / e["N"]) ** 3 if kernel != "kspace" else (N * N * (N // 2 + 1)) / (e["N"] ** 2 * (e["N"] // 2 + 1))
+    return e["bytes"] * scale
 
 
 def cpu_reference_sample(N: int, steps: int, warm: int = 1):
