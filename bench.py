@@ -258,7 +258,7 @@ def main():
     precisions = [("fp32", gb.FP32)] + ([] if args.no_fp64 else [("fp64", gb.FP64)])
     clocks = None
     for name, prec in precisions:
-        lat = gb.Lattice(N, gws=gws, precision=prec, device=local)
+        lat = gb.Lattice(N, gws=gws, precision=prec, device=local, tile_shape="auto")
         stream = torch.cuda.ExternalStream(lat.stream_ptr)
         # ---- device-resident leg
         lat.upload_ptrs(hf.data_ptr(), hd.data_ptr(), None, None, a0, adot0)
@@ -305,7 +305,8 @@ def main():
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))
         legs[name] = {"ms": ms, "ms_e2e": ms_e2e, "phases": phases, "energies": en, "finite": finite,
                       "nonfinite_e2e": nonfinite_e2e, "device_bytes": lat.device_bytes,
-                      "launches_per_step": lat.launches_per_step}
+                      "launches_per_step": lat.launches_per_step,
+                      "tile": [lat.params.tile_shape, lat.params.tile_ci]}
         lat.close()
         torch.cuda.empty_cache()
 
@@ -361,6 +362,7 @@ def main():
         "gpu_launches": K * L32["launches_per_step"],
         "clocks": clocks,
         "finite": L32["finite"],
+        "tile": {"fp32": L32["tile"], "fp64": legs.get("fp64", {}).get("tile")},
         "device_bytes": L32["device_bytes"],
     }
     line.update(extra)

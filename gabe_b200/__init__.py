@@ -34,6 +34,7 @@ _LIB_PATH = os.path.join(HERE, "libgabe_b200.so")
 FP64, FP32 = 0, 1
 MODEL_QUADRATIC, MODEL_LPHI4 = 0, 1
 FLAG_NO_GRAPH = 1
+FLAG_NO_OVERLAP = 2
 
 STATUS = {
     0: "GABE_OK", 1: "GABE_ERR_PARAM", 2: "GABE_ERR_CUDA", 3: "GABE_ERR_CUFFT", 4: "GABE_ERR_NOMEM",
@@ -125,8 +126,15 @@ class Lattice:
 
     def __init__(self, N: int, *, L: float = 20.0, dt: float = 0.01, gws: bool = False,
                  model: int = MODEL_LPHI4, model_c=None, precision: int = FP64, device: int = -1,
-                 gw_spec_quirk: bool = True, flags: int = 0, tile_ci: int = 0, tile_shape: int = -1):
+                 gw_spec_quirk: bool = True, flags: int = 0, tile_ci: int = 0, tile_shape=-1):
+        """tile_shape="auto" takes the tile the autotuner cached for this GPU,
+        N, precision and GW setting (gabe_b200.autotune), if any."""
         lib = library()
+        if tile_shape == "auto":
+            from .autotune import lookup
+
+            hit = lookup(int(N), int(precision), bool(gws))
+            tile_shape, tile_ci = hit if hit else (-1, tile_ci)
         p = Params()
         lib.gabe_default_params(ctypes.byref(p), int(N))
         p.L, p.dt, p.gws_on, p.model, p.precision = float(L), float(dt), int(bool(gws)), int(model), int(precision)

@@ -1,0 +1,111 @@
+"""Stencil tile autotuner.
+
+The two sweeps (include/gabe.h: tile_shape, tile_ci) are launched on a grid
+of TJ x TK column tiles that each march `ci` planes along i.  The best pair
+depends on N, the precision and whether the GW sources are written.  This
+module times candidates on the current GPU with the library's own per-phase
+CUDA events (gabe_profile_steps) and keeps the fastest per
+(GPU name, N, precision, GWs) in a JSON cache, which `Lattice(...,
+tile_shape="auto")` consults.
+
+    python -m gabe_b200.autotune 64 128 256 512 --gws 1 --precision fp32
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import numpy as np
+
+from . import FP32, FP64, GabeError, Lattice
+
+SHAPES = {0: (32, 8), 1: (16, 16), 2: (32, 4), 3: (16, 8), 4: (8, 8), 5: (4, 4)}
+CACHE = os.environ.get("GABE_TILE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "tiles.json"))
+
+
+def _gpu_name() -> str:
+    try:
+        import torch
+
+        return torch.cuda.get_device_name(0)
+    except Exception:
+        return "unknown"
+
+
+def _key(N: int, precision: int, gws: bool) -> str:
+    return f"{_gpu_name()}|N={N}|{'fp32' if precision == FP32 else 'fp64'}|gws={int(gws)}"
+
+
+def load_cache() -> dict:
+    if os.path.exists(CACHE):
+        with open(CACHE) as fh:
+            return json.load(fh)
+    return {}
+
+
+def lookup(N: int, precision: int, gws: bool):
+    """(tile_shape, tile_ci) from the cache, or None."""
+    e = load_cache().get(_key(N, precision, gws))
+    return (e["shape"], e["ci"]) if e else None
+
+
+def candidates(N: int):
+    out = []
+    for s, (tk, tj) in SHAPES.items():
+        if tk > N or tj > N or N % tk or N % tj:
+            continue
+        for ci in (16, 32, 64, 128, 256, 512):
+            if ci <= N:
+                out.append((s, ci))
+    return out
+
+
+def tune(N: int, precision: int = FP32, gws: bool = True, steps: int = 3, verbose: bool = True) -> dict:
+    """Times every candidate on a random state; returns and caches the best."""
+    rng = np.random.default_rng(0)
+    f = 0.342 + 1e-6 * rng.standard_normal((2, N, N, N))
+    f[1] -= 0.342
+    d = 1e-6 * rng.standard_normal((2, N, N, N))
+    results = []
+    for shape, ci in candidates(N):
+        try:
+            with Lattice(N, gws=gws, precision=precision, tile_shape=shape, tile_ci=ci) as lat:
+                lat.upload_state(f, d, a0=1.0, adot0=0.5)
+                lat.profile_steps(1)
+                ph = lat.profile_steps(steps)
+        except GabeError as e:
+            if verbose:
+                print(f"shape {SHAPES[shape]} ci {ci}: {e}")
+            continue
+        t = ph["stage1"] + ph["stage2"]
+        results.append({"shape": shape, "ci": ci, "sweeps_ms": t, "stage1": ph["stage1"], "stage2": ph["stage2"]})
+        if verbose:
+            print(f"shape {SHAPES[shape]} ci {ci:4d}: sweep A {ph['stage1']:.3f} ms  sweep B {ph['stage2']:.3f} ms",
+                  flush=True)
+    best = min(results, key=lambda r: r["sweeps_ms"])
+    cache = load_cache()
+    cache[_key(N, precision, gws)] = {"shape": best["shape"], "ci": best["ci"], "sweeps_ms": best["sweeps_ms"],
+                                      "tile": SHAPES[best["shape"]]}
+    with open(CACHE, "w") as fh:
+        json.dump(cache, fh, indent=1, sort_keys=True)
+    return {"best": best, "all": results}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("N", type=int, nargs="+")
+    ap.add_argument("--gws", type=int, default=1)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--steps", type=int, default=3)
+    a = ap.parse_args()
+    out = {}
+    for N in a.N:
+        r = tune(N, FP32 if a.precision == "fp32" else FP64, bool(a.gws), a.steps)
+        out[N] = r["best"]
+        print(json.dumps({"N": N, "best": r["best"]}), flush=True)
+    return out
+
+
+if __name__ == "__main__":
+    main()

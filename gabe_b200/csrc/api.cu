@@ -39,7 +39,10 @@ struct gabe_handle {
     void *G = nullptr;  // GW amplitudes h+, hx, l+, lx [4][M] complex
     double *gwnorm = nullptr;  // upload check: |h|^2, |h - TT(h)|^2, |l|^2, |l - TT(l)|^2
     void *S = nullptr;  // sources / spectra scratch / staging
+    void *S2 = nullptr; // second source buffer: lets the GW chain of step n overlap sweep A of step n+1
     size_t S_bytes = 0;
+    cudaStream_t gw_stream = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_k[2] = {nullptr, nullptr};
     int nslots = 0;
     double *partials = nullptr;
     size_t npartials = 0;
@@ -59,7 +62,8 @@ struct gabe_handle {
     int cur = 0;
     bool uploaded = false;
     bool e0_stale = false;  // stage-0 energies/adot of the current state not yet reduced
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};   // one step, by starting parity
+    cudaGraphExec_t graph2[2] = {nullptr, nullptr};  // two steps, by starting parity
     bool graph_tried = false, graph_ok = false;
     size_t dev_bytes = 0;
     std::string err;
@@ -146,13 +150,17 @@ int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
     return GABE_OK;
 }
 
-StencilArgs stencil_args(gabe_handle *h, int cur) {
+bool overlapped(const gabe_handle *h) { return h->p.gws_on && h->S2 != nullptr; }
+void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
+
+StencilArgs stencil_args(gabe_handle *h, int cur, int slot = 0) {
     StencilArgs a{};
     a.X = h->X[cur];
     a.D = h->D[cur];
     a.Xo = h->X[1 - cur];
     a.Do = h->D[1 - cur];
-    a.S = h->S;
+    a.S = source_buffer(h, slot);
+    a.slot = slot;
     a.partials = h->partials;
     a.sc = h->sc;
     a.c = h->lc;
@@ -160,67 +168,111 @@ StencilArgs stencil_args(gabe_handle *h, int cur) {
     return a;
 }
 
-int sweep(gabe_handle *h, int mode, int cur, int counter) {
-    StencilArgs a = stencil_args(h, cur);
+int sweep(gabe_handle *h, int mode, int cur, int counter, int slot = 0) {
+    StencilArgs a = stencil_args(h, cur, slot);
     a.counter = h->counters + counter;
     CK(h, h->f32 ? sweep_f32(h->shape, mode, a, h->grid, h->stream) : sweep_f64(h->shape, mode, a, h->grid, h->stream));
     return GABE_OK;
 }
 
-// Enqueues one step reading buffer `cur` and writing buffer 1-cur.  With
-// `ev` (5 events) the phase boundaries sweep A | FFT | k-space | sweep B are
-// recorded for gabe_profile_steps.
-int enqueue_step(gabe_handle *h, int cur, cudaEvent_t *ev = nullptr) {
-    if (ev) CK(h, cudaEventRecord(ev[0], h->stream));
-    int rc = sweep(h, h->p.gws_on ? MODE_A_GW : MODE_A, cur, 0);
+int gw_chain(gabe_handle *h, int slot, cudaStream_t s) {
+    void *S = source_buffer(h, slot);
+    CF(h, cufftSetStream(h->plan_src, s));
+    int rc = fft_r2c(h, h->plan_src, S, S);
     if (rc) return rc;
-    if (ev) CK(h, cudaEventRecord(ev[1], h->stream));
-    if (h->p.gws_on) {
-        rc = fft_r2c(h, h->plan_src, h->S, h->S);
-        if (rc) return rc;
-        if (ev) CK(h, cudaEventRecord(ev[2], h->stream));
-        KspaceArgs k{};
-        k.S = h->S;
-        k.G = h->G;
-        k.sc = h->sc;
-        k.c = h->lc;
-        Launch lk{dim3(148 * 8), dim3(256), 0, h->stream};
-        CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
-    } else if (ev) {
-        CK(h, cudaEventRecord(ev[2], h->stream));
-    }
-    if (ev) CK(h, cudaEventRecord(ev[3], h->stream));
-    rc = sweep(h, MODE_B, cur, 1);
-    if (rc) return rc;
-    if (ev) CK(h, cudaEventRecord(ev[4], h->stream));
+    KspaceArgs k{};
+    k.S = S;
+    k.G = h->G;
+    k.sc = h->sc;
+    k.c = h->lc;
+    k.slot = slot;
+    Launch lk{dim3(148 * 8), dim3(256), 0, s};
+    CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
     return GABE_OK;
+}
+
+// Enqueues nsteps steps starting from state buffer `cur`.  The field chain
+// (sweep A, sweep B) runs on the handle's stream.  With two source buffers
+// the GW chain of each step (FFT, k-space) forks onto gw_stream after its
+// sweep A and overlaps sweep B and the next step's sweep A; a step's sweep A
+// waits for the k-space pass two steps back (same source buffer), and the
+// enqueue ends joined on the handle's stream.  Nothing in the field chain
+// reads the GW chain (no backreaction), so only buffer reuse orders them.
+// With `ev` (5 events per step, serial only) the phase boundaries sweep A |
+// FFT | k-space | sweep B are recorded for gabe_profile_steps.
+int enqueue_steps(gabe_handle *h, int cur, int nsteps, bool serial, cudaEvent_t *ev = nullptr) {
+    const bool fork = overlapped(h) && !serial;
+    for (int s = 0; s < nsteps; s++) {
+        const int c = cur ^ (s & 1);
+        const int slot = fork ? c : 0;
+        cudaEvent_t *e = ev ? ev + 5 * s : nullptr;
+        if (fork && s >= 2) CK(h, cudaStreamWaitEvent(h->stream, h->ev_k[slot], 0));
+        if (e) CK(h, cudaEventRecord(e[0], h->stream));
+        int rc = sweep(h, h->p.gws_on ? MODE_A_GW : MODE_A, c, 0, slot);
+        if (rc) return rc;
+        if (e) CK(h, cudaEventRecord(e[1], h->stream));
+        if (h->p.gws_on) {
+            if (fork) {
+                CK(h, cudaEventRecord(h->ev_a, h->stream));
+                CK(h, cudaStreamWaitEvent(h->gw_stream, h->ev_a, 0));
+                rc = gw_chain(h, slot, h->gw_stream);
+                if (rc) return rc;
+                CK(h, cudaEventRecord(h->ev_k[slot], h->gw_stream));
+            } else {
+                CF(h, cufftSetStream(h->plan_src, h->stream));
+                rc = fft_r2c(h, h->plan_src, source_buffer(h, slot), source_buffer(h, slot));
+                if (rc) return rc;
+                if (e) CK(h, cudaEventRecord(e[2], h->stream));
+                KspaceArgs k{};
+                k.S = source_buffer(h, slot);
+                k.G = h->G;
+                k.sc = h->sc;
+                k.c = h->lc;
+                k.slot = slot;
+                Launch lk{dim3(148 * 8), dim3(256), 0, h->stream};
+                CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
+            }
+        } else if (e) {
+            CK(h, cudaEventRecord(e[2], h->stream));
+        }
+        if (e) CK(h, cudaEventRecord(e[3], h->stream));
+        rc = sweep(h, MODE_B, c, 1, slot);
+        if (rc) return rc;
+        if (e) CK(h, cudaEventRecord(e[4], h->stream));
+    }
+    if (fork && nsteps > 0) CK(h, cudaStreamWaitEvent(h->stream, h->ev_k[cur ^ ((nsteps - 1) & 1)], 0));
+    return GABE_OK;
+}
+
+int capture(gabe_handle *h, int cur, int nsteps, cudaGraphExec_t *out) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int rc = enqueue_steps(h, cur, nsteps, false);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc != GABE_OK || e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        h->err.clear();
+        return 1;
+    }
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return 1;
+    }
+    return 0;
 }
 
 int build_graphs(gabe_handle *h) {
     h->graph_tried = true;
     if (h->p.flags & GABE_FLAG_NO_GRAPH) return GABE_OK;
-    for (int par = 0; par < 2; par++) {
-        cudaGraph_t g = nullptr;
-        if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-            cudaGetLastError();
-            return GABE_OK;
-        }
-        int rc = enqueue_step(h, par);
-        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
-        if (rc != GABE_OK || e != cudaSuccess || !g) {
-            cudaGetLastError();
-            if (g) cudaGraphDestroy(g);
-            h->err.clear();
-            return GABE_OK;  // fall back to direct launches
-        }
-        e = cudaGraphInstantiate(&h->graph[par], g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            h->graph[par] = nullptr;
-            return GABE_OK;
-        }
-    }
+    for (int par = 0; par < 2; par++)
+        if (capture(h, par, 1, &h->graph[par]) || capture(h, par, 2, &h->graph2[par])) return GABE_OK;
     h->graph_ok = true;
     return GABE_OK;
 }
@@ -408,6 +460,21 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     h->nslots = p->gws_on ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
+    if (p->gws_on && !(p->flags & GABE_FLAG_NO_OVERLAP)) {
+        // optional: without it the GW chain simply runs in line
+        if (dalloc(h, &h->S2, h->S_bytes) != GABE_OK) {
+            h->S2 = nullptr;
+            h->err.clear();
+        }
+    }
+    if (cudaStreamCreateWithFlags(&h->gw_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_a, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_k[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&h->ev_k[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        set_err(h, GABE_ERR_CUDA, "stream/event creation failed");
+        return bail(GABE_ERR_CUDA);
+    }
     const size_t nblk_stencil = (size_t)h->grid.x * h->grid.y * h->grid.z;
     h->npartials = kNV * (nblk_stencil > 4096 ? nblk_stencil : 4096);
     if ((rc = dalloc(h, (void **)&h->partials, h->npartials * sizeof(double)))) return bail(rc);
@@ -432,15 +499,21 @@ int gabe_destroy(gabe_handle *h) {
     if (!h) return GABE_OK;
     cudaSetDevice(h->dev);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (int i = 0; i < 2; i++)
+    if (h->gw_stream) cudaStreamSynchronize(h->gw_stream);
+    for (int i = 0; i < 2; i++) {
         if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
+        if (h->graph2[i]) cudaGraphExecDestroy(h->graph2[i]);
+        if (h->ev_k[i]) cudaEventDestroy(h->ev_k[i]);
+    }
+    if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->have_plan_src) cufftDestroy(h->plan_src);
     if (h->have_plan_spec) cufftDestroy(h->plan_spec);
-    void *bufs[] = {h->X[0], h->X[1], h->D[0], h->D[1], h->G, h->gwnorm, h->S, h->partials, h->counters,
+    void *bufs[] = {h->X[0], h->X[1], h->D[0], h->D[1], h->G, h->gwnorm, h->S, h->S2, h->partials, h->counters,
                     h->sc, h->bin_part, h->bin_cnt_part, h->bin_sum, h->fft_work};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->gw_stream) cudaStreamDestroy(h->gw_stream);
     cudaGetLastError();
     delete h;
     return GABE_OK;
@@ -498,14 +571,17 @@ int gabe_step(gabe_handle *h, int nsteps) {
         int rc = build_graphs(h);
         if (rc) return rc;
     }
-    for (int s = 0; s < nsteps; s++) {
-        if (h->graph_ok) {
+    if (h->graph_ok) {
+        int left = nsteps;
+        for (; left >= 2; left -= 2) CK(h, cudaGraphLaunch(h->graph2[h->cur], h->stream));
+        if (left) {
             CK(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
-        } else {
-            int rc = enqueue_step(h, h->cur);
-            if (rc) return rc;
+            h->cur ^= 1;
         }
-        h->cur ^= 1;
+    } else {
+        int rc = enqueue_steps(h, h->cur, nsteps, false);
+        if (rc) return rc;
+        h->cur ^= (nsteps & 1);
     }
     if (nsteps > 0) h->e0_stale = true;
     return GABE_OK;
@@ -518,10 +594,8 @@ int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]) {
     std::vector<cudaEvent_t> ev((size_t)5 * nsteps);
     for (auto &e : ev) CK(h, cudaEventCreate(&e));
     int rc = GABE_OK;
-    for (int s = 0; s < nsteps && rc == GABE_OK; s++) {
-        rc = enqueue_step(h, h->cur, ev.data() + 5 * s);
-        h->cur ^= 1;
-    }
+    rc = enqueue_steps(h, h->cur, nsteps, true, ev.data());
+    h->cur ^= (nsteps & 1);
     h->e0_stale = true;
     double acc[4] = {0, 0, 0, 0};
     if (rc == GABE_OK && cudaStreamSynchronize(h->stream) == cudaSuccess) {

@@ -32,6 +32,10 @@ struct DevScalars {
     long long step;
     unsigned int status;
     unsigned int adot_given;  // adot[0] came from the caller (after an upload), not from adf(0)
+    // a[0], adot[0], a[1], adot[1] of the step whose GW sources sit in source
+    // buffer s, for the k-space update (which may run while the fields are
+    // already one step further on)
+    double gw[2][4];
 };
 
 enum Model : int { MODEL_QUADRATIC = 0, MODEL_LPHI4 = 1 };

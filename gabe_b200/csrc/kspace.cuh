@@ -39,6 +39,7 @@ struct KspaceArgs {
     void *G;         // complex amplitudes [4][N][N][N/2+1]: h+, hx, l+, lx
     const DevScalars *sc;
     LatticeConsts c;
+    int slot;        // which step's scalars (DevScalars::gw) to use
 };
 
 // Polarization tensors of the integer wave vector n (n != 0): the six
@@ -72,8 +73,8 @@ __global__ void __launch_bounds__(256) kspace_kernel(KspaceArgs args) {
     const LatticeConsts &c = args.c;
     const int N = c.N, nz = N / 2 + 1;
     const size_t M = (size_t)N * N * nz;
-    const DevScalars *sc = args.sc;
-    const double a0 = sc->a[0], ad0 = sc->adot[0], a1 = sc->a[1], ad1 = sc->adot[1];
+    const double *g4 = args.sc->gw[args.slot];
+    const double a0 = g4[0], ad0 = g4[1], a1 = g4[2], ad1 = g4[3];
     // derivs() coefficients (g2evolutionpert.cpp:486-501) for both stages
     const double norm0 = c.k2norm_c / a0 / a0, norm1 = c.k2norm_c / a1 / a1;
     const double om0 = c.eight_pi / a0 / a0, om1 = c.eight_pi / a1 / a1;

@@ -50,6 +50,7 @@ struct StencilArgs {
     DevScalars *sc;
     LatticeConsts c;
     int ci;              // planes per block along i
+    int slot;            // source buffer / GW scalar slot of this step
 };
 
 constexpr int kNV = 8;  // reduced values: kin0 pot0 grad0 | pot1 grad1 PP PQ QQ
@@ -212,7 +213,7 @@ __device__ __forceinline__ void store_sources(T *S, int N, int i, int j, int k, 
 // Final scalars of sweep A / E0 from the block-summed values (thread 0 of
 // the last block).
 template <typename T, int MODE>
-__device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, const double *tot) {
+__device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, const double *tot, int slot) {
     const double a0 = s->a[0];
     double ek0 = tot[0] / c.gridsize / 2.;
     double ep0 = tot[1] / c.gridsize;
@@ -244,13 +245,25 @@ __device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, 
     s->edrho[1] = rho1;
     s->adot[1] = sqrt(c.eight_pi_3 * rho1) * a1; /* adf(1), :252 */
     if (!isfinite(rho1)) s->status |= ST_NONFINITE;
+    s->gw[slot][0] = a0;
+    s->gw[slot][1] = ad0;
+    s->gw[slot][2] = a1;
+    s->gw[slot][3] = s->adot[1];
 }
 
 // ---------------------------------------------------------------------------
 // the sweep kernel
 // ---------------------------------------------------------------------------
+// FP32: cap registers so that 3 (sweep A) or 4 (sweep B, E0) blocks of 256
+// threads share an SM -- the sweeps are latency-bound at lower occupancy.
+template <typename T, int MODE>
+constexpr int sweep_min_threads() {
+    return sizeof(T) == 8 ? 0 : (MODE == MODE_A_GW || MODE == MODE_A ? 768 : 1024);
+}
+
 template <typename T, int TK, int TJ, int MODE>
-__global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
+__global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * TJ - 1) / (TK * TJ))
+    sweep_kernel(StencilArgs args) {
     using M = March<T, TK, TJ>;
     __shared__ __align__(16) T smem[2][M::NA * M::P];
     __shared__ double sred[((TK * TJ + 31) / 32) * kNV];
@@ -422,7 +435,7 @@ __global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
         double tot[kNV];
         sum_partials<kNV>(args.partials, gridDim.x * gridDim.y * gridDim.z, tot, sred);
         if (tid == 0) {
-            finish_a<T, MODE>(c, args.sc, tot);
+            finish_a<T, MODE>(c, args.sc, tot, args.slot);
             *args.counter = 0u;
         }
     } else if (tid == 0) {

@@ -64,7 +64,10 @@ enum gabe_model {
 };
 
 enum gabe_flags {
-    GABE_FLAG_NO_GRAPH = 1 /* launch kernels one by one instead of replaying a CUDA graph */
+    GABE_FLAG_NO_GRAPH = 1,  /* launch kernels one by one instead of replaying a CUDA graph */
+    GABE_FLAG_NO_OVERLAP = 2 /* one source buffer: the GW transforms and k-space update run in line
+                                instead of overlapping the next field sweeps (saves 10 N^2(N+2)
+                                words of device memory) */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two
