@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-N", type=int, default=256, help="lattice of the CPU reference sample")
     ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--ens-lattices", type=int, default=256)
+    ap.add_argument("--ens-steps", type=int, default=200, help="timed ensemble steps (multiple of --ens-every)")
+    ap.add_argument("--ens-every", type=int, default=50, help="steps between log-spectra outputs")
+    ap.add_argument("--ens-seed", type=int, default=20261203, help="master seed of the ensemble's parameters")
     return ap.parse_args()
 
 
@@ -187,6 +192,83 @@ def cpu_reference_sample(N: int, steps: int, warm: int = 1):
     po.step(stt, steps)
     dt = time.perf_counter() - t0
     return Np ** 3 * steps / dt, {"kind": "port", "cores": 1, "sample": f"oracle port, {Np}^3 GW on, {steps} steps"}
+
+
+def ensemble_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ranks):
+    """The uneven batched ensemble: lattices of N in {32,48,64,96,128},
+    g^2/lambda log-uniform [1,500], amplitude U[0.5,2], FP32 storage, GWs
+    on, 64-bin log spectra of phi, chi and GWs every `ens_every` steps.
+    Lattices are split over ranks by sum N^3 (strong scaling: the ensemble
+    is fixed); the spectra are gathered on rank 0 at the end."""
+    import numpy as np
+    import torch
+
+    import gabe_b200 as gb
+    from gabe_b200 import ensemble as ge
+
+    Ns, g, amp, seeds = ge.sample_parameters(args.ens_lattices, args.ens_seed)
+    mine = ge.partition(Ns, world)[rank]
+    every = args.ens_every
+    K = max(every, args.ens_steps // every * every)
+    ens = gb.Ensemble(Ns[mine], g[mine], amp[mine], seeds[mine], nlog=64, device=local, tiles="auto")
+    stream = torch.cuda.ExternalStream(ens.stream_ptr)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record(stream)
+    ens.init()
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms_init = max_over_ranks(ev[0].elapsed_time(ev[1]))
+    ens.step(max(3, args.warmup))
+    ens.log_spectra()
+    barrier()
+    # steps with the log-spectra output cadence (each output reads the
+    # spectra back to the host)
+    ev[0].record(stream)
+    for _ in range(K // every):
+        ens.step(every)
+        logs, _, _ = ens.log_spectra()
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms = max_over_ranks(ev[0].elapsed_time(ev[1]))
+    # the same steps without outputs
+    barrier()
+    ev[2].record(stream)
+    ens.step(K)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    ms_steps = max_over_ranks(ev[2].elapsed_time(ev[3]))
+    sc = ens.scalars()
+    logs, cnt, _ = ens.log_spectra()
+    local_rows = np.concatenate([logs.reshape(len(mine), -1), sc], axis=1)
+    launches = ens.launches_per_step
+    dev_bytes = ens.device_bytes
+    ens.close()
+    torch.cuda.empty_cache()
+    full = ge.gather_rows(mine, local_rows, args.ens_lattices, dist if world > 1 else None)
+    sites = float(np.sum(np.asarray(Ns, dtype=np.float64) ** 3))
+    nspec = args.ens_lattices * (K // every)
+    algo = sum(sum(algorithmic_bytes(int(n), 4, True).values()) for n in Ns)
+    out = {
+        "workload": f"{args.ens_lattices} lattices, N uniform on {{32,48,64,96,128}}, g^2/lambda log-uniform "
+                    f"[1,500], amplitude U[0.5,2], master seed {args.ens_seed}, FP32 storage, GWs on, "
+                    f"64-bin log spectra every {every} steps",
+        "sites": sites, "steps": K, "scaling": "strong", "n_gpus": world,
+        "site_updates_per_s": sites * K / (ms / 1e3),
+        "spectra_per_s": nspec / (ms / 1e3),
+        "ms_per_step_with_outputs": ms / K,
+        "site_updates_per_s_steps_only": sites * K / (ms_steps / 1e3),
+        "ms_per_step_steps_only": ms_steps / K,
+        "step_algorithmic_bytes": algo,
+        "step_achieved_gbs": algo / (ms_steps / K / 1e3) / 1e9,
+        "ms_init": ms_init,
+        "gpu_launches_per_step": launches,
+        "device_bytes_rank0": dev_bytes,
+    }
+    if full is not None:
+        nl = 3 * 64
+        out["finite_lattices"] = int(np.sum(np.all(np.isfinite(full[:, nl:]), axis=1)))
+        out["nonempty_log_bins_mean"] = float(np.mean(np.sum(np.isfinite(full[:, :64]), axis=1)))
+    return out
 
 
 def run_reference_arm(args, rank: int):
@@ -366,6 +448,8 @@ def main():
         "device_bytes": L32["device_bytes"],
     }
     line.update(extra)
+    if not args.no_ensemble:
+        line["ensemble"] = ensemble_leg(args, rank, world, local, dist, barrier, max_over_ranks)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         v, info = cpu_reference_sample(args.ref_N, 2, warm=1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],

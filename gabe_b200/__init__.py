@@ -288,3 +288,189 @@ class Lattice:
                 raise GabeError(5, f"unstable solution: field {q} not numerical")
             out[q] = (av, var)
         return out
+
+
+class EnsParams(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("nlat", ctypes.c_int32),
+        ("N", ctypes.POINTER(ctypes.c_int32)), ("g2_over_lambda", ctypes.POINTER(ctypes.c_double)),
+        ("amplitude", ctypes.POINTER(ctypes.c_double)), ("seed", ctypes.POINTER(ctypes.c_uint64)),
+        ("tile_shape", ctypes.POINTER(ctypes.c_int32)), ("tile_ci", ctypes.POINTER(ctypes.c_int32)),
+        ("L", ctypes.c_double), ("dt", ctypes.c_double),
+        ("lam", ctypes.c_double), ("phi0", ctypes.c_double), ("dphi0", ctypes.c_double),
+        ("gws_on", ctypes.c_int32), ("device", ctypes.c_int32), ("nlog", ctypes.c_int32),
+        ("gw_spec_quirk", ctypes.c_int32), ("flags", ctypes.c_int32), ("reserved", ctypes.c_int32),
+    ]
+
+
+def _ens_lib():
+    L = library()
+    if not getattr(L, "_ens_ready", False):
+        E = ctypes.c_void_p
+        L.gabe_ensemble_create.argtypes = [ctypes.POINTER(EnsParams), ctypes.POINTER(E)]
+        L.gabe_ensemble_destroy.argtypes = [E]
+        L.gabe_ensemble_init.argtypes = [E]
+        L.gabe_ensemble_upload.argtypes = [E, ctypes.c_int, _dp, _dp, ctypes.c_double, ctypes.c_double]
+        L.gabe_ensemble_step.argtypes = [E, ctypes.c_int]
+        L.gabe_ensemble_sync.argtypes = [E]
+        L.gabe_ensemble_scalars.argtypes = [E, _dp]
+        L.gabe_ensemble_native_bins.argtypes = [E]
+        L.gabe_ensemble_log_spectra.argtypes = [E, _dp, _dp, _dp]
+        L.gabe_ensemble_download.argtypes = [E, ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.gabe_ensemble_last_error.argtypes = [E]
+        L.gabe_ensemble_last_error.restype = ctypes.c_char_p
+        L.gabe_ensemble_device_bytes.argtypes = [E]
+        L.gabe_ensemble_device_bytes.restype = ctypes.c_size_t
+        L.gabe_ensemble_stream.argtypes = [E]
+        L.gabe_ensemble_stream.restype = ctypes.c_void_p
+        L.gabe_ensemble_launches_per_step.argtypes = [E]
+        L._ens_ready = True
+    return L
+
+
+class Ensemble:
+    """Many independent lattices evolved together (gabe_ensemble_*): FP32
+    storage, FP64 scalars, the lambda phi^4 + g^2 phi^2 chi^2 model with a
+    per-lattice g^2/lambda, fluctuation amplitude multiplier and seed."""
+
+    def __init__(self, N, g2_over_lambda, amplitude, seed, *, L: float = 20.0, dt: float = 0.01,
+                 lam: float = 9e-14, phi0: float = 0.342, dphi0: float = 0.0, gws: bool = True, nlog: int = 64,
+                 tiles="auto", device: int = -1, flags: int = 0, gw_spec_quirk: bool = True):
+        lib = _ens_lib()
+        self.N = np.ascontiguousarray(N, dtype=np.int32)
+        self.nlat = len(self.N)
+        self._g = np.ascontiguousarray(g2_over_lambda, dtype=np.float64)
+        self._amp = np.ascontiguousarray(amplitude, dtype=np.float64)
+        self._seed = np.ascontiguousarray(seed, dtype=np.uint64)
+        self.gws, self.nlog = bool(gws), int(nlog)
+        shapes = cis = None
+        if tiles == "auto":
+            from .autotune import lookup_ensemble
+
+            st = [lookup_ensemble(int(n)) for n in self.N]
+            if all(t is not None for t in st):
+                shapes = np.array([t[0] for t in st], dtype=np.int32)
+                cis = np.array([t[1] for t in st], dtype=np.int32)
+        elif tiles is not None:
+            shapes = np.ascontiguousarray(tiles[0], dtype=np.int32)
+            cis = np.ascontiguousarray(tiles[1], dtype=np.int32)
+        self._shapes, self._cis = shapes, cis
+        p = EnsParams()
+        p.struct_size = ctypes.sizeof(EnsParams)
+        p.nlat = self.nlat
+        p.N = self.N.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        p.g2_over_lambda = self._g.ctypes.data_as(_dp)
+        p.amplitude = self._amp.ctypes.data_as(_dp)
+        p.seed = self._seed.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        if shapes is not None:
+            p.tile_shape = shapes.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+            p.tile_ci = cis.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        p.L, p.dt, p.lam, p.phi0, p.dphi0 = L, dt, lam, phi0, dphi0
+        p.gws_on, p.device, p.nlog, p.gw_spec_quirk, p.flags = int(gws), device, nlog, int(gw_spec_quirk), flags
+        self._p = p
+        self._h = ctypes.c_void_p()
+        rc = lib.gabe_ensemble_create(ctypes.byref(p), ctypes.byref(self._h))
+        if rc != 0:
+            self._h = None
+            raise GabeError(rc, lib.gabe_ensemble_last_error(None).decode())
+        self.nb = lib.gabe_ensemble_native_bins(self._h)
+
+    def _check(self, rc):
+        if rc != 0:
+            raise GabeError(rc, _ens_lib().gabe_ensemble_last_error(self._h).decode())
+
+    def close(self):
+        if self._h:
+            _ens_lib().gabe_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        return _ens_lib().gabe_ensemble_device_bytes(self._h)
+
+    @property
+    def stream_ptr(self) -> int:
+        return _ens_lib().gabe_ensemble_stream(self._h) or 0
+
+    @property
+    def launches_per_step(self) -> int:
+        return _ens_lib().gabe_ensemble_launches_per_step(self._h)
+
+    def init(self):
+        self._check(_ens_lib().gabe_ensemble_init(self._h))
+
+    def upload(self, lat: int, field0, dfield0, *, a0: float = 1.0, adot0: float):
+        n = int(self.N[lat])
+        f = np.ascontiguousarray(field0, dtype=np.float64).reshape(2, n, n, n)
+        d = np.ascontiguousarray(dfield0, dtype=np.float64).reshape(2, n, n, n)
+        self._check(_ens_lib().gabe_ensemble_upload(self._h, int(lat), _ptr(f), _ptr(d), a0, adot0))
+
+    def step(self, n: int = 1):
+        self._check(_ens_lib().gabe_ensemble_step(self._h, int(n)))
+
+    def sync(self):
+        self._check(_ens_lib().gabe_ensemble_sync(self._h))
+
+    def scalars(self) -> np.ndarray:
+        """[nlat][12]: a[0], a[1], adot[0], adot[1], edkin[0..1], edpot, edgrad, edrho."""
+        out = np.zeros((self.nlat, 12))
+        self._check(_ens_lib().gabe_ensemble_scalars(self._h, _ptr(out)))
+        return out
+
+    def log_spectra(self):
+        logs = np.zeros((self.nlat, 3, self.nlog))
+        cnt = np.zeros((self.nlat, self.nlog))
+        nat = np.zeros((self.nlat, 4, self.nb))
+        self._check(_ens_lib().gabe_ensemble_log_spectra(self._h, _ptr(logs), _ptr(cnt), _ptr(nat)))
+        return logs, cnt, nat
+
+    def download(self, lat: int, want_gw: bool = True):
+        n = int(self.N[lat])
+        f = np.empty((2, n, n, n))
+        d = np.empty((2, n, n, n))
+        hh = ll = None
+        if self.gws and want_gw:
+            hh = np.empty((12, n, n, n // 2 + 1))
+            ll = np.empty((12, n, n, n // 2 + 1))
+        self._check(_ens_lib().gabe_ensemble_download(self._h, int(lat), _ptr(f), _ptr(d), _ptr(hh), _ptr(ll)))
+        return f, d, hh, ll
+
+
+def rebin_log(native: np.ndarray, N: int, nlog: int, nb_max: int, L: float, rho0: float) -> np.ndarray:
+    """Log-binned (Delta^2_phi, Delta^2_chi, Omega_gw) from native bin sums
+    and counts -- the rule of gabe_ensemble_log_spectra, for checks and for
+    single lattices (use gabe_spectra_raw's sums/counts as `native`
+    [4][nb]: phi, chi, GW sums and counts)."""
+    nbe = int(math.sqrt(3.0) * N / 2 + 1)
+    spec_norm = (L / N) ** 6 * (2 * math.pi / L) ** 3
+    hub = math.sqrt(8 * math.pi / 3) * math.sqrt(rho0)
+    norm1 = 4.e-5 / 100. ** .333 / 24. / math.pi / math.pi / L ** 3 / hub ** 2
+    out = np.full((3, nlog), np.nan)
+    cnt = np.zeros(nlog)
+    lo, hi = 1.0, float(nb_max)
+    for q in range(nlog):
+        e0 = lo * (hi / lo) ** (q / nlog)
+        e1 = lo * (hi / lo) ** ((q + 1) / nlog)
+        bs = [b for b in range(1, nbe) if b >= e0 and (b < e1 if q + 1 < nlog else b <= e1)]
+        n = sum(native[3][b] for b in bs)
+        cnt[q] = n
+        if n > 0:
+            k3 = [(b * 2 * math.pi / L) ** 3 for b in bs]
+            s = [sum(k * native[c][b] for k, b in zip(k3, bs)) for c in range(3)]
+            with np.errstate(divide="ignore"):
+                out[0, q] = np.log10(spec_norm * s[0] / n / 2 / math.pi / math.pi)
+                out[1, q] = np.log10(spec_norm * s[1] / n / 2 / math.pi / math.pi)
+                out[2, q] = np.log10(norm1 * s[2] / n)
+    return out, cnt

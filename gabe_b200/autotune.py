@@ -50,6 +50,47 @@ def lookup(N: int, precision: int, gws: bool):
     return (e["shape"], e["ci"]) if e else None
 
 
+def lookup_ensemble(N: int):
+    """(shape, ci) for ensemble lattices of size N (256-thread tiles only)."""
+    e = load_cache().get(f"{_gpu_name()}|ens|N={N}")
+    return (e["shape"], e["ci"]) if e else None
+
+
+def tune_ensemble(sizes, steps: int = 3, verbose: bool = True) -> dict:
+    """Ensemble tiles per lattice size: the 256-thread shapes (32x8, 16x16)
+    and ci in {16, 32, 64}, timed on single FP32 GW lattices of that size."""
+    out = {}
+    cache = load_cache()
+    for N in sizes:
+        rng = np.random.default_rng(1)
+        f = 0.342 + 1e-6 * rng.standard_normal((2, N, N, N))
+        f[1] -= 0.342
+        d = 1e-6 * rng.standard_normal((2, N, N, N))
+        best = None
+        for shape in (0, 1):
+            tk, tj = SHAPES[shape]
+            if N % tk or N % tj:
+                continue
+            for ci in (16, 32, 64):
+                if ci > N:
+                    continue
+                with Lattice(N, gws=True, precision=FP32, tile_shape=shape, tile_ci=ci) as lat:
+                    lat.upload_state(f, d, a0=1.0, adot0=0.5)
+                    lat.profile_steps(1)
+                    ph = lat.profile_steps(steps)
+                t = ph["stage1"] + ph["stage2"]
+                if verbose:
+                    print(f"ens N={N} shape {SHAPES[shape]} ci {ci}: {t:.4f} ms", flush=True)
+                if best is None or t < best[2]:
+                    best = (shape, ci, t)
+        cache[f"{_gpu_name()}|ens|N={N}"] = {"shape": best[0], "ci": best[1], "sweeps_ms": best[2],
+                                             "tile": SHAPES[best[0]]}
+        out[N] = best
+    with open(CACHE, "w") as fh:
+        json.dump(cache, fh, indent=1, sort_keys=True)
+    return out
+
+
 def candidates(N: int):
     out = []
     for s, (tk, tj) in SHAPES.items():
@@ -98,7 +139,10 @@ def main():
     ap.add_argument("--gws", type=int, default=1)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--ensemble", action="store_true", help="tune the ensemble's 256-thread tiles instead")
     a = ap.parse_args()
+    if a.ensemble:
+        return tune_ensemble(a.N, a.steps)
     out = {}
     for N in a.N:
         r = tune(N, FP32 if a.precision == "fp32" else FP64, bool(a.gws), a.steps)

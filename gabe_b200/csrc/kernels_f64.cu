@@ -5,7 +5,7 @@ namespace gabe {
 
 template <int TK, int TJ>
 static cudaError_t sweep_shape(int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
-    const dim3 block(TK, TJ);
+    const dim3 block(TK * TJ);
     switch (mode) {
         case MODE_A: sweep_kernel<double, TK, TJ, MODE_A><<<grid, block, 0, s>>>(a); break;
         case MODE_A_GW: sweep_kernel<double, TK, TJ, MODE_A_GW><<<grid, block, 0, s>>>(a); break;

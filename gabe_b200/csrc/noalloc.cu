@@ -78,7 +78,7 @@ __global__ void noalloc_end(const DevScalars *sc, double *out4) {
 
 template <int TK, int TJ>
 cudaError_t launch_e0(const StencilArgs &a, dim3 grid, cudaStream_t s) {
-    sweep_kernel<double, TK, TJ, MODE_E0><<<grid, dim3(TK, TJ), 0, s>>>(a);
+    sweep_kernel<double, TK, TJ, MODE_E0><<<grid, dim3(TK * TJ), 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -143,11 +143,12 @@ struct March {
     bool has_halo;
     T prev[NA], cur[NA], nxt[NA], nn[NA], hal[NA];
 
-    __device__ __forceinline__ void init(const T *X, const T *D, int N_, size_t n3) {
+    __device__ __forceinline__ void init(const T *X, const T *D, int N_, size_t n3, int j0_, int k0_) {
         src[0] = X; src[1] = X + n3; src[2] = D; src[3] = D + n3;
         N = N_;
-        tx = threadIdx.x; ty = threadIdx.y; tid = tx + TK * ty;
-        j0 = blockIdx.y * TJ; k0 = blockIdx.x * TK;
+        tid = threadIdx.x;
+        tx = tid % TK; ty = tid / TK;
+        j0 = j0_; k0 = k0_;
         has_halo = tid < NH;
         int t = tid;
         if (t < TK) { hr = 0; hc = t + 1; }
@@ -254,31 +255,38 @@ __device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, 
 // ---------------------------------------------------------------------------
 // the sweep kernel
 // ---------------------------------------------------------------------------
-// FP32: cap registers so that 3 (sweep A) or 4 (sweep B, E0) blocks of 256
-// threads share an SM -- the sweeps are latency-bound at lower occupancy.
-template <typename T, int MODE>
-constexpr int sweep_min_threads() {
-    return sizeof(T) == 8 ? 0 : (MODE == MODE_A_GW || MODE == MODE_A ? 768 : 1024);
-}
+// One tile of one lattice: the column tile (j0, k0) marched over planes
+// [i0, i1).  Shared by the single-lattice kernel below and the ensemble
+// kernel (ensemble.cuh).
+template <typename T>
+struct TileJob {
+    const T *X, *D;   // fields and momenta in, [2][N^3] each
+    T *Xo, *Do;       // sweep B outputs
+    T *S;             // GW sources [10][N][N][N+2] (sweep A with GWs)
+    const DevScalars *sc;
+    int j0, k0, i0, i1;
+};
 
+template <int TK, int TJ>
+struct SweepSmem {
+    static constexpr int P = (TK + 2) * (TJ + 2);
+};
+
+// Marches one tile; adds this thread's share of the reduced values to acc.
 template <typename T, int TK, int TJ, int MODE>
-__global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * TJ - 1) / (TK * TJ))
-    sweep_kernel(StencilArgs args) {
+__device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob<T> &job, T *smem0, T *smem1,
+                                           double (&acc)[kNV]) {
     using M = March<T, TK, TJ>;
-    __shared__ __align__(16) T smem[2][M::NA * M::P];
-    __shared__ double sred[((TK * TJ + 31) / 32) * kNV];
-    __shared__ int sflag;
-    const LatticeConsts &c = args.c;
     const int N = c.N;
     const size_t n3 = (size_t)N * N * N;
     M m;
-    m.init(static_cast<const T *>(args.X), static_cast<const T *>(args.D), N, n3);
-    const int i0 = blockIdx.z * args.ci, i1 = min(i0 + args.ci, N);
-    const DevScalars *scp = args.sc;
+    m.init(job.X, job.D, N, n3, job.j0, job.k0);
+    const int i0 = job.i0, i1 = job.i1;
+    const DevScalars *scp = job.sc;
     const double h = c.half_dt, dt = c.dt;
     const double a0 = scp->a[0];
+    auto buf = [smem0, smem1](int i) { return (i & 1) ? smem1 : smem0; };
 
-    // per-kernel constants
     double ad0 = 0., a1 = 0., ad1 = 0.;
     if constexpr (MODE == MODE_B) {
         ad0 = scp->adot[0];
@@ -308,19 +316,15 @@ __global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * T
     }
     (void)ia12f; (void)c3H0f; (void)c3H1f; (void)dtf; (void)dnf; (void)q3f; (void)c3H1;
 
-    double acc[kNV];
-#pragma unroll
-    for (int q = 0; q < kNV; q++) acc[q] = 0.;
-
     // prologue: registers for planes i0-1, i0, i0+1; shared tile of plane i0
     m.load_own(m.prev, i0 - 1);
     m.load_own(m.cur, i0);
     m.load_own(m.nxt, i0 + 1);
     m.load_halo(i0);
-    m.store(smem[i0 & 1], m.cur);
+    m.store(buf(i0), m.cur);
     __syncthreads();
 
-    T *Xo = static_cast<T *>(args.Xo), *Do = static_cast<T *>(args.Do);
+    T *Xo = job.Xo, *Do = job.Do;
     const int j = m.j0 + m.ty, k = m.k0 + m.tx;
     for (int i = i0; i < i1; i++) {
         const bool more = i + 1 < i1;
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * T
             m.load_own(m.nn, i + 2);
             m.load_halo(i + 1);
         }
-        const T *sb = smem[i & 1];
+        const T *sb = buf(i);
         Nb7<T> f0[2], d0[2];
         for (int f = 0; f < 2; f++) {
             f0[f] = m.nb(sb, f);
@@ -409,7 +413,7 @@ __global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * T
                 acc[1] += (double)v_diff32(m0, c.model, f0[0].v[0], f0[1].v[0]);
                 if constexpr (MODE != MODE_E0) acc[3] += (double)v_diff32(m1, c.model, f1c[0], f1c[1]);
             }
-            if constexpr (MODE == MODE_A_GW) store_sources(static_cast<T *>(args.S), N, i, j, k, s0, s1);
+            if constexpr (MODE == MODE_A_GW) store_sources(job.S, N, i, j, k, s0, s1);
         }
         if (more) {
 #pragma unroll
@@ -418,12 +422,65 @@ __global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * T
                 m.cur[a] = m.nxt[a];
                 m.nxt[a] = m.nn[a];
             }
-            m.store(smem[(i + 1) & 1], m.cur);
+            m.store(buf(i + 1), m.cur);
         }
         __syncthreads();
     }
+}
 
-    const int tid = m.tid;
+// End of sweep B for one lattice (thread 0 of the block that finished it
+// last): the homogeneous trajectory (FP32 path) and a[0] advance.
+template <typename T>
+__device__ __forceinline__ void finish_b(const LatticeConsts &c, DevScalars *s) {
+    const double dt = c.dt, a0 = s->a[0], ad0 = s->adot[0], a1 = s->a[1], ad1 = s->adot[1];
+    const double c3H1 = (3. * ad1) / a1;
+    if constexpr (sizeof(T) == 4) {
+        MeanTraj q = mean_traj(c, s);
+        for (int f = 0; f < 2; f++) {
+            const double dfb1 = q.pbar[f] + ad0 * q.qbar[f];
+            const double fbn = q.fb0[f] + dt * dfb1;
+            const double dfbn = q.dfb0[f] + dt * (-dv_h(c.model, c.mc, f, q.fb1[0], q.fb1[1]) - c3H1 * dfb1);
+            s->fbar[f] = fbn;
+            s->dfbar[f] = dfbn;
+        }
+    }
+    s->a[0] = a0 + dt * ad1; /* g2functions.cpp:268 */
+    s->adot_given = 0;
+    s->step += 1;
+}
+
+// FP32: cap registers so that 3 (sweep A) or 4 (sweep B, E0) blocks of 256
+// threads share an SM -- the sweeps are latency-bound at lower occupancy.
+template <typename T, int MODE>
+constexpr int sweep_min_threads() {
+    return sizeof(T) == 8 ? 0 : (MODE == MODE_A_GW || MODE == MODE_A ? 768 : 1024);
+}
+
+// Single lattice: block (x, y, z) = column tile (k, j) and plane chunk.
+template <typename T, int TK, int TJ, int MODE>
+__global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * TJ - 1) / (TK * TJ))
+    sweep_kernel(StencilArgs args) {
+    __shared__ __align__(16) T smem[2][4 * SweepSmem<TK, TJ>::P];
+    __shared__ double sred[((TK * TJ + 31) / 32) * kNV];
+    __shared__ int sflag;
+    const LatticeConsts &c = args.c;
+    TileJob<T> job;
+    job.X = static_cast<const T *>(args.X);
+    job.D = static_cast<const T *>(args.D);
+    job.Xo = static_cast<T *>(args.Xo);
+    job.Do = static_cast<T *>(args.Do);
+    job.S = static_cast<T *>(args.S);
+    job.sc = args.sc;
+    job.k0 = blockIdx.x * TK;
+    job.j0 = blockIdx.y * TJ;
+    job.i0 = blockIdx.z * args.ci;
+    job.i1 = min(job.i0 + args.ci, c.N);
+    double acc[kNV];
+#pragma unroll
+    for (int q = 0; q < kNV; q++) acc[q] = 0.;
+    sweep_tile<T, TK, TJ, MODE>(c, job, smem[0], smem[1], acc);
+
+    const int tid = threadIdx.x;
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if constexpr (MODE != MODE_B) {
         block_reduce<kNV>(acc, sred);
@@ -439,21 +496,7 @@ __global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * T
             *args.counter = 0u;
         }
     } else if (tid == 0) {
-        DevScalars *s = args.sc;
-        if constexpr (sizeof(T) == 4) {
-            // homogeneous trajectory to the end of the step, same RK2 scheme
-            MeanTraj q = mean_traj(c, s);
-            for (int f = 0; f < 2; f++) {
-                const double dfb1 = q.pbar[f] + ad0 * q.qbar[f];
-                const double fbn = q.fb0[f] + dt * dfb1;
-                const double dfbn = q.dfb0[f] + dt * (-dv_h(c.model, c.mc, f, q.fb1[0], q.fb1[1]) - c3H1 * dfb1);
-                s->fbar[f] = fbn;
-                s->dfbar[f] = dfbn;
-            }
-        }
-        s->a[0] = a0 + dt * ad1; /* g2functions.cpp:268 */
-        s->adot_given = 0;
-        s->step += 1;
+        finish_b<T>(c, args.sc);
         *args.counter = 0u;
     }
 }

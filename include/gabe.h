@@ -179,6 +179,80 @@ size_t gabe_device_bytes(const gabe_handle *h);
 /* Kernel launches one step enqueues (for launch accounting). */
 int gabe_launches_per_step(const gabe_handle *h);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble: many independent lattices of uneven size, coupling,
+ * fluctuation amplitude and seed, evolved together in FP32 storage with FP64
+ * scalars and reductions, one persistent launch per sweep and one cuFFT call
+ * per lattice size each step (replayed as a CUDA graph).  No counterpart in
+ * the reference, which runs one lattice per process; each lattice follows
+ * the same step() and specOut() as a gabe_handle.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int32_t struct_size;            /* sizeof(gabe_ensemble_params) */
+    int32_t nlat;                   /* number of lattices */
+    const int32_t *N;               /* [nlat] points per side; multiple of 16 */
+    const double *g2_over_lambda;   /* [nlat] coupling of V = lambda phi^4/4 + g^2 phi^2 chi^2/2 */
+    const double *amplitude;        /* [nlat] multiplier of the randInit amplitudes (g2init.cpp:136-143) */
+    const uint64_t *seed;           /* [nlat] generator seeds */
+    const int32_t *tile_shape;      /* [nlat] 0 = 32x8, 1 = 16x16 columns per block; NULL = default */
+    const int32_t *tile_ci;         /* [nlat] planes per block; NULL = default */
+    double L, dt;                   /* shared box side and time step */
+    double lambda, phi0, dphi0;     /* shared physical model constants (program units B = sqrt(lambda) phi0) */
+    int32_t gws_on;                 /* calc_gws */
+    int32_t device;                 /* CUDA device, -1 = current */
+    int32_t nlog;                   /* log-spaced |k| bins of gabe_ensemble_log_spectra */
+    int32_t gw_spec_quirk;          /* as in gabe_params */
+    int32_t flags;                  /* GABE_FLAG_NO_GRAPH */
+    int32_t reserved;
+} gabe_ensemble_params;
+
+typedef struct gabe_ensemble gabe_ensemble;
+
+int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out);
+int gabe_ensemble_destroy(gabe_ensemble *e);
+
+/* Draws every lattice's initial state on the device: homogeneous values
+ * phi0, dphi0 plus Gaussian random fluctuations with the reference's
+ * randInit distribution (g2init.cpp:68-189; phi first, then chi with
+ * m_eff^2 from the fluctuated phi), a = 1, adot from the homogeneous energy,
+ * h = l = 0. */
+int gabe_ensemble_init(gabe_ensemble *e);
+
+/* Replaces lattice `lat`'s state (FP64 host arrays in the reference
+ * layout; h = l = 0). */
+int gabe_ensemble_upload(gabe_ensemble *e, int lat, const double *field0, const double *dfield0, double a0,
+                         double adot0);
+
+int gabe_ensemble_step(gabe_ensemble *e, int nsteps);
+int gabe_ensemble_sync(gabe_ensemble *e);
+
+/* Per-lattice scalars, [nlat][12] in the order of gabe_scalars. */
+int gabe_ensemble_scalars(gabe_ensemble *e, double *out);
+
+/* Native |k| bins of the largest lattice: (int)(sqrt(3) Nmax/2 + 1). */
+int gabe_ensemble_native_bins(const gabe_ensemble *e);
+
+/* Log spectra of every lattice: logspec [nlat][3][nlog] = log10 of
+ * (Delta^2_phi, Delta^2_chi, Omega_gw) in nlog log-spaced bins of the native
+ * bin index b in [1, native_bins], each the count-weighted mean of the
+ * native bins' values (g2spectra.cpp:94-103,186-195), NaN where a log bin
+ * holds no native bin; counts [nlat][nlog]; native (may be NULL)
+ * [nlat][4][native_bins]: the native power sums of phi, chi, GW and the
+ * counts. */
+int gabe_ensemble_log_spectra(gabe_ensemble *e, double *logspec, double *counts, double *native);
+
+/* Copies lattice `lat`'s state to the host (reference layout, FP64). */
+int gabe_ensemble_download(gabe_ensemble *e, int lat, double *field0, double *dfield0, double *h0, double *l0);
+
+const char *gabe_ensemble_last_error(const gabe_ensemble *e);
+size_t gabe_ensemble_device_bytes(const gabe_ensemble *e);
+
+/* The cudaStream_t (as void *) every ensemble call enqueues on, for timing
+ * with events; and the library's own kernel launches per step (cuFFT's are
+ * not counted). */
+void *gabe_ensemble_stream(const gabe_ensemble *e);
+int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
+
 #ifdef __cplusplus
 }
 #endif

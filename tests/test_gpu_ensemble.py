@@ -1,0 +1,127 @@
+"""The batched ensemble (gabe_ensemble_*) against single lattices and the
+oracle.
+
+* Each ensemble lattice takes the same step as a single FP32 lattice holding
+  the same state (same per-site arithmetic; only the order of the energy
+  sums differs, so FP32 fields agree to ~1e-6 of their fluctuations).
+* The device initial conditions have the reference's randInit distribution:
+  averaged over 16 lattices and 16 oracle realisations (rand()-driven, as the
+  reference), the phi and chi spectra and the kinetic energy agree within
+  their statistical error.
+* Log spectra are the count-weighted means of the native bins (checked
+  against the numpy restatement gabe_b200.rebin_log).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import gabe_b200 as gb
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(got, want):
+    n = np.linalg.norm(want)
+    return float(np.linalg.norm(got - want) / n) if n > 0 else float(np.abs(got).max())
+
+
+def test_ensemble_steps_like_single_lattices():
+    sizes, g, amp, seeds = [32, 16, 48, 32], [100.0, 10.0, 300.0, 1.0], [1.0, 0.5, 2.0, 1.2], [11, 12, 13, 14]
+    with gb.Ensemble(sizes, g, amp, seeds, nlog=32, tiles=None) as ens:
+        ens.init()
+        sc0 = ens.scalars()
+        states = [ens.download(l) for l in range(4)]
+        for l, (f, d, _, _) in enumerate(states):
+            ens.upload(l, f, d, a0=sc0[l, 0], adot0=sc0[l, 2])
+        ens.step(8)
+        sc = ens.scalars()
+        for l, (f, d, _, _) in enumerate(states):
+            with gb.Lattice(sizes[l], gws=True, precision=gb.FP32, model_c=gb.lphi4_constants(g[l])) as lat:
+                lat.upload_state(f, d, a0=sc0[l, 0], adot0=sc0[l, 2])
+                lat.step(8)
+                s1 = lat.scalars()
+                f1, d1, h1, l1 = lat.download_state()
+            want = np.array([v for k in ("a", "adot", "edkin", "edpot", "edgrad", "edrho") for v in s1[k]])
+            rho = want[10]
+            for q in range(12):
+                tol = 1e-6 * (abs(rho) if q in (8, 9) else abs(want[q]))
+                assert abs(sc[l, q] - want[q]) <= tol, (l, q, sc[l, q], want[q])
+            fe, de, he, le = ens.download(l)
+            for fld in range(2):
+                fl = f1[fld] - f1[fld].mean()
+                assert np.abs(fe[fld] - f1[fld]).max() <= 1e-5 * np.abs(fl).max()
+            assert _rel(le, l1) <= 1e-4 and _rel(he, h1) <= 1e-4
+
+
+def test_ensemble_graph_and_direct_launches_agree():
+    sizes, g, amp, seeds = [32, 16], [100.0, 50.0], [1.0, 1.0], [3, 4]
+    out = []
+    for flags in (0, gb.FLAG_NO_GRAPH):
+        with gb.Ensemble(sizes, g, amp, seeds, nlog=16, tiles=None, flags=flags) as ens:
+            ens.init()
+            ens.step(5)
+            out.append((ens.scalars(), ens.download(0)))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    for a, b in zip(out[0][1], out[1][1]):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_ensemble_initial_conditions_have_the_reference_distribution():
+    n, nl = 32, 16
+    with gb.Ensemble([n] * nl, [100.0] * nl, [1.0] * nl, list(range(100, 100 + nl)), nlog=8, tiles=None) as ens:
+        ens.init()
+        _, _, nat = ens.log_spectra()
+        sc = ens.scalars()
+    cfg = po.Config(N=n, model=po.MODEL_LPHI4, gws=0)
+    ref_p, ref_kin = [], []
+    for s in range(nl):
+        st = po.init_state(cfg, seed=1000 + s)
+        sp = po.spectra(cfg, st.field[0], None, st.sc.edrho[0])
+        ref_p.append(sp[:, [1, 3]])  # P_phi, P_chi per native bin
+        ref_kin.append(st.sc.edkin[0])
+    ref = np.mean(ref_p, axis=0)
+    L = cfg.L
+    spec_norm = (L / n) ** 6 * (2 * math.pi / L) ** 3
+    cnt = nat[0, 3]
+    nb = len(cnt)
+    got = np.mean([[nat[l, f, :nb] * spec_norm / np.maximum(cnt, 1) for f in range(2)] for l in range(nl)], axis=0).T
+    for b in range(1, min(nb, ref.shape[0]) - 1):
+        if cnt[b] < 200:
+            continue
+        for f in range(2):
+            assert abs(got[b, f] - ref[b, f]) <= 0.15 * ref[b, f], (b, f, got[b, f], ref[b, f])
+    kin = np.mean(sc[:, 4])
+    assert abs(kin - np.mean(ref_kin)) <= 0.05 * np.mean(ref_kin)
+
+
+def test_ensemble_log_spectra_are_rebinned_native_bins():
+    sizes, g, amp, seeds = [32, 48], [100.0, 20.0], [1.0, 1.5], [7, 8]
+    nlog = 24
+    with gb.Ensemble(sizes, g, amp, seeds, nlog=nlog, tiles=None) as ens:
+        ens.init()
+        ens.step(12)
+        logs, cnt, nat = ens.log_spectra()
+        sc = ens.scalars()
+        state = ens.download(1)
+    for l in range(2):
+        want, wcnt = gb.rebin_log(nat[l], sizes[l], nlog, nat.shape[2], 20.0, sc[l, 10])
+        np.testing.assert_array_equal(cnt[l], wcnt)
+        ok = np.isfinite(want)
+        np.testing.assert_allclose(logs[l][ok], want[ok], rtol=1e-12, atol=1e-12)
+        assert np.all(np.isnan(logs[l][~ok]))
+    # native sums equal the single-lattice spectra sums of the same state
+    f, d, h, l = state
+    with gb.Lattice(48, gws=True, precision=gb.FP32, model_c=gb.lphi4_constants(20.0)) as lat:
+        lat.upload_state(f, d, h, l, a0=sc[1, 0], adot0=sc[1, 2])
+        sums, counts = lat.spectra_raw()
+    nb = len(counts)
+    np.testing.assert_array_equal(nat[1, 3, :nb], counts)
+    for s in range(3):
+        # bin 0 holds only the k = 0 mode, whose power is rounding noise for
+        # a field with zero mean: compare against a floor of the column max
+        floor = 1e-9 * sums[s].max()
+        m = sums[s] > floor
+        assert np.max(np.abs(nat[1, s, :nb][m] - sums[s][m]) / sums[s][m]) <= 1e-3
+        assert np.all(np.abs(nat[1, s, :nb][~m]) <= 10 * floor)
