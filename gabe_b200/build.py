@@ -27,6 +27,7 @@ UNITS = [
     ("kernels_f32.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("ensemble.cu", []),
+    ("mlp.cu", []),
 ]
 
 

@@ -1,0 +1,117 @@
+"""The emulator's MLP kernels (gabe_mlp_*) against the CPU oracle
+(oracle/mlp_oracle.py): initialisation, forward, gradient, the AdamW step
+and training, in FP32- and BF16-activation modes."""
+import numpy as np
+import pytest
+import torch
+
+from gabe_b200 import emulator as em
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (3, 256, 4, 192)
+
+
+def _batch(n, seed=0, nan_frac=0.3):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 3)).astype(np.float32)
+    t = rng.normal(size=(n, 192)).astype(np.float32)
+    t[rng.uniform(size=t.shape) < nan_frac] = np.nan
+    return x, t
+
+
+def _dev(a):
+    return torch.tensor(a, device="cuda")
+
+
+def _perturbed_params(seed):
+    p = mo.init_params(seed)
+    rng = np.random.default_rng(seed)
+    lay, _ = mo.layout()
+    for K, N, oW, ob in lay:
+        p[ob:ob + N] = (0.1 * rng.normal(size=N)).astype(np.float32)
+    return p
+
+
+def test_device_initialisation_equals_oracle():
+    with em.MLP(seed=1234) as net:
+        assert net.num_params == 247744
+        np.testing.assert_array_equal(net.get_params(), mo.init_params(1234))
+
+
+@pytest.mark.parametrize("fp32_act", [True, False])
+def test_forward_matches_oracle(fp32_act):
+    p = _perturbed_params(5)
+    x, _ = _batch(1000, seed=1)
+    with em.MLP(fp32_act=fp32_act, max_rows=384) as net:  # several chunks
+        net.set_params(p)
+        y = net.forward(_dev(x)).cpu().numpy()
+    y64, _, _ = mo.forward(p, x, mode="fp64")
+    if fp32_act:
+        assert np.linalg.norm(y - y64) / np.linalg.norm(y64) <= 1e-5
+    else:
+        ybf, _, _ = mo.forward(p, x, mode="bf16")
+        # same roundings as the oracle's emulation up to rare one-ulp flips
+        assert np.linalg.norm(y - ybf) / np.linalg.norm(ybf) <= 2e-3
+        assert np.linalg.norm(y - y64) / np.linalg.norm(y64) <= 2e-2
+
+
+@pytest.mark.parametrize("fp32_act", [True, False])
+def test_gradient_matches_oracle(fp32_act):
+    p = _perturbed_params(7)
+    x, t = _batch(512, seed=2)
+    with em.MLP(fp32_act=fp32_act) as net:
+        net.set_params(p)
+        loss, g = net.loss_grad(_dev(x), _dev(t))
+    mode = "fp64" if fp32_act else "bf16"
+    lref, gref = mo.loss_grad(p, x, t, mode=mode)
+    assert abs(loss - lref) <= (1e-6 if fp32_act else 2e-3) * lref
+    lay, _ = mo.layout()
+    tol = 1e-4 if fp32_act else 2e-2
+    for K, N, oW, ob in lay:
+        for a, b in ((oW, oW + K * N), (ob, ob + N)):
+            rel = np.linalg.norm(g[a:b] - gref[a:b]) / np.linalg.norm(gref[a:b])
+            assert rel <= tol, (K, N, a, rel)
+
+
+def test_adam_step_matches_oracle():
+    p = _perturbed_params(11)
+    x, t = _batch(256, seed=3)
+    perm = torch.arange(256, dtype=torch.int32, device="cuda")
+    with em.MLP(fp32_act=True, lr=3e-3, weight_decay=0.01) as net:
+        net.set_params(p)
+        _, g = net.loss_grad(_dev(x), _dev(t))
+        xd, td = _dev(x), _dev(t)
+        net.train_batches(xd, td, perm, 256, 1)
+        net.sync()
+        p1 = net.get_params()
+        loss, steps = net.train_loss()
+    assert steps == 1
+    z = np.zeros_like(p)
+    want, _, _ = mo.adamw_step(p, g, z, z.copy(), 1, lr=3e-3, wd=0.01)
+    np.testing.assert_allclose(p1, want, rtol=1e-6, atol=1e-7)
+
+
+def test_graph_and_direct_training_agree_bitwise():
+    x, t = _batch(4096, seed=4, nan_frac=0.1)
+    out = []
+    for graph in (True, False):
+        with em.MLP(graph=graph, seed=3) as net:
+            net.fit(_dev(x), _dev(t), epochs=2, batch=512, seed=9)
+            out.append(net.get_params())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_training_fits_a_smooth_map():
+    rng = np.random.default_rng(5)
+    x = rng.uniform(-1, 1, size=(8192, 3)).astype(np.float32)
+    k = np.linspace(0, 3, 192)
+    t = (np.sin(np.outer(x[:, 0], k) + x[:, 1:2]) * (1 + 0.5 * x[:, 2:3])).astype(np.float32)
+    t[:, 150:][x[:, 0] > 0.5] = np.nan  # ragged valid region
+    with em.MLP(lr=2e-3, seed=2) as net:
+        l0, _ = net.loss_grad(_dev(x[:2048]), _dev(t[:2048]), want_grad=False)
+        hist = net.fit(_dev(x), _dev(t), epochs=60, batch=256, seed=1, log_every=10)
+        l1, _ = net.loss_grad(_dev(x[:2048]), _dev(t[:2048]), want_grad=False)
+    assert hist[-1][1] < hist[0][1]
+    assert l1 < 0.02 * l0, (l0, l1)
