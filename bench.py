@@ -210,7 +210,8 @@ def ensemble_leg(args, rank: int, world: int, local: int, dist, barrier, max_ove
     mine = ge.partition(Ns, world)[rank]
     every = args.ens_every
     K = max(every, args.ens_steps // every * every)
-    ens = gb.Ensemble(Ns[mine], g[mine], amp[mine], seeds[mine], nlog=64, device=local, tiles="auto")
+    ens = gb.Ensemble(Ns[mine], g[mine], amp[mine], seeds[mine], nlog=64, device=local, tiles="auto",
+                      log_top_bin=gb.numbins(max(ge.SIZES)))
     stream = torch.cuda.ExternalStream(ens.stream_ptr)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     ev[0].record(stream)

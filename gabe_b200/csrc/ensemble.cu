@@ -56,6 +56,7 @@ struct gabe_ensemble {
     double *d_part = nullptr, *d_log = nullptr, *d_logcnt = nullptr, *d_native = nullptr;
     unsigned int *d_part_cnt = nullptr;
     int nb_max = 0;
+    int log_top = 0;  // upper end of the log bins, native-bin units
     int cur = 0;
     bool ready = false, e0_stale = false;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -222,7 +223,8 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
         return eset(nullptr, GABE_ERR_PARAM, "bad gabe_ensemble_params");
     if (p->nlat < 1 || !p->N || !p->g2_over_lambda || !p->amplitude || !p->seed)
         return eset(nullptr, GABE_ERR_PARAM, "nlat and the per-lattice arrays are required");
-    if (!(p->L > 0) || !(p->dt > 0) || !(p->lambda > 0) || !(p->phi0 != 0) || p->nlog < 1 || p->nlog > 4096)
+    if (!(p->L > 0) || !(p->dt > 0) || !(p->lambda > 0) || !(p->phi0 != 0) || p->nlog < 1 || p->nlog > 4096 ||
+        p->log_top_bin < 0 || p->log_top_bin > (1 << 20))
         return eset(nullptr, GABE_ERR_PARAM, "invalid shared parameters");
     for (int l = 0; l < p->nlat; l++) {
         const int n = p->N[l];
@@ -331,6 +333,7 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
     if ((rc = ealloc(e, (void **)&e->d_sumsq, sizeof(double) * e->nlat))) return bail(rc);
     int nmax = *std::max_element(e->N.begin(), e->N.end());
     e->nb_max = gabe_spectra_numbins(nmax);
+    e->log_top = p->log_top_bin > 0 ? p->log_top_bin : e->nb_max;
     if ((rc = ealloc(e, (void **)&e->d_part, sizeof(double) * e->nlat * kEnsBinBlocks * 3 * e->nb_max))) return bail(rc);
     if ((rc = ealloc(e, (void **)&e->d_part_cnt, sizeof(unsigned) * e->nlat * kEnsBinBlocks * e->nb_max))) return bail(rc);
     if ((rc = ealloc(e, (void **)&e->d_log, sizeof(double) * e->nlat * 3 * e->nlog))) return bail(rc);
@@ -552,7 +555,7 @@ int gabe_ensemble_log_spectra(gabe_ensemble *e, double *logspec, double *counts,
     const size_t smem = (size_t)e->nb_max * (3 * 8 + 4);
     ens_bin_kernel<<<dim3(kEnsBinBlocks, e->nlat), 256, smem, e->stream>>>(b);
     ECK(e, cudaGetLastError());
-    ens_rebin_kernel<<<e->nlat, 128, 0, e->stream>>>(b, e->nlog, e->L, e->d_log, e->d_logcnt, e->d_native);
+    ens_rebin_kernel<<<e->nlat, 128, 0, e->stream>>>(b, e->nlog, (double)e->log_top, e->L, e->d_log, e->d_logcnt, e->d_native);
     ECK(e, cudaGetLastError());
     ECK(e, cudaMemcpyAsync(logspec, e->d_log, sizeof(double) * e->nlat * 3 * e->nlog, cudaMemcpyDeviceToHost, e->stream));
     ECK(e, cudaMemcpyAsync(counts, e->d_logcnt, sizeof(double) * e->nlat * e->nlog, cudaMemcpyDeviceToHost, e->stream));

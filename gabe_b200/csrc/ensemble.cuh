@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(256) ens_bin_kernel(EnsBinArgs a) {
 // out: [nlat][3][nlog] log10 of (Delta^2_phi, Delta^2_chi, Omega_gw), NaN where
 // a log bin holds no native bin; cnt: [nlat][nlog]; native: [nlat][4][nb_max]
 // (sums of phi, chi, GW and counts) for exact checks.
-__global__ void ens_rebin_kernel(EnsBinArgs a, int nlog, double L, double *out, double *cnt, double *native) {
+__global__ void ens_rebin_kernel(EnsBinArgs a, int nlog, double hi, double L, double *out, double *cnt, double *native) {
     const int e = blockIdx.x, nb = a.nb_max;
     const EnsLat &E = a.lat[e];
     const int N = E.N;
@@ -369,7 +369,7 @@ __global__ void ens_rebin_kernel(EnsBinArgs a, int nlog, double L, double *out, 
     const double spec_norm = pow(L / (double)N, 6.) * pow(2. * M_PI / L, 3.);
     const double hub = sqrt(8. * M_PI / 3.) * sqrt(E.sc->edrho[0]);
     const double norm1 = 4.e-5 / pow(100., .333) / 24. / M_PI / M_PI / pow(L, 3.) / (hub * hub);
-    const double lo = 1.0, hi = (double)nb;
+    const double lo = 1.0;
     for (int q = threadIdx.x; q < nlog; q += blockDim.x) {
         const double e0 = lo * pow(hi / lo, (double)q / nlog), e1 = lo * pow(hi / lo, (double)(q + 1) / nlog);
         double n = 0., s0 = 0., s1 = 0., s2 = 0.;

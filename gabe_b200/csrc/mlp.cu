@@ -64,6 +64,8 @@ struct GemmArgs {
     void *Z;             // EPI_HIDDEN: pre-activation out (may be null); EPI_BWD_DATA: pre-activation in
     void *C;             // H (activation type), Y, dX or dW (FP32)
     long long ldc;
+    int kchunk;          // EPI_BWD_WEIGHT: k range of split blockIdx.z (a multiple of BK)
+    float *dbp;          // EPI_BWD_WEIGHT: column sums of B per split ([splits][N])
 };
 
 constexpr int BM = 64, BN = 64, BK = 16, kThreads = 256;
@@ -77,7 +79,12 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const TA *A = static_cast<const TA *>(g.A);
     float acc[4][4] = {};
-    for (int k0 = 0; k0 < g.K; k0 += BK) {
+    // split-K (weight gradient): this block sums k in [kb, ke) and writes
+    // its partial product to slice blockIdx.z of the output
+    const int kb = EPI == EPI_BWD_WEIGHT ? blockIdx.z * g.kchunk : 0;
+    const int ke = EPI == EPI_BWD_WEIGHT ? min(g.K, kb + g.kchunk) : g.K;
+    float csum = 0.f;  // EPI_BWD_WEIGHT, first row of tiles: column sums of B (the bias gradient)
+    for (int k0 = kb; k0 < ke; k0 += BK) {
         // A tile: 64 (m) x 16 (k); each thread 4 elements along the
         // operand's contiguous direction
         if (g.sak == 1) {
@@ -85,14 +92,14 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int gm = m0 + m, gk = k0 + kk + q;
-                As[kk + q][m] = (gm < g.M && gk < g.K) ? ldf(A, gm * g.sam + gk) : 0.f;
+                As[kk + q][m] = (gm < g.M && gk < ke) ? ldf(A, gm * g.sam + gk) : 0.f;
             }
         } else {
             const int kk = tid / 16, m = (tid % 16) * 4;
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int gm = m0 + m + q, gk = k0 + kk;
-                As[kk][m + q] = (gm < g.M && gk < g.K) ? ldf(A, gm * g.sam + gk * g.sak) : 0.f;
+                As[kk][m + q] = (gm < g.M && gk < ke) ? ldf(A, gm * g.sam + gk * g.sak) : 0.f;
             }
         }
         // B tile: 16 (k) x 64 (n)
@@ -101,17 +108,21 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int gk = k0 + kk, gn = n0 + n + q;
-                Bs[kk][n + q] = (gk < g.K && gn < g.N) ? g.B[gk * g.sbk + gn] : 0.f;
+                Bs[kk][n + q] = (gk < ke && gn < g.N) ? g.B[gk * g.sbk + gn] : 0.f;
             }
         } else {
             const int n = tid / 4, kk = (tid % 4) * 4;
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 const int gk = k0 + kk + q, gn = n0 + n;
-                Bs[kk + q][n] = (gk < g.K && gn < g.N) ? g.B[gk + gn * g.sbn] : 0.f;
+                Bs[kk + q][n] = (gk < ke && gn < g.N) ? g.B[gk + gn * g.sbn] : 0.f;
             }
         }
         __syncthreads();
+        if (EPI == EPI_BWD_WEIGHT && blockIdx.y == 0 && tid < BN) {
+#pragma unroll
+            for (int kk = 0; kk < BK; kk++) csum += Bs[kk][tid];
+        }
 #pragma unroll
         for (int kk = 0; kk < BK; kk++) {
             const float4 a = *reinterpret_cast<const float4 *>(&As[kk][ty * 4]);
@@ -124,6 +135,9 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
         }
         __syncthreads();
     }
+    if (EPI == EPI_BWD_WEIGHT && blockIdx.y == 0 && tid < BN && n0 + tid < g.N)
+        g.dbp[(long long)blockIdx.z * g.N + n0 + tid] = csum;
+    float *Cz = static_cast<float *>(g.C) + (EPI == EPI_BWD_WEIGHT ? (long long)blockIdx.z * g.M * g.ldc : 0);
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const int m = m0 + ty * 4 + i;
@@ -143,25 +157,24 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
             } else if (EPI == EPI_BWD_DATA) {
                 static_cast<float *>(g.C)[o] = v * dsilu(ldf(static_cast<const TACT *>(g.Z), o));
             } else {
-                static_cast<float *>(g.C)[o] = v;
+                Cz[o] = v;
             }
         }
     }
 }
 
-// db[n] = sum_b dZ[b][n]: 32 columns per block, 8 row groups, fixed order.
-__global__ void __launch_bounds__(256) colsum_kernel(const float *dz, int B, int N, float *db) {
-    __shared__ float red[8][33];
-    const int c = threadIdx.x % 32, rg = threadIdx.x / 32, n = blockIdx.x * 32 + c;
-    float s = 0.f;
-    if (n < N)
-        for (int b = rg; b < B; b += 8) s += dz[(long long)b * N + n];
-    red[rg][c] = s;
-    __syncthreads();
-    if (rg == 0 && n < N) {
-        float t = 0.f;
-        for (int q = 0; q < 8; q++) t += red[q][c];
-        db[n] = t;
+// dW = sum over splits of the partial products, db = sum of the partial
+// column sums; fixed order, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(256) splitk_reduce_kernel(const float *ws, const float *dbp, int splits,
+                                                            long long mn, int N, float *dW, float *db) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < mn + N;
+         i += (long long)gridDim.x * blockDim.x) {
+        float s = 0.f;
+        if (i < mn)
+            for (int z = 0; z < splits; z++) s += ws[z * mn + i];
+        else
+            for (int z = 0; z < splits; z++) s += dbp[(long long)z * N + (i - mn)];
+        (i < mn ? dW[i] : db[i - mn]) = s;
     }
 }
 
@@ -255,7 +268,8 @@ __global__ void scale_kernel(float *g, long long n, const TrainScalars *ts) {
 }
 
 struct AdamHyper {
-    float lr, b1, b2, eps, wd;
+    float lr, b1, b2, eps, wd, lr_min;
+    long long decay_steps;  // cosine from lr to lr_min over this many steps (0 = constant lr)
 };
 
 // AdamW with bias correction; the gradient is the unnormalised batch
@@ -265,15 +279,20 @@ __global__ void adam_kernel(float *p, const float *g, float *m, float *v, long l
     const float inv = ts->inv_count;
     const double t = (double)ts->step;
     const float bc1 = (float)(1. - pow((double)h.b1, t)), bc2 = (float)(1. - pow((double)h.b2, t));
+    float lr = h.lr;
+    if (h.decay_steps > 0) {
+        const double f = fmin(t - 1., (double)h.decay_steps) / (double)h.decay_steps;
+        lr = (float)(h.lr_min + 0.5 * (h.lr - h.lr_min) * (1. + cos(M_PI * f)));
+    }
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const float gi = g[i] * inv;
         float pi = p[i];
-        pi -= h.lr * h.wd * pi;
+        pi -= lr * h.wd * pi;
         const float mi = h.b1 * m[i] + (1.f - h.b1) * gi;
         const float vi = h.b2 * v[i] + (1.f - h.b2) * gi * gi;
         m[i] = mi;
         v[i] = vi;
-        p[i] = pi - h.lr * (mi / bc1) / (sqrtf(vi / bc2) + h.eps);
+        p[i] = pi - lr * (mi / bc1) / (sqrtf(vi / bc2) + h.eps);
     }
 }
 
@@ -290,6 +309,7 @@ struct gabe_mlp {
     long long P = 0;
     float *params = nullptr, *grads = nullptr, *mom = nullptr, *vel = nullptr;
     float *xb = nullptr, *tb = nullptr, *y = nullptr, *dy = nullptr, *d0 = nullptr, *d1 = nullptr;
+    float *ws = nullptr, *dbp = nullptr;  // split-K partials of the weight gradient
     void *Z = nullptr, *H = nullptr;  // [depth][max_rows][width] activation type
     double2 *part = nullptr;
     TrainScalars *ts = nullptr;
@@ -327,9 +347,11 @@ void *act_at(const gabe_mlp *m, void *base, int layer) {
     return static_cast<char *>(base) + (size_t)layer * m->p.max_rows * m->p.width * act_size(m);
 }
 
+constexpr int kMaxSplits = 16;
+
 template <typename TA, typename TACT, int EPI>
-int launch_gemm(gabe_mlp *m, const GemmArgs &g) {
-    const dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
+int launch_gemm(gabe_mlp *m, const GemmArgs &g, int splits = 1) {
+    const dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, splits);
     gemm_kernel<TA, TACT, EPI><<<grid, kThreads, 0, m->stream>>>(g);
     MCK(m, cudaGetLastError());
     return GABE_OK;
@@ -383,11 +405,22 @@ int backward_rows(gabe_mlp *m, const float *x, int rows) {
         w.B = delta;
         w.sbk = N;
         w.sbn = 1;
-        w.C = m->grads + m->offW[l];
+        w.C = m->ws;
         w.ldc = N;
-        int rc = l == 0 ? launch_gemm<float, TACT, EPI_BWD_WEIGHT>(m, w) : launch_gemm<TACT, TACT, EPI_BWD_WEIGHT>(m, w);
+        w.dbp = m->dbp;
+        // enough splits of the batch to give about two blocks per SM
+        const int tiles = ((K + BM - 1) / BM) * ((N + BN - 1) / BN);
+        int splits = (296 + tiles - 1) / tiles;
+        splits = splits < 1 ? 1 : (splits > kMaxSplits ? kMaxSplits : splits);
+        int chunk = (rows + splits - 1) / splits;
+        chunk = (chunk + BK - 1) / BK * BK;
+        splits = (rows + chunk - 1) / chunk;
+        w.kchunk = chunk;
+        int rc = l == 0 ? launch_gemm<float, TACT, EPI_BWD_WEIGHT>(m, w, splits)
+                        : launch_gemm<TACT, TACT, EPI_BWD_WEIGHT>(m, w, splits);
         if (rc) return rc;
-        colsum_kernel<<<(N + 31) / 32, 256, 0, m->stream>>>(delta, rows, N, m->grads + m->offb[l]);
+        splitk_reduce_kernel<<<148, 256, 0, m->stream>>>(m->ws, m->dbp, splits, (long long)K * N, N,
+                                                         m->grads + m->offW[l], m->grads + m->offb[l]);
         MCK(m, cudaGetLastError());
         if (l == 0) break;
         // delta_{l-1} = (delta W_l^T) * SiLU'(Z_{l-1})
@@ -428,7 +461,7 @@ int train_step(gabe_mlp *m, const float *x, const float *t, const int32_t *perm,
     loss_kernel<<<kLossBlocks, 256, 0, m->stream>>>(m->y, m->tb, (long long)B * nout, m->dy, m->part, m->ts, 1);
     MCK(m, cudaGetLastError());
     if ((rc = bwd(m, m->xb, B))) return rc;
-    AdamHyper h{m->p.lr, m->p.beta1, m->p.beta2, m->p.eps, m->p.weight_decay};
+    AdamHyper h{m->p.lr, m->p.beta1, m->p.beta2, m->p.eps, m->p.weight_decay, m->p.lr_min, m->p.decay_steps};
     adam_kernel<<<148 * 4, 256, 0, m->stream>>>(m->params, m->grads, m->mom, m->vel, m->P, h, m->ts);
     MCK(m, cudaGetLastError());
     return GABE_OK;
@@ -445,7 +478,7 @@ void free_all(gabe_mlp *m) {
     if (m->gexec) cudaGraphExecDestroy(m->gexec);
     if (m->graph) cudaGraphDestroy(m->graph);
     void *bufs[] = {m->params, m->grads, m->mom, m->vel, m->xb, m->tb, m->y, m->dy, m->d0, m->d1, m->Z, m->H,
-                    m->part, m->ts};
+                    m->part, m->ts, m->ws, m->dbp};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -469,6 +502,8 @@ void gabe_mlp_default_params(gabe_mlp_params *p) {
     p->beta2 = 0.999f;
     p->eps = 1e-8f;
     p->weight_decay = 0.f;
+    p->lr_min = 0.f;
+    p->decay_steps = 0;
     p->seed = 1;
     p->device = -1;
 }
@@ -481,7 +516,7 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         p->depth > 16 || p->n_out < 1 || p->n_out > 4096 || p->max_rows < 1 || p->max_rows > (1 << 21))
         return mset(nullptr, GABE_ERR_PARAM, "invalid MLP shape");
     if (!(p->lr >= 0) || !(p->beta1 >= 0 && p->beta1 < 1) || !(p->beta2 >= 0 && p->beta2 < 1) || !(p->eps > 0) ||
-        !(p->weight_decay >= 0))
+        !(p->weight_decay >= 0) || !(p->lr_min >= 0) || p->decay_steps < 0)
         return mset(nullptr, GABE_ERR_PARAM, "invalid optimiser parameters");
     gabe_mlp *m = new (std::nothrow) gabe_mlp();
     if (!m) return mset(nullptr, GABE_ERR_NOMEM, "host allocation failed");
@@ -523,6 +558,7 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         {(void **)&m->y, R * p->n_out * 4}, {(void **)&m->dy, R * p->n_out * 4}, {(void **)&m->d0, R * wide * 4},
         {(void **)&m->d1, R * wide * 4}, {&m->Z, (size_t)p->depth * R * W * A}, {&m->H, (size_t)p->depth * R * W * A},
         {(void **)&m->part, kLossBlocks * sizeof(double2)}, {(void **)&m->ts, sizeof(TrainScalars)},
+        {(void **)&m->ws, (size_t)kMaxSplits * wide * wide * 4}, {(void **)&m->dbp, (size_t)kMaxSplits * wide * 4},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.ptr, a.bytes) != cudaSuccess) {
@@ -649,6 +685,19 @@ int gabe_mlp_train(gabe_mlp *m, const float *x, const float *t, const int32_t *p
     return GABE_OK;
 }
 
+int gabe_mlp_set_schedule(gabe_mlp *m, float lr, float lr_min, int32_t decay_steps) {
+    if (!m || !(lr >= 0) || !(lr_min >= 0) || decay_steps < 0) return GABE_ERR_PARAM;
+    m->p.lr = lr;
+    m->p.lr_min = lr_min;
+    m->p.decay_steps = decay_steps;
+    // the captured step holds the hyper-parameters by value
+    if (m->gexec) cudaGraphExecDestroy(m->gexec);
+    if (m->graph) cudaGraphDestroy(m->graph);
+    m->gexec = nullptr;
+    m->graph = nullptr;
+    return GABE_OK;
+}
+
 int gabe_mlp_reset_batches(gabe_mlp *m) {
     if (!m) return GABE_ERR_PARAM;
     MCK(m, cudaSetDevice(m->dev));
@@ -682,6 +731,7 @@ int gabe_mlp_sync(gabe_mlp *m) {
 void *gabe_mlp_stream(const gabe_mlp *m) { return m ? (void *)m->stream : nullptr; }
 
 int gabe_mlp_launches_per_train_step(const gabe_mlp *m) { return m ? 3 + 3 * m->nl + (m->nl - 1) : 0; }
+
 
 int gabe_mlp_launches_per_forward(const gabe_mlp *m) { return m ? m->nl : 0; }
 

@@ -15,6 +15,7 @@ sweep needs around it:
 from __future__ import annotations
 
 import ctypes
+import warnings
 
 import numpy as np
 
@@ -29,7 +30,8 @@ class MLPParams(ctypes.Structure):
         ("struct_size", ctypes.c_int32), ("n_in", ctypes.c_int32), ("width", ctypes.c_int32),
         ("depth", ctypes.c_int32), ("n_out", ctypes.c_int32), ("max_rows", ctypes.c_int32),
         ("lr", ctypes.c_float), ("beta1", ctypes.c_float), ("beta2", ctypes.c_float), ("eps", ctypes.c_float),
-        ("weight_decay", ctypes.c_float), ("seed", ctypes.c_uint64), ("device", ctypes.c_int32),
+        ("weight_decay", ctypes.c_float), ("lr_min", ctypes.c_float), ("decay_steps", ctypes.c_int32),
+        ("seed", ctypes.c_uint64), ("device", ctypes.c_int32),
         ("flags", ctypes.c_int32),
     ]
 
@@ -51,6 +53,7 @@ def _mlp_lib():
         L.gabe_mlp_loss_grad.argtypes = [M, vp, vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_double), fp]
         L.gabe_mlp_train.argtypes = [M, vp, vp, vp, ctypes.c_int32, ctypes.c_int32]
         L.gabe_mlp_reset_batches.argtypes = [M]
+        L.gabe_mlp_set_schedule.argtypes = [M, ctypes.c_float, ctypes.c_float, ctypes.c_int32]
         L.gabe_mlp_train_loss.argtypes = [M, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]
         L.gabe_mlp_sync.argtypes = [M]
         L.gabe_mlp_stream.argtypes = [M]
@@ -171,6 +174,9 @@ class MLP:
         self._after_torch()
         self._check(_mlp_lib().gabe_mlp_train(self._h, x.data_ptr(), t.data_ptr(), perm.data_ptr(), batch, nbatch))
 
+    def set_schedule(self, lr: float, lr_min: float = 0.0, decay_steps: int = 0):
+        self._check(_mlp_lib().gabe_mlp_set_schedule(self._h, lr, lr_min, int(decay_steps)))
+
     def reset_batches(self):
         self._check(_mlp_lib().gabe_mlp_reset_batches(self._h))
 
@@ -182,17 +188,20 @@ class MLP:
     def sync(self):
         self._check(_mlp_lib().gabe_mlp_sync(self._h))
 
-    def fit(self, x, t, epochs: int, batch: int, seed: int = 0, log_every: int = 0):
+    def fit(self, x, t, epochs: int, batch: int, seed: int = 0, log_every: int = 0, lr_min: float | None = None):
         """Trains on all rows of x, t (device tensors) for `epochs` passes in
-        shuffled batches; the permutations of all epochs are drawn up front
-        and kept on the device.  Returns the mean batch loss per logged
-        epoch."""
+        shuffled batches; the permutations are drawn on the device.  With
+        lr_min the learning rate decays from the handle's lr to lr_min over
+        the run (cosine).  Returns the mean batch loss per logged epoch."""
         import torch
 
         n = x.shape[0]
+        if n < 1:
+            raise ValueError("no training rows")
+        batch = min(batch, n)
         nb = n // batch
-        if nb < 1:
-            raise ValueError("fewer rows than one batch")
+        if lr_min is not None:
+            self.set_schedule(self.p.lr, lr_min, epochs * nb)
         g = torch.Generator(device=x.device)
         g.manual_seed(seed)
         hist = []
@@ -233,15 +242,18 @@ class Emulator:
         return np.stack([np.log10(np.asarray(g2_over_lambda, dtype=np.float64)),
                          np.asarray(amplitude, dtype=np.float64), np.asarray(tau, dtype=np.float64)], axis=-1)
 
-    def fit(self, feats: np.ndarray, targets: np.ndarray, epochs: int, batch: int = 512, seed: int = 0):
+    def fit(self, feats: np.ndarray, targets: np.ndarray, epochs: int, batch: int = 512, seed: int = 0,
+            lr_min: float | None = 1e-5):
         import torch
 
         f = np.asarray(feats, dtype=np.float64)
         y = np.asarray(targets, dtype=np.float64)
         mu_x, sd_x = f.mean(0), f.std(0) + 1e-12
-        with np.errstate(invalid="ignore"):
-            mu_y = np.nanmean(np.where(np.isfinite(y), y, np.nan), axis=0)
-            sd_y = np.nanstd(np.where(np.isfinite(y), y, np.nan), axis=0)
+        yn = np.where(np.isfinite(y), y, np.nan)
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)  # outputs no lattice reaches
+            mu_y = np.nanmean(yn, axis=0)
+            sd_y = np.nanstd(yn, axis=0)
         mu_y = np.where(np.isfinite(mu_y), mu_y, 0.0)
         sd_y = np.where(np.isfinite(sd_y) & (sd_y > 1e-6), sd_y, 1.0)
         self.stats = (mu_x, sd_x, mu_y, sd_y)
@@ -249,7 +261,7 @@ class Emulator:
         ys = torch.tensor((y - mu_y) / sd_y, dtype=torch.float32, device="cuda")  # NaN stays NaN
         hist = []
         for k, net in enumerate(self.nets):
-            hist.append(net.fit(xs, ys, epochs, batch, seed=seed + k, log_every=max(1, epochs // 10)))
+            hist.append(net.fit(xs, ys, epochs, batch, seed=seed + k, log_every=max(1, epochs // 10), lr_min=lr_min))
         return hist
 
     def predict_members(self, feats: np.ndarray):
@@ -324,3 +336,160 @@ def queries_per_second(net: MLP, n: int = 1 << 20, reps: int = 5):
 
 
 __all__ = ["MLP", "Emulator", "nearest_neighbour", "per_bin_error", "queries_per_second"]
+
+
+# ---------------------------------------------------------------------------
+# The parameter-sweep workflow: ensembles -> training set -> emulator ->
+# held-out lattice re-runs as judge.
+# ---------------------------------------------------------------------------
+def ensemble_samples(N, g, amp, seeds, steps: int, every: int, nlog: int = 64, dt: float = 0.01, device: int = -1,
+                     log_top_bin: int | None = None):
+    """Evolves one batched ensemble and returns (features [T*nlat, 3],
+    targets [T*nlat, 3*nlog], lattice index per row, device ms).  The log
+    bins end at native bin `log_top_bin` (default: that of the largest sweep
+    size, 128^3), the same for every ensemble of a sweep."""
+    import torch
+
+    from . import Ensemble, numbins
+    from .ensemble import SIZES, evolve_and_record
+
+    top = log_top_bin if log_top_bin is not None else numbins(max(SIZES))
+    ens = Ensemble(N, g, amp, seeds, nlog=nlog, dt=dt, device=device, tiles="auto", log_top_bin=top)
+    s = torch.cuda.ExternalStream(ens.stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    ens.init()
+    taus, logs, _ = evolve_and_record(ens, steps, every, dt)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ens.close()
+    T, nlat = logs.shape[:2]
+    feats = Emulator.features(np.tile(g, T), np.tile(amp, T), np.repeat(taus, nlat))
+    targets = logs.reshape(T * nlat, 3 * nlog)
+    lat = np.tile(np.arange(nlat), T)
+    return feats, targets, lat, ms
+
+
+def run_sweep(*, nlat=256, ensembles=2, steps=2000, every=50, nlog=64, holdout=32, holdout_N=64, members=4,
+              epochs=1000, batch=512, lr=1e-3, master_seed=20261203, flag_quantile=0.9, sizes=None, log=print):
+    """Trains the emulator on `ensembles` uneven ensembles of `nlat`
+    lattices and judges it on `holdout` new parameter points evolved at
+    holdout_N^3.  Returns the report dict."""
+    import time
+
+    import torch
+
+    from .ensemble import SIZES, sample_parameters
+
+    sizes = tuple(sizes) if sizes else SIZES
+    report = {"config": dict(nlat=nlat, ensembles=ensembles, steps=steps, every=every, nlog=nlog, holdout=holdout,
+                             holdout_N=holdout_N, members=members, epochs=epochs, batch=batch, lr=lr,
+                             master_seed=master_seed, flag_quantile=flag_quantile, sizes=list(sizes))}
+    F, Y, LAT = [], [], []
+    ens_ms, sites = 0.0, 0.0
+    for e in range(ensembles):
+        N, g, amp, seeds = sample_parameters(nlat, master_seed + e, sizes=sizes)
+        f, y, lat, ms = ensemble_samples(N, g, amp, seeds, steps, every, nlog)
+        F.append(f)
+        Y.append(y)
+        LAT.append(lat + e * nlat)
+        ens_ms += ms
+        sites += float(np.sum(np.asarray(N, dtype=np.float64) ** 3))
+        log(f"ensemble {e}: {len(f)} samples in {ms / 1e3:.1f} s")
+    F, Y, LAT = np.concatenate(F), np.concatenate(Y), np.concatenate(LAT)
+    report["training_samples"] = int(len(F))
+    report["ensemble_lattice_runs_per_s"] = ensembles * nlat / (ens_ms / 1e3)
+    report["ensemble_site_updates_per_s"] = sites * steps / (ens_ms / 1e3)
+    # validation split by lattice (10 %) for the flagging threshold
+    rng = np.random.default_rng(master_seed)
+    val_lat = rng.choice(ensembles * nlat, size=max(1, ensembles * nlat // 10), replace=False)
+    is_val = np.isin(LAT, val_lat)
+    emu = Emulator(members, n_out=3 * nlog, lr=lr, seed=master_seed % 100000)
+    t0 = time.perf_counter()
+    hist = emu.fit(F[~is_val], Y[~is_val], epochs=epochs, batch=batch, seed=master_seed % 1000)
+    torch.cuda.synchronize()
+    report["train_s"] = time.perf_counter() - t0
+    report["train_loss_history"] = [[int(a), float(b)] for a, b in hist[0]]
+    steps_taken = emu.nets[0].train_loss()[1]
+    report["adam_steps_per_member"] = int(steps_taken)
+    # threshold: quantile of the per-point max spread on validation lattices
+    taus = np.unique(F[:, 2])
+    _, vspread = emu.predict(F[is_val])
+    vmask = np.isfinite(Y[is_val])
+    vpt = np.where(vmask, vspread, 0.0).max(1)
+    vlat = LAT[is_val]
+    per_point = np.array([vpt[vlat == l].max() for l in np.unique(vlat)])
+    thr = float(np.quantile(per_point, flag_quantile))
+    report["flag_threshold_dex"] = thr
+    # held-out parameter points, re-run on the lattice as judge
+    _, gh, ah, sh = sample_parameters(holdout, master_seed + 1000)
+    Nh = np.full(holdout, holdout_N, dtype=np.int32)
+    fh, yh, lath, ms_h = ensemble_samples(Nh, gh, ah, sh, steps, every, nlog)
+    report["holdout_lattice_runs_per_s"] = holdout / (ms_h / 1e3)
+    report["holdout_ms"] = ms_h
+    mean, spread = emu.predict(fh)
+    ok = np.isfinite(yh)
+    pt_spread = np.array([np.where(ok, spread, 0.0)[lath == l].max() for l in range(holdout)])
+    flagged = pt_spread > thr
+    nn = nearest_neighbour(F[~is_val], Y[~is_val], fh)
+    report["mae_dex_by_tau"] = {
+        "tau": [float(t) for t in np.unique(fh[:, 2])],
+        "emulator": [[float(np.nanmean(per_bin_error(mean[fh[:, 2] == t], yh[fh[:, 2] == t]).reshape(3, nlog)[s]))
+                      for s in range(3)] for t in np.unique(fh[:, 2])],
+    }
+    err_em = per_bin_error(mean, yh)
+    err_nn = per_bin_error(nn, yh)
+    keep = ~flagged[lath]
+    err_unflagged = per_bin_error(mean[keep], yh[keep]) if keep.any() else np.full(3 * nlog, np.nan)
+
+    def summary(err):
+        e = err.reshape(3, nlog)
+        return {"phi": float(np.nanmean(e[0])), "chi": float(np.nanmean(e[1])), "gw": float(np.nanmean(e[2])),
+                "all": float(np.nanmean(err))}
+
+    report["per_bin_mae_dex"] = {"emulator": err_em.reshape(3, nlog).tolist(),
+                                 "nearest_neighbour": err_nn.reshape(3, nlog).tolist()}
+    report["mae_dex"] = {"emulator": summary(err_em), "nearest_neighbour": summary(err_nn),
+                         "emulator_unflagged": summary(err_unflagged)}
+    report["flagged_points"] = [int(i) for i in np.flatnonzero(flagged)]
+    report["n_flagged"] = int(flagged.sum())
+    qps, qinfo = queries_per_second(emu.nets[0])
+    report["emulator_queries_per_s"] = qps
+    report["emulator_forward"] = qinfo
+    # a lattice run yields one spectrum set per output time; the emulator
+    # answers one (parameter, time) query with one spectrum set
+    report["spectra_per_s_emulator_over_lattice"] = qps / (report["holdout_lattice_runs_per_s"] * len(taus))
+    emu.close()
+    return report
+
+
+def main():
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="emulator sweep: ensembles -> training -> held-out lattice judge")
+    ap.add_argument("--lattices", type=int, default=256)
+    ap.add_argument("--ensembles", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--every", type=int, default=50)
+    ap.add_argument("--holdout", type=int, default=32)
+    ap.add_argument("--members", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=1000)
+    ap.add_argument("--batch", type=int, default=512)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    rep = run_sweep(nlat=a.lattices, ensembles=a.ensembles, steps=a.steps, every=a.every, holdout=a.holdout,
+                    members=a.members, epochs=a.epochs, batch=a.batch, lr=a.lr, master_seed=a.seed)
+    s = json.dumps(rep)
+    if a.out:
+        with open(a.out, "w") as fh:
+            fh.write(s)
+    short = {k: v for k, v in rep.items() if k not in ("per_bin_mae_dex", "train_loss_history")}
+    print(json.dumps(short, indent=1))
+
+
+if __name__ == "__main__":
+    main()

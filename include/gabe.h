@@ -203,7 +203,8 @@ typedef struct {
     int32_t nlog;                   /* log-spaced |k| bins of gabe_ensemble_log_spectra */
     int32_t gw_spec_quirk;          /* as in gabe_params */
     int32_t flags;                  /* GABE_FLAG_NO_GRAPH */
-    int32_t reserved;
+    int32_t log_top_bin;            /* upper end of the log bins in native-bin units (0 = the native
+                                       bins of the largest lattice); fix it to compare ensembles */
 } gabe_ensemble_params;
 
 typedef struct gabe_ensemble gabe_ensemble;

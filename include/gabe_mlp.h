@@ -38,6 +38,8 @@ typedef struct {
     int32_t n_out;         /* outputs (3 x 64 = 192), multiple of 64 */
     int32_t max_rows;      /* largest batch a forward/training call handles at once */
     float lr, beta1, beta2, eps, weight_decay;  /* AdamW */
+    float lr_min;          /* cosine decay of the learning rate from lr to lr_min ... */
+    int32_t decay_steps;   /* ... over this many Adam steps (0 = constant lr) */
     uint64_t seed;         /* weight initialisation */
     int32_t device;        /* CUDA device, -1 = current */
     int32_t flags;         /* GABE_MLP_* */
@@ -66,6 +68,11 @@ int gabe_mlp_loss_grad(gabe_mlp *m, const float *x, const float *t, int64_t n, d
  * i < batch, of x [*][n_in] and t [*][n_out], where s0 counts the batches
  * taken since the last gabe_mlp_reset_batches.  The caller keeps perm
  * valid for (s0 + nbatch) * batch entries. */
+/* Learning-rate schedule for the following Adam steps: cosine from lr to
+ * lr_min over decay_steps steps counted from the first step taken (0 =
+ * constant lr). */
+int gabe_mlp_set_schedule(gabe_mlp *m, float lr, float lr_min, int32_t decay_steps);
+
 int gabe_mlp_train(gabe_mlp *m, const float *x, const float *t, const int32_t *perm, int32_t batch, int32_t nbatch);
 int gabe_mlp_reset_batches(gabe_mlp *m);
 

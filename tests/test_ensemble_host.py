@@ -35,7 +35,8 @@ def _params(N, g=None, amp=None, seed=None, **kw):
     return p, (N, g, amp, seed)
 
 
-@pytest.mark.parametrize("case", ["N_not_16", "N_small", "neg_amp", "nan_g", "nlog0", "dt0", "nlat0", "size"])
+@pytest.mark.parametrize("case", ["N_not_16", "N_small", "neg_amp", "nan_g", "nlog0", "dt0", "nlat0", "size",
+                                  "log_top"])
 def test_ensemble_create_rejects_bad_params(case):
     lib = gb._ens_lib()
     N, g, amp, kw = [32, 48], None, None, {}
@@ -55,6 +56,8 @@ def test_ensemble_create_rejects_bad_params(case):
         kw = {"nlat": 0}
     elif case == "size":
         kw = {"struct_size": 8}
+    elif case == "log_top":
+        kw = {"log_top_bin": -1}
     p, keep = _params(N, g, amp, **kw)
     h = ctypes.c_void_p()
     assert lib.gabe_ensemble_create(ctypes.byref(p), ctypes.byref(h)) == 1

@@ -115,3 +115,26 @@ def test_training_fits_a_smooth_map():
         l1, _ = net.loss_grad(_dev(x[:2048]), _dev(t[:2048]), want_grad=False)
     assert hist[-1][1] < hist[0][1]
     assert l1 < 0.02 * l0, (l0, l1)
+
+
+def test_cosine_schedule_matches_oracle():
+    p = _perturbed_params(13)
+    x, t = _batch(128, seed=6)
+    perm = torch.arange(128, dtype=torch.int32, device="cuda")
+    lr0, lr1 = 4e-3, 1e-4
+    with em.MLP(fp32_act=True, lr=lr0) as net:
+        net.set_params(p)
+        net.set_schedule(lr0, lr1, 2)
+        xd, td = _dev(x), _dev(t)
+        ref, m, v = p.copy(), np.zeros_like(p), np.zeros_like(p)
+        for s in range(1, 4):
+            net.set_params(ref)
+            _, g = net.loss_grad(xd, td)
+            net.reset_batches()
+            net.train_batches(xd, td, perm, 128, 1)
+            net.sync()
+            got = net.get_params()
+            f = min(s - 1, 2) / 2
+            lr = lr1 + 0.5 * (lr0 - lr1) * (1 + np.cos(np.pi * f))
+            ref, m, v = mo.adamw_step(ref, g, m, v, s, lr=lr)
+            np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
