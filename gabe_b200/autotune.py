@@ -20,7 +20,13 @@ import numpy as np
 
 from . import FP32, FP64, GabeError, Lattice
 
-SHAPES = {0: (32, 8), 1: (16, 16), 2: (32, 4), 3: (16, 8), 4: (8, 8), 5: (4, 4)}
+SHAPES = {0: (32, 8), 1: (16, 16), 2: (32, 4), 3: (16, 8), 4: (8, 8), 5: (4, 4)}  # FP64 sweeps, ensemble
+# FP32 single-lattice sweeps (two sites per thread along k): kShapes32 in csrc/launch.h
+SHAPES32 = {0: (64, 8), 1: (64, 4), 2: (128, 4), 3: (32, 8), 4: (64, 16), 5: (32, 4), 6: (16, 8)}
+
+
+def shapes_for(precision: int) -> dict:
+    return SHAPES32 if precision == FP32 else SHAPES
 CACHE = os.environ.get("GABE_TILE_CACHE", os.path.join(os.path.dirname(os.path.abspath(__file__)), "tiles.json"))
 
 
@@ -91,9 +97,9 @@ def tune_ensemble(sizes, steps: int = 3, verbose: bool = True) -> dict:
     return out
 
 
-def candidates(N: int):
+def candidates(N: int, precision: int = FP32):
     out = []
-    for s, (tk, tj) in SHAPES.items():
+    for s, (tk, tj) in shapes_for(precision).items():
         if tk > N or tj > N or N % tk or N % tj:
             continue
         for ci in (16, 32, 64, 128, 256, 512):
@@ -109,7 +115,8 @@ def tune(N: int, precision: int = FP32, gws: bool = True, steps: int = 3, verbos
     f[1] -= 0.342
     d = 1e-6 * rng.standard_normal((2, N, N, N))
     results = []
-    for shape, ci in candidates(N):
+    table = shapes_for(precision)
+    for shape, ci in candidates(N, precision):
         try:
             with Lattice(N, gws=gws, precision=precision, tile_shape=shape, tile_ci=ci) as lat:
                 lat.upload_state(f, d, a0=1.0, adot0=0.5)
@@ -117,17 +124,17 @@ def tune(N: int, precision: int = FP32, gws: bool = True, steps: int = 3, verbos
                 ph = lat.profile_steps(steps)
         except GabeError as e:
             if verbose:
-                print(f"shape {SHAPES[shape]} ci {ci}: {e}")
+                print(f"shape {table[shape]} ci {ci}: {e}")
             continue
         t = ph["stage1"] + ph["stage2"]
         results.append({"shape": shape, "ci": ci, "sweeps_ms": t, "stage1": ph["stage1"], "stage2": ph["stage2"]})
         if verbose:
-            print(f"shape {SHAPES[shape]} ci {ci:4d}: sweep A {ph['stage1']:.3f} ms  sweep B {ph['stage2']:.3f} ms",
+            print(f"shape {table[shape]} ci {ci:4d}: sweep A {ph['stage1']:.3f} ms  sweep B {ph['stage2']:.3f} ms",
                   flush=True)
     best = min(results, key=lambda r: r["sweeps_ms"])
     cache = load_cache()
     cache[_key(N, precision, gws)] = {"shape": best["shape"], "ci": best["ci"], "sweeps_ms": best["sweeps_ms"],
-                                      "tile": SHAPES[best["shape"]]}
+                                      "tile": table[best["shape"]]}
     with open(CACHE, "w") as fh:
         json.dump(cache, fh, indent=1, sort_keys=True)
     return {"best": best, "all": results}

@@ -25,6 +25,7 @@ UNITS = [
     ("api.cu", []),
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", []),
+    ("planefft.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("ensemble.cu", []),
     ("mlp.cu", []),

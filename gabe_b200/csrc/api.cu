@@ -53,6 +53,9 @@ struct gabe_handle {
     int nbins = 0;
     cufftHandle plan_src = 0, plan_spec = 0;
     bool have_plan_src = false, have_plan_spec = false;
+    // FP32 sources: 2-D plane kernels (planefft.cuh) + a 1-D cuFFT pass along i
+    bool plane_fft = false;
+    int plane_grid = 0;
     void *fft_work = nullptr;
     size_t fft_work_bytes = 0;
     LatticeConsts lc{};
@@ -106,7 +109,8 @@ int dalloc(gabe_handle *h, void **ptr, size_t bytes) {
 }
 
 void choose_tile(gabe_handle *h) {
-    GridPlan g = plan_grid(h->N, h->p.tile_shape, h->p.tile_ci);
+    GridPlan g = h->f32 ? plan_grid32(h->N, h->p.tile_shape, h->p.tile_ci)
+                        : plan_grid(h->N, h->p.tile_shape, h->p.tile_ci);
     h->shape = g.shape;
     h->ci = g.ci;
     h->grid = g.grid;
@@ -117,7 +121,16 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    if (h->p.gws_on) {
+    h->plane_fft = h->p.gws_on && h->f32 && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
+    if (h->plane_fft) {
+        CK(h, plane_r2c_setup(h->N, &h->plane_grid));
+        // remaining pass along i: N*nz sequences of stride N*nz per source component
+        long long n1[1] = {N}, em[1] = {N};
+        CF(h, cufftCreate(&h->plan_src));
+        h->have_plan_src = true;
+        CF(h, cufftSetAutoAllocation(h->plan_src, 0));
+        CF(h, cufftMakePlanMany64(h->plan_src, 1, n1, em, N * nz, 1, em, N * nz, 1, CUFFT_C2C, N * nz, &ws_src));
+    } else if (h->p.gws_on) {
         long long inem[3] = {N, N, 2 * nz}, onem[3] = {N, N, nz};
         CF(h, cufftCreate(&h->plan_src));
         h->have_plan_src = true;
@@ -153,6 +166,20 @@ int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
 bool overlapped(const gabe_handle *h) { return h->p.gws_on && h->S2 != nullptr; }
 void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
 
+// In-place 3-D r2c of the 2*kSrc source arrays in source buffer `slot`
+// (fft_stresstensor's transforms, g2evolutionpert.cpp:190-195).
+int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
+    void *S = source_buffer(h, slot);
+    CF(h, cufftSetStream(h->plan_src, s));
+    if (!h->plane_fft) return fft_r2c(h, h->plan_src, S, S);
+    CK(h, plane_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc * h->N, h->plane_grid, s));
+    for (int q = 0; q < 2 * kSrc; q++) {
+        cufftComplex *c = static_cast<cufftComplex *>(S) + (size_t)q * h->M;
+        CF(h, cufftExecC2C(h->plan_src, c, c, CUFFT_FORWARD));
+    }
+    return GABE_OK;
+}
+
 StencilArgs stencil_args(gabe_handle *h, int cur, int slot = 0) {
     StencilArgs a{};
     a.X = h->X[cur];
@@ -171,14 +198,14 @@ StencilArgs stencil_args(gabe_handle *h, int cur, int slot = 0) {
 int sweep(gabe_handle *h, int mode, int cur, int counter, int slot = 0) {
     StencilArgs a = stencil_args(h, cur, slot);
     a.counter = h->counters + counter;
-    CK(h, h->f32 ? sweep_f32(h->shape, mode, a, h->grid, h->stream) : sweep_f64(h->shape, mode, a, h->grid, h->stream));
+    CK(h, h->f32 ? sweep32_f32(h->shape, mode, a, h->grid, h->stream)
+                 : sweep_f64(h->shape, mode, a, h->grid, h->stream));
     return GABE_OK;
 }
 
 int gw_chain(gabe_handle *h, int slot, cudaStream_t s) {
     void *S = source_buffer(h, slot);
-    CF(h, cufftSetStream(h->plan_src, s));
-    int rc = fft_r2c(h, h->plan_src, S, S);
+    int rc = source_fft(h, slot, s);
     if (rc) return rc;
     KspaceArgs k{};
     k.S = S;
@@ -219,8 +246,7 @@ int enqueue_steps(gabe_handle *h, int cur, int nsteps, bool serial, cudaEvent_t 
                 if (rc) return rc;
                 CK(h, cudaEventRecord(h->ev_k[slot], h->gw_stream));
             } else {
-                CF(h, cufftSetStream(h->plan_src, h->stream));
-                rc = fft_r2c(h, h->plan_src, source_buffer(h, slot), source_buffer(h, slot));
+                rc = source_fft(h, slot, h->stream);
                 if (rc) return rc;
                 if (e) CK(h, cudaEventRecord(e[2], h->stream));
                 KspaceArgs k{};
@@ -774,6 +800,8 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
-int gabe_launches_per_step(const gabe_handle *h) { return h ? (h->p.gws_on ? 3 : 2) : 0; }
+int gabe_launches_per_step(const gabe_handle *h) {
+    return h ? (h->p.gws_on ? (h->plane_fft ? 4 : 3) : 2) : 0;
+}
 
 }  // extern "C"

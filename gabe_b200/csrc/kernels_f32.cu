@@ -1,8 +1,45 @@
 // FP32-storage kernels; built with FMA contraction.
 #include "convert.cuh"
 #include "launch.h"
+#include "sweep32.cuh"
 
 namespace gabe {
+
+constexpr int kRingSlots = 6;
+
+template <int TK2, int TJ, int MODE>
+static cudaError_t launch32(const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    auto k = s32::sweep32_kernel<TK2, TJ, MODE, kRingSlots>;
+    const size_t smem = (size_t)kRingSlots * s32::Ring<TK2, TJ>::SLOT * sizeof(float);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k<<<grid, TK2 * TJ, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int TK2, int TJ>
+static cudaError_t sweep32_shape(int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    switch (mode) {
+        case MODE_A: return launch32<TK2, TJ, MODE_A>(a, grid, s);
+        case MODE_A_GW: return launch32<TK2, TJ, MODE_A_GW>(a, grid, s);
+        case MODE_E0: return launch32<TK2, TJ, MODE_E0>(a, grid, s);
+        default: return launch32<TK2, TJ, MODE_B>(a, grid, s);
+    }
+}
+
+// shape ids follow kShapes32 (launch.h); TK2 = TK / 2 threads along k
+cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    switch (shape) {
+        case 0: return sweep32_shape<32, 8>(mode, a, grid, s);
+        case 1: return sweep32_shape<32, 4>(mode, a, grid, s);
+        case 2: return sweep32_shape<64, 4>(mode, a, grid, s);
+        case 3: return sweep32_shape<16, 8>(mode, a, grid, s);
+        case 4: return sweep32_shape<32, 16>(mode, a, grid, s);
+        case 5: return sweep32_shape<16, 4>(mode, a, grid, s);
+        case 6: return sweep32_shape<8, 8>(mode, a, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
 
 template <int TK, int TJ>
 static cudaError_t sweep_shape(int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {

@@ -84,8 +84,30 @@ inline GridPlan plan_grid(int N, int want_shape, int want_ci) {
     return GridPlan{shape, ci, dim3(N / TK, N / TJ, (N + ci - 1) / ci)};
 }
 
+// FP32 sweeps (sweep32.cuh): tile shapes (TK x TJ), two sites per thread along k.
+constexpr int kNumShapes32 = 7;
+constexpr int kShapes32[kNumShapes32][2] = {{64, 8}, {64, 4}, {128, 4}, {32, 8}, {64, 16}, {32, 4}, {16, 8}};
+
+inline GridPlan plan_grid32(int N, int want_shape, int want_ci) {
+    auto fits = [N](int s) {
+        const int tk = kShapes32[s][0], tj = kShapes32[s][1];
+        return tk <= N && tj <= N && N % tk == 0 && N % tj == 0;
+    };
+    int shape = (want_shape >= 0 && want_shape < kNumShapes32 && fits(want_shape)) ? want_shape : -1;
+    for (int q = 0; shape < 0 && q < kNumShapes32; q++)
+        if (fits(q)) shape = q;
+    const int TK = kShapes32[shape][0], TJ = kShapes32[shape][1];
+    const int bxy = (N / TK) * (N / TJ);
+    int ci = want_ci > 0 ? want_ci : N;
+    if (want_ci <= 0)
+        while (ci > 4 && (long long)bxy * ((N + ci - 1) / ci) < 4 * 148) ci /= 2;
+    if (ci > N) ci = N;
+    return GridPlan{shape, ci, dim3(N / TK, N / TJ, (N + ci - 1) / ci)};
+}
+
 cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
+cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l);
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);
 cudaError_t bins_f64(const BinArgs &a, const Launch &l);
@@ -102,6 +124,11 @@ cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *
                      cudaStream_t s);
 cudaError_t to_fluct(const double *x, size_t n, const double *mean, float *out, cudaStream_t s);
 cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out, cudaStream_t s);
+
+// FP32 2-D r2c over the (j, k) planes of the source array (planefft.cuh).
+bool plane_r2c_supported(int N);
+cudaError_t plane_r2c_setup(int N, int *grid);
+cudaError_t plane_r2c_f32(int N, float *S, int nplanes, int grid, cudaStream_t s);
 
 cudaError_t bin_reduce(const double *part_sum, const unsigned int *part_cnt, int nblocks, int nseries, int nbins,
                        double *sum, double *cnt, cudaStream_t s);

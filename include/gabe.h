@@ -65,9 +65,12 @@ enum gabe_model {
 
 enum gabe_flags {
     GABE_FLAG_NO_GRAPH = 1,  /* launch kernels one by one instead of replaying a CUDA graph */
-    GABE_FLAG_NO_OVERLAP = 2 /* one source buffer: the GW transforms and k-space update run in line
-                                instead of overlapping the next field sweeps (saves 10 N^2(N+2)
-                                words of device memory) */
+    GABE_FLAG_NO_OVERLAP = 2, /* one source buffer: the GW transforms and k-space update run in line
+                                 instead of overlapping the next field sweeps (saves 10 N^2(N+2)
+                                 words of device memory) */
+    GABE_FLAG_PLANE_FFT = 4   /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
+                                 library's 2-D plane kernel (one thread-block cluster per (j, k) plane)
+                                 and a 1-D cuFFT pass along i instead of cuFFT's 3-D r2c plan */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two

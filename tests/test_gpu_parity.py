@@ -225,13 +225,15 @@ def test_runs_are_deterministic():
     assert out[0][1] == out[1][1]
 
 
-@pytest.mark.parametrize("gws", [0, 1])
-def test_fp32_against_fp64(gws):
-    """FP32 storage of fluctuations vs the FP64 path: energies <= 1e-4."""
-    N, steps = 32, 200
+@pytest.mark.parametrize("N,gws,flags", [(32, 0, 0), (32, 1, 0), (64, 1, 0), (64, 1, gb.FLAG_PLANE_FFT)])
+def test_fp32_against_fp64(N, gws, flags):
+    """FP32 storage of fluctuations vs the FP64 path: energies <= 1e-4.  With
+    GABE_FLAG_PLANE_FFT the FP32 GW sources go through the library's plane
+    transforms, otherwise through cuFFT's 3-D plan."""
+    steps = 200
     cfg = po.Config(N=N, model=po.MODEL_LPHI4, gws=gws)
     st = po.init_state(cfg)
-    with _lattice(cfg, precision=gb.FP64) as l64, _lattice(cfg, precision=gb.FP32) as l32:
+    with _lattice(cfg, precision=gb.FP64) as l64, _lattice(cfg, precision=gb.FP32, flags=flags) as l32:
         _upload(l64, st)
         _upload(l32, st)
         e64, e32 = l64.calc_energy(), l32.calc_energy()
