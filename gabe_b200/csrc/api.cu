@@ -42,6 +42,7 @@ struct gabe_handle {
     void *S2 = nullptr; // second source buffer: lets the GW chain of step n overlap sweep A of step n+1
     size_t S_bytes = 0;
     cudaStream_t gw_stream = nullptr;
+    int prio_low = 0;  // priority of gw_stream (the handle's stream has the highest)
     cudaEvent_t ev_a = nullptr, ev_k[2] = {nullptr, nullptr};
     int nslots = 0;
     double *partials = nullptr;
@@ -53,7 +54,9 @@ struct gabe_handle {
     int nbins = 0;
     cufftHandle plan_src = 0, plan_spec = 0;
     bool have_plan_src = false, have_plan_spec = false;
-    // FP32 sources: 2-D plane kernels (planefft.cuh) + a 1-D cuFFT pass along i
+    // FP32 sources: 2-D (j, k) transforms (cuFFT 2-D plan, or the plane kernel
+    // of planefft.cuh) and the k-space update with the pass along i fused in
+    bool ks_fused = false;
     bool plane_fft = false;
     int plane_grid = 0;
     void *fft_work = nullptr;
@@ -121,15 +124,18 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    h->plane_fft = h->p.gws_on && h->f32 && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
+    h->ks_fused = h->p.gws_on && h->f32 && kspace_fused_supported(h->N) && (h->p.flags & GABE_FLAG_FUSED_KSPACE);
+    h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
     if (h->plane_fft) {
         CK(h, plane_r2c_setup(h->N, &h->plane_grid));
-        // remaining pass along i: N*nz sequences of stride N*nz per source component
-        long long n1[1] = {N}, em[1] = {N};
+    } else if (h->ks_fused) {
+        // 2-D r2c of every (source, i) plane: N x (N+2) reals in, N x nz complex out, in place
+        long long n2[2] = {N, N}, inem[2] = {N, 2 * nz}, onem[2] = {N, nz};
         CF(h, cufftCreate(&h->plan_src));
         h->have_plan_src = true;
         CF(h, cufftSetAutoAllocation(h->plan_src, 0));
-        CF(h, cufftMakePlanMany64(h->plan_src, 1, n1, em, N * nz, 1, em, N * nz, 1, CUFFT_C2C, N * nz, &ws_src));
+        CF(h, cufftMakePlanMany64(h->plan_src, 2, n2, inem, 1, N * 2 * nz, onem, 1, N * nz, CUFFT_R2C,
+                                  2 * kSrc * N, &ws_src));
     } else if (h->p.gws_on) {
         long long inem[3] = {N, N, 2 * nz}, onem[3] = {N, N, nz};
         CF(h, cufftCreate(&h->plan_src));
@@ -166,17 +172,34 @@ int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
 bool overlapped(const gabe_handle *h) { return h->p.gws_on && h->S2 != nullptr; }
 void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
 
-// In-place 3-D r2c of the 2*kSrc source arrays in source buffer `slot`
-// (fft_stresstensor's transforms, g2evolutionpert.cpp:190-195).
+// In-place transforms of the 2*kSrc source arrays in source buffer `slot`
+// (fft_stresstensor's transforms, g2evolutionpert.cpp:190-195): the full 3-D
+// r2c, or -- with the fused k-space update, which does the pass along i --
+// the 2-D r2c of every (j, k) plane.
 int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
     void *S = source_buffer(h, slot);
-    CF(h, cufftSetStream(h->plan_src, s));
-    if (!h->plane_fft) return fft_r2c(h, h->plan_src, S, S);
-    CK(h, plane_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc * h->N, h->plane_grid, s));
-    for (int q = 0; q < 2 * kSrc; q++) {
-        cufftComplex *c = static_cast<cufftComplex *>(S) + (size_t)q * h->M;
-        CF(h, cufftExecC2C(h->plan_src, c, c, CUFFT_FORWARD));
+    if (h->plane_fft) {
+        CK(h, plane_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc * h->N, h->plane_grid, s));
+        return GABE_OK;
     }
+    CF(h, cufftSetStream(h->plan_src, s));
+    return fft_r2c(h, h->plan_src, S, S);
+}
+
+// TT projection and both RK2 stages of h, l (kspace.cuh / kspace_fused.cuh).
+int kspace(gabe_handle *h, int slot, cudaStream_t s) {
+    KspaceArgs k{};
+    k.S = source_buffer(h, slot);
+    k.G = h->G;
+    k.sc = h->sc;
+    k.c = h->lc;
+    k.slot = slot;
+    if (h->ks_fused) {
+        CK(h, kspace_fused_f32(h->N, k, s));
+        return GABE_OK;
+    }
+    Launch lk{dim3(148 * 8), dim3(256), 0, s};
+    CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
     return GABE_OK;
 }
 
@@ -204,18 +227,9 @@ int sweep(gabe_handle *h, int mode, int cur, int counter, int slot = 0) {
 }
 
 int gw_chain(gabe_handle *h, int slot, cudaStream_t s) {
-    void *S = source_buffer(h, slot);
     int rc = source_fft(h, slot, s);
     if (rc) return rc;
-    KspaceArgs k{};
-    k.S = S;
-    k.G = h->G;
-    k.sc = h->sc;
-    k.c = h->lc;
-    k.slot = slot;
-    Launch lk{dim3(148 * 8), dim3(256), 0, s};
-    CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
-    return GABE_OK;
+    return kspace(h, slot, s);
 }
 
 // Enqueues nsteps steps starting from state buffer `cur`.  The field chain
@@ -249,14 +263,8 @@ int enqueue_steps(gabe_handle *h, int cur, int nsteps, bool serial, cudaEvent_t 
                 rc = source_fft(h, slot, h->stream);
                 if (rc) return rc;
                 if (e) CK(h, cudaEventRecord(e[2], h->stream));
-                KspaceArgs k{};
-                k.S = source_buffer(h, slot);
-                k.G = h->G;
-                k.sc = h->sc;
-                k.c = h->lc;
-                k.slot = slot;
-                Launch lk{dim3(148 * 8), dim3(256), 0, h->stream};
-                CK(h, h->f32 ? kspace_f32(k, lk) : kspace_f64(k, lk));
+                rc = kspace(h, slot, h->stream);
+                if (rc) return rc;
             }
         } else if (e) {
             CK(h, cudaEventRecord(e[2], h->stream));
@@ -284,7 +292,8 @@ int capture(gabe_handle *h, int cur, int nsteps, cudaGraphExec_t *out) {
         h->err.clear();
         return 1;
     }
-    e = cudaGraphInstantiate(out, g, 0);
+    // keep the captured per-kernel stream priorities (field chain high, GW chain low)
+    e = cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -462,7 +471,17 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     choose_tile(h);
     h->nbins = gabe_spectra_numbins(p->N);
 
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    // The field chain (sweeps) is on the critical path of every step; the GW
+    // chain (transforms, k-space) of step n may run until sweep A of step n+2.
+    // The field stream gets the highest priority so that its blocks take SMs
+    // as the GW chain's blocks retire instead of queueing behind them.
+    int prio_low = 0, prio_high = 0;
+    if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) {
+        cudaGetLastError();
+        prio_low = prio_high = 0;
+    }
+    h->prio_low = prio_low;
+    if (cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess) {
         cudaGetLastError();
         set_err(h, GABE_ERR_CUDA, "cudaStreamCreate failed");
         return bail(GABE_ERR_CUDA);
@@ -493,7 +512,7 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
             h->err.clear();
         }
     }
-    if (cudaStreamCreateWithFlags(&h->gw_stream, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaStreamCreateWithPriority(&h->gw_stream, cudaStreamNonBlocking, h->prio_low) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_a, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_k[0], cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&h->ev_k[1], cudaEventDisableTiming) != cudaSuccess) {

@@ -1,6 +1,7 @@
 // FP32-storage kernels; built with FMA contraction.
 #include "convert.cuh"
 #include "launch.h"
+#include "kspace_fused.cuh"
 #include "sweep32.cuh"
 
 namespace gabe {
@@ -61,6 +62,33 @@ cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cuda
         case 3: return sweep_shape<16, 8>(mode, a, grid, s);
         case 4: return sweep_shape<8, 8>(mode, a, grid, s);
         case 5: return sweep_shape<4, 4>(mode, a, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int N>
+static cudaError_t kspace_fused_n(const KspaceArgs &a, cudaStream_t s) {
+    using G = ksf::KsGeom<N>;
+    auto k = ksf::kspace_fused_kernel<N>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G::T, G::SMEM_BYTES)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    k<<<nsm * per_sm, G::T, G::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
+
+bool kspace_fused_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
+
+cudaError_t kspace_fused_f32(int N, const KspaceArgs &a, cudaStream_t s) {
+    switch (N) {
+        case 64: return kspace_fused_n<64>(a, s);
+        case 128: return kspace_fused_n<128>(a, s);
+        case 256: return kspace_fused_n<256>(a, s);
+        case 512: return kspace_fused_n<512>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -125,6 +125,11 @@ cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *
 cudaError_t to_fluct(const double *x, size_t n, const double *mean, float *out, cudaStream_t s);
 cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out, cudaStream_t s);
 
+// FP32 k-space update with the FFT pass along i fused in (kspace_fused.cuh);
+// S holds the 2-D (j, k) transforms of the sources.
+bool kspace_fused_supported(int N);
+cudaError_t kspace_fused_f32(int N, const KspaceArgs &a, cudaStream_t s);
+
 // FP32 2-D r2c over the (j, k) planes of the source array (planefft.cuh).
 bool plane_r2c_supported(int N);
 cudaError_t plane_r2c_setup(int N, int *grid);

@@ -68,9 +68,14 @@ enum gabe_flags {
     GABE_FLAG_NO_OVERLAP = 2, /* one source buffer: the GW transforms and k-space update run in line
                                  instead of overlapping the next field sweeps (saves 10 N^2(N+2)
                                  words of device memory) */
-    GABE_FLAG_PLANE_FFT = 4   /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
-                                 library's 2-D plane kernel (one thread-block cluster per (j, k) plane)
-                                 and a 1-D cuFFT pass along i instead of cuFFT's 3-D r2c plan */
+    GABE_FLAG_FUSED_KSPACE = 8, /* FP32 with N in {64, 128, 256, 512}: transform the GW sources over each
+                                   (j, k) plane only and do the FFT along i inside the k-space update,
+                                   instead of cuFFT's 3-D r2c plan followed by the k-space pass (the
+                                   default, and faster on B200: the fused form reads its columns in
+                                   32-byte pieces) */
+    GABE_FLAG_PLANE_FFT = 4     /* with GABE_FLAG_FUSED_KSPACE: the 2-D (j, k) transforms by the
+                                   library's plane kernel (one thread-block cluster per plane) instead
+                                   of cuFFT's batched 2-D plan */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two

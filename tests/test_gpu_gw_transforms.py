@@ -1,0 +1,95 @@
+"""FP32 GW-source transforms and the fused k-space update against cuFFT's 3-D
+plan with the separate k-space pass.
+
+By default the library keeps the reference's structure: one 3-D r2c per
+source array (fft_stresstensor, g2evolutionpert.cpp:183-195, cuFFT) and a
+separate k-space pass (TT projection + both RK2 stages of h, l).  With FP32
+storage, N in {64, 128, 256, 512} and GABE_FLAG_FUSED_KSPACE it transforms the
+ten GW source arrays over each (j, k) plane only (cuFFT's batched 2-D plan, or
+with GABE_FLAG_PLANE_FFT its own cluster plane kernel) and does the FFT along i
+inside the k-space update.  All forms evolve the same state through the C ABI; h, l and the
+GW spectrum must agree to FP32 transform rounding (the forms order their sums
+differently), the fields bit for bit (they do not depend on the GW chain).
+512^3 runs the 16-CTA cluster configuration of the plane kernel and is
+compared through the spectra only, so that no 512^3 GW state crosses to the
+host.
+"""
+import numpy as np
+import pytest
+
+import gabe_b200 as gb
+
+pytestmark = pytest.mark.gpu
+
+FFT_TOL = 1e-5  # relative, FP32 transforms of ~1e5..1e8 terms
+FORMS = {"fused": gb.FLAG_FUSED_KSPACE, "plane": gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT}
+
+
+def _norm_rel(got, want):
+    return float(np.linalg.norm(got - want) / np.linalg.norm(want))
+
+
+def _state(N, seed=7):
+    from gabe_b200.ic import random_state
+
+    f, d, a0, ad0 = random_state(N, seed=seed, device="cuda")
+    return f.cpu().numpy(), d.cpu().numpy(), a0, ad0
+
+
+def _gw_cols_close(got, want):
+    g, w = got[:, 5:7], want[:, 5:7]
+    floor = 1e-9 * np.abs(w).max(axis=0, keepdims=True)
+    return float(np.max((np.abs(g - w) - floor) / np.abs(w).clip(min=1e-300)))
+
+
+def _run(N, flags, state, steps):
+    f, d, a0, ad0 = state
+    with gb.Lattice(N, gws=True, precision=gb.FP32, flags=flags) as lat:
+        assert lat.launches_per_step == (4 if flags & gb.FLAG_PLANE_FFT else 3)
+        lat.upload_state(f, d, a0=a0, adot0=ad0)
+        lat.step(steps)
+        return lat.download_state(), lat.spec_out()
+
+
+@pytest.mark.parametrize("form", sorted(FORMS))
+@pytest.mark.parametrize("N", [64, 128, 256])
+def test_gw_transform_forms_match_cufft_3d(N, form):
+    st = _state(N)
+    (f0, d0, h0, l0), s0 = _run(N, FORMS[form], st, 3)
+    (f1, d1, h1, l1), s1 = _run(N, 0, st, 3)
+    np.testing.assert_array_equal(f0, f1)
+    np.testing.assert_array_equal(d0, d1)
+    assert np.linalg.norm(l1) > 0
+    assert _norm_rel(h0, h1) <= FFT_TOL
+    assert _norm_rel(l0, l1) <= FFT_TOL
+    # field spectra: same fields; the binning's FP64 shared-memory sums vary in the last bit
+    np.testing.assert_allclose(s0[:, :5], s1[:, :5], rtol=1e-12, atol=0)
+    assert _gw_cols_close(s0, s1) <= FFT_TOL
+
+
+@pytest.mark.parametrize("flags", [gb.FLAG_NO_OVERLAP, gb.FLAG_NO_GRAPH])
+@pytest.mark.parametrize("form", sorted(FORMS))
+def test_gw_transform_launch_forms_agree(form, flags):
+    """Overlapped graph, in-line and direct launches run the same kernels on
+    the same data: bit-identical results."""
+    N = 64
+    st = _state(N, seed=11)
+    a = _run(N, FORMS[form], st, 5)[0]
+    b = _run(N, FORMS[form] | flags, st, 5)[0]
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_gw_transforms_512_match_cufft_3d():
+    N = 512
+    f, d, a0, ad0 = _state(N, seed=3)
+    specs = {}
+    for name, flags in (("fused", FORMS["fused"]), ("plane", FORMS["plane"]), ("3d", 0)):
+        with gb.Lattice(N, gws=True, precision=gb.FP32, flags=flags) as lat:
+            lat.upload_state(f, d, a0=a0, adot0=ad0)
+            lat.step(2)
+            specs[name] = lat.spec_out()
+    assert np.abs(specs["3d"][:, 5]).max() > 0
+    for name in ("fused", "plane"):
+        assert np.all(np.isfinite(specs[name]))
+        assert _gw_cols_close(specs[name], specs["3d"]) <= FFT_TOL, name
