@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-N", type=int, default=256, help="lattice of the CPU reference sample")
     ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--lattice-flags", type=int, default=0,
+                    help="gabe_params.flags of the lattices (e.g. 16: GABE_FLAG_OWN_FFT, 8: GABE_FLAG_FUSED_KSPACE)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--ens-lattices", type=int, default=256)
     ap.add_argument("--ens-steps", type=int, default=200, help="timed ensemble steps (multiple of --ens-every)")
@@ -341,7 +343,7 @@ def main():
     precisions = [("fp32", gb.FP32)] + ([] if args.no_fp64 else [("fp64", gb.FP64)])
     clocks = None
     for name, prec in precisions:
-        lat = gb.Lattice(N, gws=gws, precision=prec, device=local, tile_shape="auto")
+        lat = gb.Lattice(N, gws=gws, precision=prec, device=local, tile_shape="auto", flags=args.lattice_flags)
         stream = torch.cuda.ExternalStream(lat.stream_ptr)
         # ---- device-resident leg
         lat.upload_ptrs(hf.data_ptr(), hd.data_ptr(), None, None, a0, adot0)
@@ -438,7 +440,8 @@ def main():
         "config": {"workload": f"GABE RK2 step, {N}^3 lattice, GWs on, FP32 storage / FP64 scalars",
                    "N": N, "gws": int(gws), "L": 20.0, "dt": 0.01, "model": "lambda phi^4, g^2/lambda=100",
                    "ic": "Gaussian random field with the reference's randInit distribution (torch generator)",
-                   "l2": "inputs larger than L2 (state alone is 2 GiB)"},
+                   "l2": "inputs larger than L2 (state alone is 2 GiB)",
+                   **({"lattice_flags": args.lattice_flags} if args.lattice_flags else {})},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_total": L32["ms_e2e"]},
         "roofline": roofline,

@@ -26,6 +26,7 @@ UNITS = [
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", []),
     ("planefft.cu", []),
+    ("fft3d.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("ensemble.cu", []),
     ("mlp.cu", []),

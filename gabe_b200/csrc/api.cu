@@ -56,6 +56,7 @@ struct gabe_handle {
     bool have_plan_src = false, have_plan_spec = false;
     // FP32 sources: 2-D (j, k) transforms (cuFFT 2-D plan, or the plane kernel
     // of planefft.cuh) and the k-space update with the pass along i fused in
+    bool own_fft = false;   // the library's three-pass 3-D r2c (fft3d.cuh)
     bool ks_fused = false;
     bool plane_fft = false;
     int plane_grid = 0;
@@ -126,8 +127,11 @@ int make_plans(gabe_handle *h) {
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
     h->ks_fused = h->p.gws_on && h->f32 && kspace_fused_supported(h->N) && (h->p.flags & GABE_FLAG_FUSED_KSPACE);
     h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
+    h->own_fft = h->p.gws_on && h->f32 && !h->ks_fused && fft3d_supported(h->N) && (h->p.flags & GABE_FLAG_OWN_FFT);
     if (h->plane_fft) {
         CK(h, plane_r2c_setup(h->N, &h->plane_grid));
+    } else if (h->own_fft) {
+        // no plan: fft3d.cuh
     } else if (h->ks_fused) {
         // 2-D r2c of every (source, i) plane: N x (N+2) reals in, N x nz complex out, in place
         long long n2[2] = {N, N}, inem[2] = {N, 2 * nz}, onem[2] = {N, nz};
@@ -180,6 +184,10 @@ int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
     void *S = source_buffer(h, slot);
     if (h->plane_fft) {
         CK(h, plane_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc * h->N, h->plane_grid, s));
+        return GABE_OK;
+    }
+    if (h->own_fft) {
+        CK(h, fft3d_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc, s));
         return GABE_OK;
     }
     CF(h, cufftSetStream(h->plan_src, s));
@@ -820,7 +828,7 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
 int gabe_launches_per_step(const gabe_handle *h) {
-    return h ? (h->p.gws_on ? (h->plane_fft ? 4 : 3) : 2) : 0;
+    return h ? (h->p.gws_on ? (h->own_fft ? 6 : h->plane_fft ? 4 : 3) : 2) : 0;
 }
 
 }  // extern "C"

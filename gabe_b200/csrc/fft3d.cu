@@ -1,0 +1,59 @@
+// Host side of the FP32 three-pass 3-D r2c (fft3d.cuh): persistent grids
+// sized from the occupancy of each pass.
+#include "fft3d.cuh"
+#include "launch.h"
+
+namespace gabe {
+
+namespace {
+
+template <typename K>
+cudaError_t persistent_grid(K kernel, int threads, size_t smem, int *grid) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int dev = 0, nsm = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem)) != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    *grid = nsm * per_sm;
+    return cudaSuccess;
+}
+
+template <int N>
+cudaError_t fft3d_n(float *S, int ncomp, cudaStream_t s) {
+    constexpr long long nz = N / 2 + 1;
+    int g1 = 0, g2 = 0;
+    cudaError_t e = persistent_grid(f3d::row_r2c_kernel<N>, f3d::kFftThreads, f3d::RowGeom<N>::SMEM_BYTES, &g1);
+    if (e != cudaSuccess) return e;
+    e = persistent_grid(f3d::col_fft_kernel<N>, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, &g2);
+    if (e != cudaSuccess) return e;
+    // pass 1: rows along k
+    f3d::row_r2c_kernel<N><<<g1, f3d::kFftThreads, f3d::RowGeom<N>::SMEM_BYTES, s>>>(S, (long long)ncomp * N * N);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    float2 *X = reinterpret_cast<float2 *>(S);
+    // pass 2: along j within every (component, i) plane
+    f3d::ColArgs aj{X, (long long)N * nz, 0, nz, ncomp * N, 1, (int)nz};
+    f3d::col_fft_kernel<N><<<g2, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(aj);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // pass 3: along i for every (component, j)
+    f3d::ColArgs ai{X, (long long)N * N * nz, nz, (long long)N * nz, ncomp, N, (int)nz};
+    f3d::col_fft_kernel<N><<<g2, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(ai);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool fft3d_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
+
+cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s) {
+    switch (N) {
+        case 64: return fft3d_n<64>(S, ncomp, s);
+        case 128: return fft3d_n<128>(S, ncomp, s);
+        case 256: return fft3d_n<256>(S, ncomp, s);
+        case 512: return fft3d_n<512>(S, ncomp, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace gabe

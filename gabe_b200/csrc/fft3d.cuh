@@ -1,0 +1,251 @@
+// FP32 3-D r2c of the GW source arrays in three streaming passes.
+//
+// The reference transforms each source array with one 3-D r2c FFT
+// (fft_stresstensor, g2evolutionpert.cpp:183-195).  Each 512^3 array is
+// larger than the chip's on-chip storage, so the transform is three passes
+// over HBM, one per axis.  Each pass here is a persistent batched 1-D FFT
+// whose global accesses are whole 128-byte lines:
+//   pass 1 (row_r2c_kernel): rows along k, N reals -> N/2+1 complex, in
+//          place in the N+2 reals of the row.  Two real rows travel as one
+//          complex sequence z = x_a + i x_b (four-step FFT in shared memory)
+//          and are separated with X_a[k] = (Z[k] + conj Z[N-k]) / 2,
+//          X_b[k] = (Z[k] - conj Z[N-k]) / 2i;
+//   pass 2 (col_fft_kernel along j) and pass 3 (along i): complex columns of
+//          stride nz (resp. N nz); a tile is 16 adjacent columns (16 complex
+//          = one 128-byte line per row) of one plane (resp. one row j).
+// The layout is that of a library in-place r2c: S[q][i][j][N+2] reals before,
+// S[q][kx][ky][kz] complex (kz < N/2+1) after.  Forward sign e^{-i},
+// unnormalised (FFTW's convention).
+#pragma once
+
+#include "planefft.cuh"
+#include "sweep32.cuh"
+
+namespace gabe {
+namespace f3d {
+
+using pfft::PlaneCfg;
+
+constexpr int kFftThreads = 512;
+constexpr int kFftBufs = 2;  // tile buffers: copies run one tile ahead (a third buffer measured slower)
+
+// W_N^(n1 k2) for the four-step split N = L1 L2, stored [k2][n1].
+template <int N>
+__device__ __forceinline__ void twiddles(float2 *tw) {
+    constexpr int L1 = PlaneCfg<N>::L1;
+    for (int m = threadIdx.x; m < N; m += blockDim.x) {
+        const int k2 = m / L1, n1 = m % L1;
+        double sn, cs;
+        sincospi(2.0 * (n1 * k2) / N, &sn, &cs);
+        tw[m] = make_float2((float)cs, (float)-sn);
+    }
+}
+
+// Both passes are persistent, one 512-thread CTA per SM, with a ring of
+// kFftBufs tile buffers in shared memory: the copies (cp.async) of the next
+// two tiles are in flight while the current one is transformed, so HBM
+// streams during the FFT arithmetic.
+
+// ---------------------------------------------------------------------------
+// pass 1: r2c along k of every row (nrows rows of N+2 reals)
+// ---------------------------------------------------------------------------
+template <int N>
+struct RowGeom {
+    using C_ = PlaneCfg<N>;
+    static constexpr int L1 = C_::L1, L2 = C_::L2, G = C_::G, PITCH = C_::PITCH;
+    static constexpr int R = N >= 256 ? 32 : 64, P = R / 2, T = kFftThreads;  // rows per tile, pairs
+    static constexpr int BUF = R * PITCH;                                        // floats per tile buffer
+    static constexpr int SMEM_FLOATS = kFftBufs * BUF + 2 * N;
+    static constexpr size_t SMEM_BYTES = (size_t)SMEM_FLOATS * sizeof(float);
+    static constexpr int NT2 = (P * L2 + T - 1) / T;  // pass-2 tasks per thread
+    __device__ static __forceinline__ int pad(int s) { return s + s / G; }
+};
+
+template <int N>
+__global__ void __launch_bounds__(kFftThreads, 1) row_r2c_kernel(float *S, long long nrows) {
+    using Gm = RowGeom<N>;
+    constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2;
+    constexpr int RP = N + 2, NH = N / 2 + 1;
+    extern __shared__ __align__(16) float smem[];
+    float2 *tw = reinterpret_cast<float2 *>(smem + kFftBufs * Gm::BUF);
+    const int tid = threadIdx.x;
+    twiddles<N>(tw);
+    const long long ntiles = nrows / R;
+    // rows of tile `tile` into buffer `b` (two 4-byte copies per pair of reals:
+    // the padded positions are not 8-byte aligned)
+    auto issue = [&](long long tile, int b) {
+        const float *g = S + tile * R * RP;
+        float *rows = smem + b * Gm::BUF;
+        for (int t = tid; t < R * (N / 2); t += T) {
+            const int jj = t / (N / 2), m = t % (N / 2);
+            float *dst = rows + jj * PITCH + Gm::pad(2 * m);
+            s32::cp_async4(dst, g + jj * RP + 2 * m);
+            s32::cp_async4(dst + 1, g + jj * RP + 2 * m + 1);
+        }
+    };
+#pragma unroll
+    for (int q = 0; q < kFftBufs - 1; q++) {
+        if (blockIdx.x + q * (long long)gridDim.x < ntiles) issue(blockIdx.x + q * (long long)gridDim.x, q);
+        s32::cp_commit();
+    }
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        float *rows = smem + (it % kFftBufs) * Gm::BUF;
+        float *g = S + tile * R * RP;
+        s32::cp_wait<kFftBufs - 2>();
+        __syncthreads();  // this tile landed; the buffer of tile it-1 is consumed
+        const long long ahead = tile + (long long)(kFftBufs - 1) * gridDim.x;
+        if (ahead < ntiles) issue(ahead, (it + kFftBufs - 1) % kFftBufs);
+        s32::cp_commit();
+        for (int t = tid; t < P * L1; t += T) {
+            const int p = t / L1, n1 = t % L1;
+            float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+            float2 x[L2];
+#pragma unroll
+            for (int n2 = 0; n2 < L2; n2++) {
+                const int a = Gm::pad(n1 + L1 * n2);
+                x[n2] = make_float2(re[a], im[a]);
+            }
+            pfft::fft_reg<L2>(x);
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) {
+                const float2 y = k2 ? pfft::cmul(x[k2], tw[k2 * L1 + n1]) : x[k2];
+                const int a = Gm::pad(n1 + L1 * k2);
+                re[a] = y.x;
+                im[a] = y.y;
+            }
+        }
+        __syncthreads();
+        {
+            float2 y[NT2][L1];
+#pragma unroll
+            for (int q = 0; q < NT2; q++) {
+                const int t = q * T + tid, p = t / L2, k2 = t % L2;
+                if (t < P * L2) {
+                    const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+#pragma unroll
+                    for (int n1 = 0; n1 < L1; n1++) {
+                        const int a = Gm::pad(n1 + L1 * k2);
+                        y[q][n1] = make_float2(re[a], im[a]);
+                    }
+                    pfft::fft_reg<L1>(y[q]);
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < NT2; q++) {
+                const int t = q * T + tid, p = t / L2, k2 = t % L2;
+                if (t < P * L2) {
+                    float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+#pragma unroll
+                    for (int k1 = 0; k1 < L1; k1++) {
+                        const int a = Gm::pad(k2 + L2 * k1);
+                        re[a] = y[q][k1].x;
+                        im[a] = y[q][k1].y;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // separate each pair and write N/2+1 complex values per row
+        for (int t = tid; t < P * NH; t += T) {
+            const int p = t / NH, k = t % NH, km = (N - k) & (N - 1);
+            const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+            const float zr = re[Gm::pad(k)], zi = im[Gm::pad(k)], mr = re[Gm::pad(km)], mi = im[Gm::pad(km)];
+            __stcs(reinterpret_cast<float2 *>(g + (2 * p) * RP) + k, make_float2(0.5f * (zr + mr), 0.5f * (zi - mi)));
+            __stcs(reinterpret_cast<float2 *>(g + (2 * p + 1) * RP) + k,
+                   make_float2(0.5f * (zi + mi), 0.5f * (mr - zr)));
+        }
+    }
+    s32::cp_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// passes 2 and 3: forward C2C along a strided axis
+// ---------------------------------------------------------------------------
+// Lines: for b1 < n1, b2 < n2 and column c < ncol the N values at
+// base + b1 s1 + b2 s2 + n sn + c (complex units).
+struct ColArgs {
+    float2 *X;
+    long long s1, s2, sn;
+    int n1, n2, ncol;
+};
+
+template <int N>
+struct ColGeom {
+    static constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2;
+    static constexpr int W = 16, T = kFftThreads;  // columns per tile
+    static constexpr int BUF = N * W;                // complex per tile buffer
+    static constexpr int SMEM_C = kFftBufs * BUF + N;  // tile ring + twiddles (complex)
+    static constexpr size_t SMEM_BYTES = (size_t)SMEM_C * sizeof(float2);
+};
+
+template <int N>
+__global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
+    using Gm = ColGeom<N>;
+    constexpr int L1 = Gm::L1, L2 = Gm::L2, W = Gm::W, T = Gm::T;
+    extern __shared__ __align__(16) float2 cs[];
+    float2 *tw = cs + kFftBufs * Gm::BUF;  // [k2][n1]
+    const int tid = threadIdx.x;
+    twiddles<N>(tw);
+    const int ncb = (a.ncol + W - 1) / W;
+    const long long ntiles = (long long)a.n1 * a.n2 * ncb;
+    auto tile_base = [&](long long tile, int &wn) {
+        const int cb = (int)(tile % ncb);
+        const long long b = tile / ncb;
+        const int b2 = (int)(b % a.n2), b1 = (int)(b / a.n2);
+        wn = min(W, a.ncol - cb * W);  // columns in this tile
+        return a.X + b1 * a.s1 + b2 * a.s2 + cb * W;
+    };
+    auto issue = [&](long long tile, int b) {
+        int wn;
+        const float2 *base = tile_base(tile, wn);
+        float2 *col = cs + b * Gm::BUF;
+        for (int t = tid; t < N * W; t += T) {
+            const int n = t / W, w = t % W;
+            if (w < wn) s32::cp_async8(col + t, base + n * a.sn + w);
+        }
+    };
+#pragma unroll
+    for (int q = 0; q < kFftBufs - 1; q++) {
+        if (blockIdx.x + q * (long long)gridDim.x < ntiles) issue(blockIdx.x + q * (long long)gridDim.x, q);
+        s32::cp_commit();
+    }
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        float2 *col = cs + (it % kFftBufs) * Gm::BUF;
+        int wn;
+        float2 *base = tile_base(tile, wn);
+        s32::cp_wait<kFftBufs - 2>();
+        __syncthreads();  // this tile landed; the buffer of tile it-1 is consumed
+        const long long ahead = tile + (long long)(kFftBufs - 1) * gridDim.x;
+        if (ahead < ntiles) issue(ahead, (it + kFftBufs - 1) % kFftBufs);
+        s32::cp_commit();
+        // four-step pass 1: L2-point FFTs over n2, twiddle, in place
+        for (int t = tid; t < W * L1; t += T) {
+            const int w = t % W, n1 = t / W;
+            float2 x[L2];
+#pragma unroll
+            for (int n2 = 0; n2 < L2; n2++) x[n2] = col[(n1 + L1 * n2) * W + w];
+            pfft::fft_reg<L2>(x);
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) col[(n1 + L1 * k2) * W + w] = k2 ? pfft::cmul(x[k2], tw[k2 * L1 + n1]) : x[k2];
+        }
+        __syncthreads();
+        // pass 2: L1-point FFTs over n1, straight to HBM in natural order
+        for (int t = tid; t < W * L2; t += T) {
+            const int w = t % W, k2 = t / W;
+            float2 y[L1];
+#pragma unroll
+            for (int n1 = 0; n1 < L1; n1++) y[n1] = col[(n1 + L1 * k2) * W + w];
+            pfft::fft_reg<L1>(y);
+            if (w < wn)
+#pragma unroll
+                for (int k1 = 0; k1 < L1; k1++) __stcs(base + (k2 + L2 * k1) * a.sn + w, y[k1]);
+        }
+    }
+    s32::cp_wait<0>();
+}
+
+}  // namespace f3d
+}  // namespace gabe

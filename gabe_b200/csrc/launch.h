@@ -125,6 +125,10 @@ cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *
 cudaError_t to_fluct(const double *x, size_t n, const double *mean, float *out, cudaStream_t s);
 cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out, cudaStream_t s);
 
+// FP32 in-place 3-D r2c of ncomp arrays [N][N][N+2] in three passes (fft3d.cuh).
+bool fft3d_supported(int N);
+cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s);
+
 // FP32 k-space update with the FFT pass along i fused in (kspace_fused.cuh);
 // S holds the 2-D (j, k) transforms of the sources.
 bool kspace_fused_supported(int N);

@@ -70,12 +70,15 @@ enum gabe_flags {
                                  words of device memory) */
     GABE_FLAG_FUSED_KSPACE = 8, /* FP32 with N in {64, 128, 256, 512}: transform the GW sources over each
                                    (j, k) plane only and do the FFT along i inside the k-space update,
-                                   instead of cuFFT's 3-D r2c plan followed by the k-space pass (the
+                                   instead of a full 3-D transform followed by the k-space pass (the
                                    default, and faster on B200: the fused form reads its columns in
                                    32-byte pieces) */
-    GABE_FLAG_PLANE_FFT = 4     /* with GABE_FLAG_FUSED_KSPACE: the 2-D (j, k) transforms by the
+    GABE_FLAG_PLANE_FFT = 4,    /* with GABE_FLAG_FUSED_KSPACE: the 2-D (j, k) transforms by the
                                    library's plane kernel (one thread-block cluster per plane) instead
                                    of cuFFT's batched 2-D plan */
+    GABE_FLAG_OWN_FFT = 16      /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
+                                   library's three-pass 3-D r2c instead of cuFFT's 3-D plan (no cuFFT
+                                   call on the step path; about 7% slower than cuFFT at 512^3 on B200) */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two

@@ -1,13 +1,15 @@
 """FP32 GW-source transforms and the fused k-space update against cuFFT's 3-D
 plan with the separate k-space pass.
 
-By default the library keeps the reference's structure: one 3-D r2c per
-source array (fft_stresstensor, g2evolutionpert.cpp:183-195, cuFFT) and a
-separate k-space pass (TT projection + both RK2 stages of h, l).  With FP32
-storage, N in {64, 128, 256, 512} and GABE_FLAG_FUSED_KSPACE it transforms the
-ten GW source arrays over each (j, k) plane only (cuFFT's batched 2-D plan, or
-with GABE_FLAG_PLANE_FFT its own cluster plane kernel) and does the FFT along i
-inside the k-space update.  All forms evolve the same state through the C ABI; h, l and the
+By default the library keeps the reference's structure -- one 3-D r2c per
+source array (fft_stresstensor, g2evolutionpert.cpp:183-195, here cuFFT's 3-D
+plan) and a separate k-space pass (TT projection + both RK2 stages of h, l);
+that is the reference form of the comparisons below.  With FP32 storage and N
+in {64, 128, 256, 512}: GABE_FLAG_OWN_FFT does the 3-D r2c with the library's
+own three-pass FFT; GABE_FLAG_FUSED_KSPACE transforms the ten source arrays
+over each (j, k) plane only (cuFFT's batched 2-D plan, or with
+GABE_FLAG_PLANE_FFT the library's cluster plane kernel) and does the FFT along
+i inside the k-space update.  All forms evolve the same state through the C ABI; h, l and the
 GW spectrum must agree to FP32 transform rounding (the forms order their sums
 differently), the fields bit for bit (they do not depend on the GW chain).
 512^3 runs the 16-CTA cluster configuration of the plane kernel and is
@@ -22,7 +24,8 @@ import gabe_b200 as gb
 pytestmark = pytest.mark.gpu
 
 FFT_TOL = 1e-5  # relative, FP32 transforms of ~1e5..1e8 terms
-FORMS = {"fused": gb.FLAG_FUSED_KSPACE, "plane": gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT}
+FORMS = {"own": gb.FLAG_OWN_FFT, "fused": gb.FLAG_FUSED_KSPACE, "plane": gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT}
+LAUNCHES = {gb.FLAG_OWN_FFT: 6, gb.FLAG_FUSED_KSPACE: 3, gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT: 4, 0: 3}
 
 
 def _norm_rel(got, want):
@@ -45,7 +48,7 @@ def _gw_cols_close(got, want):
 def _run(N, flags, state, steps):
     f, d, a0, ad0 = state
     with gb.Lattice(N, gws=True, precision=gb.FP32, flags=flags) as lat:
-        assert lat.launches_per_step == (4 if flags & gb.FLAG_PLANE_FFT else 3)
+        assert lat.launches_per_step == LAUNCHES[flags & ~(gb.FLAG_NO_OVERLAP | gb.FLAG_NO_GRAPH)]
         lat.upload_state(f, d, a0=a0, adot0=ad0)
         lat.step(steps)
         return lat.download_state(), lat.spec_out()
@@ -84,12 +87,12 @@ def test_gw_transforms_512_match_cufft_3d():
     N = 512
     f, d, a0, ad0 = _state(N, seed=3)
     specs = {}
-    for name, flags in (("fused", FORMS["fused"]), ("plane", FORMS["plane"]), ("3d", 0)):
+    for name, flags in [*FORMS.items(), ("3d", 0)]:
         with gb.Lattice(N, gws=True, precision=gb.FP32, flags=flags) as lat:
             lat.upload_state(f, d, a0=a0, adot0=ad0)
             lat.step(2)
             specs[name] = lat.spec_out()
     assert np.abs(specs["3d"][:, 5]).max() > 0
-    for name in ("fused", "plane"):
+    for name in FORMS:
         assert np.all(np.isfinite(specs[name]))
         assert _gw_cols_close(specs[name], specs["3d"]) <= FFT_TOL, name

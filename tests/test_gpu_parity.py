@@ -225,12 +225,14 @@ def test_runs_are_deterministic():
     assert out[0][1] == out[1][1]
 
 
-@pytest.mark.parametrize("N,gws,flags", [(32, 0, 0), (32, 1, 0), (64, 1, 0), (64, 1, gb.FLAG_FUSED_KSPACE),
+@pytest.mark.parametrize("N,gws,flags", [(32, 0, 0), (32, 1, 0), (64, 1, 0), (64, 1, gb.FLAG_OWN_FFT),
+                                         (64, 1, gb.FLAG_FUSED_KSPACE),
                                          (64, 1, gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT)])
 def test_fp32_against_fp64(N, gws, flags):
     """FP32 storage of fluctuations vs the FP64 path: energies <= 1e-4.  The
-    FP32 GW sources go through cuFFT's 3-D plan and the separate k-space pass,
-    or (GABE_FLAG_FUSED_KSPACE) through 2-D plane transforms -- cuFFT's, or the
+    FP32 GW sources go through cuFFT's 3-D plan, or the library's three-pass
+    3-D FFT (GABE_FLAG_OWN_FFT), and the separate k-space pass, or
+    (GABE_FLAG_FUSED_KSPACE) through 2-D plane transforms -- cuFFT's, or the
     library's with GABE_FLAG_PLANE_FFT -- and the k-space update with the FFT
     along i fused in."""
     steps = 200
