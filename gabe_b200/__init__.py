@@ -129,9 +129,11 @@ class Lattice:
 
     def __init__(self, N: int, *, L: float = 20.0, dt: float = 0.01, gws: bool = False,
                  model: int = MODEL_LPHI4, model_c=None, precision: int = FP64, device: int = -1,
-                 gw_spec_quirk: bool = True, flags: int = 0, tile_ci: int = 0, tile_shape=-1):
+                 gw_spec_quirk: bool = True, flags: int = 0, tile_ci: int = 0, tile_shape=-1, expansion: int = 1):
         """tile_shape="auto" takes the tile the autotuner cached for this GPU,
-        N, precision and GW setting (gabe_b200.autotune), if any."""
+        N, precision and GW setting (gabe_b200.autotune), if any.  expansion
+        is the reference's expansion_type (g2parameters.h:62): 1 self-consistent
+        Friedmann expansion, 0 none, 2 type 1 without tensor-mode evolution."""
         lib = library()
         if tile_shape == "auto":
             from .autotune import lookup
@@ -146,6 +148,7 @@ class Lattice:
         p.model_c[0], p.model_c[1] = float(model_c[0]), float(model_c[1])
         p.device, p.gw_spec_quirk, p.flags = int(device), int(bool(gw_spec_quirk)), int(flags)
         p.tile_ci, p.tile_shape = int(tile_ci), int(tile_shape)
+        p.expansion = int(expansion)
         self.params = p
         self.N, self.gws, self.precision = int(N), bool(gws), int(precision)
         self.nz = self.N // 2 + 1

@@ -56,6 +56,7 @@ struct gabe_handle {
     bool have_plan_src = false, have_plan_spec = false;
     // FP32 sources: 2-D (j, k) transforms (cuFFT 2-D plan, or the plane kernel
     // of planefft.cuh) and the k-space update with the pass along i fused in
+    bool evolve_gw = false; // calc_gws with expansion_type 1: the step evolves h, l (types 0 and 2 do not)
     bool own_fft = false;   // the library's three-pass 3-D r2c (fft3d.cuh)
     bool ks_fused = false;
     bool plane_fft = false;
@@ -125,9 +126,9 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    h->ks_fused = h->p.gws_on && h->f32 && kspace_fused_supported(h->N) && (h->p.flags & GABE_FLAG_FUSED_KSPACE);
+    h->ks_fused = h->evolve_gw && h->f32 && kspace_fused_supported(h->N) && (h->p.flags & GABE_FLAG_FUSED_KSPACE);
     h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
-    h->own_fft = h->p.gws_on && h->f32 && !h->ks_fused && fft3d_supported(h->N) && (h->p.flags & GABE_FLAG_OWN_FFT);
+    h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && fft3d_supported(h->N) && (h->p.flags & GABE_FLAG_OWN_FFT);
     if (h->plane_fft) {
         CK(h, plane_r2c_setup(h->N, &h->plane_grid));
     } else if (h->own_fft) {
@@ -140,7 +141,7 @@ int make_plans(gabe_handle *h) {
         CF(h, cufftSetAutoAllocation(h->plan_src, 0));
         CF(h, cufftMakePlanMany64(h->plan_src, 2, n2, inem, 1, N * 2 * nz, onem, 1, N * nz, CUFFT_R2C,
                                   2 * kSrc * N, &ws_src));
-    } else if (h->p.gws_on) {
+    } else if (h->evolve_gw) {
         long long inem[3] = {N, N, 2 * nz}, onem[3] = {N, N, nz};
         CF(h, cufftCreate(&h->plan_src));
         h->have_plan_src = true;
@@ -173,7 +174,7 @@ int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
     return GABE_OK;
 }
 
-bool overlapped(const gabe_handle *h) { return h->p.gws_on && h->S2 != nullptr; }
+bool overlapped(const gabe_handle *h) { return h->evolve_gw && h->S2 != nullptr; }
 void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
 
 // In-place transforms of the 2*kSrc source arrays in source buffer `slot`
@@ -257,10 +258,10 @@ int enqueue_steps(gabe_handle *h, int cur, int nsteps, bool serial, cudaEvent_t 
         cudaEvent_t *e = ev ? ev + 5 * s : nullptr;
         if (fork && s >= 2) CK(h, cudaStreamWaitEvent(h->stream, h->ev_k[slot], 0));
         if (e) CK(h, cudaEventRecord(e[0], h->stream));
-        int rc = sweep(h, h->p.gws_on ? MODE_A_GW : MODE_A, c, 0, slot);
+        int rc = sweep(h, h->evolve_gw ? MODE_A_GW : MODE_A, c, 0, slot);
         if (rc) return rc;
         if (e) CK(h, cudaEventRecord(e[1], h->stream));
-        if (h->p.gws_on) {
+        if (h->evolve_gw) {
             if (fork) {
                 CK(h, cudaEventRecord(h->ev_a, h->stream));
                 CK(h, cudaStreamWaitEvent(h->gw_stream, h->ev_a, 0));
@@ -435,8 +436,8 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     if (p->N < 4 || p->N > 1290 || (p->N & 1))
         return set_err(nullptr, GABE_ERR_PARAM, "N must be even and in [4, 1290], got %d", p->N);
     if (p->nflds != 2) return set_err(nullptr, GABE_ERR_PARAM, "nflds must be 2, got %d", p->nflds);
-    if (p->expansion != 1)
-        return set_err(nullptr, GABE_ERR_PARAM, "only expansion_type 1 is implemented, got %d", p->expansion);
+    if (p->expansion < 0 || p->expansion > 2)
+        return set_err(nullptr, GABE_ERR_PARAM, "expansion_type must be 0, 1 or 2, got %d", p->expansion);
     if (p->gws_on != 0 && p->gws_on != 1) return set_err(nullptr, GABE_ERR_PARAM, "calc_gws must be 0 or 1");
     if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4)
         return set_err(nullptr, GABE_ERR_PARAM, "unknown model %d", p->model);
@@ -510,10 +511,11 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
         if ((rc = dalloc(h, (void **)&h->gwnorm, 4 * sizeof(double)))) return bail(rc);
     }
     // sources need 10 padded slots; spectra need 2; uploads stage one FP64 field array
-    h->nslots = p->gws_on ? 2 * kSrc : 2;
+    h->evolve_gw = p->gws_on && p->expansion == 1;
+    h->nslots = h->evolve_gw ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
-    if (p->gws_on && !(p->flags & GABE_FLAG_NO_OVERLAP)) {
+    if (h->evolve_gw && !(p->flags & GABE_FLAG_NO_OVERLAP)) {
         // optional: without it the GW chain simply runs in line
         if (dalloc(h, &h->S2, h->S_bytes) != GABE_OK) {
             h->S2 = nullptr;
@@ -583,6 +585,10 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
     DevScalars s{};
     s.a[0] = a0;
     s.adot[0] = adot0;
+    if (h->p.expansion == 0) {  // both stages keep the initial expansion (g2init.cpp:18-24)
+        s.a[1] = a0;
+        s.adot[1] = adot0;
+    }
     s.adot_given = 1;
     CK(h, cudaMemcpyAsync(h->sc, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
     const size_t nf = h->n3;
@@ -828,7 +834,7 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
 int gabe_launches_per_step(const gabe_handle *h) {
-    return h ? (h->p.gws_on ? (h->own_fft ? 6 : h->plane_fft ? 4 : 3) : 2) : 0;
+    return h ? (h->evolve_gw ? (h->own_fft ? 6 : h->plane_fft ? 4 : 3) : 2) : 0;
 }
 
 }  // extern "C"

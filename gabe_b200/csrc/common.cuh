@@ -46,6 +46,7 @@ enum Model : int { MODEL_QUADRATIC = 0, MODEL_LPHI4 = 1 };
 struct LatticeConsts {
     int N;
     int model;
+    int expansion;          // expansion_type: 0 none, 1 Friedmann, 2 Friedmann without tensor modes
     double dt, half_dt;     // dt, .5*dt
     double inv_dx2_div;     // dx*dx (the reference divides by it)
     double dn, c13, c23;    // 1/(dx*dx), (1./3.)*dn, (2./3.)*dn  (g2evolutionpert.cpp:53-116)

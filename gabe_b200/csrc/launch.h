@@ -32,6 +32,7 @@ inline LatticeConsts make_lattice_consts(const gabe_params &p) {
     LatticeConsts c{};
     c.N = p.N;
     c.model = p.model;
+    c.expansion = p.expansion;
     const double L = p.L, dt = p.dt;
     const double dx = L / ((double)p.N);
     c.dt = dt;

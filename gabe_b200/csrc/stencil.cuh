@@ -229,9 +229,12 @@ __device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, 
     s->edpot[0] = ep0;
     s->edgrad[0] = eg0;
     s->edrho[0] = rho0;
-    if (!s->adot_given) s->adot[0] = sqrt(c.eight_pi_3 * rho0) * a0; /* adf(0), g2functions.cpp:270 */
+    // adf(0), g2functions.cpp:270; without expansion (type 0, :207-232) a and
+    // adot keep their initial values and only calcEnergy(0) is taken (:231)
+    if (!s->adot_given && c.expansion != 0) s->adot[0] = sqrt(c.eight_pi_3 * rho0) * a0;
     if (!isfinite(rho0)) s->status |= ST_NONFINITE;
     if constexpr (MODE == MODE_E0) return;
+    if (c.expansion == 0) return;
     const double ad0 = s->adot[0];
     const double a1 = a0 + c.half_dt * ad0; /* :250 */
     const double ek1 = (tot[5] + 2. * ad0 * tot[6] + ad0 * ad0 * tot[7]) / c.gridsize / 2.;
@@ -444,7 +447,7 @@ __device__ __forceinline__ void finish_b(const LatticeConsts &c, DevScalars *s) 
             s->dfbar[f] = dfbn;
         }
     }
-    s->a[0] = a0 + dt * ad1; /* g2functions.cpp:268 */
+    if (c.expansion != 0) s->a[0] = a0 + dt * ad1; /* g2functions.cpp:268 (type 2: :299) */
     s->adot_given = 0;
     s->step += 1;
 }

@@ -90,7 +90,9 @@ typedef struct {
     int32_t N;              /* points per side (g2parameters.h:57) */
     int32_t nflds;          /* must be 2 (g2parameters.h:43) */
     int32_t gws_on;         /* calc_gws: 0/1 (g2parameters.h:55) */
-    int32_t expansion;      /* expansion_type: must be 1 (g2parameters.h:62) */
+    int32_t expansion;      /* expansion_type (g2parameters.h:62): 1 Friedmann expansion with tensor modes
+                               (g2functions.cpp:234-271), 0 none (a, adot fixed, :207-232), 2 type 1
+                               without tensor modes (:272-302) */
     int32_t model;          /* enum gabe_model */
     int32_t precision;      /* enum gabe_precision */
     int32_t gw_spec_quirk;  /* 1: GW spectrum reads l at kz=N/2 for the kz=0 plane, as g2spectra.cpp:149-164 does */

@@ -203,10 +203,18 @@ void ora_init(const ora_params *p, int seed, const double f0[2], const double df
             field[fld * n3 + x] = f0[fld];
             dfield[fld * n3 + x] = df0[fld];
         }
-    /* initexpansion (g2init.cpp:26-29) */
-    sc->a[0] = 1;
-    set_energy(p, field, dfield, sc, 0);
-    sc->adot[0] = ora_adf(sc->edrho[0], sc->a[0]);
+    /* initexpansion (g2init.cpp:16-43) */
+    if (p->expansion == 0) {
+        sc->a[0] = 1;
+        sc->adot[0] = 0;
+        sc->a[1] = 1;
+        sc->adot[1] = 0;
+        set_energy(p, field, dfield, sc, 0);
+    } else {
+        sc->a[0] = 1;
+        set_energy(p, field, dfield, sc, 0);
+        sc->adot[0] = ora_adf(sc->edrho[0], sc->a[0]);
+    }
     /* initfields, second call: fluctuations (g2model.cpp:132-140) */
     int nz = N / 2 + 1;
     size_t nc = (size_t)N * N * nz;
@@ -409,11 +417,14 @@ void ora_step(const ora_params *p, double *field, double *dfield, double *h, dou
                     f1[fld * n3 + x] = f0[fld * n3 + x] + .5 * dt * d0[fld * n3 + x];
                     d1[fld * n3 + x] = d0[fld * n3 + x] + .5 * dt * dd;
                 }
-    if (p->gws) evolve_perts(p, 0, 1, 0.5 * dt, field, h, l, T_gw, sc); /* :247 */
-    /* :250-252 */
-    sc->a[1] = sc->a[0] + .5 * dt * sc->adot[0];
-    set_energy(p, f1, d1, sc, 1);
-    sc->adot[1] = ora_adf(sc->edrho[1], sc->a[1]);
+    const int ex = p->expansion, gw = p->gws && ex == 1;
+    if (gw) evolve_perts(p, 0, 1, 0.5 * dt, field, h, l, T_gw, sc); /* :247 */
+    if (ex != 0) {
+        /* :250-252 (type 2: :286-288) */
+        sc->a[1] = sc->a[0] + .5 * dt * sc->adot[0];
+        set_energy(p, f1, d1, sc, 1);
+        sc->adot[1] = ora_adf(sc->edrho[1], sc->a[1]);
+    }
     /* stage 2 (g2functions.cpp:254-262) */
     for (int fld = 0; fld < F; fld++)
         for (int i = 0; i < N; i++)
@@ -427,11 +438,15 @@ void ora_step(const ora_params *p, double *field, double *dfield, double *h, dou
                     f0[fld * n3 + x] = f0[fld * n3 + x] + dt * d1[fld * n3 + x];
                     d0[fld * n3 + x] = d0[fld * n3 + x] + dt * dd;
                 }
-    if (p->gws) evolve_perts(p, 1, 0, dt, field, h, l, T_gw, sc); /* :265 */
-    /* :268-270 */
-    sc->a[0] = sc->a[0] + dt * sc->adot[1];
-    set_energy(p, f0, d0, sc, 0);
-    sc->adot[0] = ora_adf(sc->edrho[0], sc->a[0]);
+    if (gw) evolve_perts(p, 1, 0, dt, field, h, l, T_gw, sc); /* :265 */
+    if (ex != 0) {
+        /* :268-270 (type 2: :299-301) */
+        sc->a[0] = sc->a[0] + dt * sc->adot[1];
+        set_energy(p, f0, d0, sc, 0);
+        sc->adot[0] = ora_adf(sc->edrho[0], sc->a[0]);
+    } else {
+        set_energy(p, f0, d0, sc, 0); /* :231 */
+    }
     if (own_T) free(T_gw);
 }
 

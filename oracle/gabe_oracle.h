@@ -29,7 +29,7 @@ typedef struct {
     int model;        /* ORA_MODEL_* */
     int gws;          /* 0/1 */
     int gw_spec_quirk;/* 1: read l at kz=N/2 for the kz=0 plane as g2spectra.cpp:149-164 does */
-    int pad;
+    int expansion;    /* expansion_type 0, 1 or 2 (g2parameters.h:62); callers set it */
     /* model constants, see ora_model_constants() */
     double mc[6];
 } ora_params;
@@ -55,13 +55,17 @@ double ora_adf(double edrho_s, double a_s);
 /* The reference initialisation sequence initfields(); initexpansion();
  * initfields() (g2main.cpp:111-118, g2model.cpp:113-144, g2init.cpp:16-189)
  * with srand(seed) and rand() in single-thread order.  Writes stage 0 of
- * field/dfield and the stage-0 scalars. */
+ * field/dfield and the scalars.  expansion_type 0 starts from a = 1,
+ * adot = 0 in both stages (g2init.cpp:18-24); expansion_type 2 leaves the
+ * start to the user (g2init.cpp:32-41) and is started here as type 1. */
 void ora_init(const ora_params *p, int seed, const double f0[2], const double df0[2],
               double rescale_B, double *field, double *dfield, ora_scalars *sc);
 
-/* One step() for expansion_type 1 (g2functions.cpp:234-271), including
- * evolve_perts (g2evolutionpert.cpp:343-455) when p->gws.  T_gw may be NULL
- * (then allocated internally). */
+/* One step() (g2functions.cpp:201-304): expansion_type 1 (:234-271)
+ * including evolve_perts (g2evolutionpert.cpp:343-455) when p->gws;
+ * expansion_type 0 (:207-232: a and adot fixed, no tensor modes, only
+ * calcEnergy(0) at the end); expansion_type 2 (:272-302: type 1's update
+ * without the tensor modes).  T_gw may be NULL (then allocated internally). */
 void ora_step(const ora_params *p, double *field, double *dfield, double *h, double *l,
               double *T_gw, ora_scalars *sc);
 

@@ -33,7 +33,7 @@ class _Params(ctypes.Structure):
         ("N", ctypes.c_int), ("nflds", ctypes.c_int),
         ("L", ctypes.c_double), ("dt", ctypes.c_double),
         ("model", ctypes.c_int), ("gws", ctypes.c_int),
-        ("gw_spec_quirk", ctypes.c_int), ("pad", ctypes.c_int),
+        ("gw_spec_quirk", ctypes.c_int), ("expansion", ctypes.c_int),
         ("mc", ctypes.c_double * 6),
     ]
 
@@ -103,11 +103,13 @@ class Config:
     model: int = MODEL_LPHI4
     gws: int = 0
     gw_spec_quirk: int = 1
+    expansion: int = 1  # expansion_type (g2parameters.h:62)
 
     def params(self) -> _Params:
         p = _Params()
         p.N, p.nflds, p.L, p.dt = self.N, 2, self.L, self.dt
         p.model, p.gws, p.gw_spec_quirk = self.model, self.gws, self.gw_spec_quirk
+        p.expansion = self.expansion
         c0, c1, *_ = model_constants(self.model)
         lib().ora_model_constants(ctypes.byref(p), c0, c1)
         return p
@@ -260,8 +262,9 @@ def read_dump(path: str, cfg: Config | None = None) -> State:
     return st
 
 
-def ref_binary(model: int, N: int, gws: int, parallel: int) -> str:
-    return os.path.join(REF_DIR, f"ref_m{model}_n{N}_g{gws}_p{parallel}")
+def ref_binary(model: int, N: int, gws: int, parallel: int, expansion: int = 1) -> str:
+    suffix = "" if expansion == 1 else f"_e{expansion}"
+    return os.path.join(REF_DIR, f"ref_m{model}_n{N}_g{gws}_p{parallel}{suffix}")
 
 
 def run_ref(binary: str, args: list[str], cwd: str, threads: int | None = None, timeout: float = 600) -> str:

@@ -100,7 +100,10 @@ const gNum L = GABE_L;
 const gNum starttime = 0.;
 const gNum endtime = GABE_ENDTIME;
 const gNum dt = GABE_DT;
-#define expansion_type 1
+#ifndef GABE_EXPANSION
+#define GABE_EXPANSION 1
+#endif
+#define expansion_type GABE_EXPANSION
 
 #define rand_init 1
 #define field_full_rand 1

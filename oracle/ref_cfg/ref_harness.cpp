@@ -165,6 +165,14 @@ int main(int argc, char **argv)
     } else {
         initfields();
         initexpansion();
+#if expansion_type == 2
+        // expansion_type 2 leaves the initial expansion to the user
+        // (g2init.cpp:32-41 is commented out); this harness starts it as
+        // expansion_type 1 does (g2init.cpp:26-29)
+        a[0] = 1.;
+        calcEnergy(0);
+        adot[0] = adf(0);
+#endif
         initfields();
     }
     double t_init1 = omp_get_wtime();

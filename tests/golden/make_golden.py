@@ -31,12 +31,17 @@ sys.path.insert(0, ROOT)
 from oracle import pyoracle as po  # noqa: E402
 
 CASES = [
-    # (model, N, gws, steps at which to dump, steps at which to write spectra)
+    # (model, N, gws, steps at which to dump, steps at which to write spectra[, expansion_type])
     (1, 16, 1, [0, 1, 2, 5, 10, 50], [0, 10, 50]),
     (0, 32, 1, [0, 1, 10, 50], [0, 50]),
     (1, 32, 0, [0, 1, 10, 100, 200], [0, 200]),
     (1, 64, 0, [0, 1, 10, 100, 200], [0, 200]),
     (1, 64, 1, [0, 1, 10], [0, 10]),
+    # expansion_type 0 (no expansion) and 2 (type 1 without tensor modes; the
+    # harness starts the user-defined expansion as type 1)
+    (1, 32, 0, [0, 1, 10, 100], [0, 100], 0),
+    (1, 32, 1, [0, 1, 10, 50], [0, 50], 0),
+    (1, 32, 1, [0, 1, 10, 50], [0, 50], 2),
 ]
 
 
@@ -59,15 +64,18 @@ def record(st: po.State) -> dict:
 
 def main() -> None:
     golden = {"generator": "tests/golden/make_golden.py", "seed": 44463132, "L": 20.0, "dt": 0.01, "cases": {}}
-    for model, N, gws, dumps, specs in CASES:
-        name = f"m{model}_n{N}_g{gws}"
-        binary = po.ref_binary(model, N, gws, 0)
+    for model, N, gws, dumps, specs, *rest in CASES:
+        expansion = rest[0] if rest else 1
+        name = f"m{model}_n{N}_g{gws}" + ("" if expansion == 1 else f"_e{expansion}")
+        binary = po.ref_binary(model, N, gws, 0, expansion)
         with tempfile.TemporaryDirectory() as d:
             steps = max(dumps + specs)
             po.run_ref(binary, ["--steps", str(steps), "--dump-prefix", "s_", "--dump-at", ",".join(map(str, dumps)),
                                 "--spectra-at", ",".join(map(str, specs))], d)
-            cfg = po.Config(N=N, model=model, gws=gws)
+            cfg = po.Config(N=N, model=model, gws=gws, expansion=expansion)
             entry = {"model": model, "N": N, "gws": gws, "steps": {}, "spectra": {}}
+            if expansion != 1:
+                entry["expansion"] = expansion
             for s in dumps:
                 st = po.read_dump(os.path.join(d, f"s_{s}.bin"), cfg)
                 entry["steps"][str(s)] = record(st)

@@ -47,7 +47,7 @@ def test_params_struct_matches_header():
     assert gb.numbins(256) == 222 and gb.numbins(512) == 444 and gb.numbins(1024) == 887
 
 
-@pytest.mark.parametrize("field,value", [("N", 63), ("N", 2), ("nflds", 3), ("expansion", 0),
+@pytest.mark.parametrize("field,value", [("N", 63), ("N", 2), ("nflds", 3), ("expansion", 3), ("expansion", -1),
                                          ("model", 7), ("precision", 5), ("dt", -1.0), ("gws_on", 2)])
 def test_create_rejects_bad_params(field, value):
     lib = gb.library()

@@ -116,6 +116,40 @@ def test_fp64_matches_oracle(model, N, gws, steps):
                     assert abs(sc[k][s] - want) <= _scalar_tol(k, want, st.sc.edrho[s]), (k, s, sc[k][s], want)
 
 
+@pytest.mark.parametrize("expansion,gws", [(0, 0), (0, 1), (2, 1)])
+def test_expansion_types_match_oracle(expansion, gws):
+    """expansion_type 0 (a, adot fixed, no tensor modes, only calcEnergy(0)
+    per step, g2functions.cpp:207-232) and 2 (type 1 without tensor modes,
+    :272-302): FP64 pointwise against the oracle, which reproduces the
+    reference builds of both types bit for bit (tests/test_oracle_golden.py);
+    FP32 energies against FP64."""
+    N, steps = 32, 100
+    cfg = po.Config(N=N, model=po.MODEL_LPHI4, gws=gws, expansion=expansion)
+    st = po.init_state(cfg)
+    first = st.copy()
+    with _lattice(cfg, expansion=expansion) as lat, _lattice(cfg, precision=gb.FP32, expansion=expansion) as l32:
+        _upload(lat, st)
+        _upload(l32, st)
+        lat.step(steps)
+        l32.step(steps)
+        po.step(st, steps)
+        f, d, h, l = lat.download_state()
+        assert _pointwise_rel(f, st.field[0]) <= 1e-10
+        assert _pointwise_rel(d, st.dfield[0]) <= 1e-10
+        if gws:  # tensor modes are not evolved: they keep their initial (zero) values
+            assert np.abs(h).max() == 0 and np.abs(l).max() == 0
+        sc = lat.scalars()
+        for k in ("a", "adot", "edkin", "edpot", "edgrad", "edrho"):
+            for s in (0, 1):
+                want = getattr(st.sc, k)[s]
+                assert abs(sc[k][s] - want) <= _scalar_tol(k, want, st.sc.edrho[s]), (k, s, sc[k][s], want)
+        if expansion == 0:
+            assert sc["a"] == (first.sc.a[0], first.sc.a[0]) and sc["adot"] == (0.0, 0.0)
+        e64, e32 = lat.calc_energy(), l32.calc_energy()
+        for k in ("kin", "pot", "rho", "a", "adot"):
+            assert abs(e32[k] - e64[k]) <= 1e-4 * abs(e64[k]) + (1e-300 if k == "adot" else 0), (k, e32[k], e64[k])
+
+
 def test_fp64_from_reference_dump():
     """Start from the state the reference itself wrote after 10 steps."""
     d = np.load(os.path.join(HERE, "golden", "ref_m1_n16_g1_step10.npz"))
