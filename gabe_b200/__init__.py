@@ -92,6 +92,10 @@ def library():
     L.gabe_spectra_numbins.argtypes = [ctypes.c_int]
     L.gabe_spectra.argtypes = [H, _dp, ctypes.c_int, ctypes.c_int]
     L.gabe_spectra_raw.argtypes = [H, _dp, _dp, ctypes.c_int, ctypes.c_int]
+    L.gabe_meansvars.argtypes = [H, _dp]
+    L.gabe_field_slice_rows.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.gabe_field_slice_rows.restype = ctypes.c_size_t
+    L.gabe_field_slice.argtypes = [H, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_size_t]
     L.gabe_last_error.argtypes = [H]
     L.gabe_last_error.restype = ctypes.c_char_p
     L.gabe_device_bytes.argtypes = [H]
@@ -283,16 +287,19 @@ class Lattice:
 
     def meansvars(self) -> np.ndarray:
         """Mean and variance of each field (meansvars, g2output.cpp:70-121),
-        from a downloaded state: rows (mean, var) per field.  Raises
+        reduced on the device: rows (mean, var) per field.  Raises
         GabeError(GABE_ERR_NONFINITE) where the reference would exit(1)."""
-        f, _, _, _ = self.download_state(want_gw=False)
-        out = np.zeros((2, 2))
-        for q in range(2):
-            av = f[q].mean()
-            var = (f[q] * f[q] - av * av).mean()
-            if av != 0.0 and not np.isfinite(av):
-                raise GabeError(5, f"unstable solution: field {q} not numerical")
-            out[q] = (av, var)
+        out = np.zeros(4)
+        self._check(library().gabe_meansvars(self._h, _ptr(out)))
+        return out.reshape(2, 2)
+
+    def field_slice(self, outdim: int = 2, skip: int = 2) -> np.ndarray:
+        """The rows outputfield (g2output.cpp:25-68) writes for field_outdim
+        `outdim` and field_sliceskip `skip`: (phi, chi, calcrho) per sampled
+        point, in the reference's loop order, computed on the device."""
+        rows = library().gabe_field_slice_rows(self.N, int(outdim), int(skip))
+        out = np.zeros((rows, 3))
+        self._check(library().gabe_field_slice(self._h, int(outdim), int(skip), _ptr(out), out.size))
         return out
 
 

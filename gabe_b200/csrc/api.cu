@@ -50,6 +50,7 @@ struct gabe_handle {
     unsigned int *counters = nullptr;
     DevScalars *sc = nullptr;
     double *bin_part = nullptr, *bin_sum = nullptr;
+    double *outres = nullptr;  // meansvars results [8]
     unsigned int *bin_cnt_part = nullptr;
     int nbins = 0;
     cufftHandle plan_src = 0, plan_spec = 0;
@@ -539,6 +540,7 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     if ((rc = dalloc(h, (void **)&h->bin_cnt_part, (size_t)kBinBlocks * h->nbins * sizeof(unsigned int))))
         return bail(rc);
     if ((rc = dalloc(h, (void **)&h->bin_sum, (size_t)4 * h->nbins * sizeof(double)))) return bail(rc);
+    if ((rc = dalloc(h, (void **)&h->outres, 8 * sizeof(double)))) return bail(rc);
     if (cudaMemset(h->counters, 0, 8 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMemset(h->sc, 0, sizeof(DevScalars)) != cudaSuccess) {
         cudaGetLastError();
@@ -564,7 +566,7 @@ int gabe_destroy(gabe_handle *h) {
     if (h->have_plan_src) cufftDestroy(h->plan_src);
     if (h->have_plan_spec) cufftDestroy(h->plan_spec);
     void *bufs[] = {h->X[0], h->X[1], h->D[0], h->D[1], h->G, h->gwnorm, h->S, h->S2, h->partials, h->counters,
-                    h->sc, h->bin_part, h->bin_cnt_part, h->bin_sum, h->fft_work};
+                    h->sc, h->bin_part, h->bin_cnt_part, h->bin_sum, h->fft_work, h->outres};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -745,6 +747,71 @@ int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double 
 }
 
 int gabe_spectra_numbins(int N) { return ((int)(sqrt(3.) * N / 2 + 1)); }
+
+namespace {
+OutArgs out_args(gabe_handle *h) {
+    OutArgs a{};
+    a.X = h->X[h->cur];
+    a.D = h->D[h->cur];
+    a.sc = h->sc;
+    a.c = h->lc;
+    a.partials = h->partials;
+    a.counter = h->counters + 6;
+    a.res = h->outres;
+    return a;
+}
+}  // namespace
+
+int gabe_meansvars(gabe_handle *h, double out4[4]) {
+    if (!h || !out4) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "meansvars before upload");
+    CK(h, cudaSetDevice(h->dev));
+    const OutArgs a = out_args(h);
+    const int nblocks = 148 * 8;  // partials hold >= 2 * nblocks doubles
+    for (int pass = 0; pass < 2; pass++)
+        CK(h, h->f32 ? meansvars_f32(a, pass, nblocks, h->stream) : meansvars_f64(a, pass, nblocks, h->stream));
+    double r[4];
+    CK(h, cudaMemcpyAsync(r, h->outres, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+    CK(h, cudaStreamSynchronize(h->stream));
+    for (int f = 0; f < 2; f++) {
+        out4[2 * f] = r[f];
+        out4[2 * f + 1] = r[2 + f];
+    }
+    for (int f = 0; f < 2; f++) {
+        const double av = r[f];
+        if (av != 0. && av / av != 1.)  // g2output.cpp:106
+            return set_err(h, GABE_ERR_NONFINITE, "Unstable solution developed. Field %d not numerical", f);
+    }
+    return GABE_OK;
+}
+
+size_t gabe_field_slice_rows(int N, int outdim, int skip) {
+    if (N <= 0 || outdim < 1 || outdim > 3 || skip < 1) return 0;
+    const size_t n = (size_t)((N + skip - 1) / skip);
+    return outdim == 1 ? n : outdim == 2 ? n * n : n * n * n;
+}
+
+int gabe_field_slice(gabe_handle *h, int outdim, int skip, double *out, size_t out_len) {
+    if (!h || !out) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "field slice before upload");
+    const size_t rows = gabe_field_slice_rows(h->N, outdim, skip);
+    if (rows == 0) return set_err(h, GABE_ERR_PARAM, "outdim must be 1..3 and skip >= 1");
+    if (out_len < 3 * rows) return set_err(h, GABE_ERR_PARAM, "out holds %zu doubles, %zu needed", out_len, 3 * rows);
+    CK(h, cudaSetDevice(h->dev));
+    const int n = (h->N + skip - 1) / skip;
+    const int nj = outdim > 1 ? n : 1, nk = n;
+    const OutArgs a = out_args(h);
+    double *stage = static_cast<double *>(h->S);  // free between steps (the step's last wait covers the GW chain)
+    const size_t chunk = h->S_bytes / (3 * sizeof(double));
+    for (size_t r0 = 0; r0 < rows; r0 += chunk) {
+        const size_t cnt = rows - r0 < chunk ? rows - r0 : chunk;
+        CK(h, h->f32 ? slice_f32(a, nj, nk, skip, r0, cnt, stage, h->stream)
+                     : slice_f64(a, nj, nk, skip, r0, cnt, stage, h->stream));
+        CK(h, cudaMemcpyAsync(out + 3 * r0, stage, cnt * 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(h, cudaStreamSynchronize(h->stream));
+    }
+    return GABE_OK;
+}
 
 int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries) {
     if (!h) return GABE_ERR_PARAM;

@@ -48,6 +48,7 @@ struct LatticeConsts {
     int model;
     int expansion;          // expansion_type: 0 none, 1 Friedmann, 2 Friedmann without tensor modes
     double dt, half_dt;     // dt, .5*dt
+    double dx;              // L/((double)N) (g2parameters.h:93)
     double inv_dx2_div;     // dx*dx (the reference divides by it)
     double dn, c13, c23;    // 1/(dx*dx), (1./3.)*dn, (2./3.)*dn  (g2evolutionpert.cpp:53-116)
     double mc[5];           // model constants (see model_consts on the host)

@@ -130,4 +130,15 @@ cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out
     return cudaGetLastError();
 }
 
+cudaError_t meansvars_f32(const OutArgs &a, int pass, int nblocks, cudaStream_t s) {
+    meansvars_kernel<float><<<nblocks, 256, 0, s>>>(a, pass);
+    return cudaGetLastError();
+}
+
+cudaError_t slice_f32(const OutArgs &a, int nj, int nk, int skip, size_t r0, size_t cnt, double *out, cudaStream_t s) {
+    const int blocks = (int)((cnt + 255) / 256 < 4 * 148 ? (cnt + 255) / 256 : 4 * 148);
+    slice_kernel<float><<<blocks > 0 ? blocks : 1, 256, 0, s>>>(a, nj, nk, skip, r0, cnt, out);
+    return cudaGetLastError();
+}
+
 }  // namespace gabe

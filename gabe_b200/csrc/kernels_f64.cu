@@ -61,4 +61,15 @@ cudaError_t bin_reduce(const double *part_sum, const unsigned int *part_cnt, int
     return cudaGetLastError();
 }
 
+cudaError_t meansvars_f64(const OutArgs &a, int pass, int nblocks, cudaStream_t s) {
+    meansvars_kernel<double><<<nblocks, 256, 0, s>>>(a, pass);
+    return cudaGetLastError();
+}
+
+cudaError_t slice_f64(const OutArgs &a, int nj, int nk, int skip, size_t r0, size_t cnt, double *out, cudaStream_t s) {
+    const int blocks = (int)((cnt + 255) / 256 < 4 * 148 ? (cnt + 255) / 256 : 4 * 148);
+    slice_kernel<double><<<blocks > 0 ? blocks : 1, 256, 0, s>>>(a, nj, nk, skip, r0, cnt, out);
+    return cudaGetLastError();
+}
+
 }  // namespace gabe

@@ -10,6 +10,7 @@
 
 #include "../../include/gabe.h"
 #include "kspace.cuh"
+#include "output.cuh"
 #include "spectra.cuh"
 #include "stencil.cuh"
 
@@ -35,6 +36,7 @@ inline LatticeConsts make_lattice_consts(const gabe_params &p) {
     c.expansion = p.expansion;
     const double L = p.L, dt = p.dt;
     const double dx = L / ((double)p.N);
+    c.dx = dx;
     c.dt = dt;
     c.half_dt = .5 * dt;
     c.inv_dx2_div = dx * dx;
@@ -120,6 +122,12 @@ cudaError_t gw_pack_f32(const double *src, size_t cnt, size_t m0, int N, size_t 
                         cudaStream_t s);
 cudaError_t gw_unpack_f64(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s);
 cudaError_t gw_unpack_f32(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s);
+
+// meansvars() and outputfield() rows on the device (output.cuh)
+cudaError_t meansvars_f64(const OutArgs &a, int pass, int nblocks, cudaStream_t s);
+cudaError_t meansvars_f32(const OutArgs &a, int pass, int nblocks, cudaStream_t s);
+cudaError_t slice_f64(const OutArgs &a, int nj, int nk, int skip, size_t r0, size_t cnt, double *out, cudaStream_t s);
+cudaError_t slice_f32(const OutArgs &a, int nj, int nk, int skip, size_t r0, size_t cnt, double *out, cudaStream_t s);
 
 cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *counter, double *out, int nblocks,
                      cudaStream_t s);

@@ -1,21 +1,22 @@
 /*
- * gabe_dropin.cpp -- GABE's step(), specOut() and specClear() on top of the
- * B200 library (include/gabe.h).
+ * gabe_dropin.cpp -- GABE's step(), specOut(), specClear() and
+ * outputslice() on top of the B200 library (include/gabe.h).
  *
  * Compiled inside a GABE source tree (it includes that tree's g2header.h and
- * g2parameters.h) together with the unmodified g2main.cpp, g2output.cpp,
- * g2init.cpp, model file and g2evolutionpert.cpp, and with g2functions.cpp
- * and g2spectra.cpp built with -Dstep=gabe_reference_cpu_step and
- * -DspecOut=gabe_reference_specOut -DspecClear=gabe_reference_specClear so
- * that these definitions take the driver's calls (g2main.cpp:126,
- * g2output.cpp:161, g2main.cpp:335).
+ * g2parameters.h) together with the unmodified g2main.cpp, g2init.cpp, model
+ * file and g2evolutionpert.cpp, and with g2functions.cpp, g2spectra.cpp and
+ * g2output.cpp built with -Dstep=gabe_reference_cpu_step,
+ * -DspecOut=gabe_reference_specOut -DspecClear=gabe_reference_specClear and
+ * -Doutputslice=gabe_reference_outputslice so that these definitions take
+ * the driver's calls (g2main.cpp:122,126,129,335).
  *
  * State ownership follows the reference: the host arrays stay the
  * program's; the device copy is made once, after the reference's own
- * initialisation (g2main.cpp:111-118), and the host mirrors are refreshed
- * as the output code needs them -- the per-stage scalars after every step,
- * field[0]/dfield[0] on the steps where outputslice() writes
- * (g2output.cpp:136-149).  Spectra are computed on the device.
+ * initialisation (g2main.cpp:111-118), and the per-stage scalars are copied
+ * back after every step (96 bytes).  The output slices need no state
+ * download: the field-slice rows with calcrho (outputfield), the means and
+ * variances (meansvars) and the spectra (specOut) are computed on the
+ * device and only the printed numbers cross to the host.
  *
  * Knobs (compile-time, like the rest of GABE):
  *   GABE_B200_MODEL      0: the shipped model (g2model.cpp; constants mphi,
@@ -89,13 +90,79 @@ void ensure_device_state()
     if (rc != GABE_OK) gabe_die("gabe_upload_state", rc);
 }
 
-// outputslice() writes after the n-th step when n is a multiple of its
-// wait (g2output.cpp:136-149); the first call at t = starttime always writes.
-bool output_due(long n)
+#if field_outdim != 0
+// outputfield(first) (g2output.cpp:25-68): the same rows and format, computed
+// on the device (gabe_field_slice).
+void device_outputfield(int first)
 {
-    const int w = slicewait == 0 ? (int)(endtime / dt / slicenumber) : slicewait;
-    return w <= 1 || n % w == 0;
+    ensure_device_state();
+    const size_t rows = gabe_field_slice_rows(N, field_outdim, field_sliceskip);
+    double *buf = (double *)malloc(sizeof(double) * 3 * rows);
+    if (!buf) {
+        fprintf(stderr, "gabe_b200: host allocation failed\n");
+        exit(1);
+    }
+    int rc = gabe_field_slice(g_gpu, field_outdim, field_sliceskip, buf, 3 * rows);
+    if (rc != GABE_OK) gabe_die("gabe_field_slice", rc);
+    char name[64];
+    snprintf(name, sizeof(name), "./slices/slices_fields_%d.dat", first);
+    FILE *f = fopen(name, "w");
+    if (!f) {
+        fprintf(stderr, "gabe_b200: cannot open %s\n", name);
+        exit(1);
+    }
+    for (size_t r = 0; r < rows; r++) {
+        for (int c = 0; c < 3; c++) {
+#if fftw_flag == 1
+            fprintf(f, "%Le ", (long double)buf[3 * r + c]);
+#else
+            fprintf(f, "%e ", buf[3 * r + c]);
+#endif
+        }
+        fprintf(f, "\n");
+    }
+    fclose(f);
+    free(buf);
 }
+#endif
+
+#if var_output != 0
+// meansvars() (g2output.cpp:70-121): the same line of meansvariances.dat and
+// the same stop on a non-numerical field mean, from gabe_meansvars.
+void device_meansvars()
+{
+    ensure_device_state();
+    double mv[4];
+    int rc = gabe_meansvars(g_gpu, mv);
+    if (rc != GABE_OK && rc != GABE_ERR_NONFINITE) gabe_die("gabe_meansvars", rc);
+    FILE *out = fopen("./slices/meansvariances.dat", "a");
+#if fftw_flag == 1
+    fprintf(out, "%Lf", t);
+#else
+    fprintf(out, "%f", t);
+#endif
+    for (int fld = 0; fld < nflds; fld++) {
+        const double av = mv[2 * fld], var = mv[2 * fld + 1];
+#if fftw_flag == 1
+        fprintf(out, " %Le %Le", (long double)av, (long double)var);
+#else
+        fprintf(out, " %e %e", av, var);
+#endif
+        if (av != 0. && av / av != 1.) {
+#if fftw_flag == 1
+            printf("Unstable solution developed. Field %d not numerical at t=%Le\n", fld, t);
+#else
+            printf("Unstable solution developed. Field %d not numerical at t=%e\n", fld, t);
+#endif
+            output_parameters();
+            fflush(out);
+            exit(1);
+        }
+    }
+    fprintf(out, "\n");
+    fclose(out);
+}
+#endif
 
 }  // namespace
 
@@ -106,10 +173,47 @@ void step()
     if (rc != GABE_OK) gabe_die("gabe_step", rc);
     g_steps++;
     pull_scalars();
-    if (output_due(g_steps)) {
-        rc = gabe_download_state(g_gpu, &field[0][0][0][0][0], &dfield[0][0][0][0][0], nullptr, nullptr);
-        if (rc != GABE_OK) gabe_die("gabe_download_state", rc);
+}
+
+// outputslice() (g2output.cpp:129-186): the same cadence, the same files in
+// the same order, with the field slice and means/variances from the device.
+void outputslice()
+{
+    static FILE *slicetime;
+    static int first = 0;
+    static int lastslice, lastspec;
+    static int slicewaitm;
+    if (first == 0) {
+        slicewaitm = slicewait == 0 ? slicewaitf() : slicewait;
+        lastslice = slicewaitm;
+        lastspec = specnumber;
     }
+    lastslice++;
+    if (lastslice < slicewaitm) return;
+#if field_outdim != 0
+    device_outputfield(first);
+#endif
+#if spec_output == 1
+    lastspec++;
+    if (lastspec >= specnumber) {
+        specOut(first / specnumber);
+        lastspec = 0;
+    }
+#endif
+#if var_output != 0
+    device_meansvars();
+#endif
+    slicetime = fopen("./slices/slices_time.dat", "a");
+#if fftw_flag == 1
+    fprintf(slicetime, "%Le %Le %Le %Le %Le %Le %Le %Le\n", t, a[0], adot[0], adot[0] / a[0], edkin[0], edpot[0],
+            edgrad[0], edrho[0]);
+#else
+    fprintf(slicetime, "%e %e %e %e %e %e %e %e\n", t, a[0], adot[0], adot[0] / a[0], edkin[0], edpot[0], edgrad[0],
+            edrho[0]);
+#endif
+    fclose(slicetime);
+    first++;
+    lastslice = 0;
 }
 
 #if spec_output == 1

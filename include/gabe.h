@@ -165,6 +165,26 @@ int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols);
  * rebin these exactly (e.g. into log-spaced |k| bins). */
 int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries);
 
+/* meansvars() (g2output.cpp:70-121) of the current state without the file
+ * write: out4 = {mean, variance} of each field, variance as the reference
+ * forms it, sum(f^2 - mean^2)/N^3.  All four values are written; the return
+ * is GABE_ERR_NONFINITE where the reference would print "Unstable solution
+ * developed" and exit (a field mean with mean != 0 and mean/mean != 1).
+ * Synchronises. */
+int gabe_meansvars(gabe_handle *h, double out4[4]);
+
+/* Rows that outputfield() (g2output.cpp:25-68) writes for field_outdim
+ * outdim (1..3) and field_sliceskip skip: ceil(N/skip)^outdim. */
+size_t gabe_field_slice_rows(int N, int outdim, int skip);
+
+/* The rows of outputfield(): for i (stepping by skip if outdim > 2, else
+ * i = 0), j (if outdim > 1, else 0) and k, in that loop order, the nflds
+ * field values and calcrho(0, i, j, k) (g2functions.cpp:176-186, with the
+ * fourth-order gradients of :70-98), computed on the device.  out holds
+ * out_len >= 3 * gabe_field_slice_rows(N, outdim, skip) doubles, row-major.
+ * Synchronises. */
+int gabe_field_slice(gabe_handle *h, int outdim, int skip, double *out, size_t out_len);
+
 /* Stage-0 energies {kin, pot, grad, rho} (calcEnergy(0)) of a state the
  * caller already holds in device memory, without allocating anything: for
  * callers that cannot allocate device memory at that point (a framework

@@ -213,6 +213,51 @@ def spectra(cfg: Config, field0: np.ndarray, l0: np.ndarray | None, edrho0: floa
     return out
 
 
+def meansvars(field0: np.ndarray) -> np.ndarray:
+    """meansvars (g2output.cpp:70-121): rows (mean, variance) per field, the
+    variance as the reference forms it, sum(f^2 - mean^2) / N^3 (numpy's sum
+    order, not the reference's serial one)."""
+    out = np.zeros((field0.shape[0], 2))
+    for q in range(field0.shape[0]):
+        f = field0[q]
+        av = f.sum() / f.size
+        out[q] = av, (f * f - av * av).sum() / f.size
+    return out
+
+
+def _potential(cfg: Config, P: np.ndarray, C: np.ndarray) -> np.ndarray:
+    """potential (g2model.cpp:66-69; lphi4 in ref_cfg/g2model_lphi4.cpp), operation order kept."""
+    mc = list(cfg.params().mc)
+    if cfg.model == MODEL_QUADRATIC:
+        return 0.5 * P * P + mc[1] * P * P * C * C
+    return mc[2] * P * P * P * P + mc[3] * P * P * C * C
+
+
+def field_slice(cfg: Config, field0: np.ndarray, dfield0: np.ndarray, a0: float, outdim: int, skip: int) -> np.ndarray:
+    """The rows outputfield (g2output.cpp:25-68) writes: per sampled point
+    (i stepping by skip if outdim > 2 else 0, j likewise if outdim > 1, k),
+    the two field values and calcrho(0, i, j, k) (g2functions.cpp:176-186)
+    with the fourth-order gradients dfdi/dfdj/dfdk (:70-98) and gradF2
+    (:118-122), each in the reference's operation order."""
+    N = cfg.N
+    dx = cfg.L / float(N)
+
+    def d4(f, axis):
+        r = lambda s: np.roll(f, s, axis=axis)  # r(2)[i] = f[i-2]
+        return ((1. / 12.) * r(2) + ((-2.) / 3.) * r(1) + (2. / 3.) * r(-1) + ((-1.) / 12.) * r(-2)) / dx
+
+    rho = _potential(cfg, field0[0], field0[1])
+    for q in range(2):
+        gi, gj, gk = d4(field0[q], 0), d4(field0[q], 1), d4(field0[q], 2)
+        g2 = gi * gi + gj * gj + gk * gk
+        rho = rho + (.5 * dfield0[q] * dfield0[q] + .5 * g2 / a0 / a0)
+    ii = range(0, N, skip) if outdim > 2 else [0]
+    jj = range(0, N, skip) if outdim > 1 else [0]
+    kk = range(0, N, skip)
+    rows = [(field0[0, i, j, k], field0[1, i, j, k], rho[i, j, k]) for i in ii for j in jj for k in kk]
+    return np.array(rows)
+
+
 # ---------------------------------------------------------------------------
 # binary dumps (include/gabe_dump.h)
 # ---------------------------------------------------------------------------

@@ -1,11 +1,13 @@
-"""The drop-in: GABE's own driver and output code (g2main.cpp,
-g2output.cpp) with step()/specOut() taken by gabe_b200/host/gabe_dropin.cpp
-on the GPU, against the same program built entirely from the reference
-sources.  Every file under slices/ must match to the precision the reference
-prints (%e, 7 significant digits), apart from two quantities the reference
-computes with cancellation: the variance column of meansvariances.dat
-(sum of f^2 - mean^2 with f ~ 0.34) and the gradient-energy column of
-slices_time.dat (sum of -f lap f).
+"""The drop-in: GABE's own driver (g2main.cpp) with step(), specOut() and
+outputslice() taken by gabe_b200/host/gabe_dropin.cpp -- the field slices,
+means/variances and spectra computed on the GPU, no state download -- against
+the same program built entirely from the reference sources.  Every file under
+slices/ must match to the precision the reference prints (%e, 7 significant
+digits), apart from quantities the reference computes with cancellation: the
+mean and variance columns of meansvariances.dat (a serial mean of f ~ 0.34,
+then sum of f^2 - mean^2: noise ~ eps mean^2 sqrt(N^3), and chi's mean, zero
+in exact arithmetic) and the gradient-energy column of slices_time.dat (sum
+of -f lap f).
 
 Both programs are compiled by `make -C oracle full dropin` where the
 reference tree is mounted; the binaries travel with the repository."""
@@ -55,8 +57,13 @@ def test_dropin_program_matches_reference_program(cfg, tmp_path):
             assert _close(got[:, 6], want[:, 6], 1e-4), n
         elif n == "meansvariances.dat":
             # columns: t, then (mean, variance) per field
-            assert _close(got[:, [0, 1, 3]], want[:, [0, 1, 3]], 2e-6), n
-            assert _close(got[:, [2, 4]], want[:, [2, 4]], 1e-3), n
+            assert _close(got[:, [0, 1]], want[:, [0, 1]], 2e-6), n
+            assert np.all(np.abs(got[:, 3] - want[:, 3]) <= 1e-20), n  # chi: rounding noise of a zero mean
+            N = 32
+            for c in (2, 4):
+                av = want[:, c - 1]
+                tol = 1e-3 * np.abs(want[:, c]) + 16 * np.finfo(float).eps * av * av * N ** 1.5
+                assert np.all(np.abs(got[:, c] - want[:, c]) <= tol), n
         elif n.startswith("slices_spectra_"):
             assert _close(got, want, 1e-5, floor_frac=1e-10), n
         else:

@@ -358,12 +358,57 @@ def test_step_before_upload_is_an_error():
         assert ei.value.code == 7
 
 
-def test_meansvars_matches_numpy():
-    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=0)
+def _variance_tol(var, av, N):
+    """Variance sum(f^2 - mean^2)/N^3 of a field with mean ~0.34 and ~1e-7
+    fluctuations: absolute rounding noise ~ eps mean^2 sqrt(N^3) (both sides
+    form it this way, with different summation orders)."""
+    return 1e-6 * abs(var) + 16 * np.finfo(float).eps * av * av * N ** 1.5
+
+
+@pytest.mark.parametrize("precision", [gb.FP64, gb.FP32])
+def test_meansvars_and_field_slice_match_oracle(precision):
+    """gabe_meansvars and gabe_field_slice (meansvars and the outputfield rows
+    with calcrho, g2output.cpp:25-121, g2functions.cpp:70-122,176-186)
+    against the oracle's restatements, which tests/test_oracle_output.py pins
+    to the reference program's own files."""
+    cfg = po.Config(N=32, model=po.MODEL_LPHI4, gws=1)
     st = po.init_state(cfg)
-    with _lattice(cfg) as lat:
+    po.step(st, 20)
+    with _lattice(cfg, precision=precision) as lat:
         _upload(lat, st)
         mv = lat.meansvars()
+        slices = {(d, sk): lat.field_slice(d, sk) for d, sk in ((1, 1), (2, 2), (3, 3))}
+    want_mv = po.meansvars(st.field[0])
     for q in range(2):
-        av = st.field[0, q].mean()
-        assert abs(mv[q, 0] - av) <= 1e-15 + 1e-13 * abs(av)
+        av, var = want_mv[q]
+        rms = float(np.sqrt(np.mean(st.field[0, q] ** 2)))
+        tol = 1e-13 * abs(av) + 16 * np.finfo(float).eps * rms
+        if precision == gb.FP32:  # fluctuations stored in FP32: ~eps32 rms(fluctuation) in the mean
+            tol += np.finfo(np.float32).eps * float(np.std(st.field[0, q]))
+        assert abs(mv[q, 0] - av) <= tol, (q, mv[q, 0], av)
+        assert abs(mv[q, 1] - var) <= _variance_tol(var, av, cfg.N), (q, mv[q, 1], var)
+    for (d, sk), got in slices.items():
+        want = po.field_slice(cfg, st.field[0], st.dfield[0], st.sc.a[0], d, sk)
+        assert got.shape == want.shape == (((cfg.N + sk - 1) // sk) ** d, 3)
+        if precision == gb.FP64:
+            np.testing.assert_array_equal(got[:, :2], want[:, :2])
+            assert np.all(np.abs(got[:, 2] - want[:, 2]) <= 1e-13 * np.abs(want[:, 2]))
+        else:  # FP32 fluctuations about the FP64 homogeneous values
+            assert np.all(np.abs(got[:, :2] - want[:, :2]) <= 1e-12 * np.abs(want[:, :2]).max())
+            assert np.all(np.abs(got[:, 2] - want[:, 2]) <= 1e-6 * np.abs(want[:, 2]))
+
+
+def test_field_slice_rejects_bad_arguments():
+    import ctypes
+
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=0)
+    st = po.init_state(cfg)
+    lib = gb.library()
+    with _lattice(cfg) as lat:
+        _upload(lat, st)
+        buf = np.zeros(3 * 64)
+        ptr = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        assert lib.gabe_field_slice(lat.handle, 0, 1, ptr, buf.size) == 1
+        assert lib.gabe_field_slice(lat.handle, 2, 0, ptr, buf.size) == 1
+        assert lib.gabe_field_slice(lat.handle, 2, 1, ptr, buf.size) == 1  # 256 rows do not fit
+        assert lib.gabe_field_slice(lat.handle, 2, 2, ptr, buf.size) == 0
