@@ -46,10 +46,19 @@ def _potential(model: int, mc, p: float, c: float) -> float:
 
 def random_state(N: int, *, L: float = 20.0, seed: int = 44463132, model: int = MODEL_LPHI4, model_c=None,
                  f0=(0.342, 0.0), df0=(0.0, 0.0), rescale_B: float | None = None, amplitude: float = 1.0,
+                 spec_cut_off: float | None = None, spec_smooth: float = 0.5, full_rand: bool = True,
                  device: str | torch.device = "cpu"):
     """Returns (field0, dfield0, a0, adot0): float64 tensors [2][N][N][N] on
     `device` and the two scalars.  `amplitude` multiplies every fluctuation
-    amplitude (the ensemble's amplitude multiplier)."""
+    amplitude (the ensemble's amplitude multiplier).  The reference's
+    initial-spectrum knobs (g2parameters.h:72-74, g2init.cpp:117-165):
+    `spec_cut_off` (with `spec_smooth`) multiplies every mode's amplitude by
+    (1 - tanh(spec_smooth (|n| - N spec_cut_off)))/2; `full_rand=False`
+    (field_full_rand 0, which the reference only defines with the cut-off)
+    replaces the random draws by the deterministic real amplitude
+    sqrt(1/(2 omega_k L^3)) and fdot_k = -H0 f_k."""
+    if not full_rand and spec_cut_off is None:
+        raise ValueError("full_rand=False needs spec_cut_off (the reference's field_full_rand 0 uses it)")
     if model_c is None:
         model_c = (1.0 / 0.342 ** 2, 100.0 / 0.342 ** 2) if model == MODEL_LPHI4 else (1e-6, 2.5e-7)
     if rescale_B is None:
@@ -73,14 +82,30 @@ def random_state(N: int, *, L: float = 20.0, seed: int = 44463132, model: int = 
     dk2 = 4.0 * math.pi * math.pi / L / L
     n2 = i2[:, None, None] + i2[None, :, None] + k2[None, None, :]
     L3 = L * L * L
+    cut = None
+    if spec_cut_off is not None:
+        cut = (1.0 - torch.tanh(spec_smooth * (torch.sqrt(n2) - N * spec_cut_off))) / 2.0
     for q in range(2):
         m2 = _dv_m2(model, model_c, f[0], f[1], q)
         wk = torch.sqrt(dk2 * n2 + m2)
+        if not full_rand:
+            amp = amplitude * rescale_B * torch.sqrt(1.0 / (2.0 * wk * L3)) * cut
+            fk = torch.complex(amp, torch.zeros_like(amp))
+            fd = torch.complex(-H0 * amp, torch.zeros_like(amp))
+            fk[0, 0, 0] = 0
+            fd[0, 0, 0] = 0
+            scale = float(N) ** 3  # FFTW's c2r is unnormalised
+            f[q] += torch.fft.irfftn(fk, s=(N, N, N)) * scale
+            d[q] += torch.fft.irfftn(fd, s=(N, N, N)) * scale
+            del fk, fd, amp, wk
+            continue
         draws = []
         for _ in range(2):
             u = 1.0 - torch.rand((N, N, nz), generator=gen, device=dev, dtype=torch.float64)
             th = 2.0 * math.pi * torch.rand((N, N, nz), generator=gen, device=dev, dtype=torch.float64)
             r = amplitude * rescale_B * torch.sqrt(-torch.log(u) / (2.0 * wk * L3))
+            if cut is not None:
+                r = r * cut
             draws.append((r * torch.cos(th), r * torch.sin(th)))
             del u, th, r
         (r1, i1), (r2, i2_) = draws

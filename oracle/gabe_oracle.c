@@ -151,7 +151,9 @@ static void set_energy(const ora_params *p, const double *f, const double *df, o
 static void rand_init(const ora_params *p, double *f, double *df, double d2vdf2, double H0,
                       double rescale_B, double *fk, double *fkd, double *inic, fftw_plan pf, fftw_plan pd)
 {
-    /* randInit (g2init.cpp:68-189), field_full_rand == 1, no spectral cut-off */
+    /* randInit (g2init.cpp:68-189): field_full_rand 1 without (variant 0) or
+     * with (1) the spectral cut-off, or field_full_rand 0 (2) */
+    const int var = p->ic_variant;
     int N = p->N, nz = N / 2 + 1;
     double L = p->L;
     double dk2 = 4. * M_PI * M_PI / L / L;
@@ -168,15 +170,33 @@ static void rand_init(const ora_params *p, double *f, double *df, double d2vdf2,
                     continue;
                 }
                 double wk = sqrt(dk2 * ((double)i2 + (double)j2 + (double)k2) + d2vdf2);
+                if (var == 2) { /* :155-163 */
+                    fk[2 * x] = rescale_B * sqrt(1 / (2. * wk * L * L * L)) *
+                                (1. - tanh(p->spec_smooth * (sqrt(i2 + j2 + k2) - N * p->spec_cut))) / 2.;
+                    fk[2 * x + 1] = 0.;
+                    fkd[2 * x] = -H0 * fk[2 * x];
+                    fkd[2 * x + 1] = 0.;
+                    continue;
+                }
                 double u, th, r1[2], r2[2];
                 u = (double)rand() / (double)RAND_MAX;
                 th = 2. * M_PI * (double)rand() / (double)RAND_MAX;
-                r1[0] = rescale_B * cos(th) * sqrt(-log(u) / (2. * wk * L * L * L));
-                r1[1] = rescale_B * sin(th) * sqrt(-log(u) / (2. * wk * L * L * L));
-                u = (double)rand() / (double)RAND_MAX;
-                th = 2. * M_PI * (double)rand() / (double)RAND_MAX;
-                r2[0] = rescale_B * cos(th) * sqrt(-log(u) / (2. * wk * L * L * L));
-                r2[1] = rescale_B * sin(th) * sqrt(-log(u) / (2. * wk * L * L * L));
+                if (var == 1) { /* :120-131 */
+                    const double cut = p->spec_smooth * (sqrt(i2 + j2 + k2) - N * p->spec_cut);
+                    r1[0] = rescale_B * cos(th) * sqrt(-log(u) / (2. * wk * L * L * L)) * (1. - tanh(cut)) / 2.;
+                    r1[1] = rescale_B * sin(th) * sqrt(-log(u) / (2. * wk * L * L * L)) * (1. - tanh(cut)) / 2.;
+                    u = (double)rand() / (double)RAND_MAX;
+                    th = 2. * M_PI * (double)rand() / (double)RAND_MAX;
+                    r2[0] = rescale_B * cos(th) * sqrt(-log(u) / (2. * wk * L * L * L)) * (1. - tanh(cut)) / 2.;
+                    r2[1] = rescale_B * sin(th) * sqrt(-log(u) / (2. * wk * L * L * L)) * (1. - tanh(cut)) / 2.;
+                } else { /* :135-143 */
+                    r1[0] = rescale_B * cos(th) * sqrt(-log(u) / (2. * wk * L * L * L));
+                    r1[1] = rescale_B * sin(th) * sqrt(-log(u) / (2. * wk * L * L * L));
+                    u = (double)rand() / (double)RAND_MAX;
+                    th = 2. * M_PI * (double)rand() / (double)RAND_MAX;
+                    r2[0] = rescale_B * cos(th) * sqrt(-log(u) / (2. * wk * L * L * L));
+                    r2[1] = rescale_B * sin(th) * sqrt(-log(u) / (2. * wk * L * L * L));
+                }
                 fk[2 * x] = (r1[0] + r2[0]) / sqrt(2.);
                 fk[2 * x + 1] = (r1[1] + r2[1]) / sqrt(2.);
                 fkd[2 * x] = (r2[1] - r1[1]) * wk / sqrt(2.) - H0 * fk[2 * x];

@@ -32,6 +32,12 @@ typedef struct {
     int expansion;    /* expansion_type 0, 1 or 2 (g2parameters.h:62); callers set it */
     /* model constants, see ora_model_constants() */
     double mc[6];
+    /* initial spectrum (randInit, g2init.cpp:117-165): 0 field_full_rand 1
+     * without cut-off; 1 field_full_rand 1 with spec_cut_off/spec_smooth;
+     * 2 field_full_rand 0 (deterministic amplitudes) with the cut-off */
+    int ic_variant;
+    int ic_pad;
+    double spec_cut, spec_smooth;
 } ora_params;
 
 typedef struct {

@@ -35,6 +35,8 @@ class _Params(ctypes.Structure):
         ("model", ctypes.c_int), ("gws", ctypes.c_int),
         ("gw_spec_quirk", ctypes.c_int), ("expansion", ctypes.c_int),
         ("mc", ctypes.c_double * 6),
+        ("ic_variant", ctypes.c_int), ("ic_pad", ctypes.c_int),
+        ("spec_cut", ctypes.c_double), ("spec_smooth", ctypes.c_double),
     ]
 
 
@@ -104,12 +106,16 @@ class Config:
     gws: int = 0
     gw_spec_quirk: int = 1
     expansion: int = 1  # expansion_type (g2parameters.h:62)
+    ic_variant: int = 0  # 0 field_full_rand 1; 1 with spec_cut_off; 2 field_full_rand 0 (g2init.cpp:117-165)
+    spec_cut: float = math.sqrt(3.) / 8.  # spec_cut_off, spec_smooth (the reference's g2parameters.h:73-74)
+    spec_smooth: float = 0.5
 
     def params(self) -> _Params:
         p = _Params()
         p.N, p.nflds, p.L, p.dt = self.N, 2, self.L, self.dt
         p.model, p.gws, p.gw_spec_quirk = self.model, self.gws, self.gw_spec_quirk
         p.expansion = self.expansion
+        p.ic_variant, p.spec_cut, p.spec_smooth = self.ic_variant, self.spec_cut, self.spec_smooth
         c0, c1, *_ = model_constants(self.model)
         lib().ora_model_constants(ctypes.byref(p), c0, c1)
         return p
@@ -307,8 +313,8 @@ def read_dump(path: str, cfg: Config | None = None) -> State:
     return st
 
 
-def ref_binary(model: int, N: int, gws: int, parallel: int, expansion: int = 1) -> str:
-    suffix = "" if expansion == 1 else f"_e{expansion}"
+def ref_binary(model: int, N: int, gws: int, parallel: int, expansion: int = 1, ic_variant: int = 0) -> str:
+    suffix = ("" if expansion == 1 else f"_e{expansion}") + ("", "_rc", "_rd")[ic_variant]
     return os.path.join(REF_DIR, f"ref_m{model}_n{N}_g{gws}_p{parallel}{suffix}")
 
 

@@ -18,6 +18,9 @@
  *   GABE_PARALLEL 0 -> one thread, deterministic rand() order (reference :53,97-100)
  *   GABE_SEED     randseed                            (reference :56)
  *   GABE_ENDTIME, GABE_SLICEWAIT, GABE_FIELD_OUTDIM, GABE_VAR_OUTPUT
+ *   GABE_EXPANSION expansion_type                     (reference :62)
+ *   GABE_FULL_RAND field_full_rand                    (reference :72)
+ *   GABE_SPEC_CUT, GABE_SPEC_SMOOTH  spec_cut_off, spec_smooth (reference :73-74)
  *                 run length and output knobs (reference :60,80,84,86) for
  *                 builds that use the reference's own g2main.cpp/g2output.cpp
  *
@@ -106,7 +109,14 @@ const gNum dt = GABE_DT;
 #define expansion_type GABE_EXPANSION
 
 #define rand_init 1
-#define field_full_rand 1
+#ifndef GABE_FULL_RAND
+#define GABE_FULL_RAND 1
+#endif
+#define field_full_rand GABE_FULL_RAND
+#ifdef GABE_SPEC_CUT /* reference :73-74 (commented out there: sqrt(3.)/8., 0.5) */
+#define spec_cut_off GABE_SPEC_CUT
+#define spec_smooth GABE_SPEC_SMOOTH
+#endif
 
 const gNum screentime = 0;
 const int slicewait = GABE_SLICEWAIT;

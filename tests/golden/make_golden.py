@@ -42,6 +42,9 @@ CASES = [
     (1, 32, 0, [0, 1, 10, 100], [0, 100], 0),
     (1, 32, 1, [0, 1, 10, 50], [0, 50], 0),
     (1, 32, 1, [0, 1, 10, 50], [0, 50], 2),
+    # initial spectra with spec_cut_off (randInit variant 1) and field_full_rand 0 (variant 2)
+    (1, 32, 0, [0, 1, 10], [0, 10], 1, 1),
+    (1, 32, 0, [0, 1, 10], [0, 10], 1, 2),
 ]
 
 
@@ -66,16 +69,19 @@ def main() -> None:
     golden = {"generator": "tests/golden/make_golden.py", "seed": 44463132, "L": 20.0, "dt": 0.01, "cases": {}}
     for model, N, gws, dumps, specs, *rest in CASES:
         expansion = rest[0] if rest else 1
-        name = f"m{model}_n{N}_g{gws}" + ("" if expansion == 1 else f"_e{expansion}")
-        binary = po.ref_binary(model, N, gws, 0, expansion)
+        ic = rest[1] if len(rest) > 1 else 0
+        name = f"m{model}_n{N}_g{gws}" + ("" if expansion == 1 else f"_e{expansion}") + ("", "_rc", "_rd")[ic]
+        binary = po.ref_binary(model, N, gws, 0, expansion, ic)
         with tempfile.TemporaryDirectory() as d:
             steps = max(dumps + specs)
             po.run_ref(binary, ["--steps", str(steps), "--dump-prefix", "s_", "--dump-at", ",".join(map(str, dumps)),
                                 "--spectra-at", ",".join(map(str, specs))], d)
-            cfg = po.Config(N=N, model=model, gws=gws, expansion=expansion)
+            cfg = po.Config(N=N, model=model, gws=gws, expansion=expansion, ic_variant=ic)
             entry = {"model": model, "N": N, "gws": gws, "steps": {}, "spectra": {}}
             if expansion != 1:
                 entry["expansion"] = expansion
+            if ic:
+                entry["ic_variant"] = ic
             for s in dumps:
                 st = po.read_dump(os.path.join(d, f"s_{s}.bin"), cfg)
                 entry["steps"][str(s)] = record(st)

@@ -19,13 +19,17 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
 
 
-CASES = ["m1_n16_g1", "m0_n32_g1", "m1_n32_g0", "m1_n64_g0", "m1_n64_g1"]
+import json  # noqa: E402
+
+with open(os.path.join(HERE, "golden", "golden.json")) as _fh:
+    CASES = sorted(json.load(_fh)["cases"])  # every configuration the reference was run with
 
 
 @pytest.mark.parametrize("name", CASES)
 def test_oracle_matches_reference_bitwise(golden, name):
     g = golden["cases"][name]
-    cfg = po.Config(N=g["N"], model=g["model"], gws=g["gws"], expansion=g.get("expansion", 1))
+    cfg = po.Config(N=g["N"], model=g["model"], gws=g["gws"], expansion=g.get("expansion", 1),
+                    ic_variant=g.get("ic_variant", 0))
     st = po.init_state(cfg, seed=golden["seed"])
     steps = sorted(int(s) for s in g["steps"])
     prev = 0
@@ -49,7 +53,8 @@ def test_oracle_matches_reference_bitwise(golden, name):
 @pytest.mark.parametrize("name", CASES)
 def test_oracle_spectra_match_reference_files(golden, name):
     g = golden["cases"][name]
-    cfg = po.Config(N=g["N"], model=g["model"], gws=g["gws"], expansion=g.get("expansion", 1))
+    cfg = po.Config(N=g["N"], model=g["model"], gws=g["gws"], expansion=g.get("expansion", 1),
+                    ic_variant=g.get("ic_variant", 0))
     st = po.init_state(cfg, seed=golden["seed"])
     prev = 0
     for s in sorted(int(x) for x in g["spectra"]):
