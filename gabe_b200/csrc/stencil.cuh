@@ -129,6 +129,55 @@ __device__ __forceinline__ MeanF mean_f(const LatticeConsts &c, const double *fb
     return m;
 }
 
+// FP32 energy sums (the FP32 sweeps here and in sweep32.cuh).
+// Reduced values of sweep A / E0 are sums over sites of expressions such as
+// (dfbar + d)^2 whose large homogeneous parts are known per launch.  Each
+// thread accumulates only FP32 moments of the fluctuations (sum d, sum d^2,
+// sum Pd, ...) over a group of kGroup planes and folds them into its FP64
+// sums once per group with the exact expansions, e.g.
+//   sum (dfbar + d)^2 = n dfbar^2 + 2 dfbar sum d + sum d^2,
+// so no site needs an FP32 -> FP64 conversion (that conversion pipe, not
+// HBM, bounded the per-site FP64 form).
+constexpr int kGroup = 8;
+struct Moments {
+    float a[2];  // sum d (momentum fluctuation) per field
+    float b;     // sum over fields of d^2
+    float c[2];  // sum Pd per field (stage-1 momentum before the adot0 term)
+    float e;     // sum over fields of Pd^2
+    float f;     // sum over fields of Pd d
+    float g0, g1;  // sum over fields of f lap f, stage 0 and stage 1
+    float v0, v1;  // potential differences, stage 0 and stage 1
+};
+__device__ __forceinline__ void zero(Moments &m) {
+    m.a[0] = m.a[1] = m.b = m.c[0] = m.c[1] = m.e = m.f = m.g0 = m.g1 = m.v0 = m.v1 = 0.f;
+}
+
+// Folds the moments of n sites into the FP64 sums kin0 pot0 grad0 | pot1
+// grad1 PP PQ QQ (the kNV values finish_a expects) and clears them.  With
+// P = pbar + Pd, Q = qbar + q3 d:  sum P^2 = n pbar^2 + 2 pbar sum Pd + sum Pd^2,
+// sum PQ = n pbar qbar + pbar q3 sum d + qbar sum Pd + q3 sum Pd d,
+// sum Q^2 = n qbar^2 + 2 qbar q3 sum d + q3^2 sum d^2.
+template <int MODE>
+__device__ __forceinline__ void fold(const MeanTraj &t, float q3f, int n, Moments &m, double (&acc)[kNV]) {
+    const double dn = (double)n, q3 = (double)q3f;
+    const double a0 = m.a[0], a1 = m.a[1], b = m.b;
+    acc[0] += dn * (t.dfb0[0] * t.dfb0[0] + t.dfb0[1] * t.dfb0[1]) + 2. * (t.dfb0[0] * a0 + t.dfb0[1] * a1) + b;
+    acc[1] += (double)m.v0;
+    acc[2] -= (double)m.g0;
+    if constexpr (MODE != MODE_E0) {
+        const double c0 = m.c[0], c1 = m.c[1];
+        acc[3] += (double)m.v1;
+        acc[4] -= (double)m.g1;
+        acc[5] += dn * (t.pbar[0] * t.pbar[0] + t.pbar[1] * t.pbar[1]) + 2. * (t.pbar[0] * c0 + t.pbar[1] * c1) +
+                  (double)m.e;
+        acc[6] += dn * (t.pbar[0] * t.qbar[0] + t.pbar[1] * t.qbar[1]) + q3 * (t.pbar[0] * a0 + t.pbar[1] * a1) +
+                  (t.qbar[0] * c0 + t.qbar[1] * c1) + q3 * (double)m.f;
+        acc[7] += dn * (t.qbar[0] * t.qbar[0] + t.qbar[1] * t.qbar[1]) + 2. * q3 * (t.qbar[0] * a0 + t.qbar[1] * a1) +
+                  q3 * q3 * b;
+    }
+    zero(m);
+}
+
 // ---------------------------------------------------------------------------
 // plane march: 4 arrays (f0 phi, f0 chi, fdot0 phi, fdot0 chi)
 // ---------------------------------------------------------------------------
@@ -318,6 +367,10 @@ __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob
         }
     }
     (void)ia12f; (void)c3H0f; (void)c3H1f; (void)dtf; (void)dnf; (void)q3f; (void)c3H1;
+    Moments mom;  // FP32: fluctuation moments of the current plane group
+    zero(mom);
+    int ngroup = 0;
+    (void)ngroup;
 
     // prologue: registers for planes i0-1, i0, i0+1; shared tile of plane i0
     m.load_own(m.prev, i0 - 1);
@@ -394,27 +447,30 @@ __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob
                 float f1c[2];
                 for (int f = 0; f < 2; f++) {
                     const float lap0 = lap32(f0[f], inv_dx2f);
-                    const double kd = mt.dfb0[f] + (double)d0[f].v[0];
-                    acc[0] = fma(kd, kd, acc[0]);
-                    acc[2] -= (double)(f0[f].v[0] * lap0);
+                    const float d = d0[f].v[0];
+                    mom.a[f] += d;
+                    mom.b = fmaf(d, d, mom.b);
+                    mom.g0 = fmaf(f0[f].v[0], lap0, mom.g0);
                     if constexpr (MODE != MODE_E0) {
                         const Nb7<float> f1 = axpy7(f0[f], hf, d0[f]);
                         f1c[f] = f1.v[0];
-                        const float Pd = d0[f].v[0] + hf * (lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]));
-                        const double P = mt.pbar[f] + (double)Pd;
-                        const double Q = mt.qbar[f] + (double)(q3f * d0[f].v[0]);
-                        acc[5] = fma(P, P, acc[5]);
-                        acc[6] = fma(P, Q, acc[6]);
-                        acc[7] = fma(Q, Q, acc[7]);
-                        acc[4] -= (double)(f1.v[0] * lap32(f1, inv_dx2f));
+                        const float Pd = d + hf * (lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]));
+                        mom.c[f] += Pd;
+                        mom.e = fmaf(Pd, Pd, mom.e);
+                        mom.f = fmaf(Pd, d, mom.f);
+                        mom.g1 = fmaf(f1.v[0], lap32(f1, inv_dx2f), mom.g1);
                         if constexpr (MODE == MODE_A_GW) {
                             source_add32(dnf, f0[f], s0);
                             source_add32(dnf, f1, s1);
                         }
                     }
                 }
-                acc[1] += (double)v_diff32(m0, c.model, f0[0].v[0], f0[1].v[0]);
-                if constexpr (MODE != MODE_E0) acc[3] += (double)v_diff32(m1, c.model, f1c[0], f1c[1]);
+                mom.v0 += v_diff32(m0, c.model, f0[0].v[0], f0[1].v[0]);
+                if constexpr (MODE != MODE_E0) mom.v1 += v_diff32(m1, c.model, f1c[0], f1c[1]);
+                if (++ngroup == kGroup || i == i1 - 1) {  // one site per thread and plane
+                    fold<MODE>(mt, q3f, ngroup, mom, acc);
+                    ngroup = 0;
+                }
             }
             if constexpr (MODE == MODE_A_GW) store_sources(job.S, N, i, j, k, s0, s1);
         }

@@ -75,28 +75,6 @@ __device__ __forceinline__ Site32 site32_consts(const LatticeConsts &c, const De
     return s;
 }
 
-// Reduced values of sweep A / E0 are sums over sites of expressions such as
-// (dfbar + d)^2 whose large homogeneous parts are known per launch.  Each
-// thread accumulates only FP32 moments of the fluctuations (sum d, sum d^2,
-// sum Pd, ...) over a group of kGroup planes and folds them into its FP64
-// sums once per group with the exact expansions, e.g.
-//   sum (dfbar + d)^2 = n dfbar^2 + 2 dfbar sum d + sum d^2,
-// so no site needs an FP32 -> FP64 conversion (that conversion pipe, not
-// HBM, bounded the per-site FP64 form).
-constexpr int kGroup = 8;
-struct Moments {
-    float a[2];  // sum d (momentum fluctuation) per field
-    float b;     // sum over fields of d^2
-    float c[2];  // sum Pd per field (stage-1 momentum before the adot0 term)
-    float e;     // sum over fields of Pd^2
-    float f;     // sum over fields of Pd d
-    float g0, g1;  // sum over fields of f lap f, stage 0 and stage 1
-    float v0, v1;  // potential differences, stage 0 and stage 1
-};
-__device__ __forceinline__ void zero(Moments &m) {
-    m.a[0] = m.a[1] = m.b = m.c[0] = m.c[1] = m.e = m.f = m.g0 = m.g1 = m.v0 = m.v1 = 0.f;
-}
-
 // One site of sweep A / E0: adds to the moments, fills the sources.
 template <int MODE>
 __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s, const Nb7<float> &fp,
@@ -128,33 +106,6 @@ __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s
     }
     m.v0 += v_diff32(s.m0, c.model, fp.v[0], fc.v[0]);
     if constexpr (MODE != MODE_E0) m.v1 += v_diff32(s.m1, c.model, f1c[0], f1c[1]);
-}
-
-// Folds the moments of n sites into the FP64 sums kin0 pot0 grad0 | pot1
-// grad1 PP PQ QQ (the kNV values finish_a expects) and clears them.  With
-// P = pbar + Pd, Q = qbar + q3 d:  sum P^2 = n pbar^2 + 2 pbar sum Pd + sum Pd^2,
-// sum PQ = n pbar qbar + pbar q3 sum d + qbar sum Pd + q3 sum Pd d,
-// sum Q^2 = n qbar^2 + 2 qbar q3 sum d + q3^2 sum d^2.
-template <int MODE>
-__device__ __forceinline__ void fold(const Site32 &s, int n, Moments &m, double (&acc)[kNV]) {
-    const double dn = (double)n, q3 = (double)s.q3f;
-    const double a0 = m.a[0], a1 = m.a[1], b = m.b;
-    const MeanTraj &t = s.mt;
-    acc[0] += dn * (t.dfb0[0] * t.dfb0[0] + t.dfb0[1] * t.dfb0[1]) + 2. * (t.dfb0[0] * a0 + t.dfb0[1] * a1) + b;
-    acc[1] += (double)m.v0;
-    acc[2] -= (double)m.g0;
-    if constexpr (MODE != MODE_E0) {
-        const double c0 = m.c[0], c1 = m.c[1];
-        acc[3] += (double)m.v1;
-        acc[4] -= (double)m.g1;
-        acc[5] += dn * (t.pbar[0] * t.pbar[0] + t.pbar[1] * t.pbar[1]) + 2. * (t.pbar[0] * c0 + t.pbar[1] * c1) +
-                  (double)m.e;
-        acc[6] += dn * (t.pbar[0] * t.qbar[0] + t.pbar[1] * t.qbar[1]) + q3 * (t.pbar[0] * a0 + t.pbar[1] * a1) +
-                  (t.qbar[0] * c0 + t.qbar[1] * c1) + q3 * (double)m.f;
-        acc[7] += dn * (t.qbar[0] * t.qbar[0] + t.qbar[1] * t.qbar[1]) + 2. * q3 * (t.qbar[0] * a0 + t.qbar[1] * a1) +
-                  q3 * q3 * b;
-    }
-    zero(m);
 }
 
 // One site of sweep B: the new field and momentum of both fields.
@@ -309,7 +260,7 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
                 site_a32<MODE>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], mom, s0[v], s1[v]);
             }
             if (++ngroup == kGroup || i == i1 - 1) {
-                fold<MODE>(s, 2 * ngroup, mom, acc);
+                fold<MODE>(s.mt, s.q3f, 2 * ngroup, mom, acc);
                 ngroup = 0;
             }
             if constexpr (MODE == MODE_A_GW) {
