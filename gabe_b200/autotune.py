@@ -20,7 +20,9 @@ import numpy as np
 
 from . import FP32, FP64, GabeError, Lattice
 
-SHAPES = {0: (32, 8), 1: (16, 16), 2: (32, 4), 3: (16, 8), 4: (8, 8), 5: (4, 4)}  # FP64 sweeps, ensemble
+SHAPES = {0: (32, 8), 1: (16, 16), 2: (32, 4), 3: (16, 8), 4: (8, 8), 5: (4, 4)}  # FP64 sweeps
+# ensemble work items (sites along k x j, 256-thread blocks): ens_tile_k/j in csrc/ensemble.cuh
+ENS_SHAPES = {0: (64, 8), 1: (32, 16), 2: (16, 16)}
 # FP32 single-lattice sweeps (two sites per thread along k): kShapes32 in csrc/launch.h
 SHAPES32 = {0: (64, 8), 1: (64, 4), 2: (128, 4), 3: (32, 8), 4: (64, 16), 5: (32, 4), 6: (16, 8)}
 
@@ -57,40 +59,47 @@ def lookup(N: int, precision: int, gws: bool):
 
 
 def lookup_ensemble(N: int):
-    """(shape, ci) for ensemble lattices of size N (256-thread tiles only)."""
-    e = load_cache().get(f"{_gpu_name()}|ens|N={N}")
+    """(shape, ci) for ensemble lattices of size N, or None."""
+    e = load_cache().get(f"{_gpu_name()}|ens32|N={N}")
     return (e["shape"], e["ci"]) if e else None
 
 
-def tune_ensemble(sizes, steps: int = 3, verbose: bool = True) -> dict:
-    """Ensemble tiles per lattice size: the 256-thread shapes (32x8, 16x16)
-    and ci in {16, 32, 64}, timed on single FP32 GW lattices of that size."""
+def tune_ensemble(sizes, steps: int = 6, verbose: bool = True) -> dict:
+    """Ensemble tiles per lattice size: every shape of ENS_SHAPES that
+    divides N and ci in {8, 16, 32, 64}, timed (CUDA events on the
+    ensemble's stream) on an ensemble of ~32M sites of lattices of that size."""
+    import torch
+
+    from . import Ensemble
+
     out = {}
     cache = load_cache()
     for N in sizes:
-        rng = np.random.default_rng(1)
-        f = 0.342 + 1e-6 * rng.standard_normal((2, N, N, N))
-        f[1] -= 0.342
-        d = 1e-6 * rng.standard_normal((2, N, N, N))
+        nl = max(1, (1 << 25) // N ** 3)
         best = None
-        for shape in (0, 1):
-            tk, tj = SHAPES[shape]
+        for shape, (tk, tj) in ENS_SHAPES.items():
             if N % tk or N % tj:
                 continue
-            for ci in (16, 32, 64):
+            for ci in (8, 16, 32, 64):
                 if ci > N:
                     continue
-                with Lattice(N, gws=True, precision=FP32, tile_shape=shape, tile_ci=ci) as lat:
-                    lat.upload_state(f, d, a0=1.0, adot0=0.5)
-                    lat.profile_steps(1)
-                    ph = lat.profile_steps(steps)
-                t = ph["stage1"] + ph["stage2"]
+                with Ensemble([N] * nl, [100.0] * nl, [1.0] * nl, list(range(nl)), nlog=8,
+                              tiles=([shape] * nl, [ci] * nl)) as ens:
+                    ens.init()
+                    ens.step(2)
+                    st = torch.cuda.ExternalStream(ens.stream_ptr)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    ens.step(steps)
+                    e1.record(st)
+                    e1.synchronize()
+                    t = e0.elapsed_time(e1) / steps
                 if verbose:
-                    print(f"ens N={N} shape {SHAPES[shape]} ci {ci}: {t:.4f} ms", flush=True)
+                    print(f"ens N={N} x {nl} shape {ENS_SHAPES[shape]} ci {ci}: {t:.4f} ms/step", flush=True)
                 if best is None or t < best[2]:
                     best = (shape, ci, t)
-        cache[f"{_gpu_name()}|ens|N={N}"] = {"shape": best[0], "ci": best[1], "sweeps_ms": best[2],
-                                             "tile": SHAPES[best[0]]}
+        cache[f"{_gpu_name()}|ens32|N={N}"] = {"shape": best[0], "ci": best[1], "step_ms": best[2],
+                                               "lattices": nl, "tile": ENS_SHAPES[best[0]]}
         out[N] = best
     with open(CACHE, "w") as fh:
         json.dump(cache, fh, indent=1, sort_keys=True)
@@ -146,7 +155,7 @@ def main():
     ap.add_argument("--gws", type=int, default=1)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--ensemble", action="store_true", help="tune the ensemble's 256-thread tiles instead")
+    ap.add_argument("--ensemble", action="store_true", help="tune the ensemble's work-item tiles instead")
     a = ap.parse_args()
     if a.ensemble:
         return tune_ensemble(a.N, a.steps)

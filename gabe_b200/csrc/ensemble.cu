@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <map>
 #include <new>
@@ -50,7 +51,7 @@ struct gabe_ensemble {
     double *d_partials = nullptr;
     unsigned int *d_lat_count = nullptr;
     DevScalars *d_sc = nullptr;
-    size_t ktotal = 0;
+    int nkchunks = 0;
     void *fft_work = nullptr;
     double *d_m2 = nullptr, *d_sumsq = nullptr;
     double *d_part = nullptr, *d_log = nullptr, *d_logcnt = nullptr, *d_native = nullptr;
@@ -178,16 +179,23 @@ EnsArgs ens_args(gabe_ensemble *e, int cur) {
     return a;
 }
 
+template <int MODE>
+cudaError_t launch_sweep(const EnsArgs &a, cudaStream_t s) {
+    constexpr size_t smem = ens_ring_bytes();
+    cudaError_t r = cudaFuncSetAttribute(ens_sweep_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (r != cudaSuccess) return r;
+    ens_sweep_kernel<MODE><<<a.nitems, kEnsThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 int sweep(gabe_ensemble *e, int mode, int cur) {
     EnsArgs a = ens_args(e, cur);
-    const dim3 grid(148 * 2), block(256);
     switch (mode) {
-        case MODE_A: ens_sweep_kernel<MODE_A><<<grid, block, 0, e->stream>>>(a); break;
-        case MODE_A_GW: ens_sweep_kernel<MODE_A_GW><<<grid, block, 0, e->stream>>>(a); break;
-        case MODE_E0: ens_sweep_kernel<MODE_E0><<<grid, block, 0, e->stream>>>(a); break;
-        default: ens_sweep_kernel<MODE_B><<<grid, block, 0, e->stream>>>(a); break;
+        case MODE_A: ECK(e, launch_sweep<MODE_A>(a, e->stream)); break;
+        case MODE_A_GW: ECK(e, launch_sweep<MODE_A_GW>(a, e->stream)); break;
+        case MODE_E0: ECK(e, launch_sweep<MODE_E0>(a, e->stream)); break;
+        default: ECK(e, launch_sweep<MODE_B>(a, e->stream)); break;
     }
-    ECK(e, cudaGetLastError());
     return GABE_OK;
 }
 
@@ -196,7 +204,7 @@ int enqueue_step(gabe_ensemble *e, int cur) {
     if (rc) return rc;
     if (e->gws) {
         for (auto &G : e->groups) ECF(e, cufftExecR2C(G.plan_src, (cufftReal *)G.S, (cufftComplex *)G.S));
-        ens_kspace_kernel<<<148 * 8, 256, 0, e->stream>>>(ens_args(e, cur), e->ktotal);
+        ens_kspace_kernel<<<e->nkchunks, 256, 0, e->stream>>>(ens_args(e, cur));
         ECK(e, cudaGetLastError());
     }
     return sweep(e, MODE_B, cur);
@@ -231,8 +239,9 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
         if (n < 16 || n > 1024 || n % 16) return eset(nullptr, GABE_ERR_PARAM, "lattice %d: N=%d must be a multiple of 16 in [16,1024]", l, n);
         if (!(p->g2_over_lambda[l] >= 0) || !(p->amplitude[l] >= 0))
             return eset(nullptr, GABE_ERR_PARAM, "lattice %d: invalid coupling or amplitude", l);
-        if (p->tile_shape && (p->tile_shape[l] < 0 || p->tile_shape[l] > 1 || (p->tile_shape[l] == 0 && n % 32)))
-            return eset(nullptr, GABE_ERR_PARAM, "lattice %d: tile shape must be 0 (32x8, N%%32==0) or 1 (16x16)", l);
+        if (p->tile_shape && (p->tile_shape[l] < 0 || p->tile_shape[l] > 2 || n % ens_tile_k(p->tile_shape[l])))
+            return eset(nullptr, GABE_ERR_PARAM,
+                        "lattice %d: tile shape must be 0 (64x8, N%%64==0), 1 (32x16, N%%32==0) or 2 (16x16)", l);
     }
     gabe_ensemble *e = new (std::nothrow) gabe_ensemble();
     if (!e) return eset(nullptr, GABE_ERR_NOMEM, "host allocation failed");
@@ -252,7 +261,7 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
     e->amp.assign(p->amplitude, p->amplitude + p->nlat);
     e->seed.assign(p->seed, p->seed + p->nlat);
     for (int l = 0; l < p->nlat; l++) {
-        e->shape.push_back(p->tile_shape ? p->tile_shape[l] : (e->N[l] % 32 == 0 ? 0 : 1));
+        e->shape.push_back(p->tile_shape ? p->tile_shape[l] : (e->N[l] % 64 == 0 ? 0 : (e->N[l] % 32 == 0 ? 1 : 2)));
         int c = p->tile_ci && p->tile_ci[l] > 0 ? p->tile_ci[l] : 32;
         e->ci.push_back(std::min(c, e->N[l]));
     }
@@ -308,22 +317,26 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
             Lt.rescale_B = std::sqrt(e->lambda) * e->phi0;
         }
     }
-    // work list (lattice-major) and k-point offsets
+    // work list (lattice-major) and the k-space chunks of every lattice
     std::vector<EnsItem> items;
-    size_t kofs = 0;
+    size_t nkc = 0;
     for (int l = 0; l < e->nlat; l++) {
         EnsLat &Lt = e->h_lat[l];
-        const int n = e->N[l], TK = e->shape[l] == 0 ? 32 : 16, TJ = e->shape[l] == 0 ? 8 : 16, c = e->ci[l];
+        const int n = e->N[l], TK = ens_tile_k(e->shape[l]), TJ = ens_tile_j(e->shape[l]), c = e->ci[l];
         Lt.first_item = (int)items.size();
         for (int i0 = 0; i0 < n; i0 += c)
             for (int j0 = 0; j0 < n; j0 += TJ)
                 for (int k0 = 0; k0 < n; k0 += TK) items.push_back({l, e->shape[l], j0, k0, i0, std::min(i0 + c, n)});
         Lt.nitems = (int)items.size() - Lt.first_item;
-        Lt.kofs = kofs;
-        kofs += lattice_M(n);
+        Lt.first_kchunk = (int)nkc;
+        nkc += (lattice_M(n) + kEnsKChunk - 1) / kEnsKChunk;
+    }
+    if (items.size() > (size_t)INT32_MAX || nkc > (size_t)INT32_MAX) {
+        eset(e, GABE_ERR_PARAM, "ensemble too large for one launch");
+        return bail(GABE_ERR_PARAM);
     }
     e->nitems = (int)items.size();
-    e->ktotal = kofs;
+    e->nkchunks = (int)nkc;
     if ((rc = ealloc(e, (void **)&e->d_lat, sizeof(EnsLat) * e->nlat))) return bail(rc);
     if ((rc = ealloc(e, (void **)&e->d_items, sizeof(EnsItem) * e->nitems))) return bail(rc);
     // per-item partial sums; also the scratch of the upload's mean reduction (256 blocks)

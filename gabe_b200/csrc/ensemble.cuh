@@ -3,16 +3,17 @@
 //
 // Each step is the single-lattice step (stencil.cuh, kspace.cuh) issued once
 // for the whole ensemble:
-//   * sweep A and sweep B are persistent kernels over a work list of
-//     (lattice, column tile, plane chunk) items, 256 threads per block; each
-//     item runs the same per-tile march as the single-lattice kernel with the
-//     tile shape the autotuner chose for that lattice size (32x8 or 16x16);
-//     per-item partial sums are combined by the block that finishes the last
-//     item of a lattice, in item order, so every lattice gets its own
-//     Friedmann update without a grid-wide barrier;
+//   * sweep A and sweep B take one work item (lattice, column tile, plane
+//     chunk) per 256-thread block; each item runs the FP32 plane march of
+//     the single-lattice sweeps (sweep32.cuh: cp.async plane ring, two sites
+//     per thread) with the tile shape chosen for that lattice size (64x8,
+//     32x16 or 16x16 sites); per-item partial sums are combined by the block
+//     that finishes the last item of a lattice, in item order, so every
+//     lattice gets its own Friedmann update without a grid-wide barrier;
 //   * the GW transforms are one cuFFT call per lattice size (batch = 10 x
 //     lattices of that size, sources of a size group contiguous);
-//   * the k-space update is one kernel over the concatenated half spectra.
+//   * the k-space update is one kernel over the half spectra of all
+//     lattices, in chunks of one lattice per block.
 // The initial state is drawn on the device with the reference's randInit
 // distribution (g2init.cpp:68-189) from a counter-based generator (Philox
 // 4x32-10, Salmon et al., SC'11), so it matches the reference in
@@ -22,7 +23,7 @@
 #include <math_constants.h>
 
 #include "kspace.cuh"
-#include "stencil.cuh"
+#include "sweep32.cuh"
 
 namespace gabe {
 
@@ -32,9 +33,9 @@ struct EnsLat {
     float *S;            // [10][N][N][N+2] sources / [..][N][N][N/2+1] spectra
     Cplx<float> *G;      // [4][M] h+, hx, l+, lx
     DevScalars *sc;
-    size_t kofs;         // offset of this lattice's k-points in the ensemble k index
+    int first_kchunk;    // first block of the k-space update that takes this lattice
     int first_item, nitems;
-    int N, pad;
+    int N;
     unsigned long long seed;  // IC: counter-based generator key
     double amp;               // IC: amplitude multiplier
     double rescale_B;         // B of the program units
@@ -54,133 +55,99 @@ struct EnsArgs {
 };
 
 // ---------------------------------------------------------------------------
-// persistent sweep over the work list
+// sweeps over the work list: one item (lattice, column tile, plane chunk) per
+// block, the FP32 plane march of the single-lattice sweeps (sweep32.cuh)
 // ---------------------------------------------------------------------------
+constexpr int kEnsThreads = 256;
+constexpr int kEnsRing = 6;  // plane slots of the cp.async ring
+
+// Tile shapes of the work items, sites along k x j: 0 = 64 x 8, 1 = 32 x 16,
+// 2 = 16 x 16 (128 of the 256 threads march; for N = 16 (mod 32)).
+__host__ __device__ constexpr int ens_tile_k(int shape) { return shape == 0 ? 64 : (shape == 1 ? 32 : 16); }
+__host__ __device__ constexpr int ens_tile_j(int shape) { return shape == 0 ? 8 : 16; }
+constexpr size_t ens_ring_bytes() {
+    constexpr int a = s32::Ring<32, 8>::SLOT, b = s32::Ring<16, 16>::SLOT, c = s32::Ring<8, 16>::SLOT;
+    return sizeof(float) * kEnsRing * (a > b ? (a > c ? a : c) : (b > c ? b : c));
+}
+
 template <int MODE>
-__global__ void __launch_bounds__(256, 2) ens_sweep_kernel(EnsArgs a) {
-    __shared__ __align__(16) float smem[2][4 * SweepSmem<32, 8>::P];
-    __shared__ double sred[8 * kNV];
+__global__ void __launch_bounds__(kEnsThreads, s32::sweep32_threads_per_sm<MODE>() / kEnsThreads)
+    ens_sweep_kernel(EnsArgs a) {
+    extern __shared__ __align__(16) float ring[];
+    __shared__ double sred[(kEnsThreads / 32) * kNV];
     __shared__ int sflag;
-    static_assert(SweepSmem<16, 16>::P <= SweepSmem<32, 8>::P, "shared tile too small");
-    const int tid = threadIdx.x;
-    for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
-        const EnsItem item = a.items[it];
-        const EnsLat &L = a.lat[item.lat];
-        const LatticeConsts c = L.c;
-        TileJob<float> job;
-        job.X = L.X[a.cur];
-        job.D = L.D[a.cur];
-        job.Xo = L.X[a.cur ^ 1];
-        job.Do = L.D[a.cur ^ 1];
-        job.S = L.S;
-        job.sc = L.sc;
-        job.j0 = item.j0;
-        job.k0 = item.k0;
-        job.i0 = item.i0;
-        job.i1 = item.i1;
-        double acc[kNV];
+    const int tid = threadIdx.x, it = blockIdx.x;
+    const EnsItem item = a.items[it];
+    const EnsLat &L = a.lat[item.lat];
+    const LatticeConsts c = L.c;
+    s32::Tile32 t;
+    t.X = L.X[a.cur];
+    t.D = L.D[a.cur];
+    t.Xo = L.X[a.cur ^ 1];
+    t.Do = L.D[a.cur ^ 1];
+    t.S = L.S;
+    t.k0 = item.k0;
+    t.j0 = item.j0;
+    t.i0 = item.i0;
+    t.i1 = item.i1;
+    const s32::Site32 s = s32::site32_consts<MODE>(c, L.sc);
+    double acc[kNV];
 #pragma unroll
-        for (int q = 0; q < kNV; q++) acc[q] = 0.;
-        if (item.shape == 0) sweep_tile<float, 32, 8, MODE>(c, job, smem[0], smem[1], acc);
-        else sweep_tile<float, 16, 16, MODE>(c, job, smem[0], smem[1], acc);
-        if constexpr (MODE != MODE_B) {
-            block_reduce<kNV>(acc, sred);
-            if (tid == 0)
-                for (int q = 0; q < kNV; q++) a.partials[(size_t)it * kNV + q] = acc[q];
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) sflag = atomicAdd(&a.lat_count[item.lat], 1u) == (unsigned)(L.nitems - 1);
-        __syncthreads();
-        if (sflag) {
-            __threadfence();
-            if constexpr (MODE != MODE_B) {
-                double tot[kNV];
-                sum_partials<kNV>(a.partials + (size_t)L.first_item * kNV, L.nitems, tot, sred);
-                if (tid == 0) finish_a<float, MODE>(c, L.sc, tot, a.slot);
-            } else if (tid == 0) {
-                finish_b<float>(c, L.sc);
-            }
-            if (tid == 0) a.lat_count[item.lat] = 0u;
-        }
-        __syncthreads();
+    for (int q = 0; q < kNV; q++) acc[q] = 0.;
+    if (item.shape == 0) s32::march32<32, 8, MODE, kEnsRing, kEnsThreads>(c, s, t, ring, acc);
+    else if (item.shape == 1) s32::march32<16, 16, MODE, kEnsRing, kEnsThreads>(c, s, t, ring, acc);
+    else s32::march32<8, 16, MODE, kEnsRing, kEnsThreads>(c, s, t, ring, acc);
+    if constexpr (MODE != MODE_B) {
+        block_reduce<kNV>(acc, sred);
+        if (tid == 0)
+            for (int q = 0; q < kNV; q++) a.partials[(size_t)it * kNV + q] = acc[q];
     }
+    // the block that completes a lattice's last item takes its scalar update
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) sflag = atomicAdd(&a.lat_count[item.lat], 1u) == (unsigned)(L.nitems - 1);
+    __syncthreads();
+    if (!sflag) return;
+    __threadfence();
+    if constexpr (MODE != MODE_B) {
+        double tot[kNV];
+        sum_partials<kNV>(a.partials + (size_t)L.first_item * kNV, L.nitems, tot, sred);
+        if (tid == 0) finish_a<float, MODE>(c, L.sc, tot, a.slot);
+    } else if (tid == 0) {
+        finish_b<float>(c, L.sc);
+    }
+    if (tid == 0) a.lat_count[item.lat] = 0u;
 }
 
 // ---------------------------------------------------------------------------
-// k-space update over all lattices (same per-point arithmetic as kspace.cuh)
+// k-space update over all lattices: block b takes chunk b of the concatenated
+// half spectra (chunks never straddle two lattices), the per-point update of
+// the single-lattice kernel (kspace.cuh kspace_point)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int ens_find(const EnsLat *lat, int nlat, size_t g) {
+constexpr int kEnsKChunk = 4096;  // k-points per block
+
+__device__ __forceinline__ int ens_find_kchunk(const EnsLat *lat, int nlat, int b) {
     int lo = 0, hi = nlat - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (lat[mid].kofs <= g) lo = mid;
+        if (lat[mid].first_kchunk <= b) lo = mid;
         else hi = mid - 1;
     }
     return lo;
 }
 
-__global__ void __launch_bounds__(256) ens_kspace_kernel(EnsArgs a, size_t ktotal) {
-    for (size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x; g < ktotal; g += (size_t)gridDim.x * blockDim.x) {
-        const int e = ens_find(a.lat, a.nlat, g);
-        const EnsLat &L = a.lat[e];
-        const int N = L.N, nz = N / 2 + 1;
-        const size_t M = (size_t)N * N * nz, idx = g - L.kofs;
-        const double *g4 = L.sc->gw[a.slot];
-        const double a0 = g4[0], ad0 = g4[1], a1 = g4[2], ad1 = g4[3];
-        const LatticeConsts &c = L.c;
-        const Cplx<float> *Sc = reinterpret_cast<const Cplx<float> *>(L.S);
-        Cplx<float> s[10], gg[4];
-#pragma unroll
-        for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
-#pragma unroll
-        for (int q = 0; q < 4; q++) gg[q] = L.G[(size_t)q * M + idx];
-        const int kzi = (int)(idx % nz);
-        const size_t t = idx / nz;
-        const int j = (int)(t % N), i = (int)(t / N);
-        const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
-        const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
-        if (m2 == 0.0) continue;
-        double ep[6], ex[6];
-        pol_tensors(px, py, kzi, ep, ex);
-        const float wp[5] = {(float)(0.5 * (ep[0] - ep[5])), (float)ep[1], (float)ep[2], (float)(0.5 * (ep[3] - ep[5])),
-                             (float)ep[4]};
-        const float wx[5] = {(float)(0.5 * (ex[0] - ex[5])), (float)ex[1], (float)ex[2], (float)(0.5 * (ex[3] - ex[5])),
-                             (float)ex[4]};
-        const float kk0 = (float)(m2 * (c.k2norm_c / a0 / a0)), kk1 = (float)(m2 * (c.k2norm_c / a1 / a1));
-        const float c3H0 = (float)(3. * ad0 / a0), c3H1 = (float)(3. * ad1 / a1);
-        const float src0 = (float)(2. * (c.eight_pi / a0 / a0) * c.normmm);
-        const float src1 = (float)(2. * (c.eight_pi / a1 / a1) * c.normmm);
-        const float hdt = (float)c.half_dt, dt = (float)c.dt;
-        float Tp[2][2][2];
-#pragma unroll
-        for (int st = 0; st < 2; st++) {
-            float sr[5], si[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) { sr[q] = s[5 * st + q].re; si[q] = s[5 * st + q].im; }
-            const float f = st == 0 ? src0 : src1;
-            Tp[st][0][0] = f * pol_contract(wp, sr);
-            Tp[st][0][1] = f * pol_contract(wp, si);
-            Tp[st][1][0] = f * pol_contract(wx, sr);
-            Tp[st][1][1] = f * pol_contract(wx, si);
-        }
-#pragma unroll
-        for (int p = 0; p < 2; p++) {
-            Cplx<float> hn, ln;
-#pragma unroll
-            for (int ri = 0; ri < 2; ri++) {
-                const float h0 = ri ? gg[p].im : gg[p].re, l0 = ri ? gg[2 + p].im : gg[2 + p].re;
-                const float ld0 = -kk0 * h0 - c3H0 * l0 + Tp[0][p][ri];
-                const float h1 = h0 + hdt * l0;
-                const float l1 = l0 + hdt * ld0;
-                const float ld1 = -kk1 * h1 - c3H1 * l1 + Tp[1][p][ri];
-                (ri ? hn.im : hn.re) = h0 + dt * l1;
-                (ri ? ln.im : ln.re) = l0 + dt * ld1;
-            }
-            L.G[(size_t)p * M + idx] = hn;
-            L.G[(size_t)(2 + p) * M + idx] = ln;
-        }
-    }
+__global__ void __launch_bounds__(256) ens_kspace_kernel(EnsArgs a) {
+    __shared__ int s_lat;
+    if (threadIdx.x == 0) s_lat = ens_find_kchunk(a.lat, a.nlat, blockIdx.x);
+    __syncthreads();
+    const EnsLat &L = a.lat[s_lat];
+    const int N = L.N;
+    const size_t M = (size_t)N * N * (N / 2 + 1);
+    const size_t m0 = (size_t)(blockIdx.x - L.first_kchunk) * kEnsKChunk;
+    const size_t m1 = m0 + kEnsKChunk < M ? m0 + kEnsKChunk : M;
+    const KsCoef<float> kc = ks_coef<float>(L.c, L.sc->gw[a.slot]);
+    const Cplx<float> *Sc = reinterpret_cast<const Cplx<float> *>(L.S);
+    for (size_t idx = m0 + threadIdx.x; idx < m1; idx += blockDim.x) kspace_point<float>(kc, N, M, Sc, L.G, idx);
 }
 
 // ---------------------------------------------------------------------------

@@ -68,71 +68,95 @@ __device__ __forceinline__ T pol_contract(const T *w, const T *S) {
     return w[0] * S[0] + w[1] * S[1] + w[2] * S[2] + w[3] * S[3] + w[4] * S[4];
 }
 
+// derivs() coefficients (g2evolutionpert.cpp:486-501) of both RK2 stages of
+// one step, from the scale factor and its derivative at the two stages.
+template <typename T>
+struct KsCoef {
+    double norm0, norm1;  // k^2 / a^2 per |n|^2
+    T c3H0, c3H1, src0, src1, hdt, dt;
+};
+
+template <typename T>
+__device__ __forceinline__ KsCoef<T> ks_coef(const LatticeConsts &c, const double *g4) {
+    const double a0 = g4[0], ad0 = g4[1], a1 = g4[2], ad1 = g4[3];
+    KsCoef<T> k;
+    k.norm0 = c.k2norm_c / a0 / a0;
+    k.norm1 = c.k2norm_c / a1 / a1;
+    const double om0 = c.eight_pi / a0 / a0, om1 = c.eight_pi / a1 / a1;
+    k.c3H0 = (T)(3. * ad0 / a0);
+    k.c3H1 = (T)(3. * ad1 / a1);
+    k.src0 = (T)(2. * om0 * c.normmm);
+    k.src1 = (T)(2. * om1 * c.normmm);
+    k.hdt = (T)c.half_dt;
+    k.dt = (T)c.dt;
+    return k;
+}
+
+// Both RK2 stages of the amplitudes of k-point idx of the half spectrum
+// [N][N][N/2+1] (M points): sources Sc [10][M], amplitudes G [4][M].
+template <typename T>
+__device__ __forceinline__ void kspace_point(const KsCoef<T> &kc, int N, size_t M, const Cplx<T> *Sc, Cplx<T> *G,
+                                             size_t idx) {
+    const int nz = N / 2 + 1;
+    Cplx<T> s[10], g[4];
+#pragma unroll
+    for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
+#pragma unroll
+    for (int q = 0; q < 4; q++) g[q] = G[(size_t)q * M + idx];
+    const int kzi = (int)(idx % nz);
+    const size_t t = idx / nz;
+    const int j = (int)(t % N), i = (int)(t / N);
+    const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
+    const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
+    if (m2 == 0.0) return;  // no TT mode at k = 0; its amplitudes stay zero
+    double ep[6], ex[6];
+    pol_tensors(px, py, kzi, ep, ex);
+    // weights of (S11, S12, S13, S22, S23) in eps:S/2 with S33 = -S11-S22
+    const T wp[5] = {(T)(0.5 * (ep[0] - ep[5])), (T)ep[1], (T)ep[2], (T)(0.5 * (ep[3] - ep[5])), (T)ep[4]};
+    const T wx[5] = {(T)(0.5 * (ex[0] - ex[5])), (T)ex[1], (T)ex[2], (T)(0.5 * (ex[3] - ex[5])), (T)ex[4]};
+    const T kk0 = (T)(m2 * kc.norm0), kk1 = (T)(m2 * kc.norm1);
+    T Tp[2][2][2];  // [stage][pol][re/im], already times 2 (8 pi/a^2) dx^3
+#pragma unroll
+    for (int st = 0; st < 2; st++) {
+        T sr[5], si[5];
+#pragma unroll
+        for (int q = 0; q < 5; q++) { sr[q] = s[5 * st + q].re; si[q] = s[5 * st + q].im; }
+        const T f = st == 0 ? kc.src0 : kc.src1;
+        Tp[st][0][0] = f * pol_contract(wp, sr);
+        Tp[st][0][1] = f * pol_contract(wp, si);
+        Tp[st][1][0] = f * pol_contract(wx, sr);
+        Tp[st][1][1] = f * pol_contract(wx, si);
+    }
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+        Cplx<T> hn, ln;
+#pragma unroll
+        for (int ri = 0; ri < 2; ri++) {
+            const T h0 = ri ? g[p].im : g[p].re, l0 = ri ? g[2 + p].im : g[2 + p].re;
+            // stage 1: evolve_perts(0, 1, dt/2)
+            const T ld0 = -kk0 * h0 - kc.c3H0 * l0 + Tp[0][p][ri];
+            const T h1 = h0 + kc.hdt * l0;
+            const T l1 = l0 + kc.hdt * ld0;
+            // stage 2: evolve_perts(1, 0, dt)
+            const T ld1 = -kk1 * h1 - kc.c3H1 * l1 + Tp[1][p][ri];
+            (ri ? hn.im : hn.re) = h0 + kc.dt * l1;
+            (ri ? ln.im : ln.re) = l0 + kc.dt * ld1;
+        }
+        G[(size_t)p * M + idx] = hn;
+        G[(size_t)(2 + p) * M + idx] = ln;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) kspace_kernel(KspaceArgs args) {
     const LatticeConsts &c = args.c;
-    const int N = c.N, nz = N / 2 + 1;
-    const size_t M = (size_t)N * N * nz;
-    const double *g4 = args.sc->gw[args.slot];
-    const double a0 = g4[0], ad0 = g4[1], a1 = g4[2], ad1 = g4[3];
-    // derivs() coefficients (g2evolutionpert.cpp:486-501) for both stages
-    const double norm0 = c.k2norm_c / a0 / a0, norm1 = c.k2norm_c / a1 / a1;
-    const double om0 = c.eight_pi / a0 / a0, om1 = c.eight_pi / a1 / a1;
-    const T c3H0 = (T)(3. * ad0 / a0), c3H1 = (T)(3. * ad1 / a1);
-    const T src0 = (T)(2. * om0 * c.normmm), src1 = (T)(2. * om1 * c.normmm);
-    const T hdt = (T)c.half_dt, dt = (T)c.dt;
+    const int N = c.N;
+    const size_t M = (size_t)N * N * (N / 2 + 1);
+    const KsCoef<T> kc = ks_coef<T>(c, args.sc->gw[args.slot]);
     const Cplx<T> *Sc = static_cast<const Cplx<T> *>(args.S);
     Cplx<T> *G = static_cast<Cplx<T> *>(args.G);
-
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < M; idx += (size_t)gridDim.x * blockDim.x) {
-        Cplx<T> s[10], g[4];
-#pragma unroll
-        for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
-#pragma unroll
-        for (int q = 0; q < 4; q++) g[q] = G[(size_t)q * M + idx];
-        const int kzi = (int)(idx % nz);
-        const size_t t = idx / nz;
-        const int j = (int)(t % N), i = (int)(t / N);
-        const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
-        const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
-        if (m2 == 0.0) continue;  // no TT mode at k = 0; its amplitudes stay zero
-        double ep[6], ex[6];
-        pol_tensors(px, py, kzi, ep, ex);
-        // weights of (S11, S12, S13, S22, S23) in eps:S/2 with S33 = -S11-S22
-        const T wp[5] = {(T)(0.5 * (ep[0] - ep[5])), (T)ep[1], (T)ep[2], (T)(0.5 * (ep[3] - ep[5])), (T)ep[4]};
-        const T wx[5] = {(T)(0.5 * (ex[0] - ex[5])), (T)ex[1], (T)ex[2], (T)(0.5 * (ex[3] - ex[5])), (T)ex[4]};
-        const T kk0 = (T)(m2 * norm0), kk1 = (T)(m2 * norm1);
-        T Tp[2][2][2];  // [stage][pol][re/im], already times 2 (8 pi/a^2) dx^3
-#pragma unroll
-        for (int st = 0; st < 2; st++) {
-            T sr[5], si[5];
-#pragma unroll
-            for (int q = 0; q < 5; q++) { sr[q] = s[5 * st + q].re; si[q] = s[5 * st + q].im; }
-            const T f = st == 0 ? src0 : src1;
-            Tp[st][0][0] = f * pol_contract(wp, sr);
-            Tp[st][0][1] = f * pol_contract(wp, si);
-            Tp[st][1][0] = f * pol_contract(wx, sr);
-            Tp[st][1][1] = f * pol_contract(wx, si);
-        }
-#pragma unroll
-        for (int p = 0; p < 2; p++) {
-            Cplx<T> hn, ln;
-#pragma unroll
-            for (int ri = 0; ri < 2; ri++) {
-                const T h0 = ri ? g[p].im : g[p].re, l0 = ri ? g[2 + p].im : g[2 + p].re;
-                // stage 1: evolve_perts(0, 1, dt/2)
-                const T ld0 = -kk0 * h0 - c3H0 * l0 + Tp[0][p][ri];
-                const T h1 = h0 + hdt * l0;
-                const T l1 = l0 + hdt * ld0;
-                // stage 2: evolve_perts(1, 0, dt)
-                const T ld1 = -kk1 * h1 - c3H1 * l1 + Tp[1][p][ri];
-                (ri ? hn.im : hn.re) = h0 + dt * l1;
-                (ri ? ln.im : ln.re) = l0 + dt * ld1;
-            }
-            G[(size_t)p * M + idx] = hn;
-            G[(size_t)(2 + p) * M + idx] = ln;
-        }
-    }
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < M; idx += (size_t)gridDim.x * blockDim.x)
+        kspace_point<T>(kc, N, M, Sc, G, idx);
 }
 
 // ---------------------------------------------------------------------------

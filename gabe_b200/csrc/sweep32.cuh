@@ -135,29 +135,37 @@ constexpr int sweep32_threads_per_sm() {
     return (MODE == MODE_A_GW || MODE == MODE_A) ? 512 : 768;
 }
 
-template <int TK2, int TJ, int MODE, int S>
-__global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2 * TJ - 1) / (TK2 * TJ))
-    sweep32_kernel(StencilArgs args) {
+// Pointers and bounds of one column tile of one lattice.
+struct Tile32 {
+    const float *X, *D;  // fields and momenta of the current state, [2][N^3]
+    float *Xo, *Do;      // new fields and momenta (sweep B)
+    float *S;            // GW sources [10][N][N][N+2] (sweep A with sources)
+    int k0, j0, i0, i1;
+};
+
+// The plane march of one TK x TJ tile over planes i0 .. i1-1 by a block of NT
+// threads (NT >= TK2 TJ; threads beyond TK2 TJ only take part in the
+// barriers).  Sweep A / E0 add the tile's folded sums to acc (per-thread
+// partials, zero on idle threads); sweep B writes the new state.
+template <int TK2, int TJ, int MODE, int S, int NT>
+__device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s, const Tile32 &t, float *ring,
+                                        double (&acc)[kNV]) {
     using Rg = Ring<TK2, TJ>;
     constexpr int TK = Rg::TK, PK = Rg::PK;
     static_assert(S >= 4, "ring needs planes i-1, i, i+1 and one in flight");
     static_assert(TK2 * TJ >= 2 * TK2 + 2 * TJ, "enough threads for the halo copies");
-    extern __shared__ __align__(16) float ring[];  // S slots
-    __shared__ double sred[((TK2 * TJ + 31) / 32) * kNV];
-    __shared__ int sflag;
-
-    const LatticeConsts &c = args.c;
+    static_assert(NT >= TK2 * TJ, "block smaller than the tile");
     const int N = c.N;
-    const size_t n3 = (size_t)N * N * N;
-    const int tid = threadIdx.x, tx = tid % TK2, ty = tid / TK2;
-    const int k0 = blockIdx.x * TK, j0 = blockIdx.y * TJ;
-    const int i0 = blockIdx.z * args.ci, i1 = min(i0 + args.ci, N);
+    const int n3 = N * N * N;  // N^3 < 2^31 for N <= 1024
+    const int tid = threadIdx.x;
+    const bool act = NT == TK2 * TJ || tid < TK2 * TJ;
+    const int tx = tid % TK2, ty = tid / TK2;
+    const int k0 = t.k0, j0 = t.j0, i0 = t.i0, i1 = t.i1;
     const int j = j0 + ty, k = k0 + 2 * tx;
-    const float *X = static_cast<const float *>(args.X), *D = static_cast<const float *>(args.D);
-    const float *src[4] = {X, X + n3, D, D + n3};
+    const float *src[4] = {t.X, t.X + n3, t.D, t.D + n3};
 
-    // 32-bit element offsets (N^3 < 2^31 for N <= 1024): own pair and halo
-    // points within a plane; planes are p N^2
+    // element offsets of the own pair and the halo points within a plane;
+    // planes are p N^2
     const int NN = N * N;
     const int jm = wrapi(j0 - 1, N), jp = wrapi(j0 + TJ, N), km = wrapi(k0 - 1, N), kp = wrapi(k0 + TK, N);
     const int o_own = j * N + k;
@@ -178,6 +186,7 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
         h_go = (j0 + q) * N + (r ? kp : km);
     }
     auto issue = [&](int p, int sl) {  // plane p (wrapped) into slot sl
+        if (!act) return;
         float *slot = ring + sl * Rg::SLOT;
         const int pb = wrapi(p, N) * NN;
 #pragma unroll
@@ -191,10 +200,6 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
     };
     auto next_slot = [](int sl) { return sl + 1 == S ? 0 : sl + 1; };
 
-    const Site32 s = site32_consts<MODE>(c, args.sc);
-    double acc[kNV];
-#pragma unroll
-    for (int q = 0; q < kNV; q++) acc[q] = 0.;
     Moments mom;
     zero(mom);
     int ngroup = 0;  // planes in the current moment group
@@ -209,9 +214,7 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
     // slots of planes i-1, i, i+1 and of the plane issued next (i+S-2)
     int s_pr = 0, s_cu = 1, s_nx = 2, s_is = S - 1;
     float2 pr[4], cu[4];  // own pair of planes i-1 and i
-    float *Xo0 = static_cast<float *>(args.Xo), *Do0 = static_cast<float *>(args.Do);
-    float *Sg = static_cast<float *>(args.S);
-    const size_t sstride = (size_t)NN * (N + 2);  // one source component
+    const int sstride = NN * (N + 2);  // one source component
     const int so_row = j * (N + 2) + k;
     for (int i = i0; i < i1; i++) {
         cp_wait<S - 4>();  // planes up to i+1 have landed (this thread's copies)
@@ -219,62 +222,66 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
         if (i + S - 2 <= i1) issue(i + S - 2, s_is);  // into the slot of plane i-2
         cp_commit();
 
-        const float *sc = ring + s_cu * Rg::SLOT;
-        const float *sn = ring + s_nx * Rg::SLOT;
-        if (i == i0) {
-            const float *sp = ring + s_pr * Rg::SLOT;
+        if (act) {
+            const float *sc = ring + s_cu * Rg::SLOT;
+            const float *sn = ring + s_nx * Rg::SLOT;
+            if (i == i0) {
+                const float *sp = ring + s_pr * Rg::SLOT;
+#pragma unroll
+                for (int a = 0; a < 4; a++) {
+                    pr[a] = *reinterpret_cast<const float2 *>(sp + a * Rg::ARR + so_own);
+                    cu[a] = *reinterpret_cast<const float2 *>(sc + a * Rg::ARR + so_own);
+                }
+            }
+            Nb7<float> nb[4][2];  // [array][site]
+            float2 nx[4];
 #pragma unroll
             for (int a = 0; a < 4; a++) {
-                pr[a] = *reinterpret_cast<const float2 *>(sp + a * Rg::ARR + so_own);
-                cu[a] = *reinterpret_cast<const float2 *>(sc + a * Rg::ARR + so_own);
+                const int ao = a * Rg::ARR + so_own;
+                nx[a] = *reinterpret_cast<const float2 *>(sn + ao);
+                const float2 up = *reinterpret_cast<const float2 *>(sc + ao + PK);
+                const float2 dn = *reinterpret_cast<const float2 *>(sc + ao - PK);
+                const float lm = sc[ao - 1], rp = sc[ao + 2];
+                // reference neighbour order: centre, i+1, i-1, j+1, j-1, k+1, k-1
+                nb[a][0] = Nb7<float>{{cu[a].x, nx[a].x, pr[a].x, up.x, dn.x, cu[a].y, lm}};
+                nb[a][1] = Nb7<float>{{cu[a].y, nx[a].y, pr[a].y, up.y, dn.y, rp, cu[a].x}};
             }
-        }
-        Nb7<float> nb[4][2];  // [array][site]
-        float2 nx[4];
+            if constexpr (MODE == MODE_B) {
+                float xo[2][2], dout[2][2];  // [site][field]
 #pragma unroll
-        for (int a = 0; a < 4; a++) {
-            const int ao = a * Rg::ARR + so_own;
-            nx[a] = *reinterpret_cast<const float2 *>(sn + ao);
-            const float2 up = *reinterpret_cast<const float2 *>(sc + ao + PK);
-            const float2 dn = *reinterpret_cast<const float2 *>(sc + ao - PK);
-            const float lm = sc[ao - 1], rp = sc[ao + 2];
-            // reference neighbour order: centre, i+1, i-1, j+1, j-1, k+1, k-1
-            nb[a][0] = Nb7<float>{{cu[a].x, nx[a].x, pr[a].x, up.x, dn.x, cu[a].y, lm}};
-            nb[a][1] = Nb7<float>{{cu[a].y, nx[a].y, pr[a].y, up.y, dn.y, rp, cu[a].x}};
-        }
-        if constexpr (MODE == MODE_B) {
-            float xo[2][2], dout[2][2];  // [site][field]
+                for (int v = 0; v < 2; v++) {
+                    site_b32(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], xo[v], dout[v]);
+                }
+                const int gx = i * NN + o_own;
+                __stcs(reinterpret_cast<float2 *>(t.Xo + gx), make_float2(xo[0][0], xo[1][0]));
+                __stcs(reinterpret_cast<float2 *>(t.Xo + n3 + gx), make_float2(xo[0][1], xo[1][1]));
+                __stcs(reinterpret_cast<float2 *>(t.Do + gx), make_float2(dout[0][0], dout[1][0]));
+                __stcs(reinterpret_cast<float2 *>(t.Do + n3 + gx), make_float2(dout[0][1], dout[1][1]));
+            } else {
+                float s0[2][kSrc] = {}, s1[2][kSrc] = {};
 #pragma unroll
-            for (int v = 0; v < 2; v++) {
-                site_b32(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], xo[v], dout[v]);
+                for (int v = 0; v < 2; v++) {
+                    site_a32<MODE>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], mom, s0[v], s1[v]);
+                }
+                if (++ngroup == kGroup || i == i1 - 1) {
+                    fold<MODE>(s.mt, s.q3f, 2 * ngroup, mom, acc);
+                    ngroup = 0;
+                }
+                if constexpr (MODE == MODE_A_GW) {
+                    float *g = t.S + (i * (N * (N + 2)) + so_row);
+#pragma unroll
+                    for (int q = 0; q < kSrc; q++, g += sstride)
+                        __stcs(reinterpret_cast<float2 *>(g), make_float2(s0[0][q], s0[1][q]));
+#pragma unroll
+                    for (int q = 0; q < kSrc; q++, g += sstride)
+                        __stcs(reinterpret_cast<float2 *>(g), make_float2(s1[0][q], s1[1][q]));
+                }
             }
-            const int gx = i * NN + o_own;
-            __stcs(reinterpret_cast<float2 *>(Xo0 + gx), make_float2(xo[0][0], xo[1][0]));
-            __stcs(reinterpret_cast<float2 *>(Xo0 + n3 + gx), make_float2(xo[0][1], xo[1][1]));
-            __stcs(reinterpret_cast<float2 *>(Do0 + gx), make_float2(dout[0][0], dout[1][0]));
-            __stcs(reinterpret_cast<float2 *>(Do0 + n3 + gx), make_float2(dout[0][1], dout[1][1]));
-        } else {
-            float s0[2][kSrc] = {}, s1[2][kSrc] = {};
 #pragma unroll
-            for (int v = 0; v < 2; v++) {
-                site_a32<MODE>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], mom, s0[v], s1[v]);
+            for (int a = 0; a < 4; a++) {
+                pr[a] = cu[a];
+                cu[a] = nx[a];
             }
-            if (++ngroup == kGroup || i == i1 - 1) {
-                fold<MODE>(s.mt, s.q3f, 2 * ngroup, mom, acc);
-                ngroup = 0;
-            }
-            if constexpr (MODE == MODE_A_GW) {
-                float *g = Sg + (i * (N * (N + 2)) + so_row);
-#pragma unroll
-                for (int q = 0; q < kSrc; q++, g += sstride) __stcs(reinterpret_cast<float2 *>(g), make_float2(s0[0][q], s0[1][q]));
-#pragma unroll
-                for (int q = 0; q < kSrc; q++, g += sstride) __stcs(reinterpret_cast<float2 *>(g), make_float2(s1[0][q], s1[1][q]));
-            }
-        }
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-            pr[a] = cu[a];
-            cu[a] = nx[a];
         }
         s_pr = s_cu;
         s_cu = s_nx;
@@ -282,6 +289,35 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
         s_is = next_slot(s_is);
     }
     cp_wait<0>();
+    __syncthreads();  // the ring may be refilled by the block's next tile
+}
+
+template <int TK2, int TJ, int MODE, int S>
+__global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2 * TJ - 1) / (TK2 * TJ))
+    sweep32_kernel(StencilArgs args) {
+    extern __shared__ __align__(16) float ring[];  // S slots
+    __shared__ double sred[((TK2 * TJ + 31) / 32) * kNV];
+    __shared__ int sflag;
+
+    const LatticeConsts &c = args.c;
+    const int N = c.N;
+    const int tid = threadIdx.x;
+    Tile32 t;
+    t.X = static_cast<const float *>(args.X);
+    t.D = static_cast<const float *>(args.D);
+    t.Xo = static_cast<float *>(args.Xo);
+    t.Do = static_cast<float *>(args.Do);
+    t.S = static_cast<float *>(args.S);
+    t.k0 = blockIdx.x * 2 * TK2;
+    t.j0 = blockIdx.y * TJ;
+    t.i0 = blockIdx.z * args.ci;
+    t.i1 = min(t.i0 + args.ci, N);
+
+    const Site32 s = site32_consts<MODE>(c, args.sc);
+    double acc[kNV];
+#pragma unroll
+    for (int q = 0; q < kNV; q++) acc[q] = 0.;
+    march32<TK2, TJ, MODE, S, TK2 * TJ>(c, s, t, ring, acc);
 
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if constexpr (MODE != MODE_B) {

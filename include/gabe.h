@@ -227,7 +227,8 @@ typedef struct {
     const double *g2_over_lambda;   /* [nlat] coupling of V = lambda phi^4/4 + g^2 phi^2 chi^2/2 */
     const double *amplitude;        /* [nlat] multiplier of the randInit amplitudes (g2init.cpp:136-143) */
     const uint64_t *seed;           /* [nlat] generator seeds */
-    const int32_t *tile_shape;      /* [nlat] 0 = 32x8, 1 = 16x16 columns per block; NULL = default */
+    const int32_t *tile_shape;      /* [nlat] sites along k x j per work item: 0 = 64x8 (N%64==0),
+                                       1 = 32x16 (N%32==0), 2 = 16x16; NULL = by N */
     const int32_t *tile_ci;         /* [nlat] planes per block; NULL = default */
     double L, dt;                   /* shared box side and time step */
     double lambda, phi0, dphi0;     /* shared physical model constants (program units B = sqrt(lambda) phi0) */

@@ -65,6 +65,21 @@ def test_ensemble_create_rejects_bad_params(case):
     assert lib.gabe_ensemble_last_error(None)
 
 
+@pytest.mark.parametrize("N,shape", [(96, 0), (48, 1), (64, 3), (64, -1)])
+def test_ensemble_create_rejects_tile_shapes_that_do_not_divide_N(N, shape):
+    """Work-item shapes: 0 = 64x8 sites (N % 64 == 0), 1 = 32x16 (N % 32 == 0),
+    2 = 16x16 (any N % 16 == 0)."""
+    lib = gb._ens_lib()
+    shapes = np.array([shape], dtype=np.int32)
+    cis = np.array([16], dtype=np.int32)
+    p, keep = _params([N], tile_shape=shapes.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                      tile_ci=cis.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    h = ctypes.c_void_p()
+    assert lib.gabe_ensemble_create(ctypes.byref(p), ctypes.byref(h)) == 1
+    assert not h.value
+    assert b"tile shape" in lib.gabe_ensemble_last_error(None)
+
+
 def test_ensemble_null_handles_are_errors():
     lib = gb._ens_lib()
     assert lib.gabe_ensemble_destroy(None) == 0

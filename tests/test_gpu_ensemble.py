@@ -28,7 +28,7 @@ def _rel(got, want):
 
 
 def test_ensemble_steps_like_single_lattices():
-    sizes, g, amp, seeds = [32, 16, 48, 32], [100.0, 10.0, 300.0, 1.0], [1.0, 0.5, 2.0, 1.2], [11, 12, 13, 14]
+    sizes, g, amp, seeds = [32, 16, 48, 64], [100.0, 10.0, 300.0, 1.0], [1.0, 0.5, 2.0, 1.2], [11, 12, 13, 14]
     with gb.Ensemble(sizes, g, amp, seeds, nlog=32, tiles=None) as ens:
         ens.init()
         sc0 = ens.scalars()
@@ -53,6 +53,33 @@ def test_ensemble_steps_like_single_lattices():
                 fl = f1[fld] - f1[fld].mean()
                 assert np.abs(fe[fld] - f1[fld]).max() <= 1e-5 * np.abs(fl).max()
             assert _rel(le, l1) <= 1e-4 and _rel(he, h1) <= 1e-4
+
+
+@pytest.mark.parametrize("shapes,cis", [([0, 1], [16, 8]), ([0, 2], [64, 32]), ([1, 2], [32, 16])])
+def test_ensemble_tile_shapes_and_chunks_agree(shapes, cis):
+    """Every work-item shape (64x8, 32x16, 16x16 sites) and plane chunk gives
+    the same evolution: per-site arithmetic is shared, only the order of the
+    energy sums (and so FP32 rounding of the scalars) differs."""
+    sizes, g, amp, seeds = [64, 64], [100.0, 30.0], [1.0, 1.5], [21, 22]
+    with gb.Ensemble(sizes, g, amp, seeds, nlog=8, tiles=None) as ens:
+        ens.init()
+        ens.step(6)
+        want_sc = ens.scalars()
+        want = [ens.download(l) for l in range(2)]
+    with gb.Ensemble(sizes, g, amp, seeds, nlog=8, tiles=(shapes, cis)) as ens:
+        ens.init()
+        ens.step(6)
+        sc = ens.scalars()
+        got = [ens.download(l) for l in range(2)]
+    for l in range(2):
+        rho = want_sc[l, 10]
+        for q in range(12):
+            tol = 1e-6 * (abs(rho) if q in (8, 9) else abs(want_sc[l, q]))
+            assert abs(sc[l, q] - want_sc[l, q]) <= tol, (l, q, sc[l, q], want_sc[l, q])
+        for fld in range(2):
+            fl = want[l][0][fld] - want[l][0][fld].mean()
+            assert np.abs(got[l][0][fld] - want[l][0][fld]).max() <= 1e-5 * np.abs(fl).max()
+        assert _rel(got[l][3], want[l][3]) <= 1e-4
 
 
 def test_ensemble_graph_and_direct_launches_agree():
