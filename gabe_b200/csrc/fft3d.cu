@@ -24,12 +24,13 @@ template <int N>
 cudaError_t fft3d_n(float *S, int ncomp, cudaStream_t s) {
     constexpr long long nz = N / 2 + 1;
     int g1 = 0, g2 = 0;
-    cudaError_t e = persistent_grid(f3d::row_r2c_kernel<N>, f3d::kFftThreads, f3d::RowGeom<N>::SMEM_BYTES, &g1);
+    using RG = f3d::RowGeom<N>;
+    cudaError_t e = persistent_grid(f3d::row_r2c_kernel<N>, RG::T, RG::SMEM_BYTES, &g1);
     if (e != cudaSuccess) return e;
     e = persistent_grid(f3d::col_fft_kernel<N>, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, &g2);
     if (e != cudaSuccess) return e;
     // pass 1: rows along k
-    f3d::row_r2c_kernel<N><<<g1, f3d::kFftThreads, f3d::RowGeom<N>::SMEM_BYTES, s>>>(S, (long long)ncomp * N * N);
+    f3d::row_r2c_kernel<N><<<g1, RG::T, RG::SMEM_BYTES, s>>>(S, (long long)ncomp * N * N);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     float2 *X = reinterpret_cast<float2 *>(S);
     // pass 2: along j within every (component, i) plane

@@ -41,81 +41,95 @@ __device__ __forceinline__ void twiddles(float2 *tw) {
     }
 }
 
-// Both passes are persistent, one 512-thread CTA per SM, with a ring of
-// kFftBufs tile buffers in shared memory: the copies (cp.async) of the next
-// two tiles are in flight while the current one is transformed, so HBM
-// streams during the FFT arithmetic.
+// All passes are persistent kernels with a ring of tile buffers in shared
+// memory: the copies (cp.async) of the next tile are in flight while the
+// current one is transformed, so HBM streams during the FFT arithmetic.
 
 // ---------------------------------------------------------------------------
 // pass 1: r2c along k of every row (nrows rows of N+2 reals)
 // ---------------------------------------------------------------------------
+// 128-thread CTAs, several per SM (one computes while the others' copies
+// stream), each with two buffers of R = 16 rows.  Rows land in shared memory
+// with 8-byte cp.async copies, unpadded: within each run of L1 reals
+// (one four-step chunk) the pairs of reals are permuted by an XOR with the
+// chunk's index, so that the stride-L1 reads of the second four-step pass
+// fall on distinct banks while every pair stays 8-byte aligned.
 template <int N>
 struct RowGeom {
     using C_ = PlaneCfg<N>;
-    static constexpr int L1 = C_::L1, L2 = C_::L2, G = C_::G, PITCH = C_::PITCH;
-    static constexpr int R = N >= 256 ? 32 : 64, P = R / 2, T = kFftThreads;  // rows per tile, pairs
-    static constexpr int BUF = R * PITCH;                                        // floats per tile buffer
-    static constexpr int SMEM_FLOATS = kFftBufs * BUF + 2 * N;
+    static constexpr int L1 = C_::L1, L2 = C_::L2;
+    static constexpr int R = 16, P = R / 2, T = 128, NB = 2;  // rows per tile, pairs, threads, buffers
+    static constexpr int PITCH = N;                             // floats per shared row
+    static constexpr int BUF = R * PITCH;                       // floats per tile buffer
+    static constexpr int SMEM_FLOATS = NB * BUF + 2 * N;        // + twiddles
     static constexpr size_t SMEM_BYTES = (size_t)SMEM_FLOATS * sizeof(float);
     static constexpr int NT2 = (P * L2 + T - 1) / T;  // pass-2 tasks per thread
-    __device__ static __forceinline__ int pad(int s) { return s + s / G; }
+    static_assert(L1 % 2 == 0 && L1 <= 32, "pair swizzle within a chunk of L1 reals");
+    // shared position of real e of a row
+    __device__ static __forceinline__ int phys(int e) {
+        constexpr int CPR = 32 / L1, H = L1 / 2;  // chunks per 32-bank row, pairs per chunk
+        const int c = e / L1, q = (e % L1) >> 1;
+        return c * L1 + 2 * (q ^ ((c / CPR) % H)) + (e & 1);
+    }
 };
 
 template <int N>
-__global__ void __launch_bounds__(kFftThreads, 1) row_r2c_kernel(float *S, long long nrows) {
+__global__ void __launch_bounds__(RowGeom<N>::T, 3) row_r2c_kernel(float *S, long long nrows) {
     using Gm = RowGeom<N>;
-    constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2;
+    constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2,
+                  NB = Gm::NB;
     constexpr int RP = N + 2, NH = N / 2 + 1;
     extern __shared__ __align__(16) float smem[];
-    float2 *tw = reinterpret_cast<float2 *>(smem + kFftBufs * Gm::BUF);
+    float2 *tw = reinterpret_cast<float2 *>(smem + NB * Gm::BUF);
     const int tid = threadIdx.x;
     twiddles<N>(tw);
     const long long ntiles = nrows / R;
-    // rows of tile `tile` into buffer `b` (two 4-byte copies per pair of reals:
-    // the padded positions are not 8-byte aligned)
+    // rows of tile `tile` into buffer `b`: rows start on 8-byte boundaries (N+2 even)
     auto issue = [&](long long tile, int b) {
         const float *g = S + tile * R * RP;
         float *rows = smem + b * Gm::BUF;
+#pragma unroll 4
         for (int t = tid; t < R * (N / 2); t += T) {
             const int jj = t / (N / 2), m = t % (N / 2);
-            float *dst = rows + jj * PITCH + Gm::pad(2 * m);
-            s32::cp_async4(dst, g + jj * RP + 2 * m);
-            s32::cp_async4(dst + 1, g + jj * RP + 2 * m + 1);
+            s32::cp_async8(rows + jj * PITCH + Gm::phys(2 * m), g + jj * RP + 2 * m);
         }
     };
 #pragma unroll
-    for (int q = 0; q < kFftBufs - 1; q++) {
+    for (int q = 0; q < NB - 1; q++) {
         if (blockIdx.x + q * (long long)gridDim.x < ntiles) issue(blockIdx.x + q * (long long)gridDim.x, q);
         s32::cp_commit();
     }
     int it = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
-        float *rows = smem + (it % kFftBufs) * Gm::BUF;
+        float *rows = smem + (it % NB) * Gm::BUF;
         float *g = S + tile * R * RP;
-        s32::cp_wait<kFftBufs - 2>();
+        s32::cp_wait<NB - 2>();
         __syncthreads();  // this tile landed; the buffer of tile it-1 is consumed
-        const long long ahead = tile + (long long)(kFftBufs - 1) * gridDim.x;
-        if (ahead < ntiles) issue(ahead, (it + kFftBufs - 1) % kFftBufs);
+        const long long ahead = tile + (long long)(NB - 1) * gridDim.x;
+        if (ahead < ntiles) issue(ahead, (it + NB - 1) % NB);
         s32::cp_commit();
-        for (int t = tid; t < P * L1; t += T) {
-            const int p = t / L1, n1 = t % L1;
+        // four-step pass 1: L2-point FFTs over n2 (stride L1), twiddle W_N^(n1 k2), in place
+#pragma unroll
+        for (int t0 = 0; t0 < P * L1; t0 += T) {
+            const int t = t0 + tid, p = t / L1, n1 = t % L1;
             float *re = rows + 2 * p * PITCH, *im = re + PITCH;
             float2 x[L2];
 #pragma unroll
             for (int n2 = 0; n2 < L2; n2++) {
-                const int a = Gm::pad(n1 + L1 * n2);
+                const int a = Gm::phys(n1 + L1 * n2);
                 x[n2] = make_float2(re[a], im[a]);
             }
             pfft::fft_reg<L2>(x);
 #pragma unroll
             for (int k2 = 0; k2 < L2; k2++) {
                 const float2 y = k2 ? pfft::cmul(x[k2], tw[k2 * L1 + n1]) : x[k2];
-                const int a = Gm::pad(n1 + L1 * k2);
+                const int a = Gm::phys(n1 + L1 * k2);
                 re[a] = y.x;
                 im[a] = y.y;
             }
         }
         __syncthreads();
+        // pass 2: L1-point FFTs over n1, written back in natural order k = k2 + L2 k1
         {
             float2 y[NT2][L1];
 #pragma unroll
@@ -125,7 +139,7 @@ __global__ void __launch_bounds__(kFftThreads, 1) row_r2c_kernel(float *S, long 
                     const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
 #pragma unroll
                     for (int n1 = 0; n1 < L1; n1++) {
-                        const int a = Gm::pad(n1 + L1 * k2);
+                        const int a = Gm::phys(n1 + L1 * k2);
                         y[q][n1] = make_float2(re[a], im[a]);
                     }
                     pfft::fft_reg<L1>(y[q]);
@@ -139,7 +153,7 @@ __global__ void __launch_bounds__(kFftThreads, 1) row_r2c_kernel(float *S, long 
                     float *re = rows + 2 * p * PITCH, *im = re + PITCH;
 #pragma unroll
                     for (int k1 = 0; k1 < L1; k1++) {
-                        const int a = Gm::pad(k2 + L2 * k1);
+                        const int a = Gm::phys(k2 + L2 * k1);
                         re[a] = y[q][k1].x;
                         im[a] = y[q][k1].y;
                     }
@@ -151,7 +165,8 @@ __global__ void __launch_bounds__(kFftThreads, 1) row_r2c_kernel(float *S, long 
         for (int t = tid; t < P * NH; t += T) {
             const int p = t / NH, k = t % NH, km = (N - k) & (N - 1);
             const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
-            const float zr = re[Gm::pad(k)], zi = im[Gm::pad(k)], mr = re[Gm::pad(km)], mi = im[Gm::pad(km)];
+            const int ak = Gm::phys(k & (N - 1)), am = Gm::phys(km);
+            const float zr = re[ak], zi = im[ak], mr = re[am], mi = im[am];
             __stcs(reinterpret_cast<float2 *>(g + (2 * p) * RP) + k, make_float2(0.5f * (zr + mr), 0.5f * (zi - mi)));
             __stcs(reinterpret_cast<float2 *>(g + (2 * p + 1) * RP) + k,
                    make_float2(0.5f * (zi + mi), 0.5f * (mr - zr)));
