@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(RowGeom<N>::T, 3) row_r2c_kernel(float *S, lon
 #pragma unroll
         for (int t0 = 0; t0 < P * L1; t0 += T) {
             const int t = t0 + tid, p = t / L1, n1 = t % L1;
+            if (t >= P * L1) break;  // N = 64: fewer tasks than threads
             float *re = rows + 2 * p * PITCH, *im = re + PITCH;
             float2 x[L2];
 #pragma unroll
