@@ -78,7 +78,7 @@ enum gabe_flags {
                                    of cuFFT's batched 2-D plan */
     GABE_FLAG_OWN_FFT = 16      /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
                                    library's three-pass 3-D r2c instead of cuFFT's 3-D plan (no cuFFT
-                                   call on the step path; about 7% slower than cuFFT at 512^3 on B200) */
+                                   call on the step path; about 1% slower than cuFFT at 512^3 on B200) */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two
