@@ -42,30 +42,6 @@ cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cu
     }
 }
 
-template <int TK, int TJ>
-static cudaError_t sweep_shape(int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
-    const dim3 block(TK * TJ);
-    switch (mode) {
-        case MODE_A: sweep_kernel<float, TK, TJ, MODE_A><<<grid, block, 0, s>>>(a); break;
-        case MODE_A_GW: sweep_kernel<float, TK, TJ, MODE_A_GW><<<grid, block, 0, s>>>(a); break;
-        case MODE_E0: sweep_kernel<float, TK, TJ, MODE_E0><<<grid, block, 0, s>>>(a); break;
-        default: sweep_kernel<float, TK, TJ, MODE_B><<<grid, block, 0, s>>>(a); break;
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s) {
-    switch (shape) {
-        case 0: return sweep_shape<32, 8>(mode, a, grid, s);
-        case 1: return sweep_shape<16, 16>(mode, a, grid, s);
-        case 2: return sweep_shape<32, 4>(mode, a, grid, s);
-        case 3: return sweep_shape<16, 8>(mode, a, grid, s);
-        case 4: return sweep_shape<8, 8>(mode, a, grid, s);
-        case 5: return sweep_shape<4, 4>(mode, a, grid, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
 template <int N>
 static cudaError_t kspace_fused_n(const KspaceArgs &a, cudaStream_t s) {
     using G = ksf::KsGeom<N>;

@@ -109,7 +109,6 @@ inline GridPlan plan_grid32(int N, int want_shape, int want_ci) {
 }
 
 cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
-cudaError_t sweep_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l);
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);

@@ -23,14 +23,15 @@
 //     (:254-262).  Its last block advances a[0] (:268).
 //   mode E0: sweep A's E0 part alone, for energies asked for between steps.
 //
-// Both sweeps are radius-1 stencils: each thread owns a (j,k) column of a
-// TJ x TK tile and marches along i over `ci` planes, keeping the i-1, i, i+1
-// values of its column in registers (plus i+2 prefetched), and the (j,k)
-// neighbours of plane i in a double-buffered shared-memory tile with a
-// one-point halo, so each value is read from HBM once per sweep and there is
-// one barrier per plane.  The FP64 instantiations keep the reference's
-// operation order (compiled without FMA contraction); the FP32 ones evolve
-// fluctuations about the FP64 homogeneous trajectory (common.cuh).
+// Both sweeps are radius-1 stencils: in the FP64 kernels here each thread
+// owns a (j,k) column of a TJ x TK tile and marches along i over `ci` planes,
+// keeping the i-1, i, i+1 values of its column in registers (plus i+2
+// prefetched), and the (j,k) neighbours of plane i in a double-buffered
+// shared-memory tile with a one-point halo, so each value is read from HBM
+// once per sweep and there is one barrier per plane.  They keep the
+// reference's operation order (compiled without FMA contraction).  The FP32
+// sweeps (sweep32.cuh) evolve fluctuations about the FP64 homogeneous
+// trajectory with the per-site helpers and moment folding defined here.
 #pragma once
 
 #include "common.cuh"
@@ -308,8 +309,8 @@ __device__ __forceinline__ void finish_a(const LatticeConsts &c, DevScalars *s, 
 // the sweep kernel
 // ---------------------------------------------------------------------------
 // One tile of one lattice: the column tile (j0, k0) marched over planes
-// [i0, i1).  Shared by the single-lattice kernel below and the ensemble
-// kernel (ensemble.cuh).
+// [i0, i1) by the FP64 single-lattice kernel below (the FP32 sweeps use the
+// cp.async plane march of sweep32.cuh).
 template <typename T>
 struct TileJob {
     const T *X, *D;   // fields and momenta in, [2][N^3] each
@@ -328,6 +329,7 @@ struct SweepSmem {
 template <typename T, int TK, int TJ, int MODE>
 __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob<T> &job, T *smem0, T *smem1,
                                            double (&acc)[kNV]) {
+    static_assert(sizeof(T) == 8, "FP64 march; FP32 storage uses sweep32.cuh");
     using M = March<T, TK, TJ>;
     const int N = c.N;
     const size_t n3 = (size_t)N * N * N;
@@ -346,31 +348,7 @@ __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob
         ad1 = scp->adot[1];
     }
     const double c3H0 = (3. * ad0) / a0, c3H1 = MODE == MODE_B ? (3. * ad1) / a1 : 0.;
-    MeanTraj mt{};
-    MeanF m0{}, m1{};
-    float ia02f = 0.f, ia12f = 0.f, c3H0f = 0.f, c3H1f = 0.f, hf = 0.f, dtf = 0.f, inv_dx2f = 0.f, dnf = 0.f,
-          q3f = 0.f;
-    if constexpr (sizeof(T) == 4) {
-        mt = mean_traj(c, scp);
-        m0 = mean_f(c, mt.fb0);
-        m1 = mean_f(c, mt.fb1);
-        ia02f = (float)(1.0 / (a0 * a0));
-        hf = (float)h;
-        dtf = (float)dt;
-        inv_dx2f = (float)(1.0 / c.inv_dx2_div);
-        dnf = (float)c.dn;
-        q3f = (float)(-h * 3. / a0);
-        if constexpr (MODE == MODE_B) {
-            ia12f = (float)(1.0 / (a1 * a1));
-            c3H0f = (float)c3H0;
-            c3H1f = (float)c3H1;
-        }
-    }
-    (void)ia12f; (void)c3H0f; (void)c3H1f; (void)dtf; (void)dnf; (void)q3f; (void)c3H1;
-    Moments mom;  // FP32: fluctuation moments of the current plane group
-    zero(mom);
-    int ngroup = 0;
-    (void)ngroup;
+    (void)c3H1;
 
     // prologue: registers for planes i0-1, i0, i0+1; shared tile of plane i0
     m.load_own(m.prev, i0 - 1);
@@ -396,82 +374,39 @@ __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob
         }
         if constexpr (MODE == MODE_B) {
             const size_t gx = ((size_t)i * N + j) * N + k;
-            if constexpr (sizeof(T) == 8) {
-                const Nb7<double> f1[2] = {axpy7(f0[0], h, d0[0]), axpy7(f0[1], h, d0[1])};
-                for (int f = 0; f < 2; f++) {
-                    const double lap0 = lap64(f0[f], c.inv_dx2_div);
-                    const double dd0 = lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]) - c3H0 * d0[f].v[0];
-                    const double d1c = d0[f].v[0] + h * dd0;                  /* g2functions.cpp:242 */
-                    const double lap1 = lap64(f1[f], c.inv_dx2_div);
-                    const double dd1 = lap1 / a1 / a1 - dv64(c, f, f1[0].v[0], f1[1].v[0]) - c3H1 * d1c;
-                    Xo[f * n3 + gx] = f0[f].v[0] + dt * d1c;                  /* :259 */
-                    Do[f * n3 + gx] = d0[f].v[0] + dt * dd1;                  /* :260 */
-                }
-            } else {
-                const Nb7<float> f1[2] = {axpy7(f0[0], hf, d0[0]), axpy7(f0[1], hf, d0[1])};
-                for (int f = 0; f < 2; f++) {
-                    const float lap0 = lap32(f0[f], inv_dx2f);
-                    const float dd0 = lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]) - c3H0f * d0[f].v[0];
-                    const float d1c = d0[f].v[0] + hf * dd0;
-                    const float lap1 = lap32(f1[f], inv_dx2f);
-                    const float dd1 = lap1 * ia12f - dv_diff32(m1, c.model, f, f1[0].v[0], f1[1].v[0]) - c3H1f * d1c;
-                    Xo[f * n3 + gx] = f0[f].v[0] + dtf * d1c;
-                    Do[f * n3 + gx] = d0[f].v[0] + dtf * dd1;
-                }
+            const Nb7<double> f1[2] = {axpy7(f0[0], h, d0[0]), axpy7(f0[1], h, d0[1])};
+            for (int f = 0; f < 2; f++) {
+                const double lap0 = lap64(f0[f], c.inv_dx2_div);
+                const double dd0 = lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]) - c3H0 * d0[f].v[0];
+                const double d1c = d0[f].v[0] + h * dd0;                  /* g2functions.cpp:242 */
+                const double lap1 = lap64(f1[f], c.inv_dx2_div);
+                const double dd1 = lap1 / a1 / a1 - dv64(c, f, f1[0].v[0], f1[1].v[0]) - c3H1 * d1c;
+                Xo[f * n3 + gx] = f0[f].v[0] + dt * d1c;                  /* :259 */
+                Do[f * n3 + gx] = d0[f].v[0] + dt * dd1;                  /* :260 */
             }
         } else {
             T s0[kSrc] = {0, 0, 0, 0, 0}, s1[kSrc] = {0, 0, 0, 0, 0};
-            if constexpr (sizeof(T) == 8) {
-                for (int f = 0; f < 2; f++) {
-                    const double lap0 = lap64(f0[f], c.inv_dx2_div);
-                    acc[0] += d0[f].v[0] * d0[f].v[0];
-                    acc[2] -= f0[f].v[0] * lap0;
-                    if constexpr (MODE != MODE_E0) {
-                        const Nb7<double> f1 = axpy7(f0[f], h, d0[f]);
-                        const double P = d0[f].v[0] + h * (lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]));
-                        const double Q = -h * 3. * d0[f].v[0] / a0;
-                        acc[5] += P * P;
-                        acc[6] += P * Q;
-                        acc[7] += Q * Q;
-                        acc[4] -= f1.v[0] * lap64(f1, c.inv_dx2_div);
-                        if constexpr (MODE == MODE_A_GW) {
-                            source_add64(c, f0[f], s0);
-                            source_add64(c, f1, s1);
-                        }
+            for (int f = 0; f < 2; f++) {
+                const double lap0 = lap64(f0[f], c.inv_dx2_div);
+                acc[0] += d0[f].v[0] * d0[f].v[0];
+                acc[2] -= f0[f].v[0] * lap0;
+                if constexpr (MODE != MODE_E0) {
+                    const Nb7<double> f1 = axpy7(f0[f], h, d0[f]);
+                    const double P = d0[f].v[0] + h * (lap0 / a0 / a0 - dv64(c, f, f0[0].v[0], f0[1].v[0]));
+                    const double Q = -h * 3. * d0[f].v[0] / a0;
+                    acc[5] += P * P;
+                    acc[6] += P * Q;
+                    acc[7] += Q * Q;
+                    acc[4] -= f1.v[0] * lap64(f1, c.inv_dx2_div);
+                    if constexpr (MODE == MODE_A_GW) {
+                        source_add64(c, f0[f], s0);
+                        source_add64(c, f1, s1);
                     }
-                }
-                acc[1] += pot64(c, f0[0].v[0], f0[1].v[0]);
-                if constexpr (MODE != MODE_E0)
-                    acc[3] += pot64(c, f0[0].v[0] + h * d0[0].v[0], f0[1].v[0] + h * d0[1].v[0]);
-            } else {
-                float f1c[2];
-                for (int f = 0; f < 2; f++) {
-                    const float lap0 = lap32(f0[f], inv_dx2f);
-                    const float d = d0[f].v[0];
-                    mom.a[f] += d;
-                    mom.b = fmaf(d, d, mom.b);
-                    mom.g0 = fmaf(f0[f].v[0], lap0, mom.g0);
-                    if constexpr (MODE != MODE_E0) {
-                        const Nb7<float> f1 = axpy7(f0[f], hf, d0[f]);
-                        f1c[f] = f1.v[0];
-                        const float Pd = d + hf * (lap0 * ia02f - dv_diff32(m0, c.model, f, f0[0].v[0], f0[1].v[0]));
-                        mom.c[f] += Pd;
-                        mom.e = fmaf(Pd, Pd, mom.e);
-                        mom.f = fmaf(Pd, d, mom.f);
-                        mom.g1 = fmaf(f1.v[0], lap32(f1, inv_dx2f), mom.g1);
-                        if constexpr (MODE == MODE_A_GW) {
-                            source_add32(dnf, f0[f], s0);
-                            source_add32(dnf, f1, s1);
-                        }
-                    }
-                }
-                mom.v0 += v_diff32(m0, c.model, f0[0].v[0], f0[1].v[0]);
-                if constexpr (MODE != MODE_E0) mom.v1 += v_diff32(m1, c.model, f1c[0], f1c[1]);
-                if (++ngroup == kGroup || i == i1 - 1) {  // one site per thread and plane
-                    fold<MODE>(mt, q3f, ngroup, mom, acc);
-                    ngroup = 0;
                 }
             }
+            acc[1] += pot64(c, f0[0].v[0], f0[1].v[0]);
+            if constexpr (MODE != MODE_E0)
+                acc[3] += pot64(c, f0[0].v[0] + h * d0[0].v[0], f0[1].v[0] + h * d0[1].v[0]);
             if constexpr (MODE == MODE_A_GW) store_sources(job.S, N, i, j, k, s0, s1);
         }
         if (more) {
@@ -508,17 +443,9 @@ __device__ __forceinline__ void finish_b(const LatticeConsts &c, DevScalars *s) 
     s->step += 1;
 }
 
-// FP32: cap registers so that 3 (sweep A) or 4 (sweep B, E0) blocks of 256
-// threads share an SM -- the sweeps are latency-bound at lower occupancy.
-template <typename T, int MODE>
-constexpr int sweep_min_threads() {
-    return sizeof(T) == 8 ? 0 : (MODE == MODE_A_GW || MODE == MODE_A ? 768 : 1024);
-}
-
-// Single lattice: block (x, y, z) = column tile (k, j) and plane chunk.
+// Single lattice, FP64: block (x, y, z) = column tile (k, j) and plane chunk.
 template <typename T, int TK, int TJ, int MODE>
-__global__ void __launch_bounds__(TK *TJ, (sweep_min_threads<T, MODE>() + TK * TJ - 1) / (TK * TJ))
-    sweep_kernel(StencilArgs args) {
+__global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
     __shared__ __align__(16) T smem[2][4 * SweepSmem<TK, TJ>::P];
     __shared__ double sred[((TK * TJ + 31) / 32) * kNV];
     __shared__ int sflag;
