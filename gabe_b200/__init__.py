@@ -38,6 +38,7 @@ FLAG_NO_OVERLAP = 2
 FLAG_PLANE_FFT = 4
 FLAG_FUSED_KSPACE = 8
 FLAG_OWN_FFT = 16
+FLAG_FUSED_ROWS = 32
 
 STATUS = {
     0: "GABE_OK", 1: "GABE_ERR_PARAM", 2: "GABE_ERR_CUDA", 3: "GABE_ERR_CUFFT", 4: "GABE_ERR_NOMEM",

@@ -59,6 +59,7 @@ struct gabe_handle {
     // of planefft.cuh) and the k-space update with the pass along i fused in
     bool evolve_gw = false; // calc_gws with expansion_type 1: the step evolves h, l (types 0 and 2 do not)
     bool own_fft = false;   // the library's three-pass 3-D r2c (fft3d.cuh)
+    bool rows_fused = false;  // sweep A writes the sources transformed along k (sweeprows.cuh)
     bool ks_fused = false;
     bool plane_fft = false;
     int plane_grid = 0;
@@ -129,10 +130,13 @@ int make_plans(gabe_handle *h) {
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
     h->ks_fused = h->evolve_gw && h->f32 && kspace_fused_supported(h->N) && (h->p.flags & GABE_FLAG_FUSED_KSPACE);
     h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
-    h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && fft3d_supported(h->N) && (h->p.flags & GABE_FLAG_OWN_FFT);
+    h->rows_fused = h->evolve_gw && h->f32 && !h->ks_fused && sweep32_rows_supported(h->N) &&
+                    (h->p.flags & GABE_FLAG_FUSED_ROWS);
+    h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && !h->rows_fused && fft3d_supported(h->N) &&
+                 (h->p.flags & GABE_FLAG_OWN_FFT);
     if (h->plane_fft) {
         CK(h, plane_r2c_setup(h->N, &h->plane_grid));
-    } else if (h->own_fft) {
+    } else if (h->own_fft || h->rows_fused) {
         // no plan: fft3d.cuh
     } else if (h->ks_fused) {
         // 2-D r2c of every (source, i) plane: N x (N+2) reals in, N x nz complex out, in place
@@ -192,6 +196,10 @@ int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
         CK(h, fft3d_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc, s));
         return GABE_OK;
     }
+    if (h->rows_fused) {  // the pass along k was taken by sweep A
+        CK(h, fft3d_cols_f32(h->N, static_cast<float *>(S), 2 * kSrc, s));
+        return GABE_OK;
+    }
     CF(h, cufftSetStream(h->plan_src, s));
     return fft_r2c(h, h->plan_src, S, S);
 }
@@ -231,6 +239,10 @@ StencilArgs stencil_args(gabe_handle *h, int cur, int slot = 0) {
 int sweep(gabe_handle *h, int mode, int cur, int counter, int slot = 0) {
     StencilArgs a = stencil_args(h, cur, slot);
     a.counter = h->counters + counter;
+    if (mode == MODE_A_GW && h->rows_fused) {
+        CK(h, sweep32_rows_f32(a, h->stream));
+        return GABE_OK;
+    }
     CK(h, h->f32 ? sweep32_f32(h->shape, mode, a, h->grid, h->stream)
                  : sweep_f64(h->shape, mode, a, h->grid, h->stream));
     return GABE_OK;
@@ -901,7 +913,7 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
 int gabe_launches_per_step(const gabe_handle *h) {
-    return h ? (h->evolve_gw ? (h->own_fft ? 6 : h->plane_fft ? 4 : 3) : 2) : 0;
+    return h ? (h->evolve_gw ? (h->own_fft ? 6 : h->rows_fused ? 5 : h->plane_fft ? 4 : 3) : 2) : 0;
 }
 
 }  // extern "C"

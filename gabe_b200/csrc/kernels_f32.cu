@@ -3,6 +3,7 @@
 #include "launch.h"
 #include "kspace_fused.cuh"
 #include "sweep32.cuh"
+#include "sweeprows.cuh"
 
 namespace gabe {
 
@@ -38,6 +39,32 @@ cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cu
         case 4: return sweep32_shape<32, 16>(mode, a, grid, s);
         case 5: return sweep32_shape<16, 4>(mode, a, grid, s);
         case 6: return sweep32_shape<8, 8>(mode, a, grid, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int N>
+static cudaError_t sweep32_rows_n(StencilArgs a, int ci, cudaStream_t s) {
+    using G = s32::RowsGeom<N>;
+    auto k = s32::sweep32_rows_kernel<N>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    a.ci = ci;
+    k<<<dim3(N / 2, (N + ci - 1) / ci), G::T, G::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
+
+bool sweep32_rows_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
+
+int sweep32_rows_ci(int N) { return N >= 512 ? 64 : (N >= 256 ? 32 : (N >= 128 ? 16 : 8)); }
+
+cudaError_t sweep32_rows_f32(const StencilArgs &a, cudaStream_t s) {
+    const int ci = sweep32_rows_ci(a.c.N);
+    switch (a.c.N) {
+        case 64: return sweep32_rows_n<64>(a, ci, s);
+        case 128: return sweep32_rows_n<128>(a, ci, s);
+        case 256: return sweep32_rows_n<256>(a, ci, s);
+        case 512: return sweep32_rows_n<512>(a, ci, s);
         default: return cudaErrorInvalidValue;
     }
 }

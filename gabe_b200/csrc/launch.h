@@ -110,6 +110,11 @@ inline GridPlan plan_grid32(int N, int want_shape, int want_ci) {
 
 cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
+// FP32 sweep A with sources that writes them transformed along k (sweeprows.cuh):
+// one block per pair of rows and chunk of sweep32_rows_ci(N) planes.
+bool sweep32_rows_supported(int N);
+int sweep32_rows_ci(int N);
+cudaError_t sweep32_rows_f32(const StencilArgs &a, cudaStream_t s);
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l);
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);
 cudaError_t bins_f64(const BinArgs &a, const Launch &l);
@@ -136,6 +141,8 @@ cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out
 // FP32 in-place 3-D r2c of ncomp arrays [N][N][N+2] in three passes (fft3d.cuh).
 bool fft3d_supported(int N);
 cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s);
+// Its passes along j and i alone, for sources already transformed along k.
+cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s);
 
 // FP32 k-space update with the FFT pass along i fused in (kspace_fused.cuh);
 // S holds the 2-D (j, k) transforms of the sources.

@@ -76,9 +76,14 @@ enum gabe_flags {
     GABE_FLAG_PLANE_FFT = 4,    /* with GABE_FLAG_FUSED_KSPACE: the 2-D (j, k) transforms by the
                                    library's plane kernel (one thread-block cluster per plane) instead
                                    of cuFFT's batched 2-D plan */
-    GABE_FLAG_OWN_FFT = 16      /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
+    GABE_FLAG_OWN_FFT = 16,     /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
                                    library's three-pass 3-D r2c instead of cuFFT's 3-D plan (no cuFFT
                                    call on the step path; about 1% slower than cuFFT at 512^3 on B200) */
+    GABE_FLAG_FUSED_ROWS = 32   /* FP32 with N in {64, 128, 256, 512}: sweep A writes the GW sources already
+                                   transformed along k (one block per pair of whole rows), and the
+                                   transforms along j and i are the library's column passes (one HBM
+                                   pass fewer, but about 8% slower per step at 512^3 on B200: one
+                                   block per SM, whose transform phases leave most warps idle) */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two
