@@ -29,6 +29,7 @@ UNITS = [
     ("fft3d.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("ensemble.cu", []),
+    ("slab.cu", []),
     ("mlp.cu", []),
 ]
 

@@ -90,6 +90,7 @@ __global__ void __launch_bounds__(kEnsThreads, s32::sweep32_threads_per_sm<MODE>
     t.j0 = item.j0;
     t.i0 = item.i0;
     t.i1 = item.i1;
+    t.planes = 0;
     const s32::Site32 s = s32::site32_consts<MODE>(c, L.sc);
     double acc[kNV];
 #pragma unroll

@@ -43,6 +43,15 @@ cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cu
     }
 }
 
+cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s) {
+    switch (mode) {
+        case MODE_A: slab_finish_kernel<float, MODE_A><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
+        case MODE_E0: slab_finish_kernel<float, MODE_E0><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 template <int N>
 static cudaError_t sweep32_rows_n(StencilArgs a, int ci, cudaStream_t s) {
     using G = s32::RowsGeom<N>;

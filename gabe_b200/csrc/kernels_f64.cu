@@ -27,6 +27,15 @@ cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cuda
     }
 }
 
+cudaError_t slab_finish_f64(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s) {
+    switch (mode) {
+        case MODE_A: slab_finish_kernel<double, MODE_A><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
+        case MODE_E0: slab_finish_kernel<double, MODE_E0><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l) {
     kspace_kernel<double><<<l.grid, l.block, l.smem, l.stream>>>(a);
     return cudaGetLastError();

@@ -110,6 +110,9 @@ inline GridPlan plan_grid32(int N, int want_shape, int want_ci) {
 
 cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
 cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
+// Slab: finish_a of sweep A (mode MODE_A) or of the energies (MODE_E0) from the totals of all slabs.
+cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s);
+cudaError_t slab_finish_f64(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s);
 // FP32 sweep A with sources that writes them transformed along k (sweeprows.cuh):
 // one block per pair of rows and chunk of sweep32_rows_ci(N) planes.
 bool sweep32_rows_supported(int N);

@@ -1,0 +1,345 @@
+// One slab of a lattice split along i over several processes (GPUs), field
+// evolution without tensor modes (gabe_slab_*, include/gabe.h).
+//
+// Each rank holds its own planes i in [plane0, plane0 + nplanes) of the
+// four state arrays between two halo planes (the last own plane of the rank
+// below and the first of the rank above, periodic in i), and runs the same
+// two sweeps per step as a whole lattice (stencil.cuh / sweep32.cuh with
+// StencilArgs::planes set).  The Friedmann update of the reference's step()
+// (g2functions.cpp:234-271) needs full-volume energies, so sweep A (and the
+// energies between steps) end with their block-summed totals in device
+// memory; the caller adds the totals of all ranks (an all-reduce of kNV
+// FP64 values) and runs the finish, which every rank then takes with the
+// same totals.  After sweep B the caller exchanges the boundary planes:
+// pack -> send/recv -> unpack.  The library does no communication itself.
+#include <cmath>
+#include <cstdarg>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/gabe.h"
+#include "launch.h"
+
+using namespace gabe;
+
+namespace {
+thread_local std::string g_slab_create_error;
+}
+
+struct gabe_slab {
+    gabe_params p{};
+    LatticeConsts lc{};
+    int N = 0, plane0 = 0, nloc = 0, planes = 0, dev = 0, cur = 0;
+    bool f32 = false, uploaded = false;
+    size_t plane_elems = 0, w = 8;
+    cudaStream_t stream = nullptr;
+    void *X[2] = {nullptr, nullptr}, *D[2] = {nullptr, nullptr};
+    DevScalars *sc = nullptr;
+    double *partials = nullptr, *sums = nullptr, *stage = nullptr;
+    unsigned int *counters = nullptr;
+    void *send[2] = {nullptr, nullptr}, *recv[2] = {nullptr, nullptr};  // [lo, hi]: 4 planes each
+    int shape = 0, ci = 1;
+    dim3 grid;
+    std::string err;
+};
+
+namespace {
+
+int serr(gabe_slab *s, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (s) s->err = buf;
+    else g_slab_create_error = buf;
+    return code;
+}
+
+#define SCK(s, x)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess) return serr(s, GABE_ERR_CUDA, "%s: %s", #x, cudaGetErrorString(e_)); \
+    } while (0)
+
+int salloc(gabe_slab *s, void **p, size_t bytes) {
+    if (cudaMalloc(p, bytes ? bytes : 256) != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return serr(s, GABE_ERR_NOMEM, "cudaMalloc(%zu bytes) failed", bytes);
+    }
+    return GABE_OK;
+}
+
+// Device address of array a (0 phi, 1 chi, 2 phidot, 3 chidot) at buffer plane p of state c.
+char *plane_ptr(gabe_slab *s, int c, int a, int p) {
+    char *base = static_cast<char *>(a < 2 ? s->X[c] : s->D[c]);
+    return base + ((size_t)(a & 1) * s->planes + p) * s->plane_elems * s->w;
+}
+
+double *dev_mean(gabe_slab *s, bool momentum, int f) {
+    const size_t off = momentum ? offsetof(DevScalars, dfbar) : offsetof(DevScalars, fbar);
+    return reinterpret_cast<double *>(reinterpret_cast<char *>(s->sc) + off) + f;
+}
+
+StencilArgs slab_args(gabe_slab *s, int counter, double *sums_out) {
+    StencilArgs a{};
+    a.X = s->X[s->cur];
+    a.D = s->D[s->cur];
+    a.Xo = s->X[s->cur ^ 1];
+    a.Do = s->D[s->cur ^ 1];
+    a.S = nullptr;
+    a.partials = s->partials;
+    a.counter = s->counters + counter;
+    a.sc = s->sc;
+    a.c = s->lc;
+    a.ci = s->ci;
+    a.slot = 0;
+    a.planes = s->planes;
+    a.sums_out = sums_out;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab **out) {
+    if (!out) return serr(nullptr, GABE_ERR_PARAM, "out is NULL");
+    *out = nullptr;
+    if (!p || p->struct_size != (int32_t)sizeof(gabe_params)) return serr(nullptr, GABE_ERR_PARAM, "bad gabe_params");
+    if (!sp || sp->struct_size != (int32_t)sizeof(gabe_slab_params))
+        return serr(nullptr, GABE_ERR_PARAM, "bad gabe_slab_params");
+    const int N = p->N;
+    if (N < 16 || N > 1024 || N % 16 || p->nflds != 2)
+        return serr(nullptr, GABE_ERR_PARAM, "N must be a multiple of 16 in [16, 1024] and nflds 2");
+    if (p->gws_on) return serr(nullptr, GABE_ERR_PARAM, "slabs evolve the fields only (gws_on must be 0)");
+    if (p->precision != GABE_FP64 && p->precision != GABE_FP32) return serr(nullptr, GABE_ERR_PARAM, "bad precision");
+    if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4) return serr(nullptr, GABE_ERR_PARAM, "bad model");
+    if (p->expansion < 0 || p->expansion > 2) return serr(nullptr, GABE_ERR_PARAM, "expansion must be 0, 1 or 2");
+    if (!(p->L > 0) || !(p->dt > 0)) return serr(nullptr, GABE_ERR_PARAM, "L and dt must be positive");
+    if (sp->nplanes < 1 || sp->plane0 < 0 || sp->plane0 + sp->nplanes > N)
+        return serr(nullptr, GABE_ERR_PARAM, "planes [%d, %d) outside [0, %d)", sp->plane0, sp->plane0 + sp->nplanes, N);
+    gabe_slab *s = new (std::nothrow) gabe_slab();
+    if (!s) return serr(nullptr, GABE_ERR_NOMEM, "host allocation failed");
+    auto bail = [&](int code) {
+        g_slab_create_error = s->err;
+        gabe_slab_destroy(s);
+        return code;
+    };
+    s->p = *p;
+    s->N = N;
+    s->plane0 = sp->plane0;
+    s->nloc = sp->nplanes;
+    s->planes = sp->nplanes + 2;
+    s->f32 = p->precision == GABE_FP32;
+    s->w = s->f32 ? 4 : 8;
+    s->plane_elems = (size_t)N * N;
+    s->lc = make_lattice_consts(*p);
+    if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) {
+        cudaGetLastError();
+        serr(s, GABE_ERR_CUDA, "cudaSetDevice(%d) failed", p->device);
+        return bail(GABE_ERR_CUDA);
+    }
+    if (cudaGetDevice(&s->dev) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        serr(s, GABE_ERR_CUDA, "no CUDA device");
+        return bail(GABE_ERR_CUDA);
+    }
+    // the whole lattice's tile and plane chunk, with the chunks cut from this slab's planes
+    GridPlan g = s->f32 ? plan_grid32(N, p->tile_shape, p->tile_ci) : plan_grid(N, p->tile_shape, p->tile_ci);
+    s->shape = g.shape;
+    s->ci = g.ci < s->nloc ? g.ci : s->nloc;
+    s->grid = dim3(g.grid.x, g.grid.y, (s->nloc + s->ci - 1) / s->ci);
+    const size_t arr = 2 * (size_t)s->planes * s->plane_elems * s->w;  // both fields of one array kind
+    const size_t nblk = (size_t)s->grid.x * s->grid.y * s->grid.z;
+    int rc;
+    for (int b = 0; b < 2; b++) {
+        if ((rc = salloc(s, &s->X[b], arr)) || (rc = salloc(s, &s->D[b], arr))) return bail(rc);
+        if ((rc = salloc(s, &s->send[b], 4 * s->plane_elems * s->w)) || (rc = salloc(s, &s->recv[b], 4 * s->plane_elems * s->w)))
+            return bail(rc);
+    }
+    if ((rc = salloc(s, (void **)&s->sc, sizeof(DevScalars))) ||
+        (rc = salloc(s, (void **)&s->partials, kNV * sizeof(double) * (nblk > 4096 ? nblk : 4096))) ||
+        (rc = salloc(s, (void **)&s->sums, kNV * sizeof(double))) ||
+        (rc = salloc(s, (void **)&s->counters, 4 * sizeof(unsigned int))))
+        return bail(rc);
+    if (s->f32 && (rc = salloc(s, (void **)&s->stage, (size_t)s->nloc * s->plane_elems * sizeof(double)))) return bail(rc);
+    if (cudaMemset(s->counters, 0, 4 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMemset(s->sc, 0, sizeof(DevScalars)) != cudaSuccess) {
+        cudaGetLastError();
+        serr(s, GABE_ERR_CUDA, "device initialisation failed");
+        return bail(GABE_ERR_CUDA);
+    }
+    *out = s;
+    return GABE_OK;
+}
+
+int gabe_slab_destroy(gabe_slab *s) {
+    if (!s) return GABE_OK;
+    cudaSetDevice(s->dev);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    void *bufs[] = {s->X[0], s->X[1], s->D[0], s->D[1], s->send[0], s->send[1], s->recv[0], s->recv[1],
+                    s->sc, s->partials, s->sums, s->stage, s->counters};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    cudaGetLastError();
+    delete s;
+    return GABE_OK;
+}
+
+const char *gabe_slab_last_error(gabe_slab *s) { return s ? s->err.c_str() : g_slab_create_error.c_str(); }
+
+int gabe_slab_upload(gabe_slab *s, const double *field0, const double *dfield0, const double mean[4], double a0,
+                     double adot0) {
+    if (!s) return GABE_ERR_PARAM;
+    if (!field0 || !dfield0) return serr(s, GABE_ERR_PARAM, "field0/dfield0 must not be NULL");
+    if (s->f32 && !mean) return serr(s, GABE_ERR_PARAM, "FP32 storage needs the whole lattice's means");
+    if (!(a0 > 0) || !std::isfinite(a0) || !std::isfinite(adot0)) return serr(s, GABE_ERR_PARAM, "bad a0/adot0");
+    SCK(s, cudaSetDevice(s->dev));
+    DevScalars d{};
+    d.a[0] = a0;
+    d.adot[0] = adot0;
+    if (s->p.expansion == 0) {
+        d.a[1] = a0;
+        d.adot[1] = adot0;
+    }
+    d.adot_given = 1;
+    if (s->f32)
+        for (int f = 0; f < 2; f++) {
+            d.fbar[f] = mean[f];
+            d.dfbar[f] = mean[2 + f];
+        }
+    SCK(s, cudaMemcpyAsync(s->sc, &d, sizeof(d), cudaMemcpyHostToDevice, s->stream));
+    const size_t nf = (size_t)s->nloc * s->plane_elems;  // own values of one field
+    const double *src[2] = {field0, dfield0};
+    for (int a = 0; a < 4; a++) {
+        const double *h = src[a >> 1] + (size_t)(a & 1) * nf;
+        char *dst = plane_ptr(s, 0, a, 1);
+        if (!s->f32) {
+            SCK(s, cudaMemcpyAsync(dst, h, nf * 8, cudaMemcpyHostToDevice, s->stream));
+        } else {
+            SCK(s, cudaMemcpyAsync(s->stage, h, nf * 8, cudaMemcpyHostToDevice, s->stream));
+            SCK(s, to_fluct(s->stage, nf, dev_mean(s, a >= 2, a & 1), reinterpret_cast<float *>(dst), s->stream));
+        }
+    }
+    SCK(s, cudaStreamSynchronize(s->stream));
+    s->cur = 0;
+    s->uploaded = true;
+    return GABE_OK;
+}
+
+int gabe_slab_download(gabe_slab *s, double *field0, double *dfield0) {
+    if (!s) return GABE_ERR_PARAM;
+    if (!s->uploaded) return serr(s, GABE_ERR_STATE, "download before upload");
+    SCK(s, cudaSetDevice(s->dev));
+    const size_t nf = (size_t)s->nloc * s->plane_elems;
+    double *dst[2] = {field0, dfield0};
+    for (int a = 0; a < 4; a++) {
+        double *h = dst[a >> 1];
+        if (!h) continue;
+        h += (size_t)(a & 1) * nf;
+        const char *src = plane_ptr(s, s->cur, a, 1);
+        if (!s->f32) {
+            SCK(s, cudaMemcpyAsync(h, src, nf * 8, cudaMemcpyDeviceToHost, s->stream));
+        } else {
+            SCK(s, from_fluct(reinterpret_cast<const float *>(src), nf, dev_mean(s, a >= 2, a & 1), s->stage, s->stream));
+            SCK(s, cudaMemcpyAsync(h, s->stage, nf * 8, cudaMemcpyDeviceToHost, s->stream));
+        }
+    }
+    SCK(s, cudaStreamSynchronize(s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_buffers(gabe_slab *s, double **sums, void **send_lo, void **send_hi, void **recv_lo, void **recv_hi,
+                      size_t *halo_bytes) {
+    if (!s) return GABE_ERR_PARAM;
+    if (sums) *sums = s->sums;
+    if (send_lo) *send_lo = s->send[0];
+    if (send_hi) *send_hi = s->send[1];
+    if (recv_lo) *recv_lo = s->recv[0];
+    if (recv_hi) *recv_hi = s->recv[1];
+    if (halo_bytes) *halo_bytes = 4 * s->plane_elems * s->w;
+    return GABE_OK;
+}
+
+int gabe_slab_pack(gabe_slab *s) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "pack before upload") : GABE_ERR_PARAM;
+    SCK(s, cudaSetDevice(s->dev));
+    const size_t pb = s->plane_elems * s->w;
+    for (int a = 0; a < 4; a++) {
+        SCK(s, cudaMemcpyAsync(static_cast<char *>(s->send[0]) + a * pb, plane_ptr(s, s->cur, a, 1), pb,
+                               cudaMemcpyDeviceToDevice, s->stream));
+        SCK(s, cudaMemcpyAsync(static_cast<char *>(s->send[1]) + a * pb, plane_ptr(s, s->cur, a, s->nloc), pb,
+                               cudaMemcpyDeviceToDevice, s->stream));
+    }
+    return GABE_OK;
+}
+
+int gabe_slab_unpack(gabe_slab *s) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "unpack before upload") : GABE_ERR_PARAM;
+    SCK(s, cudaSetDevice(s->dev));
+    const size_t pb = s->plane_elems * s->w;
+    for (int a = 0; a < 4; a++) {
+        SCK(s, cudaMemcpyAsync(plane_ptr(s, s->cur, a, 0), static_cast<char *>(s->recv[0]) + a * pb, pb,
+                               cudaMemcpyDeviceToDevice, s->stream));
+        SCK(s, cudaMemcpyAsync(plane_ptr(s, s->cur, a, s->nloc + 1), static_cast<char *>(s->recv[1]) + a * pb, pb,
+                               cudaMemcpyDeviceToDevice, s->stream));
+    }
+    return GABE_OK;
+}
+
+int gabe_slab_sweep(gabe_slab *s, int which) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "sweep before upload") : GABE_ERR_PARAM;
+    if (which < 0 || which > 2) return serr(s, GABE_ERR_PARAM, "which must be 0 (sweep A), 1 (sweep B) or 2 (energies)");
+    SCK(s, cudaSetDevice(s->dev));
+    const int mode = which == 0 ? MODE_A : (which == 1 ? MODE_B : MODE_E0);
+    StencilArgs a = slab_args(s, which, which == 1 ? nullptr : s->sums);
+    SCK(s, s->f32 ? sweep32_f32(s->shape, mode, a, s->grid, s->stream) : sweep_f64(s->shape, mode, a, s->grid, s->stream));
+    if (which == 1) s->cur ^= 1;
+    return GABE_OK;
+}
+
+int gabe_slab_finish(gabe_slab *s, int which) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "finish before upload") : GABE_ERR_PARAM;
+    if (which != 0 && which != 2) return serr(s, GABE_ERR_PARAM, "which must be 0 (after sweep A) or 2 (energies)");
+    SCK(s, cudaSetDevice(s->dev));
+    const int mode = which == 0 ? MODE_A : MODE_E0;
+    SCK(s, s->f32 ? slab_finish_f32(mode, s->lc, s->sc, s->sums, s->stream)
+                  : slab_finish_f64(mode, s->lc, s->sc, s->sums, s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_stream(gabe_slab *s, void **stream) {
+    if (!s || !stream) return GABE_ERR_PARAM;
+    *stream = s->stream;
+    return GABE_OK;
+}
+
+int gabe_slab_sync(gabe_slab *s) {
+    if (!s) return GABE_ERR_PARAM;
+    SCK(s, cudaSetDevice(s->dev));
+    SCK(s, cudaStreamSynchronize(s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_scalars(gabe_slab *s, double out12[12]) {
+    if (!s || !out12) return GABE_ERR_PARAM;
+    SCK(s, cudaSetDevice(s->dev));
+    SCK(s, cudaStreamSynchronize(s->stream));
+    DevScalars d;
+    SCK(s, cudaMemcpy(&d, s->sc, sizeof(d), cudaMemcpyDeviceToHost));
+    const double *src[6] = {d.a, d.adot, d.edkin, d.edpot, d.edgrad, d.edrho};
+    for (int q = 0; q < 6; q++) {
+        out12[2 * q] = src[q][0];
+        out12[2 * q + 1] = src[q][1];
+    }
+    if (d.status & ST_NONFINITE) return serr(s, GABE_ERR_NONFINITE, "non-finite energy density at step %lld", d.step);
+    return GABE_OK;
+}
+
+}  // extern "C"

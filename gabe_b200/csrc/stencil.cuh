@@ -52,6 +52,14 @@ struct StencilArgs {
     LatticeConsts c;
     int ci;              // planes per block along i
     int slot;            // source buffer / GW scalar slot of this step
+    // Slab of a lattice split along i (slab.cu): X, D, Xo, Do hold `planes`
+    // planes per field -- own planes 1 .. planes-2 between two halo planes --
+    // addressed without wrap along i.  0: the whole periodic lattice.
+    int planes;
+    // Slab: the last block writes the block-summed totals (kNV doubles) here
+    // instead of finishing the stage; the caller adds the totals of all
+    // slabs and finishes with slab_finish_kernel.
+    double *sums_out;
 };
 
 constexpr int kNV = 8;  // reduced values: kin0 pot0 grad0 | pot1 grad1 PP PQ QQ
@@ -188,14 +196,16 @@ struct March {
     static constexpr int NH = 2 * TK + 2 * TJ;  // halo points of a plane tile
     const T *src[NA];
     int N, j0, k0, tx, ty, tid;
+    bool wrap;  // periodic along i (whole lattice) or slab planes addressed as they are
     // halo duty of this thread: (row, col) in the tile and global (j, k)
     int hr, hc, hj, hk;
     bool has_halo;
     T prev[NA], cur[NA], nxt[NA], nn[NA], hal[NA];
 
-    __device__ __forceinline__ void init(const T *X, const T *D, int N_, size_t n3, int j0_, int k0_) {
+    __device__ __forceinline__ void init(const T *X, const T *D, int N_, size_t n3, int j0_, int k0_, bool wrap_) {
         src[0] = X; src[1] = X + n3; src[2] = D; src[3] = D + n3;
         N = N_;
+        wrap = wrap_;
         tid = threadIdx.x;
         tx = tid % TK; ty = tid / TK;
         j0 = j0_; k0 = k0_;
@@ -208,10 +218,11 @@ struct March {
         hj = wrapi(j0 + hr - 1, N);
         hk = wrapi(k0 + hc - 1, N);
     }
+    __device__ __forceinline__ int plane(int i) const { return wrap ? wrapi(i, N) : i; }
     __device__ __forceinline__ size_t own(int i) const {
-        return ((size_t)wrapi(i, N) * N + (j0 + ty)) * N + (k0 + tx);
+        return ((size_t)plane(i) * N + (j0 + ty)) * N + (k0 + tx);
     }
-    __device__ __forceinline__ size_t halo(int i) const { return ((size_t)wrapi(i, N) * N + hj) * N + hk; }
+    __device__ __forceinline__ size_t halo(int i) const { return ((size_t)plane(i) * N + hj) * N + hk; }
     __device__ __forceinline__ void load_own(T (&dst)[NA], int i) const {
         const size_t o = own(i);
 #pragma unroll
@@ -318,6 +329,7 @@ struct TileJob {
     T *S;             // GW sources [10][N][N][N+2] (sweep A with GWs)
     const DevScalars *sc;
     int j0, k0, i0, i1;
+    int planes;       // planes per field in the arrays (slab); 0 = N, periodic
 };
 
 template <int TK, int TJ>
@@ -332,9 +344,9 @@ __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob
     static_assert(sizeof(T) == 8, "FP64 march; FP32 storage uses sweep32.cuh");
     using M = March<T, TK, TJ>;
     const int N = c.N;
-    const size_t n3 = (size_t)N * N * N;
+    const size_t n3 = (size_t)(job.planes ? job.planes : N) * N * N;
     M m;
-    m.init(job.X, job.D, N, n3, job.j0, job.k0);
+    m.init(job.X, job.D, N, n3, job.j0, job.k0, job.planes == 0);
     const int i0 = job.i0, i1 = job.i1;
     const DevScalars *scp = job.sc;
     const double h = c.half_dt, dt = c.dt;
@@ -459,8 +471,10 @@ __global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
     job.sc = args.sc;
     job.k0 = blockIdx.x * TK;
     job.j0 = blockIdx.y * TJ;
-    job.i0 = blockIdx.z * args.ci;
-    job.i1 = min(job.i0 + args.ci, c.N);
+    job.planes = args.planes;
+    const int first = args.planes ? 1 : 0, end = args.planes ? args.planes - 1 : c.N;  // own planes
+    job.i0 = first + blockIdx.z * args.ci;
+    job.i1 = min(job.i0 + args.ci, end);
     double acc[kNV];
 #pragma unroll
     for (int q = 0; q < kNV; q++) acc[q] = 0.;
@@ -478,13 +492,22 @@ __global__ void __launch_bounds__(TK *TJ) sweep_kernel(StencilArgs args) {
         double tot[kNV];
         sum_partials<kNV>(args.partials, gridDim.x * gridDim.y * gridDim.z, tot, sred);
         if (tid == 0) {
-            finish_a<T, MODE>(c, args.sc, tot, args.slot);
+            if (args.sums_out)
+                for (int q = 0; q < kNV; q++) args.sums_out[q] = tot[q];
+            else
+                finish_a<T, MODE>(c, args.sc, tot, args.slot);
             *args.counter = 0u;
         }
     } else if (tid == 0) {
         finish_b<T>(c, args.sc);
         *args.counter = 0u;
     }
+}
+
+// Slab: the end of sweep A / E0 from the totals of all slabs (one thread).
+template <typename T, int MODE>
+__global__ void slab_finish_kernel(LatticeConsts c, DevScalars *sc, const double *tot, int slot) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) finish_a<T, MODE>(c, sc, tot, slot);
 }
 
 }  // namespace gabe

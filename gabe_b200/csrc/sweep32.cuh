@@ -141,6 +141,7 @@ struct Tile32 {
     float *Xo, *Do;      // new fields and momenta (sweep B)
     float *S;            // GW sources [10][N][N][N+2] (sweep A with sources)
     int k0, j0, i0, i1;
+    int planes;          // planes per field in X, D, Xo, Do (slab, no wrap along i); 0 = N, periodic
 };
 
 // The plane march of one TK x TJ tile over planes i0 .. i1-1 by a block of NT
@@ -156,7 +157,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     static_assert(TK2 * TJ >= 2 * TK2 + 2 * TJ, "enough threads for the halo copies");
     static_assert(NT >= TK2 * TJ, "block smaller than the tile");
     const int N = c.N;
-    const int n3 = N * N * N;  // N^3 < 2^31 for N <= 1024
+    const int n3 = (t.planes ? t.planes : N) * N * N;  // < 2^31 for N <= 1024
     const int tid = threadIdx.x;
     const bool act = NT == TK2 * TJ || tid < TK2 * TJ;
     const int tx = tid % TK2, ty = tid / TK2;
@@ -188,7 +189,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     auto issue = [&](int p, int sl) {  // plane p (wrapped) into slot sl
         if (!act) return;
         float *slot = ring + sl * Rg::SLOT;
-        const int pb = wrapi(p, N) * NN;
+        const int pb = (t.planes ? p : wrapi(p, N)) * NN;
 #pragma unroll
         for (int a = 0; a < 4; a++) {
             float *sa = slot + a * Rg::ARR;
@@ -310,8 +311,10 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
     t.S = static_cast<float *>(args.S);
     t.k0 = blockIdx.x * 2 * TK2;
     t.j0 = blockIdx.y * TJ;
-    t.i0 = blockIdx.z * args.ci;
-    t.i1 = min(t.i0 + args.ci, N);
+    t.planes = args.planes;
+    const int first = args.planes ? 1 : 0, end = args.planes ? args.planes - 1 : N;  // own planes
+    t.i0 = first + blockIdx.z * args.ci;
+    t.i1 = min(t.i0 + args.ci, end);
 
     const Site32 s = site32_consts<MODE>(c, args.sc);
     double acc[kNV];
@@ -330,7 +333,10 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
         double tot[kNV];
         sum_partials<kNV>(args.partials, gridDim.x * gridDim.y * gridDim.z, tot, sred);
         if (tid == 0) {
-            finish_a<float, MODE>(c, args.sc, tot, args.slot);
+            if (args.sums_out)
+                for (int q = 0; q < kNV; q++) args.sums_out[q] = tot[q];
+            else
+                finish_a<float, MODE>(c, args.sc, tot, args.slot);
             *args.counter = 0u;
         }
     } else if (tid == 0) {

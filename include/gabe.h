@@ -293,6 +293,64 @@ size_t gabe_ensemble_device_bytes(const gabe_ensemble *e);
 void *gabe_ensemble_stream(const gabe_ensemble *e);
 int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
 
+/* ------------------------------------------------------------------------
+ * One slab of a lattice split along i over several processes (one GPU each).
+ *
+ * The reference evolves one lattice in one process (step(),
+ * g2functions.cpp:234-271, OpenMP over i).  A lattice larger than one GPU
+ * is split into slabs of whole planes i in [plane0, plane0 + nplanes); each
+ * rank creates one slab and, per step, makes the calls below, with the
+ * communication between them its own (e.g. NCCL through torch.distributed):
+ *
+ *   gabe_slab_sweep(s, 0)     sweep A: stage-1 sums of this slab -> sums
+ *   all-reduce(sums, kNV = 8 FP64 values, sum) over the ranks
+ *   gabe_slab_finish(s, 0)    adot0, a[1], adot[1] from the global sums
+ *   gabe_slab_sweep(s, 1)     sweep B: new state, a[0]
+ *   gabe_slab_pack(s)         own boundary planes -> send_lo / send_hi
+ *   exchange: send_lo -> rank below's recv_hi, send_hi -> rank above's recv_lo
+ *                             (periodic in i)
+ *   gabe_slab_unpack(s)       recv_lo / recv_hi -> halo planes
+ *
+ * After gabe_slab_upload, exchange the halos (pack, exchange, unpack) and
+ * take the energies with gabe_slab_sweep(s, 2), all-reduce, and
+ * gabe_slab_finish(s, 2), as calcEnergy(0) after the reference's
+ * initialisation.  All calls enqueue on the slab's stream
+ * (gabe_slab_stream); order the exchange after it.  Fields only: gws_on
+ * must be 0 (the distributed 3-D transform of the GW sources is not part
+ * of this interface).  No counterpart in the reference. */
+typedef struct gabe_slab gabe_slab;
+typedef struct {
+    int32_t struct_size; /* sizeof(gabe_slab_params) */
+    int32_t plane0;      /* first own plane (global index i) */
+    int32_t nplanes;     /* own planes, >= 1 */
+    int32_t reserved;
+} gabe_slab_params;
+
+int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab **out);
+int gabe_slab_destroy(gabe_slab *s);
+const char *gabe_slab_last_error(gabe_slab *s); /* NULL: the last failed create on this thread */
+
+/* Own planes of stage 0, [2][nplanes][N][N] FP64 (the reference's layout
+ * restricted to the slab).  mean = {<phi>, <chi>, <phidot>, <chidot>} of the
+ * whole lattice (FP32 storage; ignored for FP64). */
+int gabe_slab_upload(gabe_slab *s, const double *field0, const double *dfield0, const double mean[4], double a0,
+                     double adot0);
+int gabe_slab_download(gabe_slab *s, double *field0, double *dfield0);
+
+/* Device buffers: the kNV stage sums, and the packed boundary planes (four
+ * arrays phi, chi, phidot, chidot of N^2 values in the storage precision:
+ * halo_bytes each). */
+int gabe_slab_buffers(gabe_slab *s, double **sums, void **send_lo, void **send_hi, void **recv_lo, void **recv_hi,
+                      size_t *halo_bytes);
+int gabe_slab_sweep(gabe_slab *s, int which);  /* 0 sweep A, 1 sweep B, 2 energies of the current state */
+int gabe_slab_finish(gabe_slab *s, int which); /* 0 after sweep A, 2 after the energies */
+int gabe_slab_pack(gabe_slab *s);
+int gabe_slab_unpack(gabe_slab *s);
+int gabe_slab_stream(gabe_slab *s, void **stream);
+int gabe_slab_sync(gabe_slab *s);
+/* a, adot, edkin, edpot, edgrad, edrho, two stages each (synchronises) */
+int gabe_slab_scalars(gabe_slab *s, double out12[12]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,141 @@
+"""A lattice split into slabs along i (gabe_slab_* through gabe_b200.slab)
+against the same lattice on one handle (gabe_create), fields only.
+
+* One slab holds the whole lattice between two halo planes that are copies
+  of its own end planes: same tiles, same plane chunks, the same block sums
+  in the same order, so FP64 results are bit for bit those of the handle --
+  through the in-process communicator and through a one-rank NCCL group.
+* Several slabs in one process (the ranks' kernels never wait on each
+  other: sums are added on the host, halos copied between steps) differ
+  from the handle only in the order of the energy sums: FP64 to ~1e-12,
+  FP32 (fluctuations about the FP64 mean) to its rounding.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+
+import gabe_b200 as gb
+from gabe_b200 import slab as gs
+from gabe_b200.ic import random_state
+
+pytestmark = pytest.mark.gpu
+
+STEPS = 6
+
+
+def _state(N, seed=5):
+    f, d, a0, ad0 = random_state(N, seed=seed)
+    return f.numpy(), d.numpy(), a0, ad0
+
+
+def _whole(N, precision, st, steps):
+    f, d, a0, ad0 = st
+    with gb.Lattice(N, precision=precision) as lat:
+        lat.upload_state(f, d, a0=a0, adot0=ad0)
+        lat.step(steps)
+        sc = lat.scalars()
+        f1, d1, _, _ = lat.download_state()
+    want = np.array([v for k in ("a", "adot", "edkin", "edpot", "edgrad", "edrho") for v in sc[k]])
+    return f1, d1, want
+
+
+def _slabs(N, precision, st, steps, comm):
+    f, d, a0, ad0 = st
+    with gs.SlabLattice(N, comm, precision=precision) as lat:
+        fs = [f[:, p0:p0 + n] for p0, n in lat.planes]
+        ds = [d[:, p0:p0 + n] for p0, n in lat.planes]
+        lat.upload(fs if len(fs) > 1 else fs[0], ds if len(ds) > 1 else ds[0], a0, ad0)
+        lat.step(steps)
+        sc = lat.scalars()
+        per = [s.scalars() for s in lat.slabs]
+        out = lat.download()
+    f1 = np.concatenate([o[0] for o in out], axis=1)
+    d1 = np.concatenate([o[1] for o in out], axis=1)
+    for p in per[1:]:
+        np.testing.assert_array_equal(p, per[0])  # every slab holds the same scalars
+    return f1, d1, sc
+
+
+def test_one_slab_is_the_whole_lattice_bitwise():
+    N = 32
+    st = _state(N)
+    f0, d0, s0 = _whole(N, gb.FP64, st, STEPS)
+    f1, d1, s1 = _slabs(N, gb.FP64, st, STEPS, gs.LocalComm(1))
+    np.testing.assert_array_equal(f1, f0)
+    np.testing.assert_array_equal(d1, d0)
+    np.testing.assert_array_equal(s1, s0)
+
+
+@pytest.mark.parametrize("world", [2, 3, 4])
+def test_slabs_match_the_whole_lattice_fp64(world):
+    N = 32
+    st = _state(N, seed=9)
+    f0, d0, s0 = _whole(N, gb.FP64, st, STEPS)
+    f1, d1, s1 = _slabs(N, gb.FP64, st, STEPS, gs.LocalComm(world))
+    # the fields see the scalars only through a and adot, which differ in the last bits
+    for x, y in ((f1, f0), (d1, d0)):
+        for fld in range(2):
+            fl = y[fld] - y[fld].mean()
+            assert np.abs(x[fld] - y[fld]).max() <= 1e-10 * np.abs(fl).max()
+    rho = s0[10]
+    for q in range(12):
+        tol = 1e-12 * (abs(rho) if q in (8, 9) else abs(s0[q]))
+        assert abs(s1[q] - s0[q]) <= tol, (q, s1[q], s0[q])
+
+
+def test_slabs_match_the_whole_lattice_fp32():
+    N = 64
+    st = _state(N, seed=13)
+    f0, d0, s0 = _whole(N, gb.FP32, st, STEPS)
+    f1, d1, s1 = _slabs(N, gb.FP32, st, STEPS, gs.LocalComm(3))
+    for x, y in ((f1, f0), (d1, d0)):
+        for fld in range(2):
+            fl = y[fld] - y[fld].mean()
+            assert np.abs(x[fld] - y[fld]).max() <= 1e-5 * np.abs(fl).max()
+    rho = s0[10]
+    for q in range(12):
+        tol = 1e-6 * (abs(rho) if q in (8, 9) else abs(s0[q]))
+        assert abs(s1[q] - s0[q]) <= tol, (q, s1[q], s0[q])
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def test_one_rank_nccl_group_is_the_whole_lattice_bitwise():
+    import datetime
+
+    import torch.distributed as dist
+
+    N = 32
+    st = _state(N, seed=21)
+    f0, d0, s0 = _whole(N, gb.FP64, st, STEPS)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        f1, d1, s1 = _slabs(N, gb.FP64, st, STEPS, gs.DistComm())
+    finally:
+        dist.destroy_process_group()
+    np.testing.assert_array_equal(f1, f0)
+    np.testing.assert_array_equal(d1, d0)
+    np.testing.assert_array_equal(s1, s0)
+
+
+def test_slab_rejects_sweeps_before_upload():
+    s = gs.Slab(32, 0, 32)
+    try:
+        with pytest.raises(gb.GabeError):
+            s.sweep(0)
+        with pytest.raises(gb.GabeError):
+            s.sweep(7)
+    finally:
+        s.close()

@@ -1,0 +1,161 @@
+"""Host side of the slab decomposition (gabe_b200.slab, gabe_slab_*), on the
+CPU: the plane split, gabe_slab_create's parameter checks (made before any
+CUDA call), and the per-step protocol -- all-reduce of the stage sums and
+the periodic ring exchange of boundary planes -- through a world-size-3 gloo
+process group with stand-in slabs that hold CPU tensors."""
+import ctypes
+import datetime
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import gabe_b200 as gb
+from gabe_b200 import slab as gs
+
+
+@pytest.mark.parametrize("N,world", [(32, 1), (32, 3), (64, 4), (48, 5), (16, 16)])
+def test_split_planes_covers_the_lattice(N, world):
+    parts = gs.split_planes(N, world)
+    assert len(parts) == world
+    assert parts[0][0] == 0 and sum(n for _, n in parts) == N
+    for (p0, n), (q0, _) in zip(parts, parts[1:]):
+        assert q0 == p0 + n
+    sizes = [n for _, n in parts]
+    assert max(sizes) - min(sizes) <= 1 and min(sizes) >= 1
+
+
+def test_split_planes_rejects_more_ranks_than_planes():
+    with pytest.raises(ValueError):
+        gs.split_planes(16, 17)
+
+
+@pytest.mark.parametrize("case", ["gws", "planes_hi", "planes_neg", "empty", "N", "size"])
+def test_slab_create_rejects_bad_params(case):
+    lib = gs._lib()
+    p = gb.Params()
+    lib.gabe_default_params(ctypes.byref(p), 32)
+    sp = gs.SlabParams(ctypes.sizeof(gs.SlabParams), 0, 8, 0)
+    if case == "gws":
+        p.gws_on = 1
+    elif case == "planes_hi":
+        sp.plane0, sp.nplanes = 28, 8
+    elif case == "planes_neg":
+        sp.plane0 = -1
+    elif case == "empty":
+        sp.nplanes = 0
+    elif case == "N":
+        p.N = 40
+    elif case == "size":
+        sp.struct_size = 4
+    h = ctypes.c_void_p()
+    assert lib.gabe_slab_create(ctypes.byref(p), ctypes.byref(sp), ctypes.byref(h)) == 1
+    assert not h.value
+    assert lib.gabe_slab_last_error(None)
+
+
+class FakeSlab:
+    """Stands in for gs.Slab: CPU tensors for the sums and boundary planes,
+    and a log of the stage calls.  Its 'sweeps' put rank-dependent values in
+    the sums; 'pack' writes a pattern naming the rank and the side."""
+
+    def __init__(self, rank, plane0, nplanes, log):
+        self.rank, self.plane0, self.nplanes, self.log = rank, plane0, nplanes, log
+        self.t = {"sums": torch.zeros(gs.KNV, dtype=torch.float64)}
+        for k in ("send_lo", "send_hi", "recv_lo", "recv_hi"):
+            self.t[k] = torch.zeros(16, dtype=torch.uint8)
+        self.finished = []
+
+    def tensor(self, name):
+        return self.t[name]
+
+    def sync(self):
+        pass
+
+    def sweep(self, which):
+        self.log.append(("sweep", which))
+        if which in (0, 2):
+            self.t["sums"][:] = torch.arange(gs.KNV, dtype=torch.float64) + 10.0 * (self.rank + 1) + which
+
+    def finish(self, which):
+        self.log.append(("finish", which))
+        self.finished.append(self.t["sums"].clone())
+
+    def pack(self):
+        self.log.append(("pack",))
+        self.t["send_lo"][:] = 10 * self.rank + 1
+        self.t["send_hi"][:] = 10 * self.rank + 2
+
+    def unpack(self):
+        self.log.append(("unpack",))
+
+    def upload(self, f, d, mean, a0, adot0):
+        self.log.append(("upload", None if mean is None else tuple(np.round(mean, 12))))
+
+    def close(self):
+        pass
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _protocol_worker(rank, world, port, N, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        log = []
+        made = []
+
+        def factory(p0, n):
+            made.append(FakeSlab(rank, p0, n, log))
+            return made[-1]
+
+        lat = gs.SlabLattice(N, gs.DistComm(), precision=gb.FP32, slab_factory=factory)
+        (s,) = made
+        ok = lat.planes == [gs.split_planes(N, world)[rank]]
+        # upload: the whole lattice's means come from the ranks' own planes
+        p0, n = lat.planes[0]
+        f = np.zeros((2, n, N, N))
+        f[0] += 1.0 + p0  # phi differs per rank
+        d = np.ones((2, n, N, N))
+        lat.upload(f, d, 1.0, 0.5)
+        want_phi = sum((1.0 + a) * b for a, b in gs.split_planes(N, world)) * N * N / float(N) ** 3
+        ok &= log[0][0] == "upload" and abs(log[0][1][0] - want_phi) < 1e-12 and log[0][1][2] == 1.0
+        log.clear()
+        s.finished.clear()
+        lat.step(2)
+        want_log = [("sweep", 0), ("finish", 0), ("sweep", 1), ("pack",), ("unpack",)] * 2
+        ok &= log == want_log
+        # every rank finished with the sum over ranks of its stage sums
+        tot = sum(torch.arange(gs.KNV, dtype=torch.float64) + 10.0 * (r + 1) for r in range(world))
+        ok &= all(torch.equal(t, tot) for t in s.finished)
+        # ring: recv_lo holds the top plane of the rank below, recv_hi the bottom plane of the rank above
+        lo, hi = (rank - 1) % world, (rank + 1) % world
+        ok &= bool((s.tensor("recv_lo") == 10 * lo + 2).all()) and bool((s.tensor("recv_hi") == 10 * hi + 1).all())
+        q.put(bool(ok))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_protocol_over_gloo_ranks(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_protocol_worker, args=(r, world, port, 24, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    assert all(q.get(timeout=5) for _ in range(world))
