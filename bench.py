@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--lattice-flags", type=int, default=0,
                     help="gabe_params.flags of the lattices (e.g. 16: GABE_FLAG_OWN_FFT, 8: GABE_FLAG_FUSED_KSPACE)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
+    ap.add_argument("--no-slab", action="store_true", help="skip the slab leg (one lattice split over the ranks)")
+    ap.add_argument("--slab-N", type=int, default=512, help="lattice of the slab leg")
+    ap.add_argument("--slab-steps", type=int, default=20)
     ap.add_argument("--ens-lattices", type=int, default=256)
     ap.add_argument("--ens-steps", type=int, default=200, help="timed ensemble steps (multiple of --ens-every)")
     ap.add_argument("--ens-every", type=int, default=50, help="steps between log-spectra outputs")
@@ -194,6 +197,60 @@ def cpu_reference_sample(N: int, steps: int, warm: int = 1):
     po.step(stt, steps)
     dt = time.perf_counter() - t0
     return Np ** 3 * steps / dt, {"kind": "port", "cores": 1, "sample": f"oracle port, {Np}^3 GW on, {steps} steps"}
+
+
+def slab_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ranks):
+    """One lattice split into slabs of planes along i over the ranks (fields
+    only, FP32 storage): per step sweep A, an all-reduce of the 8 stage sums,
+    the finish, sweep B and the exchange of boundary planes (strong scaling:
+    the lattice is fixed).  Timed with CUDA events on the slab's stream,
+    which record the whole step including the waits for the exchanges; max
+    over ranks."""
+    import numpy as np
+    import torch
+
+    import gabe_b200 as gb
+    from gabe_b200 import slab as gs
+    from gabe_b200.ic import random_state
+
+    N, K, W = args.slab_N, args.slab_steps, max(3, args.warmup)
+    lat = None
+    ok = 1.0
+    try:
+        comm = gs.DistComm() if dist else gs.LocalComm(1)
+        lat = gs.SlabLattice(N, comm, precision=gb.FP32, device=local)
+        (p0, n), = lat.planes
+        f, d, a0, ad0 = random_state(N, seed=11, device="cuda")
+        fl, dl = f[:, p0:p0 + n].cpu().numpy(), d[:, p0:p0 + n].cpu().numpy()
+        mean = np.array([float(f[0].mean()), float(f[1].mean()), float(d[0].mean()), float(d[1].mean())])
+        del f, d
+        torch.cuda.empty_cache()
+    except Exception as e:  # noqa: BLE001 -- reported in the line, and every rank skips together
+        ok, err = 0.0, f"{type(e).__name__}: {e}"
+    if max_over_ranks(-ok) > -1.0:  # some rank failed its setup
+        if lat:
+            lat.close()
+        return {"skipped": err if ok == 0.0 else "setup failed on another rank"}
+    lat.upload(fl, dl, a0, ad0, mean=mean)
+    lat.step(W)
+    (s,) = lat.slabs
+    stream = torch.cuda.ExternalStream(s.stream_ptr)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    barrier()
+    ev[0].record(stream)
+    lat.step(K)
+    ev[1].record(stream)
+    ev[1].synchronize()
+    ms = max_over_ranks(ev[0].elapsed_time(ev[1]))
+    sc = lat.scalars()
+    lat.close()
+    sites = float(N) ** 3
+    return {"workload": f"{N}^3 lattice split into {world} slab(s) of planes along i, fields only (GWs off), "
+                        f"FP32 storage; per step: sweep A, all-reduce of 8 FP64 sums, finish, sweep B, "
+                        f"boundary-plane exchange",
+            "planes": [list(pp) for pp in gs.split_planes(N, world)], "scaling": "strong", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": ms / K, "site_updates_per_s": sites * K / (ms / 1e3),
+            "halo_bytes_per_rank_per_step": 2 * s.halo_bytes, "finite": bool(np.all(np.isfinite(sc)))}
 
 
 def ensemble_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ranks):
@@ -454,6 +511,8 @@ def main():
     line.update(extra)
     if not args.no_ensemble:
         line["ensemble"] = ensemble_leg(args, rank, world, local, dist, barrier, max_over_ranks)
+    if not args.no_slab:
+        line["slab"] = slab_leg(args, rank, world, local, dist, barrier, max_over_ranks)
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         v, info = cpu_reference_sample(args.ref_N, 2, warm=1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
