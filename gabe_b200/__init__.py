@@ -314,6 +314,8 @@ class EnsParams(ctypes.Structure):
         ("lam", ctypes.c_double), ("phi0", ctypes.c_double), ("dphi0", ctypes.c_double),
         ("gws_on", ctypes.c_int32), ("device", ctypes.c_int32), ("nlog", ctypes.c_int32),
         ("gw_spec_quirk", ctypes.c_int32), ("flags", ctypes.c_int32), ("log_top_bin", ctypes.c_int32),
+        ("spec_cut_off", ctypes.c_double), ("spec_smooth", ctypes.c_double),
+        ("ic_deterministic", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -349,7 +351,8 @@ class Ensemble:
 
     def __init__(self, N, g2_over_lambda, amplitude, seed, *, L: float = 20.0, dt: float = 0.01,
                  lam: float = 9e-14, phi0: float = 0.342, dphi0: float = 0.0, gws: bool = True, nlog: int = 64,
-                 tiles="auto", device: int = -1, flags: int = 0, gw_spec_quirk: bool = True, log_top_bin: int = 0):
+                 tiles="auto", device: int = -1, flags: int = 0, gw_spec_quirk: bool = True, log_top_bin: int = 0,
+                 spec_cut_off: float | None = None, spec_smooth: float = 0.5, full_rand: bool = True):
         lib = _ens_lib()
         self.N = np.ascontiguousarray(N, dtype=np.int32)
         self.nlat = len(self.N)
@@ -382,6 +385,10 @@ class Ensemble:
         p.L, p.dt, p.lam, p.phi0, p.dphi0 = L, dt, lam, phi0, dphi0
         p.gws_on, p.device, p.nlog, p.gw_spec_quirk, p.flags = int(gws), device, nlog, int(gw_spec_quirk), flags
         p.log_top_bin = int(log_top_bin)
+        # the reference's spec_cut_off / spec_smooth / field_full_rand (as gabe_b200.ic.random_state)
+        p.spec_cut_off = float(spec_cut_off) if spec_cut_off is not None else 0.0
+        p.spec_smooth = float(spec_smooth)
+        p.ic_deterministic = 0 if full_rand else 1
         self._p = p
         self._h = ctypes.c_void_p()
         rc = lib.gabe_ensemble_create(ctypes.byref(p), ctypes.byref(self._h))

@@ -29,7 +29,8 @@ constexpr int kEnsBinBlocks = 32;  // binning blocks per lattice
 }  // namespace
 
 struct gabe_ensemble {
-    int nlat = 0, dev = 0, nlog = 0, quirk = 1, gws = 1, flags = 0;
+    int nlat = 0, dev = 0, nlog = 0, quirk = 1, gws = 1, flags = 0, ic_det = 0;
+    double spec_cut = 0., spec_smooth = 0.5;
     double L = 20., dt = 0.01, lambda = 9e-14, phi0 = 0.342, dphi0 = 0.;
     std::vector<int> N, shape, ci;
     std::vector<double> g, amp;
@@ -232,7 +233,9 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
     if (p->nlat < 1 || !p->N || !p->g2_over_lambda || !p->amplitude || !p->seed)
         return eset(nullptr, GABE_ERR_PARAM, "nlat and the per-lattice arrays are required");
     if (!(p->L > 0) || !(p->dt > 0) || !(p->lambda > 0) || !(p->phi0 != 0) || p->nlog < 1 || p->nlog > 4096 ||
-        p->log_top_bin < 0 || p->log_top_bin > (1 << 20))
+        p->log_top_bin < 0 || p->log_top_bin > (1 << 20) || !(p->spec_cut_off >= 0) ||
+        (p->spec_cut_off > 0 && !(p->spec_smooth > 0 && std::isfinite(p->spec_smooth))) ||
+        (p->ic_deterministic != 0 && p->ic_deterministic != 1) || (p->ic_deterministic && !(p->spec_cut_off > 0)))
         return eset(nullptr, GABE_ERR_PARAM, "invalid shared parameters");
     for (int l = 0; l < p->nlat; l++) {
         const int n = p->N[l];
@@ -255,6 +258,9 @@ int gabe_ensemble_create(const gabe_ensemble_params *p, gabe_ensemble **out) {
     e->gws = p->gws_on ? 1 : 0;
     e->nlog = p->nlog;
     e->quirk = p->gw_spec_quirk;
+    e->spec_cut = p->spec_cut_off;
+    e->spec_smooth = p->spec_smooth;
+    e->ic_det = p->ic_deterministic;
     e->flags = p->flags;
     e->N.assign(p->N, p->N + p->nlat);
     e->g.assign(p->g2_over_lambda, p->g2_over_lambda + p->nlat);
@@ -423,7 +429,8 @@ int gabe_ensemble_init(gabe_ensemble *e) {
     std::vector<double> m2(e->nlat, 3. * lam_pr * e->phi0 * e->phi0);
     for (int fld = 0; fld < 2; fld++) {
         ECK(e, cudaMemcpyAsync(e->d_m2, m2.data(), sizeof(double) * e->nlat, cudaMemcpyHostToDevice, e->stream));
-        ens_ic_modes_kernel<<<dim3(gx, e->nlat), 256, 0, e->stream>>>(e->d_lat, fld, e->d_m2, H0, e->L);
+        ens_ic_modes_kernel<<<dim3(gx, e->nlat), 256, 0, e->stream>>>(e->d_lat, fld, e->d_m2, H0, e->L, e->spec_cut,
+                                                                    e->spec_smooth, e->ic_det);
         ECK(e, cudaGetLastError());
         ens_ic_symm_kernel<<<dim3(64, e->nlat), 256, 0, e->stream>>>(e->d_lat);
         ECK(e, cudaGetLastError());

@@ -177,7 +177,8 @@ __device__ __forceinline__ double u01(unsigned x) { return ((double)x + 0.5) * (
 // (R1+R2)/sqrt2, fdot_k = i-rotated (R2-R1) omega/sqrt2 - H0 f_k, zero mode 0.
 // Writes f_k to complex slot 0 and fdot_k to slot 1 of the lattice's buffer.
 __global__ void __launch_bounds__(256) ens_ic_modes_kernel(const EnsLat *lats, int fld, const double *m2,
-                                                           double H0, double L) {
+                                                           double H0, double L, double cut, double smooth,
+                                                           int deterministic) {
     const EnsLat &E = lats[blockIdx.y];
     const int N = E.N, nz = N / 2 + 1;
     const size_t M = (size_t)N * N * nz;
@@ -199,10 +200,19 @@ __global__ void __launch_bounds__(256) ens_ic_modes_kernel(const EnsLat *lats, i
         }
         const double i2 = i < N / 2 + 1 ? (double)i * i : (double)(N - i) * (N - i);
         const double j2 = j < N / 2 + 1 ? (double)j * j : (double)(N - j) * (N - j);
-        const double wk = sqrt(dk2 * (i2 + j2 + (double)kz * kz) + m2e);
+        const double n2 = i2 + j2 + (double)kz * kz;
+        const double wk = sqrt(dk2 * n2 + m2e);
+        // spectral window of spec_cut_off (g2init.cpp:117-165); 1 without a cut-off
+        const double win = cut > 0 ? 0.5 * (1. - tanh(smooth * (sqrt(n2) - N * cut))) : 1.;
+        if (deterministic) {  // field_full_rand 0: real amplitude, no draws
+            const double amp = B * sqrt(1. / (2. * wk * L3)) * win;
+            fk[idx] = Cplx<float>{(float)amp, 0.f};
+            fd[idx] = Cplx<float>{(float)(-H0 * amp), 0.f};
+            continue;
+        }
         const uint4 r = philox4x32_10(make_uint4((unsigned)idx, (unsigned)(idx >> 32), 0u, 0u), key);
-        const double a1 = B * sqrt(-log(u01(r.x)) / (2. * wk * L3)), th1 = 2. * M_PI * u01(r.y);
-        const double a2 = B * sqrt(-log(u01(r.z)) / (2. * wk * L3)), th2 = 2. * M_PI * u01(r.w);
+        const double a1 = win * B * sqrt(-log(u01(r.x)) / (2. * wk * L3)), th1 = 2. * M_PI * u01(r.y);
+        const double a2 = win * B * sqrt(-log(u01(r.z)) / (2. * wk * L3)), th2 = 2. * M_PI * u01(r.w);
         const double r1re = a1 * cos(th1), r1im = a1 * sin(th1), r2re = a2 * cos(th2), r2im = a2 * sin(th2);
         const double fre = (r1re + r2re) / s2, fim = (r1im + r2im) / s2;
         fk[idx] = Cplx<float>{(float)fre, (float)fim};

@@ -244,6 +244,14 @@ typedef struct {
     int32_t flags;                  /* GABE_FLAG_NO_GRAPH */
     int32_t log_top_bin;            /* upper end of the log bins in native-bin units (0 = the native
                                        bins of the largest lattice); fix it to compare ensembles */
+    /* initial-spectrum knobs of the reference's randInit (g2init.cpp:117-165), for every lattice:
+       spec_cut_off > 0 multiplies each mode's amplitude by
+       (1 - tanh(spec_smooth (|n| - N spec_cut_off))) / 2 (spec_cut_off, spec_smooth); 0 = none.
+       ic_deterministic = 1 replaces the random draws by the real amplitude sqrt(1/(2 omega L^3))
+       and fdot_k = -H0 f_k (field_full_rand 0; needs spec_cut_off > 0, as in the reference). */
+    double spec_cut_off, spec_smooth;
+    int32_t ic_deterministic;
+    int32_t reserved;
 } gabe_ensemble_params;
 
 typedef struct gabe_ensemble gabe_ensemble;

@@ -36,7 +36,7 @@ def _params(N, g=None, amp=None, seed=None, **kw):
 
 
 @pytest.mark.parametrize("case", ["N_not_16", "N_small", "neg_amp", "nan_g", "nlog0", "dt0", "nlat0", "size",
-                                  "log_top"])
+                                  "log_top", "cut_neg", "smooth0", "det_without_cut", "det_2"])
 def test_ensemble_create_rejects_bad_params(case):
     lib = gb._ens_lib()
     N, g, amp, kw = [32, 48], None, None, {}
@@ -58,6 +58,14 @@ def test_ensemble_create_rejects_bad_params(case):
         kw = {"struct_size": 8}
     elif case == "log_top":
         kw = {"log_top_bin": -1}
+    elif case == "cut_neg":
+        kw = {"spec_cut_off": -0.1}
+    elif case == "smooth0":
+        kw = {"spec_cut_off": 0.25, "spec_smooth": 0.0}
+    elif case == "det_without_cut":
+        kw = {"ic_deterministic": 1}
+    elif case == "det_2":
+        kw = {"spec_cut_off": 0.25, "spec_smooth": 0.5, "ic_deterministic": 2}
     p, keep = _params(N, g, amp, **kw)
     h = ctypes.c_void_p()
     assert lib.gabe_ensemble_create(ctypes.byref(p), ctypes.byref(h)) == 1

@@ -152,3 +152,44 @@ def test_ensemble_log_spectra_are_rebinned_native_bins():
         m = sums[s] > floor
         assert np.max(np.abs(nat[1, s, :nb][m] - sums[s][m]) / sums[s][m]) <= 1e-3
         assert np.all(np.abs(nat[1, s, :nb][~m]) <= 10 * floor)
+
+
+def test_deterministic_initial_spectrum_matches_the_host_generator():
+    """field_full_rand 0 with spec_cut_off: no random draws, so the device
+    generator's state is the host generator's (gabe_b200.ic) up to FP32
+    storage and transform rounding."""
+    from gabe_b200.ic import random_state
+
+    sizes, g, amp = [32, 48], [100.0, 20.0], [1.0, 1.5]
+    with gb.Ensemble(sizes, g, amp, [1, 2], nlog=8, tiles=None, spec_cut_off=0.25, spec_smooth=0.5,
+                     full_rand=False) as ens:
+        ens.init()
+        got = [ens.download(l) for l in range(2)]
+    for l, n in enumerate(sizes):
+        f, d, _, _ = random_state(n, model_c=gb.lphi4_constants(g[l]), amplitude=amp[l], spec_cut_off=0.25,
+                                  spec_smooth=0.5, full_rand=False)
+        f, d = f.numpy(), d.numpy()
+        for x, y in ((got[l][0], f), (got[l][1], d)):
+            for fld in range(2):
+                fl = y[fld] - y[fld].mean()
+                assert np.abs(fl).max() > 0
+                assert np.abs((x[fld] - x[fld].mean()) - fl).max() <= 1e-4 * np.abs(fl).max(), (l, fld)
+
+
+def test_spectral_cut_off_windows_the_random_initial_spectrum():
+    """spec_cut_off with random draws: the draws are the same as without the
+    cut, so the phi spectrum (its effective mass does not depend on the
+    fluctuations) is the uncut one times the window squared: unchanged well
+    below N * cut, suppressed well above."""
+    n, cut, smooth = 64, 0.25, 0.5
+    nat = []
+    for c in (None, cut):
+        with gb.Ensemble([n], [100.0], [1.0], [31], nlog=8, tiles=None, gws=False, spec_cut_off=c,
+                         spec_smooth=smooth) as ens:
+            ens.init()
+            nat.append(ens.log_spectra()[2][0])
+    (p0, p1) = (nat[0][0], nat[1][0])  # phi native-bin sums
+    for b in range(1, int(n * cut) - 10):
+        assert abs(p1[b] / p0[b] - 1.0) <= 1e-3, (b, p1[b], p0[b])
+    for b in range(int(n * cut) + 10, int(n * cut) + 20):
+        assert p1[b] <= 1e-6 * p0[b], (b, p1[b], p0[b])
