@@ -512,7 +512,10 @@ def main():
     if not args.no_ensemble:
         line["ensemble"] = ensemble_leg(args, rank, world, local, dist, barrier, max_over_ranks)
     if not args.no_slab:
-        line["slab"] = slab_leg(args, rank, world, local, dist, barrier, max_over_ranks)
+        try:
+            line["slab"] = slab_leg(args, rank, world, local, dist, barrier, max_over_ranks)
+        except Exception as e:  # noqa: BLE001 -- the headline line is still printed
+            line["slab"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         v, info = cpu_reference_sample(args.ref_N, 2, warm=1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
