@@ -31,9 +31,9 @@ def _state(N, seed=5):
     return f.numpy(), d.numpy(), a0, ad0
 
 
-def _whole(N, precision, st, steps):
+def _whole(N, precision, st, steps, **kw):
     f, d, a0, ad0 = st
-    with gb.Lattice(N, precision=precision) as lat:
+    with gb.Lattice(N, precision=precision, **kw) as lat:
         lat.upload_state(f, d, a0=a0, adot0=ad0)
         lat.step(steps)
         sc = lat.scalars()
@@ -42,9 +42,9 @@ def _whole(N, precision, st, steps):
     return f1, d1, want
 
 
-def _slabs(N, precision, st, steps, comm):
+def _slabs(N, precision, st, steps, comm, **kw):
     f, d, a0, ad0 = st
-    with gs.SlabLattice(N, comm, precision=precision) as lat:
+    with gs.SlabLattice(N, comm, precision=precision, **kw) as lat:
         fs = [f[:, p0:p0 + n] for p0, n in lat.planes]
         ds = [d[:, p0:p0 + n] for p0, n in lat.planes]
         lat.upload(fs if len(fs) > 1 else fs[0], ds if len(ds) > 1 else ds[0], a0, ad0)
@@ -84,6 +84,36 @@ def test_slabs_match_the_whole_lattice_fp64(world):
     for q in range(12):
         tol = 1e-12 * (abs(rho) if q in (8, 9) else abs(s0[q]))
         assert abs(s1[q] - s0[q]) <= tol, (q, s1[q], s0[q])
+
+
+@pytest.mark.parametrize("case", ["expansion0", "expansion2", "quadratic", "one_plane_slabs"])
+def test_slab_variants_match_the_whole_lattice_fp64(case):
+    """expansion_type 0 and 2, the shipped m^2 phi^2 + g^2 phi^2 chi^2 model,
+    and slabs of a single plane (every halo plane is a neighbour's)."""
+    N, world, kw = 32, 4, {}
+    if case == "expansion0":
+        kw = {"expansion": 0}
+    elif case == "expansion2":
+        kw = {"expansion": 2}
+    elif case == "quadratic":
+        kw = {"model": gb.MODEL_QUADRATIC, "model_c": (1e-6, 2.5e-7)}
+    else:
+        N, world = 16, 16
+    if case == "quadratic":
+        f, d, a0, ad0 = random_state(N, seed=17, model=gb.MODEL_QUADRATIC, model_c=(1e-6, 2.5e-7), f0=(1.0, 0.0))
+        st = (f.numpy(), d.numpy(), a0, ad0)
+    else:
+        st = _state(N, seed=17)
+    f0, d0, s0 = _whole(N, gb.FP64, st, STEPS, **kw)
+    f1, d1, s1 = _slabs(N, gb.FP64, st, STEPS, gs.LocalComm(world), **kw)
+    for x, y in ((f1, f0), (d1, d0)):
+        for fld in range(2):
+            fl = y[fld] - y[fld].mean()
+            assert np.abs(x[fld] - y[fld]).max() <= 1e-10 * max(np.abs(fl).max(), 1e-300)
+    rho = s0[10]
+    for q in range(12):
+        tol = 1e-12 * (abs(rho) if q in (8, 9) else abs(s0[q])) + 1e-300
+        assert abs(s1[q] - s0[q]) <= tol, (case, q, s1[q], s0[q])
 
 
 def test_slabs_match_the_whole_lattice_fp32():
