@@ -22,6 +22,7 @@ the halos copied device to device).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 
 import numpy as np
@@ -175,14 +176,29 @@ class Slab:
         return out
 
 
+def _on_slab_stream(s):
+    """Torch work inside this context is ordered on the slab's CUDA stream
+    (after the library's kernels, before its next ones), so no host
+    synchronisation is needed around it; CPU stand-ins need none."""
+    if s.tensor("sums").is_cuda:
+        import torch
+
+        return torch.cuda.stream(torch.cuda.ExternalStream(s.stream_ptr))
+    return contextlib.nullcontext()
+
+
 class LocalComm:
     """Every slab of the lattice in this process (one GPU or several):
-    sums added on the host in rank order, halos copied device to device."""
+    sums added on the host in rank order, halos copied device to device.
+    A single slab needs neither: its sums are the totals, and its halos are
+    copies of its own end planes, taken on its stream."""
 
     def __init__(self, world: int):
         self.world = int(world)
 
     def allreduce_sums(self, slabs):
+        if len(slabs) == 1:
+            return
         for s in slabs:
             s.sync()
         tot = np.zeros(KNV)
@@ -199,6 +215,12 @@ class LocalComm:
     def exchange(self, slabs):
         import torch
 
+        if len(slabs) == 1:
+            (s,) = slabs
+            with _on_slab_stream(s):
+                s.tensor("recv_lo").copy_(s.tensor("send_hi"))
+                s.tensor("recv_hi").copy_(s.tensor("send_lo"))
+            return
         for s in slabs:
             s.sync()
         W = len(slabs)
@@ -224,18 +246,17 @@ class DistComm:
 
     def allreduce_sums(self, slabs):
         (s,) = slabs
-        s.sync()
-        self.dist.all_reduce(s.tensor("sums"), group=self.group)
-        _sync_torch(s)
+        with _on_slab_stream(s):  # NCCL: ordered on the slab's stream, no host round trip
+            self.dist.all_reduce(s.tensor("sums"), group=self.group)
 
     def exchange(self, slabs):
         (s,) = slabs
-        s.sync()
         W, r, d = self.world, self.rank, self.dist
-        if W == 1:
-            s.tensor("recv_lo").copy_(s.tensor("send_hi"))
-            s.tensor("recv_hi").copy_(s.tensor("send_lo"))
-        else:
+        with _on_slab_stream(s):
+            if W == 1:
+                s.tensor("recv_lo").copy_(s.tensor("send_hi"))
+                s.tensor("recv_hi").copy_(s.tensor("send_lo"))
+                return
             lo, hi = (r - 1) % W, (r + 1) % W
             g = lambda p: d.get_global_rank(self.group, p) if self.group is not None else p  # noqa: E731
             ops = [d.P2POp(d.isend, s.tensor("send_hi"), g(hi), self.group, tag=1),
@@ -243,16 +264,7 @@ class DistComm:
                    d.P2POp(d.irecv, s.tensor("recv_lo"), g(lo), self.group, tag=1),
                    d.P2POp(d.irecv, s.tensor("recv_hi"), g(hi), self.group, tag=0)]
             for w in d.batch_isend_irecv(ops):
-                w.wait()
-        _sync_torch(s)
-
-
-def _sync_torch(s):
-    t = s.tensor("sums")
-    if t.is_cuda:
-        import torch
-
-        torch.cuda.synchronize(t.device)
+                w.wait()  # NCCL: the slab's stream waits; gloo: the host waits
 
 
 class SlabLattice:
