@@ -59,6 +59,15 @@ cudaError_t fft3d_n(float *S, int ncomp, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int N>
+cudaError_t col_pass_n(const f3d::ColArgs &a, cudaStream_t s) {
+    int g = 0;
+    cudaError_t e = persistent_grid(f3d::col_fft_kernel<N>, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, &g);
+    if (e != cudaSuccess) return e;
+    f3d::col_fft_kernel<N><<<g, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 bool fft3d_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
@@ -69,6 +78,18 @@ cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s) {
         case 128: return fft3d_cols_n<128>(S, ncomp, s);
         case 256: return fft3d_cols_n<256>(S, ncomp, s);
         case 512: return fft3d_cols_n<512>(S, ncomp, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long long sn, int n1, int n2, int ncol,
+                             cudaStream_t s) {
+    f3d::ColArgs a{static_cast<float2 *>(X), s1, s2, sn, n1, n2, ncol};
+    switch (N) {
+        case 64: return col_pass_n<64>(a, s);
+        case 128: return col_pass_n<128>(a, s);
+        case 256: return col_pass_n<256>(a, s);
+        case 512: return col_pass_n<512>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

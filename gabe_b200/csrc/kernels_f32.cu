@@ -1,8 +1,11 @@
 // FP32-storage kernels; built with FMA contraction.
+#include <algorithm>
+
 #include "convert.cuh"
 #include "launch.h"
 #include "kspace_fused.cuh"
 #include "sweep32.cuh"
+#include "slabgw.cuh"
 #include "sweeprows.cuh"
 
 namespace gabe {
@@ -46,9 +49,41 @@ cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cu
 cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s) {
     switch (mode) {
         case MODE_A: slab_finish_kernel<float, MODE_A><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
+        case MODE_A_GW: slab_finish_kernel<float, MODE_A_GW><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
         case MODE_E0: slab_finish_kernel<float, MODE_E0><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+static unsigned slab_grid(size_t n) { return (unsigned)std::min<size_t>(148 * 8, (n + 255) / 256); }
+
+cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, cudaStream_t s) {
+    const size_t n = (size_t)10 * nloc * N * (N / 2 + 1);
+    slab_gw_pack_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(S), static_cast<Cplx<float> *>(send),
+                                                     N, nloc, Split(N, W));
+    return cudaGetLastError();
+}
+
+cudaError_t slab_gw_unpack_f32(const void *recv, void *T, int N, int m, int W, cudaStream_t s) {
+    const size_t n = (size_t)10 * N * m * (N / 2 + 1);
+    slab_gw_unpack_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(recv), static_cast<Cplx<float> *>(T),
+                                                       N, m, Split(N, W));
+    return cudaGetLastError();
+}
+
+cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
+                            cudaStream_t s) {
+    const size_t n = (size_t)c.N * m * (c.N / 2 + 1);
+    slab_kspace_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(T), static_cast<Cplx<float> *>(G), sc,
+                                                    c, m, y0);
+    return cudaGetLastError();
+}
+
+cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
+                                   cudaStream_t s) {
+    slab_gw_unpack_amplitudes_kernel<<<slab_grid(cnt), 256, 0, s>>>(static_cast<const Cplx<float> *>(G), cnt, m0, N, m,
+                                                                    y0, which, dst);
     return cudaGetLastError();
 }
 

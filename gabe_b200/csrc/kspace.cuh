@@ -92,21 +92,17 @@ __device__ __forceinline__ KsCoef<T> ks_coef(const LatticeConsts &c, const doubl
     return k;
 }
 
-// Both RK2 stages of the amplitudes of k-point idx of the half spectrum
-// [N][N][N/2+1] (M points): sources Sc [10][M], amplitudes G [4][M].
+// Both RK2 stages of the amplitudes of the k-point with integer wave vector
+// (px, py, kzi) stored at element idx of arrays of M points: sources Sc
+// [10][M], amplitudes G [4][M].
 template <typename T>
-__device__ __forceinline__ void kspace_point(const KsCoef<T> &kc, int N, size_t M, const Cplx<T> *Sc, Cplx<T> *G,
-                                             size_t idx) {
-    const int nz = N / 2 + 1;
+__device__ __forceinline__ void kspace_update(const KsCoef<T> &kc, int px, int py, int kzi, size_t M,
+                                              const Cplx<T> *Sc, Cplx<T> *G, size_t idx) {
     Cplx<T> s[10], g[4];
 #pragma unroll
     for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
 #pragma unroll
     for (int q = 0; q < 4; q++) g[q] = G[(size_t)q * M + idx];
-    const int kzi = (int)(idx % nz);
-    const size_t t = idx / nz;
-    const int j = (int)(t % N), i = (int)(t / N);
-    const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
     const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
     if (m2 == 0.0) return;  // no TT mode at k = 0; its amplitudes stay zero
     double ep[6], ex[6];
@@ -145,6 +141,18 @@ __device__ __forceinline__ void kspace_point(const KsCoef<T> &kc, int N, size_t 
         G[(size_t)p * M + idx] = hn;
         G[(size_t)(2 + p) * M + idx] = ln;
     }
+}
+
+// k-point idx of the half spectrum [N][N][N/2+1] (M points).
+template <typename T>
+__device__ __forceinline__ void kspace_point(const KsCoef<T> &kc, int N, size_t M, const Cplx<T> *Sc, Cplx<T> *G,
+                                             size_t idx) {
+    const int nz = N / 2 + 1;
+    const int kzi = (int)(idx % nz);
+    const size_t t = idx / nz;
+    const int j = (int)(t % N), i = (int)(t / N);
+    const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
+    kspace_update<T>(kc, px, py, kzi, M, Sc, G, idx);
 }
 
 template <typename T>

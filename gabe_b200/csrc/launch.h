@@ -113,6 +113,14 @@ cudaError_t sweep32_f32(int shape, int mode, const StencilArgs &a, dim3 grid, cu
 // Slab: finish_a of sweep A (mode MODE_A) or of the energies (MODE_E0) from the totals of all slabs.
 cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s);
 cudaError_t slab_finish_f64(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s);
+// Slab GW branch, FP32 (slabgw.cuh): pack the 2-D transforms for the all-to-all, unpack what
+// arrived into [10][N][m][nz], the k-space update of the rank's k-points, amplitudes -> 12 components.
+cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, cudaStream_t s);
+cudaError_t slab_gw_unpack_f32(const void *recv, void *T, int N, int m, int W, cudaStream_t s);
+cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
+                            cudaStream_t s);
+cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
+                                   cudaStream_t s);
 // FP32 sweep A with sources that writes them transformed along k (sweeprows.cuh):
 // one block per pair of rows and chunk of sweep32_rows_ci(N) planes.
 bool sweep32_rows_supported(int N);
@@ -144,6 +152,10 @@ cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out
 // FP32 in-place 3-D r2c of ncomp arrays [N][N][N+2] in three passes (fft3d.cuh).
 bool fft3d_supported(int N);
 cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s);
+// One column pass (fft3d.cuh col_fft_kernel): for b1 < n1, b2 < n2, c < ncol the N complex
+// values at X + b1 s1 + b2 s2 + n sn + c.
+cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long long sn, int n1, int n2, int ncol,
+                             cudaStream_t s);
 // Its passes along j and i alone, for sources already transformed along k.
 cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s);
 

@@ -20,8 +20,11 @@
 #include <new>
 #include <string>
 
+#include <cufft.h>
+
 #include "../../include/gabe.h"
 #include "launch.h"
+#include "slabsplit.h"
 
 using namespace gabe;
 
@@ -43,6 +46,16 @@ struct gabe_slab {
     void *send[2] = {nullptr, nullptr}, *recv[2] = {nullptr, nullptr};  // [lo, hi]: 4 planes each
     int shape = 0, ci = 1;
     dim3 grid;
+    // GW branch (FP32): the ranks' split, sources [10][nloc][N][N+2] (2-D transformed in place,
+    // then the all-to-all receive buffer), the send buffer (then T[10][N][m][nz]), amplitudes
+    // [4][N][m][nz] of this rank's ky columns [plane0, plane0 + nloc)
+    bool gws = false;
+    int W = 1, rank = 0;
+    float *S = nullptr;
+    void *Tb = nullptr, *G = nullptr, *fft_work = nullptr;
+    size_t nz = 0, cplx_loc = 0;  // complex values of one component over this rank's planes or columns
+    cufftHandle plan2d = 0;
+    bool have_plan = false;
     std::string err;
 };
 
@@ -91,7 +104,7 @@ StencilArgs slab_args(gabe_slab *s, int counter, double *sums_out) {
     a.D = s->D[s->cur];
     a.Xo = s->X[s->cur ^ 1];
     a.Do = s->D[s->cur ^ 1];
-    a.S = nullptr;
+    a.S = s->S;
     a.partials = s->partials;
     a.counter = s->counters + counter;
     a.sc = s->sc;
@@ -116,13 +129,23 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     const int N = p->N;
     if (N < 16 || N > 1024 || N % 16 || p->nflds != 2)
         return serr(nullptr, GABE_ERR_PARAM, "N must be a multiple of 16 in [16, 1024] and nflds 2");
-    if (p->gws_on) return serr(nullptr, GABE_ERR_PARAM, "slabs evolve the fields only (gws_on must be 0)");
+    if (p->gws_on && (p->precision != GABE_FP32 || (N != 64 && N != 128 && N != 256 && N != 512)))
+        return serr(nullptr, GABE_ERR_PARAM, "slabs with GWs need FP32 storage and N in {64, 128, 256, 512}");
     if (p->precision != GABE_FP64 && p->precision != GABE_FP32) return serr(nullptr, GABE_ERR_PARAM, "bad precision");
     if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4) return serr(nullptr, GABE_ERR_PARAM, "bad model");
     if (p->expansion < 0 || p->expansion > 2) return serr(nullptr, GABE_ERR_PARAM, "expansion must be 0, 1 or 2");
     if (!(p->L > 0) || !(p->dt > 0)) return serr(nullptr, GABE_ERR_PARAM, "L and dt must be positive");
     if (sp->nplanes < 1 || sp->plane0 < 0 || sp->plane0 + sp->nplanes > N)
         return serr(nullptr, GABE_ERR_PARAM, "planes [%d, %d) outside [0, %d)", sp->plane0, sp->plane0 + sp->nplanes, N);
+    int rank = 0;
+    if (p->gws_on) {  // the transpose needs every rank's planes: the standard split of nranks
+        if (sp->nranks < 1 || sp->nranks > N) return serr(nullptr, GABE_ERR_PARAM, "GWs need nranks in [1, N]");
+        const Split spl(N, sp->nranks);
+        rank = spl.owner(sp->plane0);
+        if (spl.p0(rank) != sp->plane0 || spl.n(rank) != sp->nplanes)
+            return serr(nullptr, GABE_ERR_PARAM, "with GWs the planes must be rank %d's share of %d ranks", rank,
+                        sp->nranks);
+    }
     gabe_slab *s = new (std::nothrow) gabe_slab();
     if (!s) return serr(nullptr, GABE_ERR_NOMEM, "host allocation failed");
     auto bail = [&](int code) {
@@ -139,6 +162,11 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     s->w = s->f32 ? 4 : 8;
     s->plane_elems = (size_t)N * N;
     s->lc = make_lattice_consts(*p);
+    s->gws = p->gws_on != 0;
+    s->W = p->gws_on ? sp->nranks : 1;
+    s->rank = rank;
+    s->nz = (size_t)N / 2 + 1;
+    s->cplx_loc = (size_t)s->nloc * N * s->nz;
     if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) {
         cudaGetLastError();
         serr(s, GABE_ERR_CUDA, "cudaSetDevice(%d) failed", p->device);
@@ -168,6 +196,29 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         (rc = salloc(s, (void **)&s->counters, 4 * sizeof(unsigned int))))
         return bail(rc);
     if (s->f32 && (rc = salloc(s, (void **)&s->stage, (size_t)s->nloc * s->plane_elems * sizeof(double)))) return bail(rc);
+    if (s->gws) {
+        if ((rc = salloc(s, (void **)&s->S, 10 * s->cplx_loc * 8)) || (rc = salloc(s, &s->Tb, 10 * s->cplx_loc * 8)) ||
+            (rc = salloc(s, &s->G, 4 * s->cplx_loc * 8)))
+            return bail(rc);
+        long long n2[2] = {N, N}, inem[2] = {N, N + 2}, onem[2] = {N, (long long)s->nz};
+        size_t ws = 0;
+        if (cufftCreate(&s->plan2d) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "cufftCreate failed");
+            return bail(GABE_ERR_CUFFT);
+        }
+        s->have_plan = true;
+        if (cufftSetAutoAllocation(s->plan2d, 0) != CUFFT_SUCCESS ||
+            cufftMakePlanMany64(s->plan2d, 2, n2, inem, 1, (long long)N * (N + 2), onem, 1, (long long)N * s->nz,
+                                CUFFT_R2C, 10LL * s->nloc, &ws) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "2-D r2c plan of the slab's source planes failed");
+            return bail(GABE_ERR_CUFFT);
+        }
+        if ((rc = salloc(s, &s->fft_work, ws))) return bail(rc);
+        if (cufftSetWorkArea(s->plan2d, s->fft_work) != CUFFT_SUCCESS || cufftSetStream(s->plan2d, s->stream) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "cuFFT work area / stream");
+            return bail(GABE_ERR_CUFFT);
+        }
+    }
     if (cudaMemset(s->counters, 0, 4 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMemset(s->sc, 0, sizeof(DevScalars)) != cudaSuccess) {
         cudaGetLastError();
@@ -182,8 +233,9 @@ int gabe_slab_destroy(gabe_slab *s) {
     if (!s) return GABE_OK;
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->have_plan) cufftDestroy(s->plan2d);
     void *bufs[] = {s->X[0], s->X[1], s->D[0], s->D[1], s->send[0], s->send[1], s->recv[0], s->recv[1],
-                    s->sc, s->partials, s->sums, s->stage, s->counters};
+                    s->sc, s->partials, s->sums, s->stage, s->counters, s->S, s->Tb, s->G, s->fft_work};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -227,6 +279,7 @@ int gabe_slab_upload(gabe_slab *s, const double *field0, const double *dfield0, 
             SCK(s, to_fluct(s->stage, nf, dev_mean(s, a >= 2, a & 1), reinterpret_cast<float *>(dst), s->stream));
         }
     }
+    if (s->gws) SCK(s, cudaMemsetAsync(s->G, 0, 4 * s->cplx_loc * 8, s->stream));  // h, l start at zero
     SCK(s, cudaStreamSynchronize(s->stream));
     s->cur = 0;
     s->uploaded = true;
@@ -297,7 +350,7 @@ int gabe_slab_sweep(gabe_slab *s, int which) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "sweep before upload") : GABE_ERR_PARAM;
     if (which < 0 || which > 2) return serr(s, GABE_ERR_PARAM, "which must be 0 (sweep A), 1 (sweep B) or 2 (energies)");
     SCK(s, cudaSetDevice(s->dev));
-    const int mode = which == 0 ? MODE_A : (which == 1 ? MODE_B : MODE_E0);
+    const int mode = which == 0 ? (s->gws ? MODE_A_GW : MODE_A) : (which == 1 ? MODE_B : MODE_E0);
     StencilArgs a = slab_args(s, which, which == 1 ? nullptr : s->sums);
     SCK(s, s->f32 ? sweep32_f32(s->shape, mode, a, s->grid, s->stream) : sweep_f64(s->shape, mode, a, s->grid, s->stream));
     if (which == 1) s->cur ^= 1;
@@ -308,9 +361,65 @@ int gabe_slab_finish(gabe_slab *s, int which) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "finish before upload") : GABE_ERR_PARAM;
     if (which != 0 && which != 2) return serr(s, GABE_ERR_PARAM, "which must be 0 (after sweep A) or 2 (energies)");
     SCK(s, cudaSetDevice(s->dev));
-    const int mode = which == 0 ? MODE_A : MODE_E0;
+    const int mode = which == 0 ? (s->gws ? MODE_A_GW : MODE_A) : MODE_E0;
     SCK(s, s->f32 ? slab_finish_f32(mode, s->lc, s->sc, s->sums, s->stream)
                   : slab_finish_f64(mode, s->lc, s->sc, s->sums, s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_gw_buffers(gabe_slab *s, void **send, void **recv, int64_t *send_bytes, int64_t *recv_bytes) {
+    if (!s) return GABE_ERR_PARAM;
+    if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
+    if (send) *send = s->Tb;
+    if (recv) *recv = s->S;
+    const Split spl(s->N, s->W);
+    for (int r = 0; r < s->W; r++) {
+        if (send_bytes) send_bytes[r] = (int64_t)10 * s->nloc * spl.n(r) * s->nz * 8;
+        if (recv_bytes) recv_bytes[r] = (int64_t)10 * spl.n(r) * s->nloc * s->nz * 8;
+    }
+    return GABE_OK;
+}
+
+int gabe_slab_gw_transform(gabe_slab *s) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "transform before upload") : GABE_ERR_PARAM;
+    if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
+    SCK(s, cudaSetDevice(s->dev));
+    if (cufftExecR2C(s->plan2d, (cufftReal *)s->S, (cufftComplex *)s->S) != CUFFT_SUCCESS)
+        return serr(s, GABE_ERR_CUFFT, "2-D r2c of the source planes failed");
+    SCK(s, slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_gw_update(gabe_slab *s) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "update before upload") : GABE_ERR_PARAM;
+    if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
+    SCK(s, cudaSetDevice(s->dev));
+    const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
+    SCK(s, slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, s->stream));
+    // pass along i: for every component and column (y, kz), the N values of stride m nz
+    SCK(s, fft_col_pass_f32(s->N, s->Tb, N * m * nz, nz, m * nz, 10, (int)m, (int)nz, s->stream));
+    SCK(s, slab_kspace_f32(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_gw_download(gabe_slab *s, double *h0, double *l0) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "download before upload") : GABE_ERR_PARAM;
+    if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
+    SCK(s, cudaSetDevice(s->dev));
+    const size_t M = s->cplx_loc;  // this rank's k-points: N kx x nloc ky x (N/2+1) kz
+    const size_t chunk = 10 * s->cplx_loc * 8 / (12 * sizeof(double));  // points staged in the send buffer
+    double *stage = static_cast<double *>(s->Tb);
+    double *dst[2] = {h0, l0};
+    for (int w = 0; w < 2; w++) {
+        if (!dst[w]) continue;
+        for (size_t m0 = 0; m0 < M; m0 += chunk) {
+            const size_t cnt = M - m0 < chunk ? M - m0 : chunk;
+            SCK(s, slab_gw_amplitudes_f32(s->G, cnt, m0, s->N, s->nloc, s->plane0, w, stage, s->stream));
+            SCK(s, cudaMemcpy2DAsync(dst[w] + m0, M * sizeof(double), stage, cnt * sizeof(double), cnt * sizeof(double),
+                                     12, cudaMemcpyDeviceToHost, s->stream));
+        }
+    }
+    SCK(s, cudaStreamSynchronize(s->stream));
     return GABE_OK;
 }
 

@@ -1,0 +1,98 @@
+// GW branch of a lattice split into slabs along i (slab.cu), FP32 storage.
+//
+// The 3-D transform of the ten source arrays (fft_stresstensor,
+// g2evolutionpert.cpp:183-195) runs as
+//   1. a 2-D r2c over (j, k) of every own plane (cuFFT, in place):
+//      S[q][il][ky][kz], il < nplanes;
+//   2. a transpose between the ranks: rank r' receives the ky columns it
+//      owns, [y0_r', y0_r' + m_r'), of every plane -- pack (below), an
+//      all-to-all by the caller, unpack (below) into T[q][i][y][kz] with i
+//      the global plane;
+//   3. the pass along i (fft3d.cuh col_fft_kernel) on T;
+// and the k-space update (kspace.cuh kspace_update) takes the rank's own
+// k-points, (kx, y0 + y, kz), from T with the amplitudes G[4][kx][y][kz].
+// Planes (i) and columns (ky) are split over the ranks with one rule:
+// rank r owns [p0(r), p0(r) + n(r)), n(r) = N/W + (r < N%W), contiguous.
+#pragma once
+
+#include "kspace.cuh"
+#include "slabsplit.h"
+
+namespace gabe {
+
+
+// 2-D transforms of this rank's planes -> send buffer, blocks by destination
+// rank r' (offset 10 nloc nz p0(r') complex), each [10][nloc][n(r')][nz].
+__global__ void __launch_bounds__(256) slab_gw_pack_kernel(const Cplx<float> *S, Cplx<float> *send, int N, int nloc,
+                                                           Split sp) {
+    const int nz = N / 2 + 1;
+    const size_t total = (size_t)10 * nloc * N * nz;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % nz);
+        size_t t = idx / nz;
+        const int j = (int)(t % N);
+        t /= N;
+        const int il = (int)(t % nloc), q = (int)(t / nloc);
+        const int r = sp.owner(j), m = sp.n(r), y = j - sp.p0(r);
+        const size_t off = (size_t)10 * nloc * nz * sp.p0(r);
+        send[off + (((size_t)q * nloc + il) * m + y) * nz + kz] = S[idx];
+    }
+}
+
+// Receive buffer (blocks by source rank r, offset 10 m nz p0(r), each
+// [10][n(r)][m][nz]) -> T[10][N][m][nz].
+__global__ void __launch_bounds__(256) slab_gw_unpack_kernel(const Cplx<float> *recv, Cplx<float> *T, int N, int m,
+                                                             Split sp) {
+    const int nz = N / 2 + 1;
+    const size_t total = (size_t)10 * N * m * nz;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % nz);
+        size_t t = idx / nz;
+        const int y = (int)(t % m);
+        t /= m;
+        const int i = (int)(t % N), q = (int)(t / N);
+        const int r = sp.owner(i), nr = sp.n(r), il = i - sp.p0(r);
+        const size_t off = (size_t)10 * m * nz * sp.p0(r);
+        T[idx] = recv[off + (((size_t)q * nr + il) * m + y) * nz + kz];
+    }
+}
+
+// TT projection and both RK2 stages for this rank's k-points (kspace.cuh).
+__global__ void __launch_bounds__(256) slab_kspace_kernel(const Cplx<float> *T, Cplx<float> *G, const DevScalars *sc,
+                                                          LatticeConsts c, int m, int y0) {
+    const int N = c.N, nz = N / 2 + 1;
+    const size_t M = (size_t)N * m * nz;
+    const KsCoef<float> kc = ks_coef<float>(c, sc->gw[0]);
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < M; idx += (size_t)gridDim.x * blockDim.x) {
+        const int kz = (int)(idx % nz);
+        const size_t t = idx / nz;
+        const int y = (int)(t % m), i = (int)(t / m), j = y0 + y;
+        const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
+        kspace_update<float>(kc, px, py, kz, M, T, G, idx);
+    }
+}
+
+// Amplitudes -> the reference's 12 components (h or l: which = 0 / 1) for
+// points m0 .. m0+cnt-1 of this rank's [N][m][nz] k-points; dst [12][cnt].
+__global__ void slab_gw_unpack_amplitudes_kernel(const Cplx<float> *G, size_t cnt, size_t m0, int N, int m, int y0,
+                                                 int which, double *dst) {
+    const int nz = N / 2 + 1;
+    const size_t M = (size_t)N * m * nz;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
+        const size_t idx = m0 + q;
+        const int kz = (int)(idx % nz);
+        const size_t t = idx / nz;
+        const int y = (int)(t % m), i = (int)(t / m), j = y0 + y;
+        const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
+        double ep[6] = {0, 0, 0, 0, 0, 0}, ex[6] = {0, 0, 0, 0, 0, 0};
+        if (px || py || kz) pol_tensors(px, py, kz, ep, ex);
+        const Cplx<float> ap = G[(size_t)(2 * which) * M + idx], ax = G[(size_t)(2 * which + 1) * M + idx];
+#pragma unroll
+        for (int c6 = 0; c6 < 6; c6++) {
+            dst[(size_t)(2 * c6) * cnt + q] = ep[c6] * (double)ap.re + ex[c6] * (double)ax.re;
+            dst[(size_t)(2 * c6 + 1) * cnt + q] = ep[c6] * (double)ap.im + ex[c6] * (double)ax.im;
+        }
+    }
+}
+
+}  // namespace gabe

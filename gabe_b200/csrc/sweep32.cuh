@@ -139,7 +139,7 @@ constexpr int sweep32_threads_per_sm() {
 struct Tile32 {
     const float *X, *D;  // fields and momenta of the current state, [2][N^3]
     float *Xo, *Do;      // new fields and momenta (sweep B)
-    float *S;            // GW sources [10][N][N][N+2] (sweep A with sources)
+    float *S;            // GW sources [10][N][N][N+2] (sweep A with sources; a slab: its own planes)
     int k0, j0, i0, i1;
     int planes;          // planes per field in X, D, Xo, Do (slab, no wrap along i); 0 = N, periodic
 };
@@ -215,7 +215,9 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     // slots of planes i-1, i, i+1 and of the plane issued next (i+S-2)
     int s_pr = 0, s_cu = 1, s_nx = 2, s_is = S - 1;
     float2 pr[4], cu[4];  // own pair of planes i-1 and i
-    const int sstride = NN * (N + 2);  // one source component
+    // sources [10][planes][N][N+2]: the whole lattice, or a slab's own planes (plane i at i - 1)
+    const int splanes = t.planes ? t.planes - 2 : N, sfirst = t.planes ? 1 : 0;
+    const int sstride = splanes * N * (N + 2);  // one source component
     const int so_row = j * (N + 2) + k;
     for (int i = i0; i < i1; i++) {
         cp_wait<S - 4>();  // planes up to i+1 have landed (this thread's copies)
@@ -269,7 +271,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
                     ngroup = 0;
                 }
                 if constexpr (MODE == MODE_A_GW) {
-                    float *g = t.S + (i * (N * (N + 2)) + so_row);
+                    float *g = t.S + ((i - sfirst) * (N * (N + 2)) + so_row);
 #pragma unroll
                     for (int q = 0; q < kSrc; q++, g += sstride)
                         __stcs(reinterpret_cast<float2 *>(g), make_float2(s0[0][q], s0[1][q]));

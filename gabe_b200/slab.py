@@ -34,7 +34,7 @@ KNV = 8  # stage sums per sweep
 
 class SlabParams(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_int32), ("plane0", ctypes.c_int32), ("nplanes", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("nranks", ctypes.c_int32)]
 
 
 _bound = False
@@ -58,6 +58,11 @@ def _lib():
             getattr(L, f).argtypes = [H]
         L.gabe_slab_stream.argtypes = [H, ctypes.POINTER(H)]
         L.gabe_slab_scalars.argtypes = [H, _dp]
+        i64p = ctypes.POINTER(ctypes.c_int64)
+        L.gabe_slab_gw_buffers.argtypes = [H, ctypes.POINTER(H), ctypes.POINTER(H), i64p, i64p]
+        for f in ("gabe_slab_gw_transform", "gabe_slab_gw_update"):
+            getattr(L, f).argtypes = [H]
+        L.gabe_slab_gw_download.argtypes = [H, _dp, _dp]
         _bound = True
     return L
 
@@ -88,17 +93,18 @@ class Slab:
 
     def __init__(self, N: int, plane0: int, nplanes: int, *, L: float = 20.0, dt: float = 0.01,
                  model: int = MODEL_LPHI4, model_c=None, precision: int = FP64, device: int = -1,
-                 tile_shape: int = -1, tile_ci: int = 0, expansion: int = 1):
+                 tile_shape: int = -1, tile_ci: int = 0, expansion: int = 1, gws: bool = False, nranks: int = 1):
         lib = _lib()
         p = Params()
         lib.gabe_default_params(ctypes.byref(p), int(N))
-        p.L, p.dt, p.gws_on, p.model, p.precision = float(L), float(dt), 0, int(model), int(precision)
+        p.L, p.dt, p.gws_on, p.model, p.precision = float(L), float(dt), int(bool(gws)), int(model), int(precision)
         if model_c is None:
             model_c = lphi4_constants() if model == MODEL_LPHI4 else (1e-6, 2.5e-7)
         p.model_c[0], p.model_c[1] = float(model_c[0]), float(model_c[1])
         p.device, p.tile_shape, p.tile_ci, p.expansion = int(device), int(tile_shape), int(tile_ci), int(expansion)
-        sp = SlabParams(ctypes.sizeof(SlabParams), int(plane0), int(nplanes), 0)
+        sp = SlabParams(ctypes.sizeof(SlabParams), int(plane0), int(nplanes), int(nranks))
         self.N, self.plane0, self.nplanes, self.precision = int(N), int(plane0), int(nplanes), int(precision)
+        self.gws, self.nranks = bool(gws), int(nranks)
         self._h = ctypes.c_void_p()
         rc = lib.gabe_slab_create(ctypes.byref(p), ctypes.byref(sp), ctypes.byref(self._h))
         if rc != 0:
@@ -114,6 +120,13 @@ class Slab:
         st = ctypes.c_void_p()
         self._check(lib.gabe_slab_stream(self._h, ctypes.byref(st)))
         self.stream_ptr = st.value or 0
+        if self.gws:
+            snd, rcv = ctypes.c_void_p(), ctypes.c_void_p()
+            sb = (ctypes.c_int64 * self.nranks)()
+            rb = (ctypes.c_int64 * self.nranks)()
+            self._check(lib.gabe_slab_gw_buffers(self._h, ctypes.byref(snd), ctypes.byref(rcv), sb, rb))
+            self._ptrs["gw_send"], self._ptrs["gw_recv"] = snd.value, rcv.value
+            self.gw_send_bytes, self.gw_recv_bytes = list(sb), list(rb)
 
     def _check(self, rc: int):
         if rc != 0:
@@ -136,6 +149,10 @@ class Slab:
 
         if name == "sums":
             return torch.as_tensor(_DeviceView(self._ptrs["sums"], KNV * 8, "<f8", 8), device="cuda")
+        if name == "gw_send":
+            return torch.as_tensor(_DeviceView(self._ptrs[name], sum(self.gw_send_bytes), "<f4", 4), device="cuda")
+        if name == "gw_recv":
+            return torch.as_tensor(_DeviceView(self._ptrs[name], sum(self.gw_recv_bytes), "<f4", 4), device="cuda")
         return torch.as_tensor(_DeviceView(self._ptrs[name], self.halo_bytes, "|u1", 1), device="cuda")
 
     # -- the stage calls ----------------------------------------------------
@@ -174,6 +191,19 @@ class Slab:
         out = np.empty(12)
         self._check(_lib().gabe_slab_scalars(self._h, out.ctypes.data_as(_dp)))
         return out
+
+    def gw_transform(self):
+        self._check(_lib().gabe_slab_gw_transform(self._h))
+
+    def gw_update(self):
+        self._check(_lib().gabe_slab_gw_update(self._h))
+
+    def gw_download(self):
+        """h, l of this slab's k-points, [12][N][nplanes][N/2+1] each (ky = plane0 + y)."""
+        shape = (12, self.N, self.nplanes, self.N // 2 + 1)
+        h, l = np.empty(shape), np.empty(shape)
+        self._check(_lib().gabe_slab_gw_download(self._h, h.ctypes.data_as(_dp), l.ctypes.data_as(_dp)))
+        return h, l
 
 
 def _on_slab_stream(s):
@@ -229,6 +259,22 @@ class LocalComm:
             s.tensor("recv_hi").copy_(slabs[(r + 1) % W].tensor("send_lo"))
         torch.cuda.synchronize()
 
+    def all_to_all(self, slabs):
+        """GW transpose: block r' of slab r's send buffer -> slab r''s receive buffer, at r."""
+        import torch
+
+        for s in slabs:
+            s.sync()
+        W = len(slabs)
+        for src in range(W):
+            snd = slabs[src].tensor("gw_send")
+            soff = np.cumsum([0] + [b // 4 for b in slabs[src].gw_send_bytes])
+            for dst in range(W):
+                rcv = slabs[dst].tensor("gw_recv")
+                roff = np.cumsum([0] + [b // 4 for b in slabs[dst].gw_recv_bytes])
+                rcv[roff[src]:roff[src + 1]].copy_(snd[soff[dst]:soff[dst + 1]])
+        torch.cuda.synchronize()
+
 
 class DistComm:
     """One slab per rank of a torch.distributed process group: the sums by
@@ -266,16 +312,26 @@ class DistComm:
             for w in d.batch_isend_irecv(ops):
                 w.wait()  # NCCL: the slab's stream waits; gloo: the host waits
 
+    def all_to_all(self, slabs):
+        """GW transpose: block r of the send buffer to rank r, arriving at this rank's place."""
+        (s,) = slabs
+        with _on_slab_stream(s):
+            self.dist.all_to_all_single(s.tensor("gw_recv"), s.tensor("gw_send"),
+                                        output_split_sizes=[b // 4 for b in s.gw_recv_bytes],
+                                        input_split_sizes=[b // 4 for b in s.gw_send_bytes], group=self.group)
+
 
 class SlabLattice:
     """The slabs of one rank (DistComm: one; LocalComm: all of them) and the
     step sequence.  Scalars are the same on every slab."""
 
-    def __init__(self, N: int, comm, *, precision: int = FP64, device: int = -1, slab_factory=None, **kw):
-        self.N, self.comm, self.precision = int(N), comm, int(precision)
+    def __init__(self, N: int, comm, *, precision: int = FP64, device: int = -1, gws: bool = False, slab_factory=None,
+                 **kw):
+        self.N, self.comm, self.precision, self.gws = int(N), comm, int(precision), bool(gws)
         parts = split_planes(self.N, comm.world)
         mine = [comm.rank] if hasattr(comm, "rank") else list(range(comm.world))
-        make = slab_factory or (lambda p0, n: Slab(self.N, p0, n, precision=precision, device=device, **kw))
+        make = slab_factory or (lambda p0, n: Slab(self.N, p0, n, precision=precision, device=device, gws=gws,
+                                                   nranks=comm.world, **kw))
         self.parts = [parts[r] for r in mine]
         self.slabs = [make(p0, n) for p0, n in self.parts]
 
@@ -344,6 +400,12 @@ class SlabLattice:
             for s in self.slabs:
                 s.sweep(0)
             self._reduce_and_finish(0)
+            if self.gws:  # sources of this step: 2-D transforms, transpose, pass along i, h/l update
+                for s in self.slabs:
+                    s.gw_transform()
+                self.comm.all_to_all(self.slabs)
+                for s in self.slabs:
+                    s.gw_update()
             for s in self.slabs:
                 s.sweep(1)
             self._exchange()
@@ -357,3 +419,8 @@ class SlabLattice:
 
     def download(self):
         return [s.download() for s in self.slabs]
+
+    def download_gw(self):
+        """(h, l) per slab of this rank: its ky columns of the reference's
+        [12][N][N][N/2+1] arrays."""
+        return [s.gw_download() for s in self.slabs]

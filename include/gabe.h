@@ -323,15 +323,26 @@ int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
  * take the energies with gabe_slab_sweep(s, 2), all-reduce, and
  * gabe_slab_finish(s, 2), as calcEnergy(0) after the reference's
  * initialisation.  All calls enqueue on the slab's stream
- * (gabe_slab_stream); order the exchange after it.  Fields only: gws_on
- * must be 0 (the distributed 3-D transform of the GW sources is not part
- * of this interface).  No counterpart in the reference. */
+ * (gabe_slab_stream); order the exchange after it.
+ *
+ * With gws_on (FP32, N in {64, 128, 256, 512}; the planes must be the
+ * standard share of `nranks` ranks: n(r) = N/nranks + (r < N%nranks),
+ * contiguous), between gabe_slab_finish(s, 0) and gabe_slab_sweep(s, 1):
+ *   gabe_slab_gw_transform(s)  2-D transforms of the own source planes ->
+ *                              send buffer, one block per rank
+ *   all-to-all: the block for rank r (send_bytes[r]) to rank r, arriving
+ *              in rank r's receive buffer at the sender's place (recv_bytes)
+ *   gabe_slab_gw_update(s)     the passes along i and the TT projection +
+ *                              h/l update of this rank's k-points: kx all,
+ *                              ky in [plane0, plane0 + nplanes), kz all.
+ * Spectra of a slab lattice are not computed.  No counterpart in the
+ * reference. */
 typedef struct gabe_slab gabe_slab;
 typedef struct {
     int32_t struct_size; /* sizeof(gabe_slab_params) */
     int32_t plane0;      /* first own plane (global index i) */
     int32_t nplanes;     /* own planes, >= 1 */
-    int32_t reserved;
+    int32_t nranks;      /* ranks of the split (needed with gws_on) */
 } gabe_slab_params;
 
 int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab **out);
@@ -358,6 +369,14 @@ int gabe_slab_stream(gabe_slab *s, void **stream);
 int gabe_slab_sync(gabe_slab *s);
 /* a, adot, edkin, edpot, edgrad, edrho, two stages each (synchronises) */
 int gabe_slab_scalars(gabe_slab *s, double out12[12]);
+/* GW branch: device send / receive buffers of the all-to-all and the bytes
+ * per rank (arrays of nranks). */
+int gabe_slab_gw_buffers(gabe_slab *s, void **send, void **recv, int64_t *send_bytes, int64_t *recv_bytes);
+int gabe_slab_gw_transform(gabe_slab *s);
+int gabe_slab_gw_update(gabe_slab *s);
+/* h, l of this rank's k-points in the reference's component order:
+ * [12][N][nplanes][N/2+1] each (ky = plane0 + y); NULL skips one. */
+int gabe_slab_gw_download(gabe_slab *s, double *h0, double *l0);
 
 #ifdef __cplusplus
 }

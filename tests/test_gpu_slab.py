@@ -1,5 +1,5 @@
 """A lattice split into slabs along i (gabe_slab_* through gabe_b200.slab)
-against the same lattice on one handle (gabe_create), fields only.
+against the same lattice on one handle (gabe_create).
 
 * One slab holds the whole lattice between two halo planes that are copies
   of its own end planes: same tiles, same plane chunks, the same block sums
@@ -9,6 +9,10 @@ against the same lattice on one handle (gabe_create), fields only.
   other: sums are added on the host, halos copied between steps) differ
   from the handle only in the order of the energy sums: FP64 to ~1e-12,
   FP32 (fluctuations about the FP64 mean) to its rounding.
+* With GWs (FP32) the slabs transform their source planes in 2-D, transpose
+  the half spectra between them by ky columns and take the pass along i
+  and the h/l update of their own k-points; h and l agree with the handle's
+  3-D cuFFT path to FP32 transform rounding.
 """
 import os
 import socket
@@ -169,3 +173,78 @@ def test_slab_rejects_sweeps_before_upload():
             s.sweep(7)
     finally:
         s.close()
+
+
+FFT_TOL = 1e-5  # relative, FP32 transforms
+
+
+def _norm_rel(got, want):
+    return float(np.linalg.norm(got - want) / np.linalg.norm(want))
+
+
+def _gw_slabs(N, st, steps, comm):
+    f, d, a0, ad0 = st
+    with gs.SlabLattice(N, comm, precision=gb.FP32, gws=True) as lat:
+        fs = [f[:, p0:p0 + n] for p0, n in lat.planes]
+        ds = [d[:, p0:p0 + n] for p0, n in lat.planes]
+        lat.upload(fs if len(fs) > 1 else fs[0], ds if len(ds) > 1 else ds[0], a0, ad0)
+        lat.step(steps)
+        sc = lat.scalars()
+        out = lat.download()
+        gw = lat.download_gw()
+    f1 = np.concatenate([o[0] for o in out], axis=1)
+    h1 = np.concatenate([g[0] for g in gw], axis=2)
+    l1 = np.concatenate([g[1] for g in gw], axis=2)
+    return f1, h1, l1, sc
+
+
+def _gw_whole(N, st, steps):
+    f, d, a0, ad0 = st
+    with gb.Lattice(N, gws=True, precision=gb.FP32) as lat:
+        lat.upload_state(f, d, a0=a0, adot0=ad0)
+        lat.step(steps)
+        sc = lat.scalars()
+        f1, _, h1, l1 = lat.download_state()
+    want = np.array([v for k in ("a", "adot", "edkin", "edpot", "edgrad", "edrho") for v in sc[k]])
+    return f1, h1, l1, want
+
+
+def _gw_compare(a, b):
+    (f1, h1, l1, s1), (f0, h0, l0, s0) = a, b
+    for fld in range(2):
+        fl = f0[fld] - f0[fld].mean()
+        assert np.abs(f1[fld] - f0[fld]).max() <= 1e-5 * np.abs(fl).max()
+    rho = s0[10]
+    for q in range(12):
+        tol = 1e-6 * (abs(rho) if q in (8, 9) else abs(s0[q]))
+        assert abs(s1[q] - s0[q]) <= tol, (q, s1[q], s0[q])
+    assert np.linalg.norm(l0) > 0
+    assert _norm_rel(h1, h0) <= FFT_TOL
+    assert _norm_rel(l1, l0) <= FFT_TOL
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_gw_slabs_match_the_whole_lattice(world):
+    N = 64
+    st = _state(N, seed=25)
+    _gw_compare(_gw_slabs(N, st, STEPS, gs.LocalComm(world)), _gw_whole(N, st, STEPS))
+
+
+def test_gw_slabs_through_a_one_rank_nccl_group():
+    import datetime
+
+    import torch.distributed as dist
+
+    N = 64
+    st = _state(N, seed=27)
+    want = _gw_whole(N, st, STEPS)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        got = _gw_slabs(N, st, STEPS, gs.DistComm())
+    finally:
+        dist.destroy_process_group()
+    _gw_compare(got, want)
+

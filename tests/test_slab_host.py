@@ -93,6 +93,24 @@ class FakeSlab:
     def unpack(self):
         self.log.append(("unpack",))
 
+    def gw_setup(self, world):
+        """Send block for rank r': 6 floats per (own rank, destination) pair, distinct per pair."""
+        self.gws = True
+        self.gw_send_bytes = [4 * 6 * (r + 1) for r in range(world)]
+        self.gw_recv_bytes = [4 * 6 * (self.rank + 1)] * world
+        self.t["gw_send"] = torch.zeros(sum(self.gw_send_bytes) // 4, dtype=torch.float32)
+        self.t["gw_recv"] = torch.full((sum(self.gw_recv_bytes) // 4,), -1.0, dtype=torch.float32)
+
+    def gw_transform(self):
+        self.log.append(("gw_transform",))
+        off = 0
+        for r, b in enumerate(self.gw_send_bytes):
+            self.t["gw_send"][off:off + b // 4] = 100.0 * self.rank + r
+            off += b // 4
+
+    def gw_update(self):
+        self.log.append(("gw_update",))
+
     def upload(self, f, d, mean, a0, adot0):
         self.log.append(("upload", None if mean is None else tuple(np.round(mean, 12))))
 
@@ -159,3 +177,46 @@ def test_slab_protocol_over_gloo_ranks(world):
         p.join(120)
     assert all(p.exitcode == 0 for p in procs)
     assert all(q.get(timeout=5) for _ in range(world))
+
+
+def _gw_worker(rank, world, port, N, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        log, made = [], []
+
+        def factory(p0, n):
+            made.append(FakeSlab(rank, p0, n, log))
+            made[-1].gw_setup(world)
+            return made[-1]
+
+        lat = gs.SlabLattice(N, gs.DistComm(), precision=gb.FP32, gws=True, slab_factory=factory)
+        (s,) = made
+        lat.step(1)
+        ok = log == [("sweep", 0), ("finish", 0), ("gw_transform",), ("gw_update",), ("sweep", 1), ("pack",),
+                     ("unpack",)]
+        # block from source rank r sits at r's place: the value 100 r + this rank
+        recv = s.tensor("gw_recv")
+        off = 0
+        for r, b in enumerate(s.gw_recv_bytes):
+            ok &= bool((recv[off:off + b // 4] == 100.0 * r + rank).all())
+            off += b // 4
+        q.put(bool(ok))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slab_gw_transpose_over_gloo_ranks():
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gw_worker, args=(r, world, port, 24, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    assert all(q.get(timeout=5) for _ in range(world))
+
