@@ -200,10 +200,12 @@ def cpu_reference_sample(N: int, steps: int, warm: int = 1):
 
 
 def slab_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ranks):
-    """One lattice split into slabs of planes along i over the ranks (fields
-    only, FP32 storage): per step sweep A, an all-reduce of the 8 stage sums,
-    the finish, sweep B and the exchange of boundary planes (strong scaling:
-    the lattice is fixed).  Timed with CUDA events on the slab's stream,
+    """One lattice split into slabs of planes along i over the ranks (FP32
+    storage, GWs on): per step sweep A, an all-reduce of the 8 stage sums,
+    the finish, 2-D transforms of the own source planes, an all-to-all
+    transpose by ky columns, the pass along i and the h/l update of the
+    rank's k-points, sweep B and the exchange of boundary planes (strong
+    scaling: the lattice is fixed).  Timed with CUDA events on the slab's stream,
     which record the whole step including the waits for the exchanges; max
     over ranks."""
     import numpy as np
@@ -218,7 +220,7 @@ def slab_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ra
     ok = 1.0
     try:
         comm = gs.DistComm() if dist else gs.LocalComm(1)
-        lat = gs.SlabLattice(N, comm, precision=gb.FP32, device=local)
+        lat = gs.SlabLattice(N, comm, precision=gb.FP32, device=local, gws=True)
         (p0, n), = lat.planes
         f, d, a0, ad0 = random_state(N, seed=11, device="cuda")
         fl, dl = f[:, p0:p0 + n].cpu().numpy(), d[:, p0:p0 + n].cpu().numpy()
@@ -245,12 +247,13 @@ def slab_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ra
     sc = lat.scalars()
     lat.close()
     sites = float(N) ** 3
-    return {"workload": f"{N}^3 lattice split into {world} slab(s) of planes along i, fields only (GWs off), "
-                        f"FP32 storage; per step: sweep A, all-reduce of 8 FP64 sums, finish, sweep B, "
-                        f"boundary-plane exchange",
+    return {"workload": f"{N}^3 lattice split into {world} slab(s) of planes along i, GWs on, FP32 storage; "
+                        f"per step: sweep A, all-reduce of 8 FP64 sums, finish, 2-D transforms of the source "
+                        f"planes, all-to-all transpose, pass along i + h/l update, sweep B, boundary-plane exchange",
             "planes": [list(pp) for pp in gs.split_planes(N, world)], "scaling": "strong", "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": ms / K, "site_updates_per_s": sites * K / (ms / 1e3),
-            "halo_bytes_per_rank_per_step": 2 * s.halo_bytes, "finite": bool(np.all(np.isfinite(sc)))}
+            "halo_bytes_per_rank_per_step": 2 * s.halo_bytes,
+            "transpose_bytes_per_rank_per_step": int(sum(s.gw_send_bytes)), "finite": bool(np.all(np.isfinite(sc)))}
 
 
 def ensemble_leg(args, rank: int, world: int, local: int, dist, barrier, max_over_ranks):
