@@ -873,11 +873,19 @@ int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols) {
     DevScalars s;
     rc = read_scalars(h, &s);
     if (rc) return rc;
+    return gabe_spectra_from_sums(&h->p, s.edrho[0], sums.data(), cnt.data(), nbins, out, ncols);
+}
+
+int gabe_spectra_from_sums(const gabe_params *p, double edrho0, const double *sums, const double *cnt, int nbins,
+                           double *out, int ncols) {
+    if (!p || !sums || !cnt || !out) return GABE_ERR_PARAM;
+    const int gws = p->gws_on;
+    if (nbins != gabe_spectra_numbins(p->N) || ncols != 5 + (gws ? 3 : 0)) return GABE_ERR_PARAM;
     // normalisation of g2spectra.cpp:27,94-103,114-117,186-195
-    const double L = h->p.L;
-    const int N = h->N;
+    const double L = p->L;
+    const int N = p->N;
     const double spec_norm = pow(L / (double)N, 6.) * pow(2. * M_PI / L, 3.);
-    const double hub = sqrt(8. * M_PI / 3.) * sqrt(s.edrho[0]);
+    const double hub = sqrt(8. * M_PI / 3.) * sqrt(edrho0);
     const double dp = 2. * M_PI / (double)L;
     const double norm1 = 4.e-5 / pow(100., .333) / 24. / M_PI / M_PI / pow(L, 3.) / (hub * hub);
     for (int b = 0; b < nbins; b++) {

@@ -115,8 +115,8 @@ cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, co
 cudaError_t slab_finish_f64(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s);
 // Slab GW branch, FP32 (slabgw.cuh): pack the 2-D transforms for the all-to-all, unpack what
 // arrived into [10][N][m][nz], the k-space update of the rank's k-points, amplitudes -> 12 components.
-cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, cudaStream_t s);
-cudaError_t slab_gw_unpack_f32(const void *recv, void *T, int N, int m, int W, cudaStream_t s);
+cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s);
+cudaError_t slab_gw_unpack_f32(const void *recv, void *T, int N, int m, int W, int ncomp, cudaStream_t s);
 cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
                             cudaStream_t s);
 cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,

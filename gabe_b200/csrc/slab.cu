@@ -30,6 +30,7 @@ using namespace gabe;
 
 namespace {
 thread_local std::string g_slab_create_error;
+constexpr int kSlabBinBlocks = 296;  // blocks of the spectrum binning (2 per SM)
 }
 
 struct gabe_slab {
@@ -49,8 +50,12 @@ struct gabe_slab {
     // GW branch (FP32): the ranks' split, sources [10][nloc][N][N+2] (2-D transformed in place,
     // then the all-to-all receive buffer), the send buffer (then T[10][N][m][nz]), amplitudes
     // [4][N][m][nz] of this rank's ky columns [plane0, plane0 + nloc)
-    bool gws = false;
-    int W = 1, rank = 0;
+    bool gws = false, spec = false;  // spec: the spectra transpose (FP32, N in {64, ..., 512})
+    int W = 1, rank = 0, nbins = 0;
+    cufftHandle plan_spec = 0;
+    bool have_plan_spec = false;
+    double *bin_part = nullptr, *bin_sum = nullptr;
+    unsigned int *bin_cnt_part = nullptr;
     float *S = nullptr;
     void *Tb = nullptr, *G = nullptr, *fft_work = nullptr;
     size_t nz = 0, cplx_loc = 0;  // complex values of one component over this rank's planes or columns
@@ -138,7 +143,8 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     if (sp->nplanes < 1 || sp->plane0 < 0 || sp->plane0 + sp->nplanes > N)
         return serr(nullptr, GABE_ERR_PARAM, "planes [%d, %d) outside [0, %d)", sp->plane0, sp->plane0 + sp->nplanes, N);
     int rank = 0;
-    if (p->gws_on) {  // the transpose needs every rank's planes: the standard split of nranks
+    const bool split_needed = p->gws_on || (p->precision == GABE_FP32 && sp->nranks >= 1);
+    if (split_needed) {  // the transposes need every rank's planes: the standard split of nranks
         if (sp->nranks < 1 || sp->nranks > N) return serr(nullptr, GABE_ERR_PARAM, "GWs need nranks in [1, N]");
         const Split spl(N, sp->nranks);
         rank = spl.owner(sp->plane0);
@@ -163,7 +169,9 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     s->plane_elems = (size_t)N * N;
     s->lc = make_lattice_consts(*p);
     s->gws = p->gws_on != 0;
-    s->W = p->gws_on ? sp->nranks : 1;
+    s->spec = s->f32 && (N == 64 || N == 128 || N == 256 || N == 512) && sp->nranks >= 1 && sp->nranks <= N;
+    s->W = (p->gws_on || s->spec) ? (sp->nranks >= 1 ? sp->nranks : 1) : 1;
+    s->nbins = gabe_spectra_numbins(N);
     s->rank = rank;
     s->nz = (size_t)N / 2 + 1;
     s->cplx_loc = (size_t)s->nloc * N * s->nz;
@@ -196,6 +204,30 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         (rc = salloc(s, (void **)&s->counters, 4 * sizeof(unsigned int))))
         return bail(rc);
     if (s->f32 && (rc = salloc(s, (void **)&s->stage, (size_t)s->nloc * s->plane_elems * sizeof(double)))) return bail(rc);
+    if (s->spec && !s->gws) {  // buffers of the two fields' transpose
+        if ((rc = salloc(s, (void **)&s->S, 2 * s->cplx_loc * 8)) || (rc = salloc(s, &s->Tb, 2 * s->cplx_loc * 8)))
+            return bail(rc);
+    }
+    if (s->spec) {
+        long long n2[2] = {N, N}, inem[2] = {N, N + 2}, onem[2] = {N, (long long)s->nz};
+        size_t ws = 0;
+        if (cufftCreate(&s->plan_spec) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "cufftCreate failed");
+            return bail(GABE_ERR_CUFFT);
+        }
+        s->have_plan_spec = true;
+        if (cufftMakePlanMany64(s->plan_spec, 2, n2, inem, 1, (long long)N * (N + 2), onem, 1, (long long)N * s->nz,
+                                CUFFT_R2C, 2LL * s->nloc, &ws) != CUFFT_SUCCESS ||
+            cufftSetStream(s->plan_spec, s->stream) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "2-D r2c plan of the slab's field planes failed");
+            return bail(GABE_ERR_CUFFT);
+        }
+        const int ns = 3, nb = s->nbins;
+        if ((rc = salloc(s, (void **)&s->bin_part, (size_t)kSlabBinBlocks * ns * nb * sizeof(double))) ||
+            (rc = salloc(s, (void **)&s->bin_cnt_part, (size_t)kSlabBinBlocks * nb * sizeof(unsigned int))) ||
+            (rc = salloc(s, (void **)&s->bin_sum, (size_t)(ns + 1) * nb * sizeof(double))))
+            return bail(rc);
+    }
     if (s->gws) {
         if ((rc = salloc(s, (void **)&s->S, 10 * s->cplx_loc * 8)) || (rc = salloc(s, &s->Tb, 10 * s->cplx_loc * 8)) ||
             (rc = salloc(s, &s->G, 4 * s->cplx_loc * 8)))
@@ -234,8 +266,10 @@ int gabe_slab_destroy(gabe_slab *s) {
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->have_plan) cufftDestroy(s->plan2d);
+    if (s->have_plan_spec) cufftDestroy(s->plan_spec);
     void *bufs[] = {s->X[0], s->X[1], s->D[0], s->D[1], s->send[0], s->send[1], s->recv[0], s->recv[1],
-                    s->sc, s->partials, s->sums, s->stage, s->counters, s->S, s->Tb, s->G, s->fft_work};
+                    s->sc, s->partials, s->sums, s->stage, s->counters, s->S, s->Tb, s->G, s->fft_work,
+                    s->bin_part, s->bin_cnt_part, s->bin_sum};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -386,7 +420,7 @@ int gabe_slab_gw_transform(gabe_slab *s) {
     SCK(s, cudaSetDevice(s->dev));
     if (cufftExecR2C(s->plan2d, (cufftReal *)s->S, (cufftComplex *)s->S) != CUFFT_SUCCESS)
         return serr(s, GABE_ERR_CUFFT, "2-D r2c of the source planes failed");
-    SCK(s, slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, s->stream));
+    SCK(s, slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
     return GABE_OK;
 }
 
@@ -395,7 +429,7 @@ int gabe_slab_gw_update(gabe_slab *s) {
     if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
     SCK(s, cudaSetDevice(s->dev));
     const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
-    SCK(s, slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, s->stream));
+    SCK(s, slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
     // pass along i: for every component and column (y, kz), the N values of stride m nz
     SCK(s, fft_col_pass_f32(s->N, s->Tb, N * m * nz, nz, m * nz, 10, (int)m, (int)nz, s->stream));
     SCK(s, slab_kspace_f32(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream));
@@ -419,6 +453,68 @@ int gabe_slab_gw_download(gabe_slab *s, double *h0, double *l0) {
                                      12, cudaMemcpyDeviceToHost, s->stream));
         }
     }
+    SCK(s, cudaStreamSynchronize(s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_spectra_transform(gabe_slab *s) {
+    if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "spectra before upload") : GABE_ERR_PARAM;
+    if (!s->spec) return serr(s, GABE_ERR_STATE, "slab spectra need FP32 storage, N in {64, ..., 512} and nranks");
+    SCK(s, cudaSetDevice(s->dev));
+    const size_t N = s->N;
+    // own planes of both fields (fluctuations) into padded rows, then 2-D r2c and the pack by ky columns
+    for (int f = 0; f < 2; f++)
+        SCK(s, cudaMemcpy2DAsync(s->S + (size_t)f * s->nloc * N * (N + 2), (N + 2) * 4, plane_ptr(s, s->cur, f, 1), N * 4,
+                                 N * 4, (size_t)s->nloc * N, cudaMemcpyDeviceToDevice, s->stream));
+    if (cufftExecR2C(s->plan_spec, (cufftReal *)s->S, (cufftComplex *)s->S) != CUFFT_SUCCESS)
+        return serr(s, GABE_ERR_CUFFT, "2-D r2c of the field planes failed");
+    SCK(s, slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
+    return GABE_OK;
+}
+
+int gabe_slab_spectra_buffers(gabe_slab *s, void **send, void **recv, int64_t *send_bytes, int64_t *recv_bytes) {
+    if (!s) return GABE_ERR_PARAM;
+    if (!s->spec) return serr(s, GABE_ERR_STATE, "slab without spectra");
+    if (send) *send = s->Tb;
+    if (recv) *recv = s->S;
+    const Split spl(s->N, s->W);
+    for (int r = 0; r < s->W; r++) {
+        if (send_bytes) send_bytes[r] = (int64_t)2 * s->nloc * spl.n(r) * s->nz * 8;
+        if (recv_bytes) recv_bytes[r] = (int64_t)2 * spl.n(r) * s->nloc * s->nz * 8;
+    }
+    return GABE_OK;
+}
+
+int gabe_slab_spectra_raw(gabe_slab *s, double *sums, double *counts) {
+    if (!s || !s->uploaded || !sums || !counts) return s ? serr(s, GABE_ERR_PARAM, "bad arguments") : GABE_ERR_PARAM;
+    if (!s->spec) return serr(s, GABE_ERR_STATE, "slab without spectra");
+    SCK(s, cudaSetDevice(s->dev));
+    const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
+    SCK(s, slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
+    SCK(s, fft_col_pass_f32(s->N, s->Tb, N * m * nz, nz, m * nz, 2, (int)m, (int)nz, s->stream));
+    SCK(s, cudaStreamSynchronize(s->stream));
+    DevScalars d;
+    SCK(s, cudaMemcpy(&d, s->sc, sizeof(d), cudaMemcpyDeviceToHost));
+    const int ns = 2 + (s->gws ? 1 : 0), nb = s->nbins;
+    BinArgs b{};
+    b.F = s->Tb;
+    b.G = s->gws ? s->G : nullptr;
+    b.part_sum = s->bin_part;
+    b.part_cnt = s->bin_cnt_part;
+    b.N = s->N;
+    b.nbins = nb;
+    b.nseries = ns;
+    b.quirk = s->p.gw_spec_quirk;
+    b.fix_zero = 1;
+    b.zero_re[0] = s->lc.gridsize * d.fbar[0];
+    b.zero_re[1] = s->lc.gridsize * d.fbar[1];
+    b.m = s->nloc;
+    b.y0 = s->plane0;
+    Launch lb{dim3(kSlabBinBlocks), dim3(256), (size_t)nb * (ns * 8 + 4), s->stream};
+    SCK(s, bins_f32(b, lb));
+    SCK(s, bin_reduce(s->bin_part, s->bin_cnt_part, kSlabBinBlocks, ns, nb, s->bin_sum, s->bin_sum + ns * nb, s->stream));
+    SCK(s, cudaMemcpyAsync(sums, s->bin_sum, (size_t)ns * nb * 8, cudaMemcpyDeviceToHost, s->stream));
+    SCK(s, cudaMemcpyAsync(counts, s->bin_sum + ns * nb, (size_t)nb * 8, cudaMemcpyDeviceToHost, s->stream));
     SCK(s, cudaStreamSynchronize(s->stream));
     return GABE_OK;
 }

@@ -22,11 +22,12 @@ namespace gabe {
 
 
 // 2-D transforms of this rank's planes -> send buffer, blocks by destination
-// rank r' (offset 10 nloc nz p0(r') complex), each [10][nloc][n(r')][nz].
+// rank r' (offset ncomp nloc nz p0(r') complex), each [ncomp][nloc][n(r')][nz]
+// (ncomp = 10 sources, or 2 fields for the spectra).
 __global__ void __launch_bounds__(256) slab_gw_pack_kernel(const Cplx<float> *S, Cplx<float> *send, int N, int nloc,
-                                                           Split sp) {
+                                                           Split sp, int ncomp) {
     const int nz = N / 2 + 1;
-    const size_t total = (size_t)10 * nloc * N * nz;
+    const size_t total = (size_t)ncomp * nloc * N * nz;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
         const int kz = (int)(idx % nz);
         size_t t = idx / nz;
@@ -34,17 +35,17 @@ __global__ void __launch_bounds__(256) slab_gw_pack_kernel(const Cplx<float> *S,
         t /= N;
         const int il = (int)(t % nloc), q = (int)(t / nloc);
         const int r = sp.owner(j), m = sp.n(r), y = j - sp.p0(r);
-        const size_t off = (size_t)10 * nloc * nz * sp.p0(r);
+        const size_t off = (size_t)ncomp * nloc * nz * sp.p0(r);
         send[off + (((size_t)q * nloc + il) * m + y) * nz + kz] = S[idx];
     }
 }
 
-// Receive buffer (blocks by source rank r, offset 10 m nz p0(r), each
-// [10][n(r)][m][nz]) -> T[10][N][m][nz].
+// Receive buffer (blocks by source rank r, offset ncomp m nz p0(r), each
+// [ncomp][n(r)][m][nz]) -> T[ncomp][N][m][nz].
 __global__ void __launch_bounds__(256) slab_gw_unpack_kernel(const Cplx<float> *recv, Cplx<float> *T, int N, int m,
-                                                             Split sp) {
+                                                             Split sp, int ncomp) {
     const int nz = N / 2 + 1;
-    const size_t total = (size_t)10 * N * m * nz;
+    const size_t total = (size_t)ncomp * N * m * nz;
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
         const int kz = (int)(idx % nz);
         size_t t = idx / nz;
@@ -52,7 +53,7 @@ __global__ void __launch_bounds__(256) slab_gw_unpack_kernel(const Cplx<float> *
         t /= m;
         const int i = (int)(t % N), q = (int)(t / N);
         const int r = sp.owner(i), nr = sp.n(r), il = i - sp.p0(r);
-        const size_t off = (size_t)10 * m * nz * sp.p0(r);
+        const size_t off = (size_t)ncomp * m * nz * sp.p0(r);
         T[idx] = recv[off + (((size_t)q * nr + il) * m + y) * nz + kz];
     }
 }

@@ -22,6 +22,8 @@ struct BinArgs {
     int N, nbins, nseries, quirk;
     double zero_re[2];      // FP32 path: N^3 fbar per field, added to F(k=0) of the fluctuations
     int fix_zero;
+    // a slab's k-points (slab.cu): F and G hold [..][N][m][N/2+1] with ky = y0 + y; m = 0: all of them
+    int m, y0;
 };
 
 template <typename T>
@@ -30,7 +32,8 @@ __global__ void __launch_bounds__(256) bin_kernel(BinArgs a) {
     double *hs = reinterpret_cast<double *>(smem_raw);                      // [nseries][nbins]
     unsigned int *hc = reinterpret_cast<unsigned int *>(hs + a.nseries * a.nbins);  // [nbins]
     const int N = a.N, nz = N / 2 + 1, nb = a.nbins, ns = a.nseries;
-    const size_t M = (size_t)N * N * nz;
+    const int ny = a.m ? a.m : N;  // ky rows held
+    const size_t M = (size_t)N * ny * nz;
     for (int q = threadIdx.x; q < ns * nb; q += blockDim.x) hs[q] = 0.0;
     for (int q = threadIdx.x; q < nb; q += blockDim.x) hc[q] = 0u;
     __syncthreads();
@@ -39,7 +42,7 @@ __global__ void __launch_bounds__(256) bin_kernel(BinArgs a) {
     for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < M; idx += (size_t)gridDim.x * blockDim.x) {
         const int kz = (int)(idx % nz);
         const size_t t = idx / nz;
-        const int j = (int)(t % N), i = (int)(t / N);
+        const int j = a.y0 + (int)(t % ny), i = (int)(t / ny);
         const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
         const int b = (int)sqrt((double)px * px + (double)py * py + (double)kz * kz);
         const bool edge = (kz == 0) || (kz == N / 2);
@@ -47,7 +50,7 @@ __global__ void __launch_bounds__(256) bin_kernel(BinArgs a) {
         atomicAdd(&hc[b], edge ? 1u : 2u);
         for (int f = 0; f < 2; f++) {
             double re = (double)F[2 * ((size_t)f * M + idx)], im = (double)F[2 * ((size_t)f * M + idx) + 1];
-            if (a.fix_zero && idx == 0) re += a.zero_re[f];
+            if (a.fix_zero && idx == 0 && a.y0 == 0) re += a.zero_re[f];  // k = 0
             atomicAdd(&hs[f * nb + b], w * (re * re + im * im));
         }
         if (ns > 2) {

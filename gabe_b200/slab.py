@@ -63,6 +63,11 @@ def _lib():
         for f in ("gabe_slab_gw_transform", "gabe_slab_gw_update"):
             getattr(L, f).argtypes = [H]
         L.gabe_slab_gw_download.argtypes = [H, _dp, _dp]
+        L.gabe_slab_spectra_buffers.argtypes = [H, ctypes.POINTER(H), ctypes.POINTER(H), i64p, i64p]
+        L.gabe_slab_spectra_transform.argtypes = [H]
+        L.gabe_slab_spectra_raw.argtypes = [H, _dp, _dp]
+        L.gabe_spectra_from_sums.argtypes = [ctypes.POINTER(Params), ctypes.c_double, _dp, _dp, ctypes.c_int, _dp,
+                                             ctypes.c_int]
         _bound = True
     return L
 
@@ -103,6 +108,7 @@ class Slab:
         p.model_c[0], p.model_c[1] = float(model_c[0]), float(model_c[1])
         p.device, p.tile_shape, p.tile_ci, p.expansion = int(device), int(tile_shape), int(tile_ci), int(expansion)
         sp = SlabParams(ctypes.sizeof(SlabParams), int(plane0), int(nplanes), int(nranks))
+        self.params = p
         self.N, self.plane0, self.nplanes, self.precision = int(N), int(plane0), int(nplanes), int(precision)
         self.gws, self.nranks = bool(gws), int(nranks)
         self._h = ctypes.c_void_p()
@@ -120,13 +126,17 @@ class Slab:
         st = ctypes.c_void_p()
         self._check(lib.gabe_slab_stream(self._h, ctypes.byref(st)))
         self.stream_ptr = st.value or 0
-        if self.gws:
+        kinds = (["gw"] if self.gws else []) + (["spec"] if self.precision == FP32 and self.N in (64, 128, 256, 512)
+                                                  and self.nranks >= 1 else [])
+        for kind in kinds:  # all-to-all buffers of the GW sources and of the spectra's two fields
             snd, rcv = ctypes.c_void_p(), ctypes.c_void_p()
             sb = (ctypes.c_int64 * self.nranks)()
             rb = (ctypes.c_int64 * self.nranks)()
-            self._check(lib.gabe_slab_gw_buffers(self._h, ctypes.byref(snd), ctypes.byref(rcv), sb, rb))
-            self._ptrs["gw_send"], self._ptrs["gw_recv"] = snd.value, rcv.value
-            self.gw_send_bytes, self.gw_recv_bytes = list(sb), list(rb)
+            fn = lib.gabe_slab_gw_buffers if kind == "gw" else lib.gabe_slab_spectra_buffers
+            self._check(fn(self._h, ctypes.byref(snd), ctypes.byref(rcv), sb, rb))
+            self._ptrs[f"{kind}_send"], self._ptrs[f"{kind}_recv"] = snd.value, rcv.value
+            setattr(self, f"{kind}_send_bytes", list(sb))
+            setattr(self, f"{kind}_recv_bytes", list(rb))
 
     def _check(self, rc: int):
         if rc != 0:
@@ -149,10 +159,9 @@ class Slab:
 
         if name == "sums":
             return torch.as_tensor(_DeviceView(self._ptrs["sums"], KNV * 8, "<f8", 8), device="cuda")
-        if name == "gw_send":
-            return torch.as_tensor(_DeviceView(self._ptrs[name], sum(self.gw_send_bytes), "<f4", 4), device="cuda")
-        if name == "gw_recv":
-            return torch.as_tensor(_DeviceView(self._ptrs[name], sum(self.gw_recv_bytes), "<f4", 4), device="cuda")
+        if name.endswith("_send") or name.endswith("_recv"):  # all-to-all buffers, as float32
+            nbytes = sum(getattr(self, f"{name}_bytes"))
+            return torch.as_tensor(_DeviceView(self._ptrs[name], nbytes, "<f4", 4), device="cuda")
         return torch.as_tensor(_DeviceView(self._ptrs[name], self.halo_bytes, "|u1", 1), device="cuda")
 
     # -- the stage calls ----------------------------------------------------
@@ -197,6 +206,16 @@ class Slab:
 
     def gw_update(self):
         self._check(_lib().gabe_slab_gw_update(self._h))
+
+    def spectra_transform(self):
+        self._check(_lib().gabe_slab_spectra_transform(self._h))
+
+    def spectra_raw(self):
+        nb = int(np.sqrt(3.0) * self.N / 2 + 1)
+        ns = 2 + int(self.gws)
+        sums, cnt = np.zeros((ns, nb)), np.zeros(nb)
+        self._check(_lib().gabe_slab_spectra_raw(self._h, sums.ctypes.data_as(_dp), cnt.ctypes.data_as(_dp)))
+        return sums, cnt
 
     def gw_download(self):
         """h, l of this slab's k-points, [12][N][nplanes][N/2+1] each (ky = plane0 + y)."""
@@ -259,26 +278,30 @@ class LocalComm:
             s.tensor("recv_hi").copy_(slabs[(r + 1) % W].tensor("send_lo"))
         torch.cuda.synchronize()
 
-    def all_to_all(self, slabs):
-        """GW transpose: block r' of slab r's send buffer -> slab r''s receive buffer, at r."""
+    def all_to_all(self, slabs, kind: str = "gw"):
+        """Transpose (kind "gw": the sources, "spec": the two fields): block r'
+        of slab r's send buffer -> slab r''s receive buffer, at r."""
         import torch
 
         if len(slabs) == 1:
             (s,) = slabs
             with _on_slab_stream(s):
-                s.tensor("gw_recv").copy_(s.tensor("gw_send"))
+                s.tensor(f"{kind}_recv").copy_(s.tensor(f"{kind}_send"))
             return
         for s in slabs:
             s.sync()
         W = len(slabs)
         for src in range(W):
-            snd = slabs[src].tensor("gw_send")
-            soff = np.cumsum([0] + [b // 4 for b in slabs[src].gw_send_bytes])
+            snd = slabs[src].tensor(f"{kind}_send")
+            soff = np.cumsum([0] + [b // 4 for b in getattr(slabs[src], f"{kind}_send_bytes")])
             for dst in range(W):
-                rcv = slabs[dst].tensor("gw_recv")
-                roff = np.cumsum([0] + [b // 4 for b in slabs[dst].gw_recv_bytes])
+                rcv = slabs[dst].tensor(f"{kind}_recv")
+                roff = np.cumsum([0] + [b // 4 for b in getattr(slabs[dst], f"{kind}_recv_bytes")])
                 rcv[roff[src]:roff[src + 1]].copy_(snd[soff[dst]:soff[dst + 1]])
         torch.cuda.synchronize()
+
+    def allreduce_host(self, v: np.ndarray) -> np.ndarray:
+        return v
 
 
 class DistComm:
@@ -317,13 +340,23 @@ class DistComm:
             for w in d.batch_isend_irecv(ops):
                 w.wait()  # NCCL: the slab's stream waits; gloo: the host waits
 
-    def all_to_all(self, slabs):
-        """GW transpose: block r of the send buffer to rank r, arriving at this rank's place."""
+    def all_to_all(self, slabs, kind: str = "gw"):
+        """Transpose: block r of the send buffer to rank r, arriving at this rank's place."""
         (s,) = slabs
         with _on_slab_stream(s):
-            self.dist.all_to_all_single(s.tensor("gw_recv"), s.tensor("gw_send"),
-                                        output_split_sizes=[b // 4 for b in s.gw_recv_bytes],
-                                        input_split_sizes=[b // 4 for b in s.gw_send_bytes], group=self.group)
+            self.dist.all_to_all_single(s.tensor(f"{kind}_recv"), s.tensor(f"{kind}_send"),
+                                        output_split_sizes=[b // 4 for b in getattr(s, f"{kind}_recv_bytes")],
+                                        input_split_sizes=[b // 4 for b in getattr(s, f"{kind}_send_bytes")],
+                                        group=self.group)
+
+    def allreduce_host(self, v: np.ndarray) -> np.ndarray:
+        import torch
+
+        t = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))
+        if self.dist.get_backend(self.group) == "nccl":
+            t = t.cuda()
+        self.dist.all_reduce(t, group=self.group)
+        return t.cpu().numpy()
 
 
 class SlabLattice:
@@ -385,15 +418,7 @@ class SlabLattice:
         self.energies()
 
     def _allreduce_host(self, v: np.ndarray) -> np.ndarray:
-        if isinstance(self.comm, DistComm):
-            import torch
-
-            t = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))
-            if self.comm.dist.get_backend(self.comm.group) == "nccl":
-                t = t.cuda()
-            self.comm.dist.all_reduce(t, group=self.comm.group)
-            return t.cpu().numpy()
-        return v
+        return self.comm.allreduce_host(v)
 
     def energies(self):
         for s in self.slabs:
@@ -424,6 +449,30 @@ class SlabLattice:
 
     def download(self):
         return [s.download() for s in self.slabs]
+
+    def spectra(self) -> np.ndarray:
+        """The table of gabe_spectra (specOut's columns) of the whole lattice,
+        the same on every rank: each rank bins its k-points after the fields'
+        transpose, the sums are added over the ranks and normalised with the
+        stage-0 energy density."""
+        sc = self.scalars()
+        for s in self.slabs:
+            s.spectra_transform()
+        self.comm.all_to_all(self.slabs, "spec")
+        raw = [s.spectra_raw() for s in self.slabs]
+        sums = sum(r[0] for r in raw)
+        cnt = sum(r[1] for r in raw)
+        flat = self._allreduce_host(np.concatenate([sums.ravel(), cnt]))
+        ns, nb = sums.shape
+        sums, cnt = np.ascontiguousarray(flat[:ns * nb].reshape(ns, nb)), np.ascontiguousarray(flat[ns * nb:])
+        ncols = 5 + (3 if self.gws else 0)
+        out = np.zeros((nb, ncols))
+        s0 = self.slabs[0]
+        rc = _lib().gabe_spectra_from_sums(ctypes.byref(s0.params), float(sc[10]), sums.ctypes.data_as(_dp),
+                                           cnt.ctypes.data_as(_dp), nb, out.ctypes.data_as(_dp), ncols)
+        if rc != 0:
+            raise GabeError(rc, "gabe_spectra_from_sums")
+        return out
 
     def download_gw(self):
         """(h, l) per slab of this rank: its ky columns of the reference's

@@ -170,6 +170,14 @@ int gabe_spectra(gabe_handle *h, double *out, int nbins, int ncols);
  * rebin these exactly (e.g. into log-spaced |k| bins). */
 int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, int nseries);
 
+/* The table of gabe_spectra from binned sums [nseries][nbins] and counts
+ * [nbins] (as gabe_spectra_raw returns them, or their sums over the slabs of
+ * a split lattice) and the stage-0 energy density edrho0: the reference's
+ * normalisation (g2spectra.cpp:27,94-103,114-117,186-195) for p's N, L and
+ * gws_on.  No device work. */
+int gabe_spectra_from_sums(const gabe_params *p, double edrho0, const double *sums, const double *counts, int nbins,
+                           double *out, int ncols);
+
 /* meansvars() (g2output.cpp:70-121) of the current state without the file
  * write: out4 = {mean, variance} of each field, variance as the reference
  * forms it, sum(f^2 - mean^2)/N^3.  All four values are written; the return
@@ -335,8 +343,12 @@ int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
  *   gabe_slab_gw_update(s)     the passes along i and the TT projection +
  *                              h/l update of this rank's k-points: kx all,
  *                              ky in [plane0, plane0 + nplanes), kz all.
- * Spectra of a slab lattice are not computed.  No counterpart in the
- * reference. */
+ * Spectra (FP32 slabs, N in {64, 128, 256, 512}): gabe_slab_spectra_transform(s)
+ * packs the 2-D transforms of the two fields; all-to-all the buffers of
+ * gabe_slab_spectra_buffers as above; gabe_slab_spectra_raw(s, ...) bins
+ * this rank's k-points (fields and, with GWs, l); add sums and counts over
+ * the ranks and pass them, with edrho[0] of gabe_slab_scalars, to
+ * gabe_spectra_from_sums.  No counterpart in the reference. */
 typedef struct gabe_slab gabe_slab;
 typedef struct {
     int32_t struct_size; /* sizeof(gabe_slab_params) */
@@ -377,6 +389,10 @@ int gabe_slab_gw_update(gabe_slab *s);
 /* h, l of this rank's k-points in the reference's component order:
  * [12][N][nplanes][N/2+1] each (ky = plane0 + y); NULL skips one. */
 int gabe_slab_gw_download(gabe_slab *s, double *h0, double *l0);
+int gabe_slab_spectra_transform(gabe_slab *s);
+int gabe_slab_spectra_buffers(gabe_slab *s, void **send, void **recv, int64_t *send_bytes, int64_t *recv_bytes);
+/* this rank's binned sums [2 + gws_on][nbins] and counts [nbins] (host arrays; synchronises) */
+int gabe_slab_spectra_raw(gabe_slab *s, double *sums, double *counts);
 
 #ifdef __cplusplus
 }

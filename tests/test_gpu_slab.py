@@ -248,3 +248,35 @@ def test_gw_slabs_through_a_one_rank_nccl_group():
         dist.destroy_process_group()
     _gw_compare(got, want)
 
+
+def _cols_close(got, want, cols):
+    g, w = got[:, cols], want[:, cols]
+    floor = 1e-9 * np.abs(w).max(axis=0, keepdims=True)
+    return float(np.max((np.abs(g - w) - floor) / np.abs(w).clip(min=1e-300)))
+
+
+@pytest.mark.parametrize("world,gws", [(1, True), (3, True), (2, False)])
+def test_slab_spectra_match_the_whole_lattice(world, gws):
+    """specOut's table of a split lattice: each slab bins its own k-points
+    after the fields' transpose; the sums over the slabs, normalised, are
+    the handle's spectra to FP32 transform rounding."""
+    N = 64
+    f, d, a0, ad0 = _state(N, seed=29)
+    with gb.Lattice(N, gws=gws, precision=gb.FP32) as lat:
+        lat.upload_state(f, d, a0=a0, adot0=ad0)
+        lat.step(STEPS)
+        want = lat.spec_out()
+    with gs.SlabLattice(N, gs.LocalComm(world), precision=gb.FP32, gws=gws) as sl:
+        fs = [f[:, p0:p0 + n] for p0, n in sl.planes]
+        ds = [d[:, p0:p0 + n] for p0, n in sl.planes]
+        sl.upload(fs if len(fs) > 1 else fs[0], ds if len(ds) > 1 else ds[0], a0, ad0)
+        sl.step(STEPS)
+        got = sl.spectra()
+    assert got.shape == want.shape
+    np.testing.assert_array_equal(got[:, 0], want[:, 0])
+    assert _cols_close(got, want, [1, 2, 3, 4]) <= 1e-5
+    if gws:
+        assert np.abs(want[:, 5]).max() > 0
+        assert _cols_close(got, want, [5, 6]) <= FFT_TOL
+        np.testing.assert_array_equal(got[:, 7], want[:, 7])
+
