@@ -136,6 +136,8 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         return serr(nullptr, GABE_ERR_PARAM, "N must be a multiple of 16 in [16, 1024] and nflds 2");
     if (p->gws_on && (p->precision != GABE_FP32 || (N != 64 && N != 128 && N != 256 && N != 512)))
         return serr(nullptr, GABE_ERR_PARAM, "slabs with GWs need FP32 storage and N in {64, 128, 256, 512}");
+    if (p->gws_on && p->expansion != 1)  // tensor modes evolve with expansion_type 1 only (g2functions.cpp:272-302)
+        return serr(nullptr, GABE_ERR_PARAM, "slabs with GWs need expansion_type 1");
     if (p->precision != GABE_FP64 && p->precision != GABE_FP32) return serr(nullptr, GABE_ERR_PARAM, "bad precision");
     if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4) return serr(nullptr, GABE_ERR_PARAM, "bad model");
     if (p->expansion < 0 || p->expansion > 2) return serr(nullptr, GABE_ERR_PARAM, "expansion must be 0, 1 or 2");

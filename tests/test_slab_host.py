@@ -34,14 +34,19 @@ def test_split_planes_rejects_more_ranks_than_planes():
         gs.split_planes(16, 17)
 
 
-@pytest.mark.parametrize("case", ["gws", "planes_hi", "planes_neg", "empty", "N", "size"])
+@pytest.mark.parametrize("case", ["gws", "gws_expansion2", "gws_split", "planes_hi", "planes_neg", "empty", "N",
+                                  "size"])
 def test_slab_create_rejects_bad_params(case):
     lib = gs._lib()
     p = gb.Params()
     lib.gabe_default_params(ctypes.byref(p), 32)
     sp = gs.SlabParams(ctypes.sizeof(gs.SlabParams), 0, 8, 0)
     if case == "gws":
-        p.gws_on = 1
+        p.gws_on = 1  # FP64
+    elif case == "gws_expansion2":  # a valid split of 64 planes over 4 ranks; only the expansion type is wrong
+        p.N, p.gws_on, p.precision, p.expansion, sp.nplanes, sp.nranks = 64, 1, gb.FP32, 2, 16, 4
+    elif case == "gws_split":  # planes [0, 8) are not a rank's share of 64 planes over 3 ranks (22, 21, 21)
+        p.N, p.gws_on, p.precision, sp.nranks = 64, 1, gb.FP32, 3
     elif case == "planes_hi":
         sp.plane0, sp.nplanes = 28, 8
     elif case == "planes_neg":
@@ -55,7 +60,12 @@ def test_slab_create_rejects_bad_params(case):
     h = ctypes.c_void_p()
     assert lib.gabe_slab_create(ctypes.byref(p), ctypes.byref(sp), ctypes.byref(h)) == 1
     assert not h.value
-    assert lib.gabe_slab_last_error(None)
+    msg = lib.gabe_slab_last_error(None)
+    assert msg
+    if case == "gws_expansion2":
+        assert b"expansion_type 1" in msg
+    elif case == "gws_split":
+        assert b"share" in msg
 
 
 class FakeSlab:
