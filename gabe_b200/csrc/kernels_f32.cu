@@ -59,14 +59,14 @@ cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, co
 static unsigned slab_grid(size_t n) { return (unsigned)std::min<size_t>(148 * 8, (n + 255) / 256); }
 
 cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s) {
-    const size_t n = (size_t)ncomp * nloc * N * (N / 2 + 1);
+    const size_t n = (size_t)ncomp * nloc * N * 32;  // one warp per row
     slab_gw_pack_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(S), static_cast<Cplx<float> *>(send),
                                                      N, nloc, Split(N, W), ncomp);
     return cudaGetLastError();
 }
 
 cudaError_t slab_gw_unpack_f32(const void *recv, void *T, int N, int m, int W, int ncomp, cudaStream_t s) {
-    const size_t n = (size_t)ncomp * N * m * (N / 2 + 1);
+    const size_t n = (size_t)ncomp * N * m * 32;  // one warp per row
     slab_gw_unpack_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(recv), static_cast<Cplx<float> *>(T),
                                                        N, m, Split(N, W), ncomp);
     return cudaGetLastError();

@@ -21,40 +21,51 @@
 namespace gabe {
 
 
+// A row of nz <= 257 complex values copied by one warp, every load issued
+// before the first store (nine per lane in flight).
+__device__ __forceinline__ void row_copy(Cplx<float> *dst, const Cplx<float> *src, int nz, int lane) {
+    constexpr int U = 9;  // ceil(257 / 32)
+    Cplx<float> v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+        if (lane + 32 * u < nz) v[u] = src[lane + 32 * u];
+#pragma unroll
+    for (int u = 0; u < U; u++)
+        if (lane + 32 * u < nz) dst[lane + 32 * u] = v[u];
+}
+
 // 2-D transforms of this rank's planes -> send buffer, blocks by destination
 // rank r' (offset ncomp nloc nz p0(r') complex), each [ncomp][nloc][n(r')][nz]
-// (ncomp = 10 sources, or 2 fields for the spectra).
+// (ncomp = 10 sources, or 2 fields for the spectra).  One warp per row of
+// nz values: the row's destination is worked out once, the copy is
+// contiguous.
 __global__ void __launch_bounds__(256) slab_gw_pack_kernel(const Cplx<float> *S, Cplx<float> *send, int N, int nloc,
                                                            Split sp, int ncomp) {
-    const int nz = N / 2 + 1;
-    const size_t total = (size_t)ncomp * nloc * N * nz;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
-        const int kz = (int)(idx % nz);
-        size_t t = idx / nz;
-        const int j = (int)(t % N);
-        t /= N;
-        const int il = (int)(t % nloc), q = (int)(t / nloc);
+    const int nz = N / 2 + 1, lane = threadIdx.x & 31;
+    const int rows = ncomp * nloc * N;  // < 2^31 for N <= 512
+    const int w0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int row = w0; row < rows; row += nw) {
+        const int j = row % N, t = row / N, il = t % nloc, q = t / nloc;
         const int r = sp.owner(j), m = sp.n(r), y = j - sp.p0(r);
-        const size_t off = (size_t)ncomp * nloc * nz * sp.p0(r);
-        send[off + (((size_t)q * nloc + il) * m + y) * nz + kz] = S[idx];
+        const size_t dst = (size_t)ncomp * nloc * nz * sp.p0(r) + (((size_t)q * nloc + il) * m + y) * nz;
+        const size_t src = (size_t)row * nz;
+        row_copy(send + dst, S + src, nz, lane);
     }
 }
 
 // Receive buffer (blocks by source rank r, offset ncomp m nz p0(r), each
-// [ncomp][n(r)][m][nz]) -> T[ncomp][N][m][nz].
+// [ncomp][n(r)][m][nz]) -> T[ncomp][N][m][nz], one warp per row of T.
 __global__ void __launch_bounds__(256) slab_gw_unpack_kernel(const Cplx<float> *recv, Cplx<float> *T, int N, int m,
                                                              Split sp, int ncomp) {
-    const int nz = N / 2 + 1;
-    const size_t total = (size_t)ncomp * N * m * nz;
-    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
-        const int kz = (int)(idx % nz);
-        size_t t = idx / nz;
-        const int y = (int)(t % m);
-        t /= m;
-        const int i = (int)(t % N), q = (int)(t / N);
+    const int nz = N / 2 + 1, lane = threadIdx.x & 31;
+    const int rows = ncomp * N * m;
+    const int w0 = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    for (int row = w0; row < rows; row += nw) {
+        const int y = row % m, t = row / m, i = t % N, q = t / N;
         const int r = sp.owner(i), nr = sp.n(r), il = i - sp.p0(r);
-        const size_t off = (size_t)ncomp * m * nz * sp.p0(r);
-        T[idx] = recv[off + (((size_t)q * nr + il) * m + y) * nz + kz];
+        const size_t src = (size_t)ncomp * m * nz * sp.p0(r) + (((size_t)q * nr + il) * m + y) * nz;
+        const size_t dst = (size_t)row * nz;
+        row_copy(T + dst, recv + src, nz, lane);
     }
 }
 
