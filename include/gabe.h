@@ -354,7 +354,8 @@ typedef struct {
     int32_t struct_size; /* sizeof(gabe_slab_params) */
     int32_t plane0;      /* first own plane (global index i) */
     int32_t nplanes;     /* own planes, >= 1 */
-    int32_t nranks;      /* ranks of the split (needed with gws_on) */
+    int32_t nranks;      /* ranks of the split: needed with gws_on and for the spectra (FP32), where
+                            [plane0, plane0 + nplanes) must be a rank's share; 0 = fields only */
 } gabe_slab_params;
 
 int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab **out);
