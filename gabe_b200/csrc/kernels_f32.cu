@@ -56,35 +56,19 @@ cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, co
     return cudaGetLastError();
 }
 
-static unsigned slab_grid(size_t n) { return (unsigned)std::min<size_t>(148 * 8, (n + 255) / 256); }
-
 cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s) {
-    const size_t n = (size_t)ncomp * nloc * N * 32;  // one warp per row
-    slab_gw_pack_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(S), static_cast<Cplx<float> *>(send),
-                                                     N, nloc, Split(N, W), ncomp);
-    return cudaGetLastError();
+    return slab_gw_pack<float>(S, send, N, nloc, W, ncomp, s);
 }
-
 cudaError_t slab_gw_unpack_f32(const void *recv, void *T, int N, int m, int W, int ncomp, cudaStream_t s) {
-    const size_t n = (size_t)ncomp * N * m * 32;  // one warp per row
-    slab_gw_unpack_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(recv), static_cast<Cplx<float> *>(T),
-                                                       N, m, Split(N, W), ncomp);
-    return cudaGetLastError();
+    return slab_gw_unpack<float>(recv, T, N, m, W, ncomp, s);
 }
-
 cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
                             cudaStream_t s) {
-    const size_t n = (size_t)c.N * m * (c.N / 2 + 1);
-    slab_kspace_kernel<<<slab_grid(n), 256, 0, s>>>(static_cast<const Cplx<float> *>(T), static_cast<Cplx<float> *>(G), sc,
-                                                    c, m, y0);
-    return cudaGetLastError();
+    return slab_kspace<float>(T, G, sc, c, m, y0, s);
 }
-
 cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
                                    cudaStream_t s) {
-    slab_gw_unpack_amplitudes_kernel<<<slab_grid(cnt), 256, 0, s>>>(static_cast<const Cplx<float> *>(G), cnt, m0, N, m,
-                                                                    y0, which, dst);
-    return cudaGetLastError();
+    return slab_gw_amplitudes<float>(G, cnt, m0, N, m, y0, which, dst, s);
 }
 
 template <int N>

@@ -1,5 +1,6 @@
 // FP64 kernels; built with -fmad=false (reference rounding, no FMA contraction).
 #include "launch.h"
+#include "slabgw.cuh"
 
 namespace gabe {
 
@@ -30,10 +31,26 @@ cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cuda
 cudaError_t slab_finish_f64(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s) {
     switch (mode) {
         case MODE_A: slab_finish_kernel<double, MODE_A><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
+        case MODE_A_GW: slab_finish_kernel<double, MODE_A_GW><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
         case MODE_E0: slab_finish_kernel<double, MODE_E0><<<1, 32, 0, s>>>(c, sc, tot, 0); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+cudaError_t slab_gw_pack_f64(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s) {
+    return slab_gw_pack<double>(S, send, N, nloc, W, ncomp, s);
+}
+cudaError_t slab_gw_unpack_f64(const void *recv, void *T, int N, int m, int W, int ncomp, cudaStream_t s) {
+    return slab_gw_unpack<double>(recv, T, N, m, W, ncomp, s);
+}
+cudaError_t slab_kspace_f64(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
+                            cudaStream_t s) {
+    return slab_kspace<double>(T, G, sc, c, m, y0, s);
+}
+cudaError_t slab_gw_amplitudes_f64(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
+                                   cudaStream_t s) {
+    return slab_gw_amplitudes<double>(G, cnt, m0, N, m, y0, which, dst, s);
 }
 
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l) {

@@ -121,6 +121,12 @@ cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const 
                             cudaStream_t s);
 cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
                                    cudaStream_t s);
+cudaError_t slab_gw_pack_f64(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s);
+cudaError_t slab_gw_unpack_f64(const void *recv, void *T, int N, int m, int W, int ncomp, cudaStream_t s);
+cudaError_t slab_kspace_f64(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
+                            cudaStream_t s);
+cudaError_t slab_gw_amplitudes_f64(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
+                                   cudaStream_t s);
 // FP32 sweep A with sources that writes them transformed along k (sweeprows.cuh):
 // one block per pair of rows and chunk of sweep32_rows_ci(N) planes.
 bool sweep32_rows_supported(int N);

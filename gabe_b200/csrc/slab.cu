@@ -59,6 +59,9 @@ struct gabe_slab {
     float *S = nullptr;
     void *Tb = nullptr, *G = nullptr, *fft_work = nullptr;
     size_t nz = 0, cplx_loc = 0;  // complex values of one component over this rank's planes or columns
+    size_t csz = 8;               // bytes of one complex value (FP32 8, FP64 16)
+    cufftHandle plan_i = 0;       // FP64: the pass along i (strided Z2Z, one component per call)
+    bool have_plan_i = false;
     cufftHandle plan2d = 0;
     bool have_plan = false;
     std::string err;
@@ -121,6 +124,28 @@ StencilArgs slab_args(gabe_slab *s, int counter, double *sums_out) {
     return a;
 }
 
+// Transform helpers by precision: the 2-D r2c of planes in place, and the
+// pass along i of ncomp components of T[ncomp][N][m][nz] in place.
+int r2c_planes(gabe_slab *s, cufftHandle plan, void *X) {
+    const cufftResult r = s->f32 ? cufftExecR2C(plan, (cufftReal *)X, (cufftComplex *)X)
+                                 : cufftExecD2Z(plan, (cufftDoubleReal *)X, (cufftDoubleComplex *)X);
+    return r == CUFFT_SUCCESS ? GABE_OK : serr(s, GABE_ERR_CUFFT, "2-D r2c of the slab's planes failed");
+}
+
+int pass_i(gabe_slab *s, void *Tb, int ncomp) {
+    const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
+    if (s->f32) {
+        SCK(s, fft_col_pass_f32(s->N, Tb, N * m * nz, nz, m * nz, ncomp, (int)m, (int)nz, s->stream));
+        return GABE_OK;
+    }
+    for (int q = 0; q < ncomp; q++) {
+        cufftDoubleComplex *X = static_cast<cufftDoubleComplex *>(Tb) + (size_t)q * N * m * nz;
+        if (cufftExecZ2Z(s->plan_i, X, X, CUFFT_FORWARD) != CUFFT_SUCCESS)
+            return serr(s, GABE_ERR_CUFFT, "pass along i failed");
+    }
+    return GABE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -134,8 +159,8 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     const int N = p->N;
     if (N < 16 || N > 1024 || N % 16 || p->nflds != 2)
         return serr(nullptr, GABE_ERR_PARAM, "N must be a multiple of 16 in [16, 1024] and nflds 2");
-    if (p->gws_on && (p->precision != GABE_FP32 || (N != 64 && N != 128 && N != 256 && N != 512)))
-        return serr(nullptr, GABE_ERR_PARAM, "slabs with GWs need FP32 storage and N in {64, 128, 256, 512}");
+    if (p->gws_on && p->precision == GABE_FP32 && N != 64 && N != 128 && N != 256 && N != 512)
+        return serr(nullptr, GABE_ERR_PARAM, "FP32 slabs with GWs need N in {64, 128, 256, 512}");
     if (p->gws_on && p->expansion != 1)  // tensor modes evolve with expansion_type 1 only (g2functions.cpp:272-302)
         return serr(nullptr, GABE_ERR_PARAM, "slabs with GWs need expansion_type 1");
     if (p->precision != GABE_FP64 && p->precision != GABE_FP32) return serr(nullptr, GABE_ERR_PARAM, "bad precision");
@@ -145,13 +170,13 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     if (sp->nplanes < 1 || sp->plane0 < 0 || sp->plane0 + sp->nplanes > N)
         return serr(nullptr, GABE_ERR_PARAM, "planes [%d, %d) outside [0, %d)", sp->plane0, sp->plane0 + sp->nplanes, N);
     int rank = 0;
-    const bool split_needed = p->gws_on || (p->precision == GABE_FP32 && sp->nranks >= 1);
+    const bool split_needed = p->gws_on || sp->nranks >= 1;
     if (split_needed) {  // the transposes need every rank's planes: the standard split of nranks
-        if (sp->nranks < 1 || sp->nranks > N) return serr(nullptr, GABE_ERR_PARAM, "GWs need nranks in [1, N]");
+        if (sp->nranks < 1 || sp->nranks > N) return serr(nullptr, GABE_ERR_PARAM, "nranks must be in [1, N]");
         const Split spl(N, sp->nranks);
         rank = spl.owner(sp->plane0);
         if (spl.p0(rank) != sp->plane0 || spl.n(rank) != sp->nplanes)
-            return serr(nullptr, GABE_ERR_PARAM, "with GWs the planes must be rank %d's share of %d ranks", rank,
+            return serr(nullptr, GABE_ERR_PARAM, "the planes must be rank %d's share of %d ranks", rank,
                         sp->nranks);
     }
     gabe_slab *s = new (std::nothrow) gabe_slab();
@@ -171,12 +196,13 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     s->plane_elems = (size_t)N * N;
     s->lc = make_lattice_consts(*p);
     s->gws = p->gws_on != 0;
-    s->spec = s->f32 && (N == 64 || N == 128 || N == 256 || N == 512) && sp->nranks >= 1 && sp->nranks <= N;
+    s->spec = (!s->f32 || N == 64 || N == 128 || N == 256 || N == 512) && sp->nranks >= 1 && sp->nranks <= N;
     s->W = (p->gws_on || s->spec) ? (sp->nranks >= 1 ? sp->nranks : 1) : 1;
     s->nbins = gabe_spectra_numbins(N);
     s->rank = rank;
     s->nz = (size_t)N / 2 + 1;
     s->cplx_loc = (size_t)s->nloc * N * s->nz;
+    s->csz = s->f32 ? 8 : 16;
     if (p->device >= 0 && cudaSetDevice(p->device) != cudaSuccess) {
         cudaGetLastError();
         serr(s, GABE_ERR_CUDA, "cudaSetDevice(%d) failed", p->device);
@@ -206,9 +232,25 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         (rc = salloc(s, (void **)&s->counters, 4 * sizeof(unsigned int))))
         return bail(rc);
     if (s->f32 && (rc = salloc(s, (void **)&s->stage, (size_t)s->nloc * s->plane_elems * sizeof(double)))) return bail(rc);
+    const cufftType r2c = s->f32 ? CUFFT_R2C : CUFFT_D2Z;
     if (s->spec && !s->gws) {  // buffers of the two fields' transpose
-        if ((rc = salloc(s, (void **)&s->S, 2 * s->cplx_loc * 8)) || (rc = salloc(s, &s->Tb, 2 * s->cplx_loc * 8)))
+        if ((rc = salloc(s, (void **)&s->S, 2 * s->cplx_loc * s->csz)) || (rc = salloc(s, &s->Tb, 2 * s->cplx_loc * s->csz)))
             return bail(rc);
+    }
+    if ((s->spec || s->gws) && !s->f32) {  // FP64 pass along i: N values of stride m nz, m nz of them
+        long long ni[1] = {N}, em[1] = {N};
+        const long long m = s->nloc, nzl = (long long)s->nz;
+        if (cufftCreate(&s->plan_i) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "cufftCreate failed");
+            return bail(GABE_ERR_CUFFT);
+        }
+        s->have_plan_i = true;
+        size_t wsi = 0;
+        if (cufftMakePlanMany64(s->plan_i, 1, ni, em, m * nzl, 1, em, m * nzl, 1, CUFFT_Z2Z, m * nzl, &wsi) != CUFFT_SUCCESS ||
+            cufftSetStream(s->plan_i, s->stream) != CUFFT_SUCCESS) {
+            serr(s, GABE_ERR_CUFFT, "plan of the pass along i failed");
+            return bail(GABE_ERR_CUFFT);
+        }
     }
     if (s->spec) {
         long long n2[2] = {N, N}, inem[2] = {N, N + 2}, onem[2] = {N, (long long)s->nz};
@@ -219,7 +261,7 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         }
         s->have_plan_spec = true;
         if (cufftMakePlanMany64(s->plan_spec, 2, n2, inem, 1, (long long)N * (N + 2), onem, 1, (long long)N * s->nz,
-                                CUFFT_R2C, 2LL * s->nloc, &ws) != CUFFT_SUCCESS ||
+                                r2c, 2LL * s->nloc, &ws) != CUFFT_SUCCESS ||
             cufftSetStream(s->plan_spec, s->stream) != CUFFT_SUCCESS) {
             serr(s, GABE_ERR_CUFFT, "2-D r2c plan of the slab's field planes failed");
             return bail(GABE_ERR_CUFFT);
@@ -231,8 +273,8 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
             return bail(rc);
     }
     if (s->gws) {
-        if ((rc = salloc(s, (void **)&s->S, 10 * s->cplx_loc * 8)) || (rc = salloc(s, &s->Tb, 10 * s->cplx_loc * 8)) ||
-            (rc = salloc(s, &s->G, 4 * s->cplx_loc * 8)))
+        if ((rc = salloc(s, (void **)&s->S, 10 * s->cplx_loc * s->csz)) ||
+            (rc = salloc(s, &s->Tb, 10 * s->cplx_loc * s->csz)) || (rc = salloc(s, &s->G, 4 * s->cplx_loc * s->csz)))
             return bail(rc);
         long long n2[2] = {N, N}, inem[2] = {N, N + 2}, onem[2] = {N, (long long)s->nz};
         size_t ws = 0;
@@ -243,7 +285,7 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         s->have_plan = true;
         if (cufftSetAutoAllocation(s->plan2d, 0) != CUFFT_SUCCESS ||
             cufftMakePlanMany64(s->plan2d, 2, n2, inem, 1, (long long)N * (N + 2), onem, 1, (long long)N * s->nz,
-                                CUFFT_R2C, 10LL * s->nloc, &ws) != CUFFT_SUCCESS) {
+                                r2c, 10LL * s->nloc, &ws) != CUFFT_SUCCESS) {
             serr(s, GABE_ERR_CUFFT, "2-D r2c plan of the slab's source planes failed");
             return bail(GABE_ERR_CUFFT);
         }
@@ -269,6 +311,7 @@ int gabe_slab_destroy(gabe_slab *s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->have_plan) cufftDestroy(s->plan2d);
     if (s->have_plan_spec) cufftDestroy(s->plan_spec);
+    if (s->have_plan_i) cufftDestroy(s->plan_i);
     void *bufs[] = {s->X[0], s->X[1], s->D[0], s->D[1], s->send[0], s->send[1], s->recv[0], s->recv[1],
                     s->sc, s->partials, s->sums, s->stage, s->counters, s->S, s->Tb, s->G, s->fft_work,
                     s->bin_part, s->bin_cnt_part, s->bin_sum};
@@ -315,7 +358,7 @@ int gabe_slab_upload(gabe_slab *s, const double *field0, const double *dfield0, 
             SCK(s, to_fluct(s->stage, nf, dev_mean(s, a >= 2, a & 1), reinterpret_cast<float *>(dst), s->stream));
         }
     }
-    if (s->gws) SCK(s, cudaMemsetAsync(s->G, 0, 4 * s->cplx_loc * 8, s->stream));  // h, l start at zero
+    if (s->gws) SCK(s, cudaMemsetAsync(s->G, 0, 4 * s->cplx_loc * s->csz, s->stream));  // h, l start at zero
     SCK(s, cudaStreamSynchronize(s->stream));
     s->cur = 0;
     s->uploaded = true;
@@ -410,8 +453,8 @@ int gabe_slab_gw_buffers(gabe_slab *s, void **send, void **recv, int64_t *send_b
     if (recv) *recv = s->S;
     const Split spl(s->N, s->W);
     for (int r = 0; r < s->W; r++) {
-        if (send_bytes) send_bytes[r] = (int64_t)10 * s->nloc * spl.n(r) * s->nz * 8;
-        if (recv_bytes) recv_bytes[r] = (int64_t)10 * spl.n(r) * s->nloc * s->nz * 8;
+        if (send_bytes) send_bytes[r] = (int64_t)10 * s->nloc * spl.n(r) * s->nz * s->csz;
+        if (recv_bytes) recv_bytes[r] = (int64_t)10 * spl.n(r) * s->nloc * s->nz * s->csz;
     }
     return GABE_OK;
 }
@@ -420,9 +463,10 @@ int gabe_slab_gw_transform(gabe_slab *s) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "transform before upload") : GABE_ERR_PARAM;
     if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
     SCK(s, cudaSetDevice(s->dev));
-    if (cufftExecR2C(s->plan2d, (cufftReal *)s->S, (cufftComplex *)s->S) != CUFFT_SUCCESS)
-        return serr(s, GABE_ERR_CUFFT, "2-D r2c of the source planes failed");
-    SCK(s, slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
+    int rc = r2c_planes(s, s->plan2d, s->S);
+    if (rc) return rc;
+    SCK(s, s->f32 ? slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream)
+                  : slab_gw_pack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
     return GABE_OK;
 }
 
@@ -430,11 +474,13 @@ int gabe_slab_gw_update(gabe_slab *s) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "update before upload") : GABE_ERR_PARAM;
     if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
     SCK(s, cudaSetDevice(s->dev));
-    const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
-    SCK(s, slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
+    SCK(s, s->f32 ? slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream)
+                  : slab_gw_unpack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
     // pass along i: for every component and column (y, kz), the N values of stride m nz
-    SCK(s, fft_col_pass_f32(s->N, s->Tb, N * m * nz, nz, m * nz, 10, (int)m, (int)nz, s->stream));
-    SCK(s, slab_kspace_f32(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream));
+    int rc = pass_i(s, s->Tb, 10);
+    if (rc) return rc;
+    SCK(s, s->f32 ? slab_kspace_f32(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream)
+                  : slab_kspace_f64(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream));
     return GABE_OK;
 }
 
@@ -443,14 +489,15 @@ int gabe_slab_gw_download(gabe_slab *s, double *h0, double *l0) {
     if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
     SCK(s, cudaSetDevice(s->dev));
     const size_t M = s->cplx_loc;  // this rank's k-points: N kx x nloc ky x (N/2+1) kz
-    const size_t chunk = 10 * s->cplx_loc * 8 / (12 * sizeof(double));  // points staged in the send buffer
+    const size_t chunk = 10 * s->cplx_loc * s->csz / (12 * sizeof(double));  // points staged in the send buffer
     double *stage = static_cast<double *>(s->Tb);
     double *dst[2] = {h0, l0};
     for (int w = 0; w < 2; w++) {
         if (!dst[w]) continue;
         for (size_t m0 = 0; m0 < M; m0 += chunk) {
             const size_t cnt = M - m0 < chunk ? M - m0 : chunk;
-            SCK(s, slab_gw_amplitudes_f32(s->G, cnt, m0, s->N, s->nloc, s->plane0, w, stage, s->stream));
+            SCK(s, s->f32 ? slab_gw_amplitudes_f32(s->G, cnt, m0, s->N, s->nloc, s->plane0, w, stage, s->stream)
+                          : slab_gw_amplitudes_f64(s->G, cnt, m0, s->N, s->nloc, s->plane0, w, stage, s->stream));
             SCK(s, cudaMemcpy2DAsync(dst[w] + m0, M * sizeof(double), stage, cnt * sizeof(double), cnt * sizeof(double),
                                      12, cudaMemcpyDeviceToHost, s->stream));
         }
@@ -461,16 +508,18 @@ int gabe_slab_gw_download(gabe_slab *s, double *h0, double *l0) {
 
 int gabe_slab_spectra_transform(gabe_slab *s) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "spectra before upload") : GABE_ERR_PARAM;
-    if (!s->spec) return serr(s, GABE_ERR_STATE, "slab spectra need FP32 storage, N in {64, ..., 512} and nranks");
+    if (!s->spec) return serr(s, GABE_ERR_STATE, "slab spectra need nranks (and, with FP32 storage, N in {64, ..., 512})");
     SCK(s, cudaSetDevice(s->dev));
-    const size_t N = s->N;
-    // own planes of both fields (fluctuations) into padded rows, then 2-D r2c and the pack by ky columns
+    const size_t N = s->N, w = s->w;
+    // own planes of both fields (FP32: fluctuations) into padded rows, then 2-D r2c and the pack by ky columns
+    char *S = reinterpret_cast<char *>(s->S);
     for (int f = 0; f < 2; f++)
-        SCK(s, cudaMemcpy2DAsync(s->S + (size_t)f * s->nloc * N * (N + 2), (N + 2) * 4, plane_ptr(s, s->cur, f, 1), N * 4,
-                                 N * 4, (size_t)s->nloc * N, cudaMemcpyDeviceToDevice, s->stream));
-    if (cufftExecR2C(s->plan_spec, (cufftReal *)s->S, (cufftComplex *)s->S) != CUFFT_SUCCESS)
-        return serr(s, GABE_ERR_CUFFT, "2-D r2c of the field planes failed");
-    SCK(s, slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
+        SCK(s, cudaMemcpy2DAsync(S + (size_t)f * s->nloc * N * (N + 2) * w, (N + 2) * w, plane_ptr(s, s->cur, f, 1), N * w,
+                                 N * w, (size_t)s->nloc * N, cudaMemcpyDeviceToDevice, s->stream));
+    int rc = r2c_planes(s, s->plan_spec, s->S);
+    if (rc) return rc;
+    SCK(s, s->f32 ? slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream)
+                  : slab_gw_pack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
     return GABE_OK;
 }
 
@@ -481,8 +530,8 @@ int gabe_slab_spectra_buffers(gabe_slab *s, void **send, void **recv, int64_t *s
     if (recv) *recv = s->S;
     const Split spl(s->N, s->W);
     for (int r = 0; r < s->W; r++) {
-        if (send_bytes) send_bytes[r] = (int64_t)2 * s->nloc * spl.n(r) * s->nz * 8;
-        if (recv_bytes) recv_bytes[r] = (int64_t)2 * spl.n(r) * s->nloc * s->nz * 8;
+        if (send_bytes) send_bytes[r] = (int64_t)2 * s->nloc * spl.n(r) * s->nz * s->csz;
+        if (recv_bytes) recv_bytes[r] = (int64_t)2 * spl.n(r) * s->nloc * s->nz * s->csz;
     }
     return GABE_OK;
 }
@@ -491,9 +540,10 @@ int gabe_slab_spectra_raw(gabe_slab *s, double *sums, double *counts) {
     if (!s || !s->uploaded || !sums || !counts) return s ? serr(s, GABE_ERR_PARAM, "bad arguments") : GABE_ERR_PARAM;
     if (!s->spec) return serr(s, GABE_ERR_STATE, "slab without spectra");
     SCK(s, cudaSetDevice(s->dev));
-    const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
-    SCK(s, slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
-    SCK(s, fft_col_pass_f32(s->N, s->Tb, N * m * nz, nz, m * nz, 2, (int)m, (int)nz, s->stream));
+    SCK(s, s->f32 ? slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream)
+                  : slab_gw_unpack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
+    int rc = pass_i(s, s->Tb, 2);
+    if (rc) return rc;
     SCK(s, cudaStreamSynchronize(s->stream));
     DevScalars d;
     SCK(s, cudaMemcpy(&d, s->sc, sizeof(d), cudaMemcpyDeviceToHost));
@@ -507,13 +557,13 @@ int gabe_slab_spectra_raw(gabe_slab *s, double *sums, double *counts) {
     b.nbins = nb;
     b.nseries = ns;
     b.quirk = s->p.gw_spec_quirk;
-    b.fix_zero = 1;
+    b.fix_zero = s->f32 ? 1 : 0;  // FP32 holds fluctuations: the k = 0 term gets N^3 fbar
     b.zero_re[0] = s->lc.gridsize * d.fbar[0];
     b.zero_re[1] = s->lc.gridsize * d.fbar[1];
     b.m = s->nloc;
     b.y0 = s->plane0;
     Launch lb{dim3(kSlabBinBlocks), dim3(256), (size_t)nb * (ns * 8 + 4), s->stream};
-    SCK(s, bins_f32(b, lb));
+    SCK(s, s->f32 ? bins_f32(b, lb) : bins_f64(b, lb));
     SCK(s, bin_reduce(s->bin_part, s->bin_cnt_part, kSlabBinBlocks, ns, nb, s->bin_sum, s->bin_sum + ns * nb, s->stream));
     SCK(s, cudaMemcpyAsync(sums, s->bin_sum, (size_t)ns * nb * 8, cudaMemcpyDeviceToHost, s->stream));
     SCK(s, cudaMemcpyAsync(counts, s->bin_sum + ns * nb, (size_t)nb * 8, cudaMemcpyDeviceToHost, s->stream));

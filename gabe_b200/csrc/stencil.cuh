@@ -261,10 +261,13 @@ __device__ __forceinline__ Nb7<T> axpy7(const Nb7<T> &x, T h, const Nb7<T> &y) {
     return r;
 }
 
+// sources [10][splanes][N][N+2]: the whole lattice (splanes = N, sfirst = 0)
+// or a slab's own planes (plane i at i - sfirst)
 template <typename T>
-__device__ __forceinline__ void store_sources(T *S, int N, int i, int j, int k, const T *s0, const T *s1) {
-    const size_t slot = (size_t)N * N * (N + 2);
-    const size_t o = ((size_t)i * N + j) * (N + 2) + k;
+__device__ __forceinline__ void store_sources(T *S, int N, int splanes, int sfirst, int i, int j, int k, const T *s0,
+                                              const T *s1) {
+    const size_t slot = (size_t)splanes * N * (N + 2);
+    const size_t o = ((size_t)(i - sfirst) * N + j) * (N + 2) + k;
 #pragma unroll
     for (int q = 0; q < kSrc; q++) {
         S[q * slot + o] = s0[q];
@@ -419,7 +422,8 @@ __device__ __forceinline__ void sweep_tile(const LatticeConsts &c, const TileJob
             acc[1] += pot64(c, f0[0].v[0], f0[1].v[0]);
             if constexpr (MODE != MODE_E0)
                 acc[3] += pot64(c, f0[0].v[0] + h * d0[0].v[0], f0[1].v[0] + h * d0[1].v[0]);
-            if constexpr (MODE == MODE_A_GW) store_sources(job.S, N, i, j, k, s0, s1);
+            if constexpr (MODE == MODE_A_GW)
+                store_sources(job.S, N, job.planes ? job.planes - 2 : N, job.planes ? 1 : 0, i, j, k, s0, s1);
         }
         if (more) {
 #pragma unroll

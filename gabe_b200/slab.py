@@ -126,8 +126,8 @@ class Slab:
         st = ctypes.c_void_p()
         self._check(lib.gabe_slab_stream(self._h, ctypes.byref(st)))
         self.stream_ptr = st.value or 0
-        kinds = (["gw"] if self.gws else []) + (["spec"] if self.precision == FP32 and self.N in (64, 128, 256, 512)
-                                                  and self.nranks >= 1 else [])
+        spec = (self.precision == FP64 or self.N in (64, 128, 256, 512)) and self.nranks >= 1
+        kinds = (["gw"] if self.gws else []) + (["spec"] if spec else [])
         for kind in kinds:  # all-to-all buffers of the GW sources and of the spectra's two fields
             snd, rcv = ctypes.c_void_p(), ctypes.c_void_p()
             sb = (ctypes.c_int64 * self.nranks)()

@@ -333,7 +333,7 @@ int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
  * initialisation.  All calls enqueue on the slab's stream
  * (gabe_slab_stream); order the exchange after it.
  *
- * With gws_on (FP32, N in {64, 128, 256, 512}; the planes must be the
+ * With gws_on (FP64, or FP32 with N in {64, 128, 256, 512}; the planes must be the
  * standard share of `nranks` ranks: n(r) = N/nranks + (r < N%nranks),
  * contiguous), between gabe_slab_finish(s, 0) and gabe_slab_sweep(s, 1):
  *   gabe_slab_gw_transform(s)  2-D transforms of the own source planes ->
@@ -343,7 +343,7 @@ int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
  *   gabe_slab_gw_update(s)     the passes along i and the TT projection +
  *                              h/l update of this rank's k-points: kx all,
  *                              ky in [plane0, plane0 + nplanes), kz all.
- * Spectra (FP32 slabs, N in {64, 128, 256, 512}): gabe_slab_spectra_transform(s)
+ * Spectra (FP64, or FP32 with N in {64, ..., 512}): gabe_slab_spectra_transform(s)
  * packs the 2-D transforms of the two fields; all-to-all the buffers of
  * gabe_slab_spectra_buffers as above; gabe_slab_spectra_raw(s, ...) bins
  * this rank's k-points (fields and, with GWs, l); add sums and counts over
@@ -354,7 +354,7 @@ typedef struct {
     int32_t struct_size; /* sizeof(gabe_slab_params) */
     int32_t plane0;      /* first own plane (global index i) */
     int32_t nplanes;     /* own planes, >= 1 */
-    int32_t nranks;      /* ranks of the split: needed with gws_on and for the spectra (FP32), where
+    int32_t nranks;      /* ranks of the split: needed with gws_on and for the spectra; when set,
                             [plane0, plane0 + nplanes) must be a rank's share; 0 = fields only */
 } gabe_slab_params;
 

@@ -9,10 +9,10 @@ against the same lattice on one handle (gabe_create).
   other: sums are added on the host, halos copied between steps) differ
   from the handle only in the order of the energy sums: FP64 to ~1e-12,
   FP32 (fluctuations about the FP64 mean) to its rounding.
-* With GWs (FP32) the slabs transform their source planes in 2-D, transpose
-  the half spectra between them by ky columns and take the pass along i
-  and the h/l update of their own k-points; h and l agree with the handle's
-  3-D cuFFT path to FP32 transform rounding.
+* With GWs the slabs transform their source planes in 2-D, transpose the
+  half spectra between them by ky columns and take the pass along i and
+  the h/l update of their own k-points; h and l agree with the handle's
+  3-D cuFFT path to transform rounding (FP32 or FP64).
 """
 import os
 import socket
@@ -176,15 +176,16 @@ def test_slab_rejects_sweeps_before_upload():
 
 
 FFT_TOL = 1e-5  # relative, FP32 transforms
+FFT_TOL64 = 1e-11  # relative, FP64 transforms
 
 
 def _norm_rel(got, want):
     return float(np.linalg.norm(got - want) / np.linalg.norm(want))
 
 
-def _gw_slabs(N, st, steps, comm):
+def _gw_slabs(N, st, steps, comm, precision=gb.FP32):
     f, d, a0, ad0 = st
-    with gs.SlabLattice(N, comm, precision=gb.FP32, gws=True) as lat:
+    with gs.SlabLattice(N, comm, precision=precision, gws=True) as lat:
         fs = [f[:, p0:p0 + n] for p0, n in lat.planes]
         ds = [d[:, p0:p0 + n] for p0, n in lat.planes]
         lat.upload(fs if len(fs) > 1 else fs[0], ds if len(ds) > 1 else ds[0], a0, ad0)
@@ -198,9 +199,9 @@ def _gw_slabs(N, st, steps, comm):
     return f1, h1, l1, sc
 
 
-def _gw_whole(N, st, steps):
+def _gw_whole(N, st, steps, precision=gb.FP32):
     f, d, a0, ad0 = st
-    with gb.Lattice(N, gws=True, precision=gb.FP32) as lat:
+    with gb.Lattice(N, gws=True, precision=precision) as lat:
         lat.upload_state(f, d, a0=a0, adot0=ad0)
         lat.step(steps)
         sc = lat.scalars()
@@ -230,6 +231,31 @@ def test_gw_slabs_match_the_whole_lattice(world):
     _gw_compare(_gw_slabs(N, st, STEPS, gs.LocalComm(world)), _gw_whole(N, st, STEPS))
 
 
+def _gw_compare64(a, b, world):
+    """FP64: one slab's fields are the handle's bit for bit (GWs do not act
+    on the fields; sweep A only also stores the sources); several slabs add
+    the energy sums in another order (~1e-12)."""
+    (f1, h1, l1, s1), (f0, h0, l0, s0) = a, b
+    if world == 1:
+        np.testing.assert_array_equal(f1, f0)
+        np.testing.assert_array_equal(s1, s0)
+    else:
+        assert np.abs(f1 - f0).max() <= 1e-11 * np.abs(f0).max()
+        for q in range(12):  # edgrad (8, 9) is ~1e-11 of rho here: measured against rho
+            tol = 1e-11 * (abs(s0[10]) if q in (8, 9) else abs(s0[q]))
+            assert abs(s1[q] - s0[q]) <= tol, (q, s1[q], s0[q])
+    assert np.linalg.norm(l0) > 0
+    assert _norm_rel(h1, h0) <= FFT_TOL64
+    assert _norm_rel(l1, l0) <= FFT_TOL64
+
+
+@pytest.mark.parametrize("N,world", [(64, 1), (64, 2), (48, 3)])
+def test_fp64_gw_slabs_match_the_whole_lattice(N, world):
+    st = _state(N, seed=31)
+    got = _gw_slabs(N, st, STEPS, gs.LocalComm(world), precision=gb.FP64)
+    _gw_compare64(got, _gw_whole(N, st, STEPS, precision=gb.FP64), world)
+
+
 def test_gw_slabs_through_a_one_rank_nccl_group():
     import datetime
 
@@ -255,18 +281,19 @@ def _cols_close(got, want, cols):
     return float(np.max((np.abs(g - w) - floor) / np.abs(w).clip(min=1e-300)))
 
 
-@pytest.mark.parametrize("world,gws", [(1, True), (3, True), (2, False)])
-def test_slab_spectra_match_the_whole_lattice(world, gws):
+@pytest.mark.parametrize("world,gws,precision", [(1, True, gb.FP32), (3, True, gb.FP32), (2, False, gb.FP32),
+                                                 (2, True, gb.FP64), (3, False, gb.FP64)])
+def test_slab_spectra_match_the_whole_lattice(world, gws, precision):
     """specOut's table of a split lattice: each slab bins its own k-points
     after the fields' transpose; the sums over the slabs, normalised, are
-    the handle's spectra to FP32 transform rounding."""
+    the handle's spectra to transform rounding (FP32 or FP64)."""
     N = 64
     f, d, a0, ad0 = _state(N, seed=29)
-    with gb.Lattice(N, gws=gws, precision=gb.FP32) as lat:
+    with gb.Lattice(N, gws=gws, precision=precision) as lat:
         lat.upload_state(f, d, a0=a0, adot0=ad0)
         lat.step(STEPS)
         want = lat.spec_out()
-    with gs.SlabLattice(N, gs.LocalComm(world), precision=gb.FP32, gws=gws) as sl:
+    with gs.SlabLattice(N, gs.LocalComm(world), precision=precision, gws=gws) as sl:
         fs = [f[:, p0:p0 + n] for p0, n in sl.planes]
         ds = [d[:, p0:p0 + n] for p0, n in sl.planes]
         sl.upload(fs if len(fs) > 1 else fs[0], ds if len(ds) > 1 else ds[0], a0, ad0)
@@ -274,9 +301,10 @@ def test_slab_spectra_match_the_whole_lattice(world, gws):
         got = sl.spectra()
     assert got.shape == want.shape
     np.testing.assert_array_equal(got[:, 0], want[:, 0])
-    assert _cols_close(got, want, [1, 2, 3, 4]) <= 1e-5
+    tol = FFT_TOL if precision == gb.FP32 else FFT_TOL64
+    assert _cols_close(got, want, [1, 2, 3, 4]) <= tol
     if gws:
         assert np.abs(want[:, 5]).max() > 0
-        assert _cols_close(got, want, [5, 6]) <= FFT_TOL
+        assert _cols_close(got, want, [5, 6]) <= tol
         np.testing.assert_array_equal(got[:, 7], want[:, 7])
 

@@ -42,7 +42,7 @@ def test_slab_create_rejects_bad_params(case):
     lib.gabe_default_params(ctypes.byref(p), 32)
     sp = gs.SlabParams(ctypes.sizeof(gs.SlabParams), 0, 8, 0)
     if case == "gws":
-        p.gws_on = 1  # FP64
+        p.gws_on, p.precision = 1, gb.FP32  # FP32 GWs need N in {64, ..., 512}
     elif case == "gws_expansion2":  # a valid split of 64 planes over 4 ranks; only the expansion type is wrong
         p.N, p.gws_on, p.precision, p.expansion, sp.nplanes, sp.nranks = 64, 1, gb.FP32, 2, 16, 4
     elif case == "gws_split":  # planes [0, 8) are not a rank's share of 64 planes over 3 ranks (22, 21, 21)
