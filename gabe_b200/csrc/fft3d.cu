@@ -68,6 +68,16 @@ cudaError_t col_pass_n(const f3d::ColArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int N>
+cudaError_t col_gather_n(const f3d::ColArgs &a, cudaStream_t s) {
+    int g = 0;
+    constexpr size_t smem = f3d::ColGeom<N>::SMEM_BYTES_GATHER;
+    cudaError_t e = persistent_grid(f3d::col_fft_kernel<N, true>, f3d::kFftThreads, smem, &g);
+    if (e != cudaSuccess) return e;
+    f3d::col_fft_kernel<N, true><<<g, f3d::kFftThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 bool fft3d_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
@@ -90,6 +100,20 @@ cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long lo
         case 128: return col_pass_n<128>(a, s);
         case 256: return col_pass_n<256>(a, s);
         case 512: return col_pass_n<512>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t fft_col_gather_f32(int N, const void *recv, void *T, int ncomp, int m, int ranks, cudaStream_t s) {
+    const long long nz = N / 2 + 1;
+    f3d::ColArgs a{static_cast<float2 *>(T), (long long)N * m * nz, nz, (long long)m * nz, ncomp, m, (int)nz};
+    a.src = static_cast<const float2 *>(recv);
+    a.ranks = ranks;
+    switch (N) {
+        case 64: return col_gather_n<64>(a, s);
+        case 128: return col_gather_n<128>(a, s);
+        case 256: return col_gather_n<256>(a, s);
+        case 512: return col_gather_n<512>(a, s);
         default: return cudaErrorInvalidValue;
     }
 }

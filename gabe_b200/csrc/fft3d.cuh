@@ -19,6 +19,7 @@
 #pragma once
 
 #include "planefft.cuh"
+#include "slabsplit.h"
 #include "sweep32.cuh"
 
 namespace gabe {
@@ -185,6 +186,14 @@ struct ColArgs {
     float2 *X;
     long long s1, s2, sn;
     int n1, n2, ncol;
+    // Gather form (col_fft_kernel<N, true>), the pass along i of a lattice
+    // split into slabs: the lines are read from the receive buffer of the
+    // transpose (slabgw.cuh), blocks by source rank r of [n1][n(r)][..]
+    // with the plane stride sn, and written to X out of place.  Value n of
+    // line (b1, b2) sits at src + (n1 p0(r) + n - p0(r) + b1 n(r)) sn + b2 s2,
+    // r the owner of plane n among `ranks`.
+    const float2 *src = nullptr;
+    int ranks = 0;
 };
 
 template <int N>
@@ -194,16 +203,27 @@ struct ColGeom {
     static constexpr int BUF = N * W;                // complex per tile buffer
     static constexpr int SMEM_C = kFftBufs * BUF + N;  // tile ring + twiddles (complex)
     static constexpr size_t SMEM_BYTES = (size_t)SMEM_C * sizeof(float2);
+    static constexpr size_t SMEM_BYTES_GATHER = SMEM_BYTES + 2 * N * sizeof(long long);  // + line offsets
 };
 
-template <int N>
+template <int N, bool GATHER = false>
 __global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
     using Gm = ColGeom<N>;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, W = Gm::W, T = Gm::T;
     extern __shared__ __align__(16) float2 cs[];
     float2 *tw = cs + kFftBufs * Gm::BUF;  // [k2][n1]
+    long long *goff = reinterpret_cast<long long *>(tw + N), *gq = goff + N;  // gather form only
     const int tid = threadIdx.x;
     twiddles<N>(tw);
+    if constexpr (GATHER) {
+        const Split sp(N, a.ranks);
+        for (int n = tid; n < N; n += T) {
+            const int r = sp.owner(n), p0 = sp.p0(r);
+            goff[n] = ((long long)a.n1 * p0 + (n - p0)) * a.sn;
+            gq[n] = (long long)sp.n(r) * a.sn;
+        }
+        __syncthreads();  // the offsets are read by the first copies
+    }
     const int ncb = (a.ncol + W - 1) / W;
     const long long ntiles = (long long)a.n1 * a.n2 * ncb;
     auto tile_base = [&](long long tile, int &wn) {
@@ -217,9 +237,20 @@ __global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
         int wn;
         const float2 *base = tile_base(tile, wn);
         float2 *col = cs + b * Gm::BUF;
-        for (int t = tid; t < N * W; t += T) {
-            const int n = t / W, w = t % W;
-            if (w < wn) s32::cp_async8(col + t, base + n * a.sn + w);
+        if constexpr (GATHER) {
+            const int cb = (int)(tile % ncb);
+            const long long bb = tile / ncb;
+            const int b2 = (int)(bb % a.n2), b1 = (int)(bb / a.n2);
+            const float2 *g = a.src + b2 * a.s2 + cb * W;
+            for (int t = tid; t < N * W; t += T) {
+                const int n = t / W, w = t % W;
+                if (w < wn) s32::cp_async8(col + t, g + goff[n] + b1 * gq[n] + w);
+            }
+        } else {
+            for (int t = tid; t < N * W; t += T) {
+                const int n = t / W, w = t % W;
+                if (w < wn) s32::cp_async8(col + t, base + n * a.sn + w);
+            }
         }
     };
 #pragma unroll

@@ -125,21 +125,24 @@ StencilArgs slab_args(gabe_slab *s, int counter, double *sums_out) {
 }
 
 // Transform helpers by precision: the 2-D r2c of planes in place, and the
-// pass along i of ncomp components of T[ncomp][N][m][nz] in place.
+// receive buffer S of a transpose -> T[ncomp][N][m][nz] transformed along i
+// (FP32: one column pass that gathers its lines from the blocks of S; FP64:
+// unpack, then a strided cuFFT Z2Z in place).
 int r2c_planes(gabe_slab *s, cufftHandle plan, void *X) {
     const cufftResult r = s->f32 ? cufftExecR2C(plan, (cufftReal *)X, (cufftComplex *)X)
                                  : cufftExecD2Z(plan, (cufftDoubleReal *)X, (cufftDoubleComplex *)X);
     return r == CUFFT_SUCCESS ? GABE_OK : serr(s, GABE_ERR_CUFFT, "2-D r2c of the slab's planes failed");
 }
 
-int pass_i(gabe_slab *s, void *Tb, int ncomp) {
+int receive_pass_i(gabe_slab *s, int ncomp) {
     const long long N = s->N, m = s->nloc, nz = (long long)s->nz;
     if (s->f32) {
-        SCK(s, fft_col_pass_f32(s->N, Tb, N * m * nz, nz, m * nz, ncomp, (int)m, (int)nz, s->stream));
+        SCK(s, fft_col_gather_f32(s->N, s->S, s->Tb, ncomp, s->nloc, s->W, s->stream));
         return GABE_OK;
     }
+    SCK(s, slab_gw_unpack_f64(s->S, s->Tb, s->N, s->nloc, s->W, ncomp, s->stream));
     for (int q = 0; q < ncomp; q++) {
-        cufftDoubleComplex *X = static_cast<cufftDoubleComplex *>(Tb) + (size_t)q * N * m * nz;
+        cufftDoubleComplex *X = static_cast<cufftDoubleComplex *>(s->Tb) + (size_t)q * N * m * nz;
         if (cufftExecZ2Z(s->plan_i, X, X, CUFFT_FORWARD) != CUFFT_SUCCESS)
             return serr(s, GABE_ERR_CUFFT, "pass along i failed");
     }
@@ -474,10 +477,8 @@ int gabe_slab_gw_update(gabe_slab *s) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "update before upload") : GABE_ERR_PARAM;
     if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
     SCK(s, cudaSetDevice(s->dev));
-    SCK(s, s->f32 ? slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream)
-                  : slab_gw_unpack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
     // pass along i: for every component and column (y, kz), the N values of stride m nz
-    int rc = pass_i(s, s->Tb, 10);
+    int rc = receive_pass_i(s, 10);
     if (rc) return rc;
     SCK(s, s->f32 ? slab_kspace_f32(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream)
                   : slab_kspace_f64(s->Tb, s->G, s->sc, s->lc, s->nloc, s->plane0, s->stream));
@@ -540,9 +541,7 @@ int gabe_slab_spectra_raw(gabe_slab *s, double *sums, double *counts) {
     if (!s || !s->uploaded || !sums || !counts) return s ? serr(s, GABE_ERR_PARAM, "bad arguments") : GABE_ERR_PARAM;
     if (!s->spec) return serr(s, GABE_ERR_STATE, "slab without spectra");
     SCK(s, cudaSetDevice(s->dev));
-    SCK(s, s->f32 ? slab_gw_unpack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream)
-                  : slab_gw_unpack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
-    int rc = pass_i(s, s->Tb, 2);
+    int rc = receive_pass_i(s, 2);
     if (rc) return rc;
     SCK(s, cudaStreamSynchronize(s->stream));
     DevScalars d;
