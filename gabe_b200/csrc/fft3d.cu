@@ -68,14 +68,31 @@ cudaError_t col_pass_n(const f3d::ColArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-template <int N>
-cudaError_t col_gather_n(const f3d::ColArgs &a, cudaStream_t s) {
+template <int N, int MODE>
+cudaError_t col_slab_n(const f3d::ColArgs &a, cudaStream_t s) {
     int g = 0;
-    constexpr size_t smem = f3d::ColGeom<N>::SMEM_BYTES_GATHER;
-    cudaError_t e = persistent_grid(f3d::col_fft_kernel<N, true>, f3d::kFftThreads, smem, &g);
+    constexpr size_t smem = f3d::ColGeom<N>::SMEM_BYTES_SLAB;
+    cudaError_t e = persistent_grid(f3d::col_fft_kernel<N, MODE>, f3d::kFftThreads, smem, &g);
     if (e != cudaSuccess) return e;
-    f3d::col_fft_kernel<N, true><<<g, f3d::kFftThreads, smem, s>>>(a);
+    f3d::col_fft_kernel<N, MODE><<<g, f3d::kFftThreads, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// 2-D r2c of the nplanes planes [N][N+2] of S (rows along k in place, then
+// along j) written to the transpose's send buffer
+template <int N>
+cudaError_t plane_scatter_n(float *S, void *send, int nplanes, int ranks, cudaStream_t s) {
+    constexpr long long nz = N / 2 + 1;
+    using RG = f3d::RowGeom<N>;
+    int g1 = 0;
+    cudaError_t e = persistent_grid(f3d::row_r2c_kernel<N>, RG::T, RG::SMEM_BYTES, &g1);
+    if (e != cudaSuccess) return e;
+    f3d::row_r2c_kernel<N><<<g1, RG::T, RG::SMEM_BYTES, s>>>(S, (long long)nplanes * N);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    f3d::ColArgs a{reinterpret_cast<float2 *>(S), (long long)N * nz, 0, nz, nplanes, 1, (int)nz};
+    a.dst = static_cast<float2 *>(send);
+    a.ranks = ranks;
+    return col_slab_n<N, f3d::kColScatter>(a, s);
 }
 
 }  // namespace
@@ -110,10 +127,20 @@ cudaError_t fft_col_gather_f32(int N, const void *recv, void *T, int ncomp, int 
     a.src = static_cast<const float2 *>(recv);
     a.ranks = ranks;
     switch (N) {
-        case 64: return col_gather_n<64>(a, s);
-        case 128: return col_gather_n<128>(a, s);
-        case 256: return col_gather_n<256>(a, s);
-        case 512: return col_gather_n<512>(a, s);
+        case 64: return col_slab_n<64, f3d::kColGather>(a, s);
+        case 128: return col_slab_n<128, f3d::kColGather>(a, s);
+        case 256: return col_slab_n<256, f3d::kColGather>(a, s);
+        case 512: return col_slab_n<512, f3d::kColGather>(a, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int ranks, cudaStream_t s) {
+    switch (N) {
+        case 64: return plane_scatter_n<64>(S, send, nplanes, ranks, s);
+        case 128: return plane_scatter_n<128>(S, send, nplanes, ranks, s);
+        case 256: return plane_scatter_n<256>(S, send, nplanes, ranks, s);
+        case 512: return plane_scatter_n<512>(S, send, nplanes, ranks, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -186,15 +186,22 @@ struct ColArgs {
     float2 *X;
     long long s1, s2, sn;
     int n1, n2, ncol;
-    // Gather form (col_fft_kernel<N, true>), the pass along i of a lattice
-    // split into slabs: the lines are read from the receive buffer of the
-    // transpose (slabgw.cuh), blocks by source rank r of [n1][n(r)][..]
-    // with the plane stride sn, and written to X out of place.  Value n of
-    // line (b1, b2) sits at src + (n1 p0(r) + n - p0(r) + b1 n(r)) sn + b2 s2,
-    // r the owner of plane n among `ranks`.
+    // Forms for a lattice split into slabs (slabgw.cuh), r the owner of
+    // index n among `ranks` ranks:
+    // gather (kColGather), the pass along i: the lines are read from the
+    // receive buffer of the transpose, blocks by source rank of
+    // [n1][n(r)][..] with the plane stride sn -- value n of line (b1, b2) at
+    // src + (n1 p0(r) + n - p0(r) + b1 n(r)) sn + b2 s2 -- and written to X;
+    // scatter (kColScatter), the pass along j (n2 = 1): lines read from X,
+    // output value n of line b1 written to the send buffer of the transpose,
+    // blocks by destination rank of [n1][n(r)][ncol], at
+    // dst + (n1 p0(r) + n - p0(r) + b1 n(r)) ncol.
     const float2 *src = nullptr;
+    float2 *dst = nullptr;
     int ranks = 0;
 };
+
+constexpr int kColInPlace = 0, kColGather = 1, kColScatter = 2;
 
 template <int N>
 struct ColGeom {
@@ -203,24 +210,26 @@ struct ColGeom {
     static constexpr int BUF = N * W;                // complex per tile buffer
     static constexpr int SMEM_C = kFftBufs * BUF + N;  // tile ring + twiddles (complex)
     static constexpr size_t SMEM_BYTES = (size_t)SMEM_C * sizeof(float2);
-    static constexpr size_t SMEM_BYTES_GATHER = SMEM_BYTES + 2 * N * sizeof(long long);  // + line offsets
+    static constexpr size_t SMEM_BYTES_SLAB = SMEM_BYTES + 2 * N * sizeof(long long);  // + per-index offsets
 };
 
-template <int N, bool GATHER = false>
+template <int N, int MODE = kColInPlace>
 __global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
     using Gm = ColGeom<N>;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, W = Gm::W, T = Gm::T;
     extern __shared__ __align__(16) float2 cs[];
     float2 *tw = cs + kFftBufs * Gm::BUF;  // [k2][n1]
-    long long *goff = reinterpret_cast<long long *>(tw + N), *gq = goff + N;  // gather form only
+    // slab forms: offset of index n for b1 = 0 and its growth per b1
+    long long *goff = reinterpret_cast<long long *>(tw + N), *gq = goff + N;
     const int tid = threadIdx.x;
     twiddles<N>(tw);
-    if constexpr (GATHER) {
+    if constexpr (MODE != kColInPlace) {
         const Split sp(N, a.ranks);
+        const long long unit = MODE == kColGather ? a.sn : (long long)a.ncol;
         for (int n = tid; n < N; n += T) {
             const int r = sp.owner(n), p0 = sp.p0(r);
-            goff[n] = ((long long)a.n1 * p0 + (n - p0)) * a.sn;
-            gq[n] = (long long)sp.n(r) * a.sn;
+            goff[n] = ((long long)a.n1 * p0 + (n - p0)) * unit;
+            gq[n] = (long long)sp.n(r) * unit;
         }
         __syncthreads();  // the offsets are read by the first copies
     }
@@ -237,7 +246,7 @@ __global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
         int wn;
         const float2 *base = tile_base(tile, wn);
         float2 *col = cs + b * Gm::BUF;
-        if constexpr (GATHER) {
+        if constexpr (MODE == kColGather) {
             const int cb = (int)(tile % ncb);
             const long long bb = tile / ncb;
             const int b2 = (int)(bb % a.n2), b1 = (int)(bb / a.n2);
@@ -286,9 +295,21 @@ __global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
 #pragma unroll
             for (int n1 = 0; n1 < L1; n1++) y[n1] = col[(n1 + L1 * k2) * W + w];
             pfft::fft_reg<L1>(y);
-            if (w < wn)
+            if (w < wn) {
+                if constexpr (MODE == kColScatter) {
+                    const int cb = (int)(tile % ncb);
+                    const long long b1 = tile / ncb / a.n2;
+                    float2 *g = a.dst + cb * W + w;
 #pragma unroll
-                for (int k1 = 0; k1 < L1; k1++) __stcs(base + (k2 + L2 * k1) * a.sn + w, y[k1]);
+                    for (int k1 = 0; k1 < L1; k1++) {
+                        const int k = k2 + L2 * k1;
+                        __stcs(g + goff[k] + b1 * gq[k], y[k1]);
+                    }
+                } else {
+#pragma unroll
+                    for (int k1 = 0; k1 < L1; k1++) __stcs(base + (k2 + L2 * k1) * a.sn + w, y[k1]);
+                }
+            }
         }
     }
     s32::cp_wait<0>();

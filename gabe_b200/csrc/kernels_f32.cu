@@ -56,9 +56,6 @@ cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, co
     return cudaGetLastError();
 }
 
-cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s) {
-    return slab_gw_pack<float>(S, send, N, nloc, W, ncomp, s);
-}
 cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
                             cudaStream_t s) {
     return slab_kspace<float>(T, G, sc, c, m, y0, s);

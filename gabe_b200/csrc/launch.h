@@ -115,7 +115,6 @@ cudaError_t slab_finish_f32(int mode, const LatticeConsts &c, DevScalars *sc, co
 cudaError_t slab_finish_f64(int mode, const LatticeConsts &c, DevScalars *sc, const double *tot, cudaStream_t s);
 // Slab GW branch, FP32 (slabgw.cuh): pack the 2-D transforms for the all-to-all, unpack what
 // arrived into [10][N][m][nz], the k-space update of the rank's k-points, amplitudes -> 12 components.
-cudaError_t slab_gw_pack_f32(const void *S, void *send, int N, int nloc, int W, int ncomp, cudaStream_t s);
 cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const LatticeConsts &c, int m, int y0,
                             cudaStream_t s);
 cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
@@ -164,6 +163,10 @@ cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long lo
 // The pass along i of a slab transpose's receive buffer (blocks by source rank of
 // [ncomp][n(r)][m][N/2+1]) into T[ncomp][N][m][N/2+1], out of place (fft3d.cuh).
 cudaError_t fft_col_gather_f32(int N, const void *recv, void *T, int ncomp, int m, int ranks, cudaStream_t s);
+// 2-D r2c over (j, k) of nplanes planes [N][N+2] of S (rows transformed in place), the
+// pass along j written to the transpose's send buffer (blocks by destination rank of
+// [nplanes][n(r)][N/2+1]), for N in {64, 128, 256, 512} (fft3d.cuh).
+cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int ranks, cudaStream_t s);
 // Its passes along j and i alone, for sources already transformed along k.
 cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s);
 

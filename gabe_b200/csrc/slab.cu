@@ -124,14 +124,22 @@ StencilArgs slab_args(gabe_slab *s, int counter, double *sums_out) {
     return a;
 }
 
-// Transform helpers by precision: the 2-D r2c of planes in place, and the
-// receive buffer S of a transpose -> T[ncomp][N][m][nz] transformed along i
-// (FP32: one column pass that gathers its lines from the blocks of S; FP64:
+// Transform helpers by precision.  The planes [ncomp][nloc][N][N+2] of S ->
+// their 2-D r2c in the send buffer Tb, blocks by destination rank (FP32: the
+// library's pass along k in place and its pass along j written straight to
+// the blocks; FP64: a cuFFT D2Z plan in place, then the pack).  The receive
+// buffer S of a transpose -> T[ncomp][N][m][nz] transformed along i (FP32:
+// one column pass that gathers its lines from the blocks of S; FP64:
 // unpack, then a strided cuFFT Z2Z in place).
-int r2c_planes(gabe_slab *s, cufftHandle plan, void *X) {
-    const cufftResult r = s->f32 ? cufftExecR2C(plan, (cufftReal *)X, (cufftComplex *)X)
-                                 : cufftExecD2Z(plan, (cufftDoubleReal *)X, (cufftDoubleComplex *)X);
-    return r == CUFFT_SUCCESS ? GABE_OK : serr(s, GABE_ERR_CUFFT, "2-D r2c of the slab's planes failed");
+int planes_to_send(gabe_slab *s, cufftHandle plan, int ncomp) {
+    if (s->f32) {
+        SCK(s, fft_plane_scatter_f32(s->N, static_cast<float *>(s->S), s->Tb, ncomp * s->nloc, s->W, s->stream));
+        return GABE_OK;
+    }
+    if (cufftExecD2Z(plan, (cufftDoubleReal *)s->S, (cufftDoubleComplex *)s->S) != CUFFT_SUCCESS)
+        return serr(s, GABE_ERR_CUFFT, "2-D r2c of the slab's planes failed");
+    SCK(s, slab_gw_pack_f64(s->S, s->Tb, s->N, s->nloc, s->W, ncomp, s->stream));
+    return GABE_OK;
 }
 
 int receive_pass_i(gabe_slab *s, int ncomp) {
@@ -255,7 +263,7 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
             return bail(GABE_ERR_CUFFT);
         }
     }
-    if (s->spec) {
+    if (s->spec && !s->f32) {
         long long n2[2] = {N, N}, inem[2] = {N, N + 2}, onem[2] = {N, (long long)s->nz};
         size_t ws = 0;
         if (cufftCreate(&s->plan_spec) != CUFFT_SUCCESS) {
@@ -269,6 +277,8 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
             serr(s, GABE_ERR_CUFFT, "2-D r2c plan of the slab's field planes failed");
             return bail(GABE_ERR_CUFFT);
         }
+    }
+    if (s->spec) {
         const int ns = 3, nb = s->nbins;
         if ((rc = salloc(s, (void **)&s->bin_part, (size_t)kSlabBinBlocks * ns * nb * sizeof(double))) ||
             (rc = salloc(s, (void **)&s->bin_cnt_part, (size_t)kSlabBinBlocks * nb * sizeof(unsigned int))) ||
@@ -279,6 +289,8 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
         if ((rc = salloc(s, (void **)&s->S, 10 * s->cplx_loc * s->csz)) ||
             (rc = salloc(s, &s->Tb, 10 * s->cplx_loc * s->csz)) || (rc = salloc(s, &s->G, 4 * s->cplx_loc * s->csz)))
             return bail(rc);
+    }
+    if (s->gws && !s->f32) {
         long long n2[2] = {N, N}, inem[2] = {N, N + 2}, onem[2] = {N, (long long)s->nz};
         size_t ws = 0;
         if (cufftCreate(&s->plan2d) != CUFFT_SUCCESS) {
@@ -466,11 +478,7 @@ int gabe_slab_gw_transform(gabe_slab *s) {
     if (!s || !s->uploaded) return s ? serr(s, GABE_ERR_STATE, "transform before upload") : GABE_ERR_PARAM;
     if (!s->gws) return serr(s, GABE_ERR_STATE, "slab without GWs");
     SCK(s, cudaSetDevice(s->dev));
-    int rc = r2c_planes(s, s->plan2d, s->S);
-    if (rc) return rc;
-    SCK(s, s->f32 ? slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream)
-                  : slab_gw_pack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 10, s->stream));
-    return GABE_OK;
+    return planes_to_send(s, s->plan2d, 10);
 }
 
 int gabe_slab_gw_update(gabe_slab *s) {
@@ -512,16 +520,12 @@ int gabe_slab_spectra_transform(gabe_slab *s) {
     if (!s->spec) return serr(s, GABE_ERR_STATE, "slab spectra need nranks (and, with FP32 storage, N in {64, ..., 512})");
     SCK(s, cudaSetDevice(s->dev));
     const size_t N = s->N, w = s->w;
-    // own planes of both fields (FP32: fluctuations) into padded rows, then 2-D r2c and the pack by ky columns
+    // own planes of both fields (FP32: fluctuations) into padded rows, then 2-D r2c into the send blocks
     char *S = reinterpret_cast<char *>(s->S);
     for (int f = 0; f < 2; f++)
         SCK(s, cudaMemcpy2DAsync(S + (size_t)f * s->nloc * N * (N + 2) * w, (N + 2) * w, plane_ptr(s, s->cur, f, 1), N * w,
                                  N * w, (size_t)s->nloc * N, cudaMemcpyDeviceToDevice, s->stream));
-    int rc = r2c_planes(s, s->plan_spec, s->S);
-    if (rc) return rc;
-    SCK(s, s->f32 ? slab_gw_pack_f32(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream)
-                  : slab_gw_pack_f64(s->S, s->Tb, s->N, s->nloc, s->W, 2, s->stream));
-    return GABE_OK;
+    return planes_to_send(s, s->plan_spec, 2);
 }
 
 int gabe_slab_spectra_buffers(gabe_slab *s, void **send, void **recv, int64_t *send_bytes, int64_t *recv_bytes) {

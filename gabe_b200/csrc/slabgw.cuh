@@ -4,13 +4,16 @@
 //
 // The 3-D transform of the ten source arrays (fft_stresstensor,
 // g2evolutionpert.cpp:183-195) runs as
-//   1. a 2-D r2c over (j, k) of every own plane (cuFFT, in place):
-//      S[q][il][ky][kz], il < nplanes;
-//   2. a transpose between the ranks: rank r' receives the ky columns it
-//      owns, [y0_r', y0_r' + m_r'), of every plane -- pack (below), an
-//      all-to-all by the caller, unpack (below) into T[q][i][y][kz] with i
-//      the global plane;
-//   3. the pass along i (fft3d.cuh col_fft_kernel) on T;
+//   1. a 2-D r2c over (j, k) of every own plane, S[q][il][ky][kz],
+//      il < nplanes, into the send buffer in blocks by destination rank:
+//      rank r' receives the ky columns it owns, [y0_r', y0_r' + m_r'), of
+//      every plane.  FP32: the library's passes (fft3d.cuh), the one along
+//      j writing the blocks directly; FP64: cuFFT D2Z in place and the
+//      pack (below);
+//   2. the all-to-all, by the caller;
+//   3. the pass along i into T[q][i][y][kz], i the global plane.  FP32: the
+//      library's column pass reading its lines from the receive blocks;
+//      FP64: the unpack (below) and a strided cuFFT Z2Z;
 // and the k-space update (kspace.cuh kspace_update) takes the rank's own
 // k-points, (kx, y0 + y, kz), from T with the amplitudes G[4][kx][y][kz].
 // Planes (i) and columns (ky) are split over the ranks with one rule:
