@@ -134,13 +134,18 @@ def algorithmic_bytes(N: int, w: int, gws: bool) -> dict:
       fft     10 real-to-complex transforms: read N^3, write N^2(N/2+1) complex each
       kspace  read 10 transformed source components and the 4 TT amplitudes
               (h+, hx, l+, lx), write the 4 amplitudes: 36 reals per k-point
-      stage2  sweep B: read f0, fdot0; write f0', fdot0'"""
+      stage2  sweep B: read f0, fdot0; write f0', fdot0'
+    and, for the library's 3-D FFT, each of its passes (one launch each):
+      fft_rows  read the N^3 reals, write N^2(N/2+1) complex per array
+      fft_j, fft_i  read and write N^2(N/2+1) complex per array"""
     n3 = N ** 3
     M = N * N * (N // 2 + 1)
     b = {"stage1": (4 + (10 if gws else 0)) * n3 * w, "stage2": 8 * n3 * w}
     if gws:
         b["fft"] = 10 * (n3 + 2 * M) * w
         b["kspace"] = 36 * M * w
+        b["fft_rows"] = 10 * (n3 + 2 * M) * w
+        b["fft_j"] = b["fft_i"] = 10 * 4 * M * w
     return b
 
 
@@ -163,8 +168,9 @@ def traffic_scaled(kernel: str, precision: str, N: int):
     e = d.get(precision, {}).get(kernel)
     if not e:
         return None
-    # DRAM bytes grow with the sites (sweeps) or k-points (k-space) processed
-    scale = (N / e["N"]) ** 3 if kernel != "kspace" else (N * N * (N // 2 + 1)) / (e["N"] ** 2 * (e["N"] // 2 + 1))
+    # DRAM bytes grow with the sites (sweeps, row pass) or k-points (k-space, column passes) processed
+    kpts = kernel in ("kspace", "fft_j", "fft_i")
+    scale = (N / e["N"]) ** 3 if not kpts else (N * N * (N // 2 + 1)) / (e["N"] ** 2 * (e["N"] // 2 + 1))
     return e["bytes"] * scale
 
 
@@ -428,6 +434,8 @@ def main():
         except gb.GabeError:
             en, finite = None, False
         phases = lat.profile_steps(args.profile_steps)
+        if lat.launches_per_step == 6:  # the library's 3-D FFT: time its passes one by one
+            phases.update(lat.profile_fft_passes(args.profile_steps))
         # ---- end-to-end leg through the C ABI with host buffers
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -463,8 +471,12 @@ def main():
     algo = algorithmic_bytes(N, w, gws)
     kern = {}
     for ph, b in algo.items():
+        if ph not in L32["phases"]:  # passes of the library's FFT when cuFFT's plan ran instead
+            continue
         t = L32["phases"][ph] / 1e3
         kern[ph] = {"ms": L32["phases"][ph], "algorithmic_bytes": b, "achieved_gbs": b / t / 1e9 if t > 0 else None}
+    # the dominant launch among the library's own kernels: the FFT phase is three launches (its passes
+    # are listed one by one when they are the library's) or cuFFT's
     own = {k: v for k, v in kern.items() if k != "fft"}
     dom = max(own, key=lambda k: own[k]["ms"])
     ach = kern[dom]["achieved_gbs"]

@@ -39,6 +39,7 @@ FLAG_PLANE_FFT = 4
 FLAG_FUSED_KSPACE = 8
 FLAG_OWN_FFT = 16
 FLAG_FUSED_ROWS = 32
+FLAG_CUFFT_3D = 64
 
 STATUS = {
     0: "GABE_OK", 1: "GABE_ERR_PARAM", 2: "GABE_ERR_CUDA", 3: "GABE_ERR_CUFFT", 4: "GABE_ERR_NOMEM",
@@ -103,6 +104,7 @@ def library():
     L.gabe_device_bytes.restype = ctypes.c_size_t
     L.gabe_launches_per_step.argtypes = [H]
     L.gabe_profile_steps.argtypes = [H, ctypes.c_int, _dp]
+    L.gabe_profile_fft_passes.argtypes = [H, ctypes.c_int, _dp]
     L.gabe_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
     L.gabe_energy_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                       ctypes.c_void_p, ctypes.c_void_p]
@@ -240,6 +242,13 @@ class Lattice:
         out = (ctypes.c_double * 4)()
         self._check(library().gabe_profile_steps(self._h, int(n), out))
         return {"stage1": out[0], "fft": out[1], "kspace": out[2], "stage2": out[3]}
+
+    def profile_fft_passes(self, n: int) -> dict:
+        """Mean ms of each pass of the library's 3-D FFT over the source
+        buffer (handles that use it: launches_per_step == 6)."""
+        out = (ctypes.c_double * 3)()
+        self._check(library().gabe_profile_fft_passes(self._h, int(n), out))
+        return {"fft_rows": out[0], "fft_j": out[1], "fft_i": out[2]}
 
     @property
     def stream_ptr(self) -> int:

@@ -132,8 +132,10 @@ int make_plans(gabe_handle *h) {
     h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
     h->rows_fused = h->evolve_gw && h->f32 && !h->ks_fused && sweep32_rows_supported(h->N) &&
                     (h->p.flags & GABE_FLAG_FUSED_ROWS);
+    // the library's 3-D r2c: on request, and by default at N = 512 (measured faster than cuFFT's plan there)
+    const bool own_default = h->N == 512 && !(h->p.flags & GABE_FLAG_CUFFT_3D);
     h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && !h->rows_fused && fft3d_supported(h->N) &&
-                 (h->p.flags & GABE_FLAG_OWN_FFT);
+                 ((h->p.flags & GABE_FLAG_OWN_FFT) || own_default);
     if (h->plane_fft) {
         CK(h, plane_r2c_setup(h->N, &h->plane_grid));
     } else if (h->own_fft || h->rows_fused) {
@@ -684,6 +686,39 @@ int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]) {
     for (int q = 0; q < 4; q++) ms_out[q] = acc[q] / nsteps;
     DevScalars sc;
     return read_scalars(h, &sc);
+}
+
+int gabe_profile_fft_passes(gabe_handle *h, int nreps, double ms_out[3]) {
+    if (!h || !ms_out || nreps < 1) return GABE_ERR_PARAM;
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "profile before upload");
+    if (!h->own_fft) return set_err(h, GABE_ERR_STATE, "this handle does not use the library's 3-D FFT");
+    CK(h, cudaSetDevice(h->dev));
+    CK(h, cudaStreamSynchronize(h->stream));  // the last step's GW chain has finished with the sources
+    std::vector<cudaEvent_t> ev((size_t)4 * nreps, nullptr);
+    cudaError_t e = cudaSuccess;
+    for (auto &x : ev)
+        if (e == cudaSuccess) e = cudaEventCreate(&x);
+    float *S = static_cast<float *>(h->S);  // transformed in place; the next sweep A rewrites it
+    for (int r = 0; r < nreps && e == cudaSuccess; r++) {
+        for (int p = 0; p < 3 && e == cudaSuccess; p++) {
+            e = cudaEventRecord(ev[4 * r + p], h->stream);
+            if (e == cudaSuccess) e = fft3d_pass_f32(h->N, S, 2 * kSrc, p, h->stream);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(ev[4 * r + 3], h->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    double acc[3] = {0, 0, 0};
+    for (int r = 0; r < nreps && e == cudaSuccess; r++)
+        for (int p = 0; p < 3; p++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[4 * r + p], ev[4 * r + p + 1]);
+            acc[p] += ms;
+        }
+    for (auto &x : ev)
+        if (x) cudaEventDestroy(x);
+    CK(h, e);
+    for (int p = 0; p < 3; p++) ms_out[p] = acc[p] / nreps;
+    return GABE_OK;
 }
 
 int gabe_stream(gabe_handle *h, void **stream) {

@@ -37,35 +37,40 @@ cudaError_t fft3d_cols_n(float *S, int ncomp, cudaStream_t s) {
 }
 
 template <int N>
-cudaError_t fft3d_n(float *S, int ncomp, cudaStream_t s) {
-    constexpr long long nz = N / 2 + 1;
-    int g1 = 0, g2 = 0;
-    using RG = f3d::RowGeom<N>;
-    cudaError_t e = persistent_grid(f3d::row_r2c_kernel<N>, RG::T, RG::SMEM_BYTES, &g1);
-    if (e != cudaSuccess) return e;
-    e = persistent_grid(f3d::col_fft_kernel<N>, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, &g2);
-    if (e != cudaSuccess) return e;
-    // pass 1: rows along k
-    f3d::row_r2c_kernel<N><<<g1, RG::T, RG::SMEM_BYTES, s>>>(S, (long long)ncomp * N * N);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    float2 *X = reinterpret_cast<float2 *>(S);
-    // pass 2: along j within every (component, i) plane
-    f3d::ColArgs aj{X, (long long)N * nz, 0, nz, ncomp * N, 1, (int)nz};
-    f3d::col_fft_kernel<N><<<g2, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(aj);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // pass 3: along i for every (component, j)
-    f3d::ColArgs ai{X, (long long)N * N * nz, nz, (long long)N * nz, ncomp, N, (int)nz};
-    f3d::col_fft_kernel<N><<<g2, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(ai);
-    return cudaGetLastError();
-}
-
-template <int N>
 cudaError_t col_pass_n(const f3d::ColArgs &a, cudaStream_t s) {
     int g = 0;
     cudaError_t e = persistent_grid(f3d::col_fft_kernel<N>, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, &g);
     if (e != cudaSuccess) return e;
     f3d::col_fft_kernel<N><<<g, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(a);
     return cudaGetLastError();
+}
+
+// one pass of the 3-D r2c: 0 rows along k, 1 along j within every (component,
+// i) plane, 2 along i for every (component, j)
+template <int N>
+cudaError_t fft3d_pass_n(float *S, int ncomp, int pass, cudaStream_t s) {
+    constexpr long long nz = N / 2 + 1;
+    float2 *X = reinterpret_cast<float2 *>(S);
+    if (pass == 0) {
+        using RG = f3d::RowGeom<N>;
+        int g1 = 0;
+        cudaError_t e = persistent_grid(f3d::row_r2c_kernel<N>, RG::T, RG::SMEM_BYTES, &g1);
+        if (e != cudaSuccess) return e;
+        f3d::row_r2c_kernel<N><<<g1, RG::T, RG::SMEM_BYTES, s>>>(S, (long long)ncomp * N * N);
+        return cudaGetLastError();
+    }
+    if (pass == 1) return col_pass_n<N>(f3d::ColArgs{X, (long long)N * nz, 0, nz, ncomp * N, 1, (int)nz}, s);
+    if (pass == 2) return col_pass_n<N>(f3d::ColArgs{X, (long long)N * N * nz, nz, (long long)N * nz, ncomp, N, (int)nz}, s);
+    return cudaErrorInvalidValue;
+}
+
+template <int N>
+cudaError_t fft3d_n(float *S, int ncomp, cudaStream_t s) {
+    for (int pass = 0; pass < 3; pass++) {
+        const cudaError_t e = fft3d_pass_n<N>(S, ncomp, pass, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 template <int N, int MODE>
@@ -141,6 +146,16 @@ cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int 
         case 128: return plane_scatter_n<128>(S, send, nplanes, ranks, s);
         case 256: return plane_scatter_n<256>(S, send, nplanes, ranks, s);
         case 512: return plane_scatter_n<512>(S, send, nplanes, ranks, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t fft3d_pass_f32(int N, float *S, int ncomp, int pass, cudaStream_t s) {
+    switch (N) {
+        case 64: return fft3d_pass_n<64>(S, ncomp, pass, s);
+        case 128: return fft3d_pass_n<128>(S, ncomp, pass, s);
+        case 256: return fft3d_pass_n<256>(S, ncomp, pass, s);
+        case 512: return fft3d_pass_n<512>(S, ncomp, pass, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -55,11 +55,11 @@ __device__ __forceinline__ void twiddles(float2 *tw) {
 // (one four-step chunk) the pairs of reals are permuted by an XOR with the
 // chunk's index, so that the stride-L1 reads of the second four-step pass
 // fall on distinct banks while every pair stays 8-byte aligned.
-template <int N>
+template <int N, int R_ = 16, int NB_ = 2>
 struct RowGeom {
     using C_ = PlaneCfg<N>;
     static constexpr int L1 = C_::L1, L2 = C_::L2;
-    static constexpr int R = 16, P = R / 2, T = 128, NB = 2;  // rows per tile, pairs, threads, buffers
+    static constexpr int R = R_, P = R / 2, T = 128, NB = NB_;  // rows per tile, pairs, threads, buffers
     static constexpr int PITCH = N;                             // floats per shared row
     static constexpr int BUF = R * PITCH;                       // floats per tile buffer
     static constexpr int SMEM_FLOATS = NB * BUF + 2 * N;        // + twiddles
@@ -74,9 +74,13 @@ struct RowGeom {
     }
 };
 
-template <int N>
-__global__ void __launch_bounds__(RowGeom<N>::T, 3) row_r2c_kernel(float *S, long long nrows) {
-    using Gm = RowGeom<N>;
+// Two CTAs per SM at N = 512: without a third CTA's register cap (149) the
+// kernel keeps more of each FFT in flight (2.37 against 2.80 ms for ten
+// 512^3 arrays, measured on B200 across R = 4 .. 32, 2 .. 4 buffers and
+// 1 .. 8 CTAs per SM).
+template <int N, int R_ = 16, int NB_ = 2, int MINB = (N >= 512 ? 2 : 3)>
+__global__ void __launch_bounds__(RowGeom<N, R_, NB_>::T, MINB) row_r2c_kernel(float *S, long long nrows) {
+    using Gm = RowGeom<N, R_, NB_>;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2,
                   NB = Gm::NB;
     constexpr int RP = N + 2, NH = N / 2 + 1;
@@ -203,19 +207,19 @@ struct ColArgs {
 
 constexpr int kColInPlace = 0, kColGather = 1, kColScatter = 2;
 
-template <int N>
+template <int N, int T_ = kFftThreads>
 struct ColGeom {
     static constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2;
-    static constexpr int W = 16, T = kFftThreads;  // columns per tile
+    static constexpr int W = 16, T = T_;  // columns per tile, threads
     static constexpr int BUF = N * W;                // complex per tile buffer
     static constexpr int SMEM_C = kFftBufs * BUF + N;  // tile ring + twiddles (complex)
     static constexpr size_t SMEM_BYTES = (size_t)SMEM_C * sizeof(float2);
     static constexpr size_t SMEM_BYTES_SLAB = SMEM_BYTES + 2 * N * sizeof(long long);  // + per-index offsets
 };
 
-template <int N, int MODE = kColInPlace>
-__global__ void __launch_bounds__(kFftThreads, 1) col_fft_kernel(ColArgs a) {
-    using Gm = ColGeom<N>;
+template <int N, int MODE = kColInPlace, int T_ = kFftThreads>
+__global__ void __launch_bounds__(T_, 1) col_fft_kernel(ColArgs a) {
+    using Gm = ColGeom<N, T_>;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, W = Gm::W, T = Gm::T;
     extern __shared__ __align__(16) float2 cs[];
     float2 *tw = cs + kFftBufs * Gm::BUF;  // [k2][n1]

@@ -156,6 +156,8 @@ cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out
 // FP32 in-place 3-D r2c of ncomp arrays [N][N][N+2] in three passes (fft3d.cuh).
 bool fft3d_supported(int N);
 cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s);
+// One of its passes: 0 rows along k, 1 along j, 2 along i.
+cudaError_t fft3d_pass_f32(int N, float *S, int ncomp, int pass, cudaStream_t s);
 // One column pass (fft3d.cuh col_fft_kernel): for b1 < n1, b2 < n2, c < ncol the N complex
 // values at X + b1 s1 + b2 s2 + n sn + c.
 cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long long sn, int n1, int n2, int ncol,

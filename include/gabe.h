@@ -78,12 +78,17 @@ enum gabe_flags {
                                    of cuFFT's batched 2-D plan */
     GABE_FLAG_OWN_FFT = 16,     /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
                                    library's three-pass 3-D r2c instead of cuFFT's 3-D plan (no cuFFT
-                                   call on the step path; about 1% slower than cuFFT at 512^3 on B200) */
-    GABE_FLAG_FUSED_ROWS = 32   /* FP32 with N in {64, 128, 256, 512}: sweep A writes the GW sources already
+                                   call on the step path).  The default for FP32 at N = 512, where it
+                                   is about 4% faster than cuFFT's plan on B200 (7.97 against 8.30 ms
+                                   for the ten transforms of a step) */
+    GABE_FLAG_FUSED_ROWS = 32,  /* FP32 with N in {64, 128, 256, 512}: sweep A writes the GW sources already
                                    transformed along k (one block per pair of whole rows), and the
                                    transforms along j and i are the library's column passes (one HBM
                                    pass fewer, but about 8% slower per step at 512^3 on B200: one
                                    block per SM, whose transform phases leave most warps idle) */
+    GABE_FLAG_CUFFT_3D = 64     /* FP32 at N = 512: cuFFT's 3-D plan for the GW sources instead of the
+                                   library's three-pass r2c (cuFFT's plan is the default at every other
+                                   size and precision) */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two
@@ -137,6 +142,14 @@ int gabe_step(gabe_handle *h, int nsteps);
  * k-space update, stage-2 sweep} (FFT and k-space are 0 without GWs).  The
  * state advances by nsteps.  Measurement hook; no reference counterpart. */
 int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]);
+
+/* For a handle whose GW sources go through the library's 3-D FFT (FP32 at
+ * N = 512 by default, or GABE_FLAG_OWN_FFT): runs its three passes nreps
+ * times on the source buffer (in place; the next step rewrites the
+ * sources) with CUDA events between them and returns the mean milliseconds
+ * of {rows along k, pass along j, pass along i}.  Measurement hook; no
+ * reference counterpart. */
+int gabe_profile_fft_passes(gabe_handle *h, int nreps, double ms_out[3]);
 
 /* The handle's CUDA stream (a cudaStream_t), so callers can order their own
  * work or events after queued steps.  No reference counterpart. */

@@ -1,12 +1,12 @@
 """FP32 GW-source transforms and the fused k-space update against cuFFT's 3-D
 plan with the separate k-space pass.
 
-By default the library keeps the reference's structure -- one 3-D r2c per
-source array (fft_stresstensor, g2evolutionpert.cpp:183-195, here cuFFT's 3-D
-plan) and a separate k-space pass (TT projection + both RK2 stages of h, l);
-that is the reference form of the comparisons below.  With FP32 storage and N
-in {64, 128, 256, 512}: GABE_FLAG_OWN_FFT does the 3-D r2c with the library's
-own three-pass FFT; GABE_FLAG_FUSED_ROWS has sweep A write the sources already
+The reference form of the comparisons below keeps the reference's structure
+-- one 3-D r2c per source array (fft_stresstensor, g2evolutionpert.cpp:183-
+195, here cuFFT's 3-D plan: the default below N = 512, GABE_FLAG_CUFFT_3D at
+512) and a separate k-space pass (TT projection + both RK2 stages of h, l).
+With FP32 storage and N in {64, 128, 256, 512}: GABE_FLAG_OWN_FFT does the
+3-D r2c with the library's own three-pass FFT (the default at 512); GABE_FLAG_FUSED_ROWS has sweep A write the sources already
 transformed along k (whole rows per block) and runs the library's passes along
 j and i; GABE_FLAG_FUSED_KSPACE transforms the ten source arrays
 over each (j, k) plane only (cuFFT's batched 2-D plan, or with
@@ -29,7 +29,7 @@ FFT_TOL = 1e-5  # relative, FP32 transforms of ~1e5..1e8 terms
 FORMS = {"own": gb.FLAG_OWN_FFT, "fused": gb.FLAG_FUSED_KSPACE, "plane": gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT,
          "rows": gb.FLAG_FUSED_ROWS}
 LAUNCHES = {gb.FLAG_OWN_FFT: 6, gb.FLAG_FUSED_KSPACE: 3, gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT: 4,
-            gb.FLAG_FUSED_ROWS: 5, 0: 3}
+            gb.FLAG_FUSED_ROWS: 5, gb.FLAG_CUFFT_3D: 3, 0: 3}
 
 
 def _norm_rel(got, want):
@@ -63,7 +63,7 @@ def _run(N, flags, state, steps):
 def test_gw_transform_forms_match_cufft_3d(N, form):
     st = _state(N)
     (f0, d0, h0, l0), s0 = _run(N, FORMS[form], st, 3)
-    (f1, d1, h1, l1), s1 = _run(N, 0, st, 3)
+    (f1, d1, h1, l1), s1 = _run(N, gb.FLAG_CUFFT_3D, st, 3)
     if form == "rows":
         # its sweep A sums the energies over other blocks: a and adot may differ in the last
         # bits, and the FP32 fluctuations with them by a rounding unit
@@ -100,12 +100,16 @@ def test_gw_transforms_512_match_cufft_3d():
     N = 512
     f, d, a0, ad0 = _state(N, seed=3)
     specs = {}
-    for name, flags in [*FORMS.items(), ("3d", 0)]:
+    for name, flags in [*FORMS.items(), ("3d", gb.FLAG_CUFFT_3D), ("default", 0)]:
         with gb.Lattice(N, gws=True, precision=gb.FP32, flags=flags) as lat:
+            if name == "default":
+                assert lat.launches_per_step == LAUNCHES[gb.FLAG_OWN_FFT]  # the library's FFT at 512
             lat.upload_state(f, d, a0=a0, adot0=ad0)
             lat.step(2)
             specs[name] = lat.spec_out()
     assert np.abs(specs["3d"][:, 5]).max() > 0
+    # same kernels; the binning's FP64 shared-memory sums vary in the last bit
+    np.testing.assert_allclose(specs["default"], specs["own"], rtol=1e-12, atol=0)
     for name in FORMS:
         assert np.all(np.isfinite(specs[name]))
         assert _gw_cols_close(specs[name], specs["3d"]) <= FFT_TOL, name
