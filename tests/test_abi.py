@@ -65,6 +65,38 @@ def test_null_handles_are_errors_not_crashes():
     assert lib.gabe_destroy(None) == 0
     assert lib.gabe_step(None, 1) == 1
     assert lib.gabe_sync(None) == 1
+    out = (ctypes.c_double * 4)()
+    assert lib.gabe_profile_steps(None, 1, out) == 1
+    assert lib.gabe_profile_fft_passes(None, 1, out) == 1
+
+
+def test_bench_counts_each_fft_pass_and_the_step_once():
+    """bench.py's byte model: each pass of the library's FFT reads and
+    writes its ten arrays once; the step's algorithmic bytes hold the
+    transforms once -- in FP32 with GWs 56 (sweep A) + 32 (sweep B) +
+    4 x 10 (1 + 2M/N^3) (one transform pass) + 4 x 36 M/N^3 (k-space) B per
+    site-update, about 240 B for the device's five traceless components
+    and four TT amplitudes (the reference's formulation, 336 B, is reported
+    separately) -- and ncu traffic of the column passes scales with the
+    k-points."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    N, w = 512, 4
+    n3, M = N ** 3, N * N * (N // 2 + 1)
+    b = bench.algorithmic_bytes(N, w, True)
+    assert b["fft_rows"] == b["fft"] == 10 * (n3 + 2 * M) * w
+    assert b["fft_j"] == b["fft_i"] == 10 * 4 * M * w
+    step = sum(v for k, v in b.items() if k not in ("fft_rows", "fft_j", "fft_i"))
+    assert step == (56 + 32) * n3 + 40 * (n3 + 2 * M) + 144 * M
+    assert abs(step / n3 - 240.4) < 0.1
+    assert bench.reference_formulation_bytes(w, True) == 336
+    assert set(bench.algorithmic_bytes(N, w, False)) == {"stage1", "stage2"}
+    t256 = bench.traffic_scaled("fft_i", "fp32", 256)
+    t512 = bench.traffic_scaled("fft_i", "fp32", 512)
+    assert t256 and abs(t512 / t256 - M / (256 * 256 * 129)) < 1e-12
 
 
 def test_oracle_library_loads():
