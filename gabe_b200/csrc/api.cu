@@ -181,7 +181,11 @@ int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
     return GABE_OK;
 }
 
-bool overlapped(const gabe_handle *h) { return h->evolve_gw && h->S2 != nullptr; }
+// The GW chain of step n overlaps the field sweeps of step n+1 (two source
+// buffers) -- except with the library's FFT, which runs in line (measured
+// faster at 512^3) and uses the second buffer as its column passes' target.
+bool overlapped(const gabe_handle *h) { return h->evolve_gw && h->S2 != nullptr && !h->own_fft; }
+float *fft_scratch(const gabe_handle *h) { return h->own_fft ? static_cast<float *>(h->S2) : nullptr; }
 void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
 
 // In-place transforms of the 2*kSrc source arrays in source buffer `slot`
@@ -195,7 +199,7 @@ int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
         return GABE_OK;
     }
     if (h->own_fft) {
-        CK(h, fft3d_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc, s));
+        CK(h, fft3d_r2c_f32(h->N, static_cast<float *>(S), fft_scratch(h), 2 * kSrc, s));
         return GABE_OK;
     }
     if (h->rows_fused) {  // the pass along k was taken by sweep A
@@ -702,7 +706,7 @@ int gabe_profile_fft_passes(gabe_handle *h, int nreps, double ms_out[3]) {
     for (int r = 0; r < nreps && e == cudaSuccess; r++) {
         for (int p = 0; p < 3 && e == cudaSuccess; p++) {
             e = cudaEventRecord(ev[4 * r + p], h->stream);
-            if (e == cudaSuccess) e = fft3d_pass_f32(h->N, S, 2 * kSrc, p, h->stream);
+            if (e == cudaSuccess) e = fft3d_pass_f32(h->N, S, fft_scratch(h), 2 * kSrc, p, h->stream);
         }
         if (e == cudaSuccess) e = cudaEventRecord(ev[4 * r + 3], h->stream);
     }

@@ -45,12 +45,32 @@ cudaError_t col_pass_n(const f3d::ColArgs &a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// one pass of the 3-D r2c: 0 rows along k, 1 along j within every (component,
-// i) plane, 2 along i for every (component, j)
 template <int N>
-cudaError_t fft3d_pass_n(float *S, int ncomp, int pass, cudaStream_t s) {
+cudaError_t col_oop_n(const f3d::ColArgs &a, cudaStream_t s) {
+    int g = 0;
+    constexpr size_t smem = f3d::ColGeom<N>::SMEM_BYTES;
+    cudaError_t e = persistent_grid(f3d::col_fft_kernel<N, f3d::kColOutOfPlace>, f3d::kFftThreads, smem, &g);
+    if (e != cudaSuccess) return e;
+    f3d::col_fft_kernel<N, f3d::kColOutOfPlace><<<g, f3d::kFftThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// one pass of the 3-D r2c: 0 rows along k, 1 along j within every (component,
+// i) plane, 2 along i for every (component, j).  With a scratch array T of
+// S's size the passes along j and i run out of place (S -> T, then T -> S):
+// on B200 a column pass that writes another array than it reads is faster.
+template <int N>
+cudaError_t fft3d_pass_n(float *S, float *T, int ncomp, int pass, cudaStream_t s) {
     constexpr long long nz = N / 2 + 1;
     float2 *X = reinterpret_cast<float2 *>(S);
+    if (T && pass > 0) {
+        float2 *Y = reinterpret_cast<float2 *>(T);
+        f3d::ColArgs a = pass == 1 ? f3d::ColArgs{Y, (long long)N * nz, 0, nz, ncomp * N, 1, (int)nz}
+                                   : f3d::ColArgs{X, (long long)N * N * nz, nz, (long long)N * nz, ncomp, N, (int)nz};
+        a.src = pass == 1 ? X : Y;
+        if (pass > 2) return cudaErrorInvalidValue;
+        return col_oop_n<N>(a, s);
+    }
     if (pass == 0) {
         using RG = f3d::RowGeom<N>;
         int g1 = 0;
@@ -65,9 +85,9 @@ cudaError_t fft3d_pass_n(float *S, int ncomp, int pass, cudaStream_t s) {
 }
 
 template <int N>
-cudaError_t fft3d_n(float *S, int ncomp, cudaStream_t s) {
+cudaError_t fft3d_n(float *S, float *T, int ncomp, cudaStream_t s) {
     for (int pass = 0; pass < 3; pass++) {
-        const cudaError_t e = fft3d_pass_n<N>(S, ncomp, pass, s);
+        const cudaError_t e = fft3d_pass_n<N>(S, T, ncomp, pass, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -150,22 +170,22 @@ cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int 
     }
 }
 
-cudaError_t fft3d_pass_f32(int N, float *S, int ncomp, int pass, cudaStream_t s) {
+cudaError_t fft3d_pass_f32(int N, float *S, float *T, int ncomp, int pass, cudaStream_t s) {
     switch (N) {
-        case 64: return fft3d_pass_n<64>(S, ncomp, pass, s);
-        case 128: return fft3d_pass_n<128>(S, ncomp, pass, s);
-        case 256: return fft3d_pass_n<256>(S, ncomp, pass, s);
-        case 512: return fft3d_pass_n<512>(S, ncomp, pass, s);
+        case 64: return fft3d_pass_n<64>(S, T, ncomp, pass, s);
+        case 128: return fft3d_pass_n<128>(S, T, ncomp, pass, s);
+        case 256: return fft3d_pass_n<256>(S, T, ncomp, pass, s);
+        case 512: return fft3d_pass_n<512>(S, T, ncomp, pass, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
-cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s) {
+cudaError_t fft3d_r2c_f32(int N, float *S, float *T, int ncomp, cudaStream_t s) {
     switch (N) {
-        case 64: return fft3d_n<64>(S, ncomp, s);
-        case 128: return fft3d_n<128>(S, ncomp, s);
-        case 256: return fft3d_n<256>(S, ncomp, s);
-        case 512: return fft3d_n<512>(S, ncomp, s);
+        case 64: return fft3d_n<64>(S, T, ncomp, s);
+        case 128: return fft3d_n<128>(S, T, ncomp, s);
+        case 256: return fft3d_n<256>(S, T, ncomp, s);
+        case 512: return fft3d_n<512>(S, T, ncomp, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -200,12 +200,14 @@ struct ColArgs {
     // output value n of line b1 written to the send buffer of the transpose,
     // blocks by destination rank of [n1][n(r)][ncol], at
     // dst + (n1 p0(r) + n - p0(r) + b1 n(r)) ncol.
+    // out of place (kColOutOfPlace): the lines are read from src with X's
+    // layout and written to X.
     const float2 *src = nullptr;
     float2 *dst = nullptr;
     int ranks = 0;
 };
 
-constexpr int kColInPlace = 0, kColGather = 1, kColScatter = 2;
+constexpr int kColInPlace = 0, kColGather = 1, kColScatter = 2, kColOutOfPlace = 3;
 
 template <int N, int T_ = kFftThreads>
 struct ColGeom {
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(T_, 1) col_fft_kernel(ColArgs a) {
     long long *goff = reinterpret_cast<long long *>(tw + N), *gq = goff + N;
     const int tid = threadIdx.x;
     twiddles<N>(tw);
-    if constexpr (MODE != kColInPlace) {
+    if constexpr (MODE == kColGather || MODE == kColScatter) {
         const Split sp(N, a.ranks);
         const long long unit = MODE == kColGather ? a.sn : (long long)a.ncol;
         for (int n = tid; n < N; n += T) {
@@ -260,9 +262,10 @@ __global__ void __launch_bounds__(T_, 1) col_fft_kernel(ColArgs a) {
                 if (w < wn) s32::cp_async8(col + t, g + goff[n] + b1 * gq[n] + w);
             }
         } else {
+            const float2 *rb = MODE == kColOutOfPlace ? a.src + (base - a.X) : base;
             for (int t = tid; t < N * W; t += T) {
                 const int n = t / W, w = t % W;
-                if (w < wn) s32::cp_async8(col + t, base + n * a.sn + w);
+                if (w < wn) s32::cp_async8(col + t, rb + n * a.sn + w);
             }
         }
     };

@@ -153,11 +153,12 @@ cudaError_t mean_f64(const double *x, size_t n, double *partials, unsigned int *
 cudaError_t to_fluct(const double *x, size_t n, const double *mean, float *out, cudaStream_t s);
 cudaError_t from_fluct(const float *x, size_t n, const double *mean, double *out, cudaStream_t s);
 
-// FP32 in-place 3-D r2c of ncomp arrays [N][N][N+2] in three passes (fft3d.cuh).
+// FP32 3-D r2c of ncomp arrays [N][N][N+2] in three passes (fft3d.cuh), result in S;
+// T (S's size, or null for in place) is the target of the pass along j, read by the pass along i.
 bool fft3d_supported(int N);
-cudaError_t fft3d_r2c_f32(int N, float *S, int ncomp, cudaStream_t s);
+cudaError_t fft3d_r2c_f32(int N, float *S, float *T, int ncomp, cudaStream_t s);
 // One of its passes: 0 rows along k, 1 along j, 2 along i.
-cudaError_t fft3d_pass_f32(int N, float *S, int ncomp, int pass, cudaStream_t s);
+cudaError_t fft3d_pass_f32(int N, float *S, float *T, int ncomp, int pass, cudaStream_t s);
 // One column pass (fft3d.cuh col_fft_kernel): for b1 < n1, b2 < n2, c < ncol the N complex
 // values at X + b1 s1 + b2 s2 + n sn + c.
 cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long long sn, int n1, int n2, int ncol,

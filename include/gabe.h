@@ -67,7 +67,9 @@ enum gabe_flags {
     GABE_FLAG_NO_GRAPH = 1,  /* launch kernels one by one instead of replaying a CUDA graph */
     GABE_FLAG_NO_OVERLAP = 2, /* one source buffer: the GW transforms and k-space update run in line
                                  instead of overlapping the next field sweeps (saves 10 N^2(N+2)
-                                 words of device memory) */
+                                 words of device memory).  With the library's 3-D FFT the chain runs
+                                 in line anyway and the second buffer is the target of its column
+                                 passes (out of place, faster); this flag makes them in place */
     GABE_FLAG_FUSED_KSPACE = 8, /* FP32 with N in {64, 128, 256, 512}: transform the GW sources over each
                                    (j, k) plane only and do the FFT along i inside the k-space update,
                                    instead of a full 3-D transform followed by the k-space pass (the
