@@ -47,12 +47,12 @@ struct gabe_slab {
     void *send[2] = {nullptr, nullptr}, *recv[2] = {nullptr, nullptr};  // [lo, hi]: 4 planes each
     int shape = 0, ci = 1;
     dim3 grid;
-    // GW branch (FP32): the ranks' split, sources [10][nloc][N][N+2] (2-D transformed in place,
-    // then the all-to-all receive buffer), the send buffer (then T[10][N][m][nz]), amplitudes
+    // GW branch: the ranks' split, sources [10][nloc][N][N+2] (the all-to-all receive buffer
+    // after the 2-D transforms), the send buffer (then T[10][N][m][nz]), amplitudes
     // [4][N][m][nz] of this rank's ky columns [plane0, plane0 + nloc)
-    bool gws = false, spec = false;  // spec: the spectra transpose (FP32, N in {64, ..., 512})
+    bool gws = false, spec = false;  // spec: the spectra transpose (FP64, or FP32 with N in {64, ..., 512})
     int W = 1, rank = 0, nbins = 0;
-    cufftHandle plan_spec = 0;
+    cufftHandle plan_spec = 0;  // FP64: 2-D D2Z of the two fields' planes
     bool have_plan_spec = false;
     double *bin_part = nullptr, *bin_sum = nullptr;
     unsigned int *bin_cnt_part = nullptr;
@@ -62,7 +62,7 @@ struct gabe_slab {
     size_t csz = 8;               // bytes of one complex value (FP32 8, FP64 16)
     cufftHandle plan_i = 0;       // FP64: the pass along i (strided Z2Z, one component per call)
     bool have_plan_i = false;
-    cufftHandle plan2d = 0;
+    cufftHandle plan2d = 0;  // FP64: 2-D D2Z of the source planes (FP32 uses the library's passes)
     bool have_plan = false;
     std::string err;
 };
