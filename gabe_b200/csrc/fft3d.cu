@@ -62,13 +62,13 @@ cudaError_t col_oop_n(const f3d::ColArgs &a, cudaStream_t s) {
 template <int N>
 cudaError_t fft3d_pass_n(float *S, float *T, int ncomp, int pass, cudaStream_t s) {
     constexpr long long nz = N / 2 + 1;
+    if (pass < 0 || pass > 2) return cudaErrorInvalidValue;
     float2 *X = reinterpret_cast<float2 *>(S);
     if (T && pass > 0) {
         float2 *Y = reinterpret_cast<float2 *>(T);
         f3d::ColArgs a = pass == 1 ? f3d::ColArgs{Y, (long long)N * nz, 0, nz, ncomp * N, 1, (int)nz}
                                    : f3d::ColArgs{X, (long long)N * N * nz, nz, (long long)N * nz, ncomp, N, (int)nz};
         a.src = pass == 1 ? X : Y;
-        if (pass > 2) return cudaErrorInvalidValue;
         return col_oop_n<N>(a, s);
     }
     if (pass == 0) {
