@@ -52,6 +52,7 @@ def parse():
                     help="gabe_params.flags of the lattices (e.g. 16: GABE_FLAG_OWN_FFT, 8: GABE_FLAG_FUSED_KSPACE)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-slab", action="store_true", help="skip the slab leg (one lattice split over the ranks)")
+    ap.add_argument("--no-energy", action="store_true", help="skip the energy-conservation block (64^3, rank 0)")
     ap.add_argument("--slab-N", type=int, default=512, help="lattice of the slab leg")
     ap.add_argument("--slab-steps", type=int, default=20)
     ap.add_argument("--ens-lattices", type=int, default=256)
@@ -357,6 +358,37 @@ def run_reference_arm(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+def energy_conservation(N: int = 64, steps: int = 500, dt: float = 0.01, device: int = 0) -> dict:
+    """Energy-conservation error (gabe_b200.energy: the continuity residual
+    eps(t) of the per-step scalars) of an FP64 and an FP32 run of one lattice
+    from the same initial state, GWs on, at a size where dt = 0.01 is inside
+    RK2's stability region (64^3: dt sqrt(12)/dx = 0.11)."""
+    import numpy as np
+
+    import gabe_b200 as gb
+    from gabe_b200 import energy
+    from gabe_b200.ic import random_state
+
+    f, d, a0, ad0 = random_state(N, seed=5, device="cuda")
+    f, d = f.cpu().numpy(), d.cpu().numpy()
+    eps = {}
+    for name, prec in (("fp64", gb.FP64), ("fp32", gb.FP32)):
+        with gb.Lattice(N, gws=True, precision=prec, device=device, dt=dt) as lat:
+            lat.upload_state(f, d, a0=a0, adot0=ad0)
+            rows = []
+            for n in range(steps + 1):
+                if n:
+                    lat.step(1)
+                e = lat.calc_energy()
+                rows.append((n * dt, e["a"], e["adot"], e["kin"], e["pot"], e["grad"], e["rho"]))
+        r = np.array(rows)
+        eps[name] = energy.continuity_residual(*(r[:, c] for c in range(7)))
+    return {"workload": f"{N}^3 lattice, GWs on, dt={dt}, {steps} steps, one initial state for both precisions",
+            "measure": "eps(t) = |rho(t) - rho(0) + int 3H(rho + p) dt| / rho(t), p = kin - grad/3 - pot",
+            "eps_fp64": float(eps["fp64"][-1]), "eps_fp32": float(eps["fp32"][-1]),
+            "max_abs_diff_fp32_vs_fp64": float(np.abs(eps["fp32"] - eps["fp64"]).max())}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -531,6 +563,11 @@ def main():
             line["slab"] = slab_leg(args, rank, world, local, dist, barrier, max_over_ranks)
         except Exception as e:  # noqa: BLE001 -- the headline line is still printed
             line["slab"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    if rank == 0 and not args.no_energy:
+        try:
+            line["energy_conservation"] = energy_conservation(device=local)
+        except Exception as e:  # noqa: BLE001 -- the headline line is still printed
+            line["energy_conservation"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         v, info = cpu_reference_sample(args.ref_N, 2, warm=1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
