@@ -371,7 +371,7 @@ def energy_conservation(N: int = 64, steps: int = 500, dt: float = 0.01, device:
 
     f, d, a0, ad0 = random_state(N, seed=5, device="cuda")
     f, d = f.cpu().numpy(), d.cpu().numpy()
-    eps = {}
+    eps, spec = {}, {}
     for name, prec in (("fp64", gb.FP64), ("fp32", gb.FP32)):
         with gb.Lattice(N, gws=True, precision=prec, device=device, dt=dt) as lat:
             lat.upload_state(f, d, a0=a0, adot0=ad0)
@@ -381,12 +381,20 @@ def energy_conservation(N: int = 64, steps: int = 500, dt: float = 0.01, device:
                     lat.step(1)
                 e = lat.calc_energy()
                 rows.append((n * dt, e["a"], e["adot"], e["kin"], e["pot"], e["grad"], e["rho"]))
+            spec[name] = lat.spec_out()
         r = np.array(rows)
         eps[name] = energy.continuity_residual(*(r[:, c] for c in range(7)))
+
+    def max_rel(cols):  # per-bin relative difference above each column's FFT noise floor
+        w, g = spec["fp64"][:, cols], spec["fp32"][:, cols]
+        floor = 1e-9 * np.abs(w).max(axis=0, keepdims=True)
+        return float(((np.abs(g - w) - floor).clip(min=0) / np.abs(w).clip(min=1e-300)).max())
+
     return {"workload": f"{N}^3 lattice, GWs on, dt={dt}, {steps} steps, one initial state for both precisions",
             "measure": "eps(t) = |rho(t) - rho(0) + int 3H(rho + p) dt| / rho(t), p = kin - grad/3 - pot",
             "eps_fp64": float(eps["fp64"][-1]), "eps_fp32": float(eps["fp32"][-1]),
-            "max_abs_diff_fp32_vs_fp64": float(np.abs(eps["fp32"] - eps["fp64"]).max())}
+            "max_abs_diff_fp32_vs_fp64": float(np.abs(eps["fp32"] - eps["fp64"]).max()),
+            "spectra_max_rel_diff_fp32_vs_fp64": {"fields": max_rel([1, 2, 3, 4]), "gw": max_rel([5, 6])}}
 
 
 def main():
