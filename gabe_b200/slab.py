@@ -236,6 +236,14 @@ def _on_slab_stream(s):
     return contextlib.nullcontext()
 
 
+def _sync_devices(slabs):
+    """Wait for the copies between slabs (CUDA); CPU stand-ins need nothing."""
+    if slabs[0].tensor("sums").is_cuda:
+        import torch
+
+        torch.cuda.synchronize()
+
+
 class LocalComm:
     """Every slab of the lattice in this process (one GPU or several):
     sums added on the host in rank order, halos copied device to device.
@@ -259,7 +267,7 @@ class LocalComm:
         t = torch.from_numpy(tot)
         for v in views:
             v.copy_(t)
-        torch.cuda.synchronize()
+        _sync_devices(slabs)
 
     def exchange(self, slabs):
         import torch
@@ -276,7 +284,7 @@ class LocalComm:
         for r, s in enumerate(slabs):
             s.tensor("recv_lo").copy_(slabs[(r - 1) % W].tensor("send_hi"))
             s.tensor("recv_hi").copy_(slabs[(r + 1) % W].tensor("send_lo"))
-        torch.cuda.synchronize()
+        _sync_devices(slabs)
 
     def all_to_all(self, slabs, kind: str = "gw"):
         """Transpose (kind "gw": the sources, "spec": the two fields): block r'
@@ -298,7 +306,7 @@ class LocalComm:
                 rcv = slabs[dst].tensor(f"{kind}_recv")
                 roff = np.cumsum([0] + [b // 4 for b in getattr(slabs[dst], f"{kind}_recv_bytes")])
                 rcv[roff[src]:roff[src + 1]].copy_(snd[soff[dst]:soff[dst + 1]])
-        torch.cuda.synchronize()
+        _sync_devices(slabs)
 
     def allreduce_host(self, v: np.ndarray) -> np.ndarray:
         return v

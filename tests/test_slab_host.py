@@ -189,6 +189,41 @@ def test_slab_protocol_over_gloo_ranks(world):
     assert all(q.get(timeout=5) for _ in range(world))
 
 
+@pytest.mark.parametrize("gws", [False, True])
+def test_local_comm_protocol_with_three_slabs(gws):
+    """All slabs in one process (LocalComm): every stage runs on every slab
+    before the exchange that follows it, each slab finishes with the sum of
+    all slabs' sums, the ring and the transpose land as over gloo."""
+    world, log, made = 3, [], []
+
+    def factory(p0, n):
+        s = FakeSlab(len(made), p0, n, log)
+        if gws:
+            s.gw_setup(world)
+        made.append(s)
+        return s
+
+    lat = gs.SlabLattice(24, gs.LocalComm(world), precision=gb.FP32, gws=gws, slab_factory=factory)
+    assert lat.parts == gs.split_planes(24, world)
+    lat.step(1)
+    each = lambda *ev: [ev] * world  # noqa: E731
+    want = each("sweep", 0) + each("finish", 0)
+    if gws:
+        want += each("gw_transform") + each("gw_update")
+    want += each("sweep", 1) + each("pack") + each("unpack")
+    assert log == want
+    tot = sum(torch.arange(gs.KNV, dtype=torch.float64) + 10.0 * (r + 1) for r in range(world))
+    for rank, s in enumerate(made):
+        assert [torch.equal(t, tot) for t in s.finished] == [True]
+        lo, hi = (rank - 1) % world, (rank + 1) % world
+        assert bool((s.tensor("recv_lo") == 10 * lo + 2).all()) and bool((s.tensor("recv_hi") == 10 * hi + 1).all())
+        if gws:
+            recv, off = s.tensor("gw_recv"), 0
+            for r, b in enumerate(s.gw_recv_bytes):
+                assert bool((recv[off:off + b // 4] == 100.0 * r + rank).all())
+                off += b // 4
+
+
 def _gw_worker(rank, world, port, N, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
