@@ -68,6 +68,26 @@ def test_slab_create_rejects_bad_params(case):
         assert b"share" in msg
 
 
+@pytest.mark.parametrize("N,world,rank", [(48, 3, 1), (64, 2, 0), (80, 5, 4)])
+def test_fp64_slabs_with_gws_pass_the_parameter_checks(N, world, rank):
+    """FP64 slabs take GWs and spectra at any N that is a multiple of 16 (the
+    pass along i is a cuFFT plan): with a rank's standard share the checks
+    pass and creation goes on to the device (none here: a CUDA error, not a
+    parameter error)."""
+    lib = gs._lib()
+    p = gb.Params()
+    lib.gabe_default_params(ctypes.byref(p), N)
+    p.gws_on, p.precision = 1, gb.FP64
+    p0, n = gs.split_planes(N, world)[rank]
+    sp = gs.SlabParams(ctypes.sizeof(gs.SlabParams), p0, n, world)
+    h = ctypes.c_void_p()
+    rc = lib.gabe_slab_create(ctypes.byref(p), ctypes.byref(sp), ctypes.byref(h))
+    if rc == 0:  # a machine with a GPU
+        assert lib.gabe_slab_destroy(h) == 0
+    else:
+        assert rc != 1 and not h.value, lib.gabe_slab_last_error(None)
+
+
 class FakeSlab:
     """Stands in for gs.Slab: CPU tensors for the sums and boundary planes,
     and a log of the stage calls.  Its 'sweeps' put rank-dependent values in
