@@ -37,6 +37,17 @@ def test_library_exports_every_declared_symbol():
         getattr(lib, n)
 
 
+def test_python_constants_match_the_header_enums():
+    """Every GABE_FLAG_*, GABE_FP* and GABE_MODEL_* value of include/gabe.h
+    has the same value in gabe_b200 (FLAG_*, FP*, MODEL_*)."""
+    src = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "gabe.h")).read(), flags=re.S)
+    enums = dict((m.group(1), int(m.group(2))) for m in re.finditer(r"\bGABE_((?:FLAG|MODEL)_\w+|FP32|FP64)\s*=\s*(\d+)",
+                                                                     src))
+    assert {"FLAG_OWN_FFT", "FLAG_CUFFT_3D", "FP32", "MODEL_LPHI4"} <= set(enums)
+    for name, value in enums.items():
+        assert getattr(gb, name) == value, name
+
+
 def test_params_struct_matches_header():
     lib = gb.library()
     p = gb.Params()
