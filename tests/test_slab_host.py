@@ -88,6 +88,32 @@ def test_fp64_slabs_with_gws_pass_the_parameter_checks(N, world, rank):
         assert rc != 1 and not h.value, lib.gabe_slab_last_error(None)
 
 
+def test_c_and_python_plane_splits_agree():
+    """gabe_slab_create checks a rank's planes against the C split
+    (slabsplit.h) before any CUDA call; gabe_b200.slab.split_planes is the
+    Python one.  Every Python share passes that check, and a share moved by
+    one plane does not."""
+    lib = gs._lib()
+    for N in (16, 48, 80, 112):
+        for world in range(1, 8):
+            for rank, (p0, n) in enumerate(gs.split_planes(N, world)):
+                p = gb.Params()
+                lib.gabe_default_params(ctypes.byref(p), N)
+                # shares hold >= 2 planes here, so a share moved by one is never another rank's
+                for q0, m, ok in ((p0, n, True), (p0 + 1, n, False)):
+                    if q0 + m > N:
+                        continue
+                    sp = gs.SlabParams(ctypes.sizeof(gs.SlabParams), q0, m, world)
+                    h = ctypes.c_void_p()
+                    rc = lib.gabe_slab_create(ctypes.byref(p), ctypes.byref(sp), ctypes.byref(h))
+                    if h.value:
+                        lib.gabe_slab_destroy(h)
+                    if ok:
+                        assert rc != 1, (N, world, rank, lib.gabe_slab_last_error(None))
+                    else:
+                        assert rc == 1 and b"share" in lib.gabe_slab_last_error(None), (N, world, rank, q0, m)
+
+
 class FakeSlab:
     """Stands in for gs.Slab: CPU tensors for the sums and boundary planes,
     and a log of the stage calls.  Its 'sweeps' put rank-dependent values in
