@@ -6,6 +6,7 @@ import glob
 import os
 import re
 import subprocess
+import sys
 
 import pytest
 
@@ -113,3 +114,23 @@ def test_bench_counts_each_fft_pass_and_the_step_once():
 def test_oracle_library_loads():
     from oracle import pyoracle as po
     assert po.numbins(64) == 56
+
+
+def test_bench_reference_arm_line():
+    """bench.py --impl reference: the reference's own step() (or the oracle
+    port when its binary is not built) prints one JSON line with the arm's
+    contract keys on rank 0; other ranks print nothing and exit 0."""
+    import json as _json
+
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "0",
+           "--ref-N", "128"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = _json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unit"] == "site-updates/s" and line["value"] > 0
+    assert line["higher_is_better"] is True and line["metric"].startswith("site-updates/s")
+    assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2")
+    other = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
+    assert other.returncode == 0 and not other.stdout.strip()
