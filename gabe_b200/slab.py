@@ -2,11 +2,16 @@
 
 The reference evolves one lattice in one process.  A lattice that does not
 fit one GPU is split here into slabs, one per rank (one GPU each).  A step is
-the whole-lattice step of the reference (step(), g2functions.cpp:234-271,
-fields only) with two exchanges between the ranks:
+the whole-lattice step of the reference (step(), g2functions.cpp:234-271)
+with two exchanges between the ranks, and a third with GWs:
 
   sweep A on every slab -> all-reduce of the 8 FP64 stage sums ->
-  finish (adot0, a[1], adot[1]) -> sweep B -> boundary-plane exchange.
+  finish (adot0, a[1], adot[1]) -> [GWs: 2-D transforms of the own source
+  planes into per-rank blocks -> all-to-all -> pass along i and the h/l
+  update of the rank's ky columns] -> sweep B -> boundary-plane exchange.
+
+The spectra take the same transpose with the two fields.  FP64 or FP32
+storage (FP32 with GWs or spectra: N in {64, 128, 256, 512}).
 
 `SlabLattice` drives the slabs of one rank through a communicator:
 `DistComm` (torch.distributed: all-reduce and a ring of point-to-point
