@@ -15,7 +15,10 @@
 //          = one 128-byte line per row) of one plane (resp. one row j).
 // The layout is that of a library in-place r2c: S[q][i][j][N+2] reals before,
 // S[q][kx][ky][kz] complex (kz < N/2+1) after.  Forward sign e^{-i},
-// unnormalised (FFTW's convention).
+// unnormalised (FFTW's convention).  The column passes also run out of place
+// (the handle's default: they write a second array faster than their input)
+// and, for a lattice split into slabs, straight into and out of the blocks
+// of the ranks' transpose (scatter along j, gather along i).
 #pragma once
 
 #include "planefft.cuh"

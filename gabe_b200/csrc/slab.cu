@@ -1,5 +1,6 @@
-// One slab of a lattice split along i over several processes (GPUs), field
-// evolution without tensor modes (gabe_slab_*, include/gabe.h).
+// One slab of a lattice split along i over several processes (GPUs):
+// field evolution, the tensor modes and the spectra (gabe_slab_*,
+// include/gabe.h; the GW transpose is in slabgw.cuh).
 //
 // Each rank holds its own planes i in [plane0, plane0 + nplanes) of the
 // four state arrays between two halo planes (the last own plane of the rank
