@@ -40,6 +40,7 @@ FLAG_FUSED_KSPACE = 8
 FLAG_OWN_FFT = 16
 FLAG_FUSED_ROWS = 32
 FLAG_CUFFT_3D = 64
+FLAG_TRANSPOSED_FFT = 128
 
 STATUS = {
     0: "GABE_OK", 1: "GABE_ERR_PARAM", 2: "GABE_ERR_CUDA", 3: "GABE_ERR_CUFFT", 4: "GABE_ERR_NOMEM",
@@ -244,11 +245,16 @@ class Lattice:
         return {"stage1": out[0], "fft": out[1], "kspace": out[2], "stage2": out[3]}
 
     def profile_fft_passes(self, n: int) -> dict:
-        """Mean ms of each pass of the library's 3-D FFT over the source
-        buffer (handles that use it: launches_per_step == 6)."""
+        """Mean ms of each pass of the library's own transforms (raises
+        GabeError GABE_ERR_STATE for a handle that uses cuFFT's plan).  The
+        three-pass 3-D FFT: {fft_rows, fft_j, fft_i}, run on the source buffer.
+        The transposed form (FLAG_TRANSPOSED_FFT): {fft_rows, fft_j,
+        fft_i_kspace}, timed inside n full steps (the state advances n steps)."""
         out = (ctypes.c_double * 3)()
         self._check(library().gabe_profile_fft_passes(self._h, int(n), out))
-        return {"fft_rows": out[0], "fft_j": out[1], "fft_i": out[2]}
+        last = "fft_i_kspace" if self.params.flags & FLAG_TRANSPOSED_FFT and self.gws and \
+            self.precision == FP32 and self.N in (64, 128, 256, 512) else "fft_i"
+        return {"fft_rows": out[0], "fft_j": out[1], last: out[2]}
 
     @property
     def stream_ptr(self) -> int:

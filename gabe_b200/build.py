@@ -27,6 +27,7 @@ UNITS = [
     ("kernels_f32.cu", []),
     ("planefft.cu", []),
     ("fft3d.cu", []),
+    ("fftt.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
     ("ensemble.cu", []),
     ("slab.cu", []),

@@ -59,6 +59,8 @@ struct gabe_handle {
     // of planefft.cuh) and the k-space update with the pass along i fused in
     bool evolve_gw = false; // calc_gws with expansion_type 1: the step evolves h, l (types 0 and 2 do not)
     bool own_fft = false;   // the library's three-pass 3-D r2c (fft3d.cuh)
+    bool fftt = false;      // the transposed three-pass transform with the pass along i fused into the
+                            // k-space update (fftt.cuh); G is then kept as [4][kz][ky][kx]
     bool rows_fused = false;  // sweep A writes the sources transformed along k (sweeprows.cuh)
     bool ks_fused = false;
     bool plane_fft = false;
@@ -128,18 +130,19 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    h->ks_fused = h->evolve_gw && h->f32 && kspace_fused_supported(h->N) && (h->p.flags & GABE_FLAG_FUSED_KSPACE);
+    h->ks_fused = h->evolve_gw && h->f32 && !h->fftt && kspace_fused_supported(h->N) &&
+                  (h->p.flags & GABE_FLAG_FUSED_KSPACE);
     h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
-    h->rows_fused = h->evolve_gw && h->f32 && !h->ks_fused && sweep32_rows_supported(h->N) &&
+    h->rows_fused = h->evolve_gw && h->f32 && !h->fftt && !h->ks_fused && sweep32_rows_supported(h->N) &&
                     (h->p.flags & GABE_FLAG_FUSED_ROWS);
     // the library's 3-D r2c: on request, and by default at N = 512 (measured faster than cuFFT's plan there)
     const bool own_default = h->N == 512 && !(h->p.flags & GABE_FLAG_CUFFT_3D);
-    h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && !h->rows_fused && fft3d_supported(h->N) &&
+    h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && !h->rows_fused && !h->fftt && fft3d_supported(h->N) &&
                  ((h->p.flags & GABE_FLAG_OWN_FFT) || own_default);
     if (h->plane_fft) {
         CK(h, plane_r2c_setup(h->N, &h->plane_grid));
-    } else if (h->own_fft || h->rows_fused) {
-        // no plan: fft3d.cuh
+    } else if (h->own_fft || h->rows_fused || h->fftt) {
+        // no plan: fft3d.cuh / fftt.cuh
     } else if (h->ks_fused) {
         // 2-D r2c of every (source, i) plane: N x (N+2) reals in, N x nz complex out, in place
         long long n2[2] = {N, N}, inem[2] = {N, 2 * nz}, onem[2] = {N, nz};
@@ -184,7 +187,7 @@ int fft_r2c(gabe_handle *h, cufftHandle plan, void *in, void *out) {
 // The GW chain of step n overlaps the field sweeps of step n+1 (two source
 // buffers) -- except with the library's FFT, which runs in line (measured
 // faster at 512^3) and uses the second buffer as its column passes' target.
-bool overlapped(const gabe_handle *h) { return h->evolve_gw && h->S2 != nullptr && !h->own_fft; }
+bool overlapped(const gabe_handle *h) { return h->evolve_gw && h->S2 != nullptr && !h->own_fft && !h->fftt; }
 float *fft_scratch(const gabe_handle *h) { return h->own_fft ? static_cast<float *>(h->S2) : nullptr; }
 void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
 
@@ -196,6 +199,11 @@ int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
     void *S = source_buffer(h, slot);
     if (h->plane_fft) {
         CK(h, plane_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc * h->N, h->plane_grid, s));
+        return GABE_OK;
+    }
+    if (h->fftt) {  // rows S -> S2, pass along j S2 -> S; the pass along i runs inside the k-space update
+        CK(h, fftt_rows_f32(h->N, static_cast<const float *>(S), h->S2, 2 * kSrc, s));
+        CK(h, fftt_cols_f32(h->N, h->S2, S, 2 * kSrc, &h->sc->status, s));
         return GABE_OK;
     }
     if (h->own_fft) {
@@ -218,6 +226,10 @@ int kspace(gabe_handle *h, int slot, cudaStream_t s) {
     k.sc = h->sc;
     k.c = h->lc;
     k.slot = slot;
+    if (h->fftt) {
+        CK(h, fftt_ikspace_f32(h->N, k.S, h->G, h->sc, h->lc, slot, &h->sc->status, s));
+        return GABE_OK;
+    }
     if (h->ks_fused) {
         CK(h, kspace_fused_f32(h->N, k, s));
         return GABE_OK;
@@ -348,6 +360,8 @@ int read_scalars(gabe_handle *h, DevScalars *out) {
     }
     CK(h, cudaStreamSynchronize(h->stream));
     CK(h, cudaMemcpy(out, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
+    if (out->status & ST_TIMEOUT)
+        return set_err(h, GABE_ERR_TIMEOUT, "a bulk copy of the GW transform did not complete (bounded wait gave up)");
     if (out->status & ST_NONFINITE)
         return set_err(h, GABE_ERR_NONFINITE, "non-finite energy density at step %lld", out->step);
     return GABE_OK;
@@ -382,7 +396,7 @@ int upload_gw(gabe_handle *h, const double *h0, const double *l0) {
             for (int q = 0; q < 12; q++)
                 CK(h, cudaMemcpyAsync(stage + (size_t)q * cnt, src[w] + (size_t)q * M + m0, cnt * 8,
                                       cudaMemcpyHostToDevice, h->stream));
-            CK(h, h->f32 ? gw_pack_f32(stage, cnt, m0, h->N, M, h->G, w, h->gwnorm + 2 * w, h->stream)
+            CK(h, h->f32 ? gw_pack_f32(stage, cnt, m0, h->N, M, h->G, w, h->gwnorm + 2 * w, h->fftt, h->stream)
                          : gw_pack_f64(stage, cnt, m0, h->N, M, h->G, w, h->gwnorm + 2 * w, h->stream));
         }
     }
@@ -406,7 +420,7 @@ int download_gw(gabe_handle *h, double *h0, double *l0) {
         if (!dst[w]) continue;
         for (size_t m0 = 0; m0 < M; m0 += chunk) {
             const size_t cnt = (M - m0) < chunk ? (M - m0) : chunk;
-            CK(h, h->f32 ? gw_unpack_f32(h->G, cnt, m0, h->N, M, w, stage, h->stream)
+            CK(h, h->f32 ? gw_unpack_f32(h->G, cnt, m0, h->N, M, w, stage, h->fftt, h->stream)
                          : gw_unpack_f64(h->G, cnt, m0, h->N, M, w, stage, h->stream));
             for (int q = 0; q < 12; q++)
                 CK(h, cudaMemcpyAsync(dst[w] + (size_t)q * M + m0, stage + (size_t)q * cnt, cnt * 8,
@@ -452,21 +466,12 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     if (!p) return set_err(nullptr, GABE_ERR_PARAM, "params is NULL");
     if (p->struct_size != (int32_t)sizeof(gabe_params))
         return set_err(nullptr, GABE_ERR_PARAM, "struct_size %d != %zu", p->struct_size, sizeof(gabe_params));
-    if (p->N < 4 || p->N > 1290 || (p->N & 1))
-        return set_err(nullptr, GABE_ERR_PARAM, "N must be even and in [4, 1290], got %d", p->N);
-    if (p->nflds != 2) return set_err(nullptr, GABE_ERR_PARAM, "nflds must be 2, got %d", p->nflds);
-    if (p->expansion < 0 || p->expansion > 2)
-        return set_err(nullptr, GABE_ERR_PARAM, "expansion_type must be 0, 1 or 2, got %d", p->expansion);
-    if (p->gws_on != 0 && p->gws_on != 1) return set_err(nullptr, GABE_ERR_PARAM, "calc_gws must be 0 or 1");
-    if (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4)
-        return set_err(nullptr, GABE_ERR_PARAM, "unknown model %d", p->model);
-    if (p->precision != GABE_FP64 && p->precision != GABE_FP32)
-        return set_err(nullptr, GABE_ERR_PARAM, "unknown precision %d", p->precision);
-    if (!(p->L > 0) || !(p->dt > 0) || !std::isfinite(p->L) || !std::isfinite(p->dt))
-        return set_err(nullptr, GABE_ERR_PARAM, "L and dt must be positive and finite");
-    if (!std::isfinite(p->model_c[0]) || !std::isfinite(p->model_c[1]) ||
-        (p->model == GABE_MODEL_QUADRATIC && p->model_c[0] == 0.0))
-        return set_err(nullptr, GABE_ERR_PARAM, "invalid model constants");
+    char msg[160];
+    if (!params_valid(*p, msg, sizeof(msg))) return set_err(nullptr, GABE_ERR_PARAM, "%s (N = %d)", msg, p->N);
+    const bool f32 = p->precision == GABE_FP32;
+    if ((f32 ? plan_grid32(p->N, p->tile_shape, p->tile_ci) : plan_grid(p->N, p->tile_shape, p->tile_ci)).shape < 0)
+        return set_err(nullptr, GABE_ERR_PARAM, "N = %d: no stencil tile divides N (%s)", p->N,
+                       f32 ? "FP32 storage needs N %% 16 == 0" : "FP64 needs N %% 4 == 0");
 
     gabe_handle *h = new (std::nothrow) gabe_handle();
     if (!h) return set_err(nullptr, GABE_ERR_NOMEM, "host allocation failed");
@@ -531,10 +536,13 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     }
     // sources need 10 padded slots; spectra need 2; uploads stage one FP64 field array
     h->evolve_gw = p->gws_on && p->expansion == 1;
+    h->fftt = h->evolve_gw && h->f32 && fftt_supported(h->N) && (p->flags & GABE_FLAG_TRANSPOSED_FFT);
     h->nslots = h->evolve_gw ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);
-    if (h->evolve_gw && !(p->flags & GABE_FLAG_NO_OVERLAP)) {
+    if (h->fftt) {  // the transposed transform's first pass writes out of place
+        if ((rc = dalloc(h, &h->S2, h->S_bytes))) return bail(rc);
+    } else if (h->evolve_gw && !(p->flags & GABE_FLAG_NO_OVERLAP)) {
         // optional: without it the GW chain simply runs in line
         if (dalloc(h, &h->S2, h->S_bytes) != GABE_OK) {
             h->S2 = nullptr;
@@ -692,9 +700,54 @@ int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]) {
     return read_scalars(h, &sc);
 }
 
+// Transposed form: nreps full steps with events around each of its three launches.
+static int profile_fftt_passes(gabe_handle *h, int nreps, double ms_out[3]) {
+    std::vector<cudaEvent_t> ev((size_t)4 * nreps, nullptr);
+    for (auto &x : ev) CK(h, cudaEventCreate(&x));
+    int rc = GABE_OK;
+    for (int r = 0; r < nreps && rc == GABE_OK; r++) {
+        const int c = h->cur ^ (r & 1);
+        cudaEvent_t *e = ev.data() + 4 * r;
+        rc = sweep(h, MODE_A_GW, c, 0, 0);
+        if (rc) break;
+        cudaError_t ce = cudaEventRecord(e[0], h->stream);
+        if (ce == cudaSuccess) ce = fftt_rows_f32(h->N, static_cast<const float *>(h->S), h->S2, 2 * kSrc, h->stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e[1], h->stream);
+        if (ce == cudaSuccess) ce = fftt_cols_f32(h->N, h->S2, h->S, 2 * kSrc, &h->sc->status, h->stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e[2], h->stream);
+        if (ce == cudaSuccess)
+            ce = fftt_ikspace_f32(h->N, h->S, h->G, h->sc, h->lc, 0, &h->sc->status, h->stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(e[3], h->stream);
+        if (ce != cudaSuccess) {
+            rc = set_err(h, GABE_ERR_CUDA, "profile launch: %s", cudaGetErrorString(ce));
+            break;
+        }
+        rc = sweep(h, MODE_B, c, 1, 0);
+    }
+    h->cur ^= (nreps & 1);
+    h->e0_stale = true;
+    double acc[3] = {0, 0, 0};
+    if (rc == GABE_OK && cudaStreamSynchronize(h->stream) == cudaSuccess)
+        for (int r = 0; r < nreps; r++)
+            for (int q = 0; q < 3; q++) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[4 * r + q], ev[4 * r + q + 1]);
+                acc[q] += ms;
+            }
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    for (int q = 0; q < 3; q++) ms_out[q] = acc[q] / nreps;
+    DevScalars sc;
+    return read_scalars(h, &sc);
+}
+
 int gabe_profile_fft_passes(gabe_handle *h, int nreps, double ms_out[3]) {
     if (!h || !ms_out || nreps < 1) return GABE_ERR_PARAM;
     if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "profile before upload");
+    if (h->fftt) {
+        CK(h, cudaSetDevice(h->dev));
+        return profile_fftt_passes(h, nreps, ms_out);
+    }
     if (!h->own_fft) return set_err(h, GABE_ERR_STATE, "this handle does not use the library's 3-D FFT");
     CK(h, cudaSetDevice(h->dev));
     CK(h, cudaStreamSynchronize(h->stream));  // the last step's GW chain has finished with the sources
@@ -886,6 +939,7 @@ int gabe_spectra_raw(gabe_handle *h, double *sums, double *counts, int nbins, in
     b.nseries = ns;
     b.quirk = h->p.gw_spec_quirk;
     b.fix_zero = h->f32 ? 1 : 0;
+    b.gt = h->fftt ? 1 : 0;
     b.zero_re[0] = h->lc.gridsize * s.fbar[0];
     b.zero_re[1] = h->lc.gridsize * s.fbar[1];
     const size_t smem = (size_t)h->nbins * (ns * 8 + 4);
@@ -960,7 +1014,7 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
 int gabe_launches_per_step(const gabe_handle *h) {
-    return h ? (h->evolve_gw ? (h->own_fft ? 6 : h->rows_fused ? 5 : h->plane_fft ? 4 : 3) : 2) : 0;
+    return h ? (h->evolve_gw ? (h->own_fft ? 6 : (h->rows_fused || h->fftt) ? 5 : h->plane_fft ? 4 : 3) : 2) : 0;
 }
 
 }  // extern "C"

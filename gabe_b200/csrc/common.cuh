@@ -21,6 +21,7 @@ namespace gabe {
 // Status bits raised on the device and read by the host at sync points.
 enum : uint32_t {
     ST_NONFINITE = 1u,
+    ST_TIMEOUT = 2u,  // a bounded wait on a bulk copy gave up (tma.cuh)
 };
 
 // Per-stage scalars, laid out like the reference's globals

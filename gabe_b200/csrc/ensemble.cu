@@ -613,7 +613,7 @@ int gabe_ensemble_download(gabe_ensemble *e, int lat, double *field0, double *df
         if (!gdst[w] || !Lt.G) continue;
         for (size_t m0 = 0; m0 < M; m0 += chunk) {
             const size_t cnt = (M - m0) < chunk ? (M - m0) : chunk;
-            ECK(e, gw_unpack_f32(Lt.G, cnt, m0, Lt.N, M, w, stage, e->stream));
+            ECK(e, gw_unpack_f32(Lt.G, cnt, m0, Lt.N, M, w, stage, 0, e->stream));
             for (int q = 0; q < 12; q++)
                 ECK(e, cudaMemcpyAsync(gdst[w] + (size_t)q * M + m0, stage + (size_t)q * cnt, cnt * 8,
                                        cudaMemcpyDeviceToHost, e->stream));

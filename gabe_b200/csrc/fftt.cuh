@@ -1,0 +1,403 @@
+// FP32 3-D r2c of the GW sources in three passes with transposed outputs,
+// the last pass fused with the TT projection and h/l update.
+//
+// The reference transforms each source array with one 3-D r2c FFT
+// (fft_stresstensor, g2evolutionpert.cpp:183-195) and then updates h and l
+// per k-point (evolve_perts, :343-455).  A 512^3 array does not fit on chip,
+// so the transform is one HBM pass per axis.  Here every pass reads whole
+// lines of its own axis as contiguous runs and writes its output transposed,
+// so that the next pass's lines are contiguous again:
+//
+//   pass 1 (rowt_kernel)   S[q][i][j][N+2] reals   -> T1[q][i][kz][j]
+//          rows along k, two real rows as one complex sequence (the row
+//          kernel of fft3d.cuh), each kz written as one 128-byte piece of
+//          16 consecutive j;
+//   pass 2 (colt_kernel)   T1 lines along j         -> T2[q][kz][ky][i]
+//          16 lines of consecutive i per tile, landed in shared memory by
+//          bulk copies (cp.async.bulk + mbarrier), each ky written as one
+//          128-byte piece of 16 consecutive i;
+//   pass 3 (ikspace_kernel) T2 lines along i + amplitudes G[p][kz][ky][kx]
+//          the ten source lines and four amplitude lines of one (kz, ky)
+//          land by bulk copies, the ten lines are transformed along i in
+//          shared memory, and the k-space update (kspace_update_vals) runs
+//          on each kx; only the amplitudes go back to HBM.
+//
+// The transformed sources never return to HBM after pass 2, and the
+// amplitudes are kept in the transposed order [p][kz][ky][kx]
+// (g_index with gt = 1) for the life of the handle.  q runs over the
+// ten source arrays (stage-0 11,12,13,22,23, then stage 1); forward sign
+// e^{-i}, unnormalised, as FFTW's r2c.
+#pragma once
+
+#include "fft3d.cuh"
+#include "kspace.cuh"
+#include "tma.cuh"
+
+namespace gabe {
+namespace f3t {
+
+using pfft::PlaneCfg;
+
+// ---------------------------------------------------------------------------
+// pass 1: rows along k -> T1[q][i][kz][j]
+// ---------------------------------------------------------------------------
+// The row kernel of fft3d.cuh (cp.async ring, four-step FFT of row pairs in a
+// swizzled unpadded layout) with its output staged per tile in shared memory
+// as [kz][16 rows] (pitch 17 complex: the pair-wise writes of the separation,
+// lanes over kz, and the piece-wise reads, lanes over rows, both hit distinct
+// banks) and written as one 128-byte piece per kz.
+template <int N>
+struct RowTGeom {
+    using RG = f3d::RowGeom<N>;
+    static constexpr int NH = N / 2 + 1, SP = RG::R + 1;  // staging pitch (complex)
+    static constexpr size_t STAGE_BYTES = (size_t)NH * SP * sizeof(float2);
+    static constexpr size_t SMEM_BYTES = RG::SMEM_BYTES + STAGE_BYTES;
+};
+
+template <int N>
+__global__ void __launch_bounds__(f3d::RowGeom<N>::T, 2) rowt_kernel(const float *S, float2 *T1, long long nrows) {
+    using Gm = f3d::RowGeom<N>;
+    constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2,
+                  NB = Gm::NB;
+    constexpr int RP = N + 2, NH = N / 2 + 1, SP = RowTGeom<N>::SP;
+    static_assert(R == 16, "one 128-byte output piece per kz");
+    extern __shared__ __align__(16) float smem[];
+    float2 *tw = reinterpret_cast<float2 *>(smem + NB * Gm::BUF);
+    float2 *st = tw + N;  // staging [NH][SP]
+    const int tid = threadIdx.x;
+    f3d::twiddles<N>(tw);
+    const long long ntiles = nrows / R;
+    auto issue = [&](long long tile, int b) {
+        const float *g = S + tile * R * RP;
+        float *rows = smem + b * Gm::BUF;
+#pragma unroll 4
+        for (int t = tid; t < R * (N / 2); t += T) {
+            const int jj = t / (N / 2), m = t % (N / 2);
+            s32::cp_async8(rows + jj * PITCH + Gm::phys(2 * m), g + jj * RP + 2 * m);
+        }
+    };
+#pragma unroll
+    for (int q = 0; q < NB - 1; q++) {
+        if (blockIdx.x + q * (long long)gridDim.x < ntiles) issue(blockIdx.x + q * (long long)gridDim.x, q);
+        s32::cp_commit();
+    }
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        float *rows = smem + (it % NB) * Gm::BUF;
+        s32::cp_wait<NB - 2>();
+        __syncthreads();  // this tile landed; the buffer and the staging of tile it-1 are consumed
+        const long long ahead = tile + (long long)(NB - 1) * gridDim.x;
+        if (ahead < ntiles) issue(ahead, (it + NB - 1) % NB);
+        s32::cp_commit();
+        // four-step pass 1: L2-point FFTs over n2 (stride L1), twiddle W_N^(n1 k2), in place
+#pragma unroll
+        for (int t0 = 0; t0 < P * L1; t0 += T) {
+            const int t = t0 + tid, p = t / L1, n1 = t % L1;
+            if (t >= P * L1) break;
+            float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+            float2 x[L2];
+#pragma unroll
+            for (int n2 = 0; n2 < L2; n2++) {
+                const int a = Gm::phys(n1 + L1 * n2);
+                x[n2] = make_float2(re[a], im[a]);
+            }
+            pfft::fft_reg<L2>(x);
+#pragma unroll
+            for (int k2 = 0; k2 < L2; k2++) {
+                const float2 y = k2 ? pfft::cmul(x[k2], tw[k2 * L1 + n1]) : x[k2];
+                const int a = Gm::phys(n1 + L1 * k2);
+                re[a] = y.x;
+                im[a] = y.y;
+            }
+        }
+        __syncthreads();
+        // pass 2: L1-point FFTs over n1, written back in natural order k = k2 + L2 k1
+        {
+            float2 y[NT2][L1];
+#pragma unroll
+            for (int q = 0; q < NT2; q++) {
+                const int t = q * T + tid, p = t / L2, k2 = t % L2;
+                if (t < P * L2) {
+                    const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+#pragma unroll
+                    for (int n1 = 0; n1 < L1; n1++) {
+                        const int a = Gm::phys(n1 + L1 * k2);
+                        y[q][n1] = make_float2(re[a], im[a]);
+                    }
+                    pfft::fft_reg<L1>(y[q]);
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < NT2; q++) {
+                const int t = q * T + tid, p = t / L2, k2 = t % L2;
+                if (t < P * L2) {
+                    float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+#pragma unroll
+                    for (int k1 = 0; k1 < L1; k1++) {
+                        const int a = Gm::phys(k2 + L2 * k1);
+                        re[a] = y[q][k1].x;
+                        im[a] = y[q][k1].y;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // separate each pair into the staging tile [kz][row]
+        for (int t = tid; t < P * NH; t += T) {
+            const int p = t / NH, k = t % NH, km = (N - k) & (N - 1);
+            const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+            const int ak = Gm::phys(k & (N - 1)), am = Gm::phys(km);
+            const float zr = re[ak], zi = im[ak], mr = re[am], mi = im[am];
+            st[k * SP + 2 * p] = make_float2(0.5f * (zr + mr), 0.5f * (zi - mi));
+            st[k * SP + 2 * p + 1] = make_float2(0.5f * (zi + mi), 0.5f * (mr - zr));
+        }
+        __syncthreads();
+        // one 128-byte piece of 16 rows per kz: T1[q][i][kz][j0 .. j0+15]
+        {
+            const long long qi = tile / (N / R);  // q N + i
+            const int j0 = (int)(tile % (N / R)) * R;
+            float2 *o = T1 + qi * NH * N + j0;
+            for (int t = tid; t < NH * R; t += T) {
+                const int kz = t / R, jj = t % R;
+                __stcs(o + (long long)kz * N + jj, st[kz * SP + jj]);
+            }
+        }
+    }
+    s32::cp_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Four-step FFT of whole lines held contiguously in shared memory
+// ---------------------------------------------------------------------------
+// Line w occupies [w * PL, w * PL + N) complex (PL = N + 2: 16-byte aligned
+// for the bulk copies, and consecutive lines 4 banks apart).  Step A: for
+// each (w, n1) the L2-point FFT of elements n1 + L1 n2, twiddled, in place
+// (lanes over n1: consecutive words).
+template <int N, int T>
+__device__ __forceinline__ void lines_step_a(float2 *buf, int nlines, const float2 *tw) {
+    constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2, PL = N + 2;
+    for (int t = threadIdx.x; t < nlines * L1; t += T) {
+        const int w = t / L1, n1 = t % L1;
+        float2 *ln = buf + w * PL;
+        float2 x[L2];
+#pragma unroll
+        for (int n2 = 0; n2 < L2; n2++) x[n2] = ln[n1 + L1 * n2];
+        pfft::fft_reg<L2>(x);
+#pragma unroll
+        for (int k2 = 0; k2 < L2; k2++) ln[n1 + L1 * k2] = k2 ? pfft::cmul(x[k2], tw[k2 * L1 + n1]) : x[k2];
+    }
+}
+
+// Step B input of task (w, k2): the L1 elements L1 k2 .. L1 k2 + L1 - 1 of
+// line w (16-byte loads), transformed in registers; y[k1] is output element
+// k2 + L2 k1.
+template <int N>
+__device__ __forceinline__ void lines_step_b(const float2 *buf, int w, int k2, float2 (&y)[PlaneCfg<N>::L1]) {
+    constexpr int L1 = PlaneCfg<N>::L1, PL = N + 2;
+    const float4 *src = reinterpret_cast<const float4 *>(buf + w * PL + L1 * k2);
+#pragma unroll
+    for (int h = 0; h < L1 / 2; h++) {
+        const float4 v = src[h];
+        y[2 * h] = make_float2(v.x, v.y);
+        y[2 * h + 1] = make_float2(v.z, v.w);
+    }
+    pfft::fft_reg<L1>(y);
+}
+
+// Shared-memory ring of NB tiles, each of nl lines of pitch N + 2, filled by
+// bulk copies; barrier b completes when tile buffer b has landed.
+template <int N, int NL, int NB>
+struct LineRing {
+    static constexpr int PL = N + 2, BUF = NL * PL;
+    static constexpr size_t HEAD = 128;  // NB mbarriers (8 bytes each)
+    static constexpr size_t SMEM_BYTES = HEAD + (size_t)N * sizeof(float2) + (size_t)NB * BUF * sizeof(float2);
+    static_assert(NB * 8 <= (int)HEAD, "barriers fit the head");
+    __device__ static uint64_t *bars(unsigned char *sm) { return reinterpret_cast<uint64_t *>(sm); }
+    __device__ static float2 *twid(unsigned char *sm) { return reinterpret_cast<float2 *>(sm + HEAD); }
+    __device__ static float2 *buf(unsigned char *sm, int b) { return twid(sm) + N + b * BUF; }
+};
+
+// ---------------------------------------------------------------------------
+// pass 2: along j, T1[q][i][kz][j] -> T2[q][kz][ky][i]
+// ---------------------------------------------------------------------------
+constexpr int kColW = 16;  // lines (consecutive i) per tile: one 128-byte output piece per ky
+
+template <int N, int T, int NB>
+__global__ void __launch_bounds__(T, 1) colt_kernel(const float2 *__restrict__ T1, float2 *__restrict__ T2, int ncomp,
+                                                    unsigned int *status) {
+    using Rg = LineRing<N, kColW, NB>;
+    constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2, NH = N / 2 + 1, W = kColW;
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *bar = Rg::bars(sm);
+    float2 *tw = Rg::twid(sm);
+    const int tid = threadIdx.x;
+    const long long ntiles = (long long)ncomp * NH * (N / W);
+    if (tid == 0) {
+        for (int b = 0; b < NB; b++) tma::mbar_init(&bar[b], 1);
+        tma::fence_barrier_init();
+    }
+    f3d::twiddles<N>(tw);
+    __syncthreads();
+    int fills[NB] = {};  // thread 0: fills issued per buffer
+    // tile = (q NH + kz) (N / W) + ib: lines i = ib W + w of (q, kz)
+    auto issue = [&](long long tile, int b) {
+        fills[b]++;
+        const int ib = (int)(tile % (N / W));
+        const long long qk = tile / (N / W);
+        const int kz = (int)(qk % NH), q = (int)(qk / NH);
+        float2 *dst = Rg::buf(sm, b);
+        tma::mbar_arrive_expect(&bar[b], W * N * (uint32_t)sizeof(float2));
+        for (int w = 0; w < W; w++)
+            tma::load(dst + w * Rg::PL, T1 + (((long long)q * N + ib * W + w) * NH + kz) * N,
+                      N * (uint32_t)sizeof(float2), &bar[b]);
+    };
+    if (tid == 0)
+        for (int q = 0; q < NB - 1; q++) {
+            const long long t = blockIdx.x + (long long)q * gridDim.x;
+            if (t < ntiles) issue(t, q);
+        }
+    int it = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+        const int b = it % NB;
+        if (tid == 0) {
+            const long long ahead = tile + (long long)(NB - 1) * gridDim.x;
+            if (ahead < ntiles) {
+                tma::fence_proxy_async();  // the buffer's last reads (tile it-1) precede its refill
+                issue(ahead, (it + NB - 1) % NB);
+            }
+        }
+        const bool ok = tma::mbar_wait(&bar[b], (uint32_t)((it / NB) & 1), status);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) tma::drain(bar, fills, NB, status);
+            break;
+        }
+        float2 *buf = Rg::buf(sm, b);
+        lines_step_a<N, T>(buf, W, tw);
+        __syncthreads();
+        const int ib = (int)(tile % (N / W));
+        const long long qk = tile / (N / W);  // q NH + kz
+        float2 *o = T2 + qk * N * N + ib * W;
+        for (int t = tid; t < W * L2; t += T) {
+            const int w = t % W, k2 = t / W;
+            float2 y[L1];
+            lines_step_b<N>(buf, w, k2, y);
+#pragma unroll
+            for (int k1 = 0; k1 < L1; k1++) __stcs(o + (long long)(k2 + L2 * k1) * N + w, y[k1]);
+        }
+        __syncthreads();  // buffer b consumed
+    }
+}
+
+// ---------------------------------------------------------------------------
+// pass 3: along i, fused with the TT projection and both RK2 stages of h, l
+// ---------------------------------------------------------------------------
+constexpr int kIkLines = 14;  // 10 source lines + 4 amplitude lines per (kz, ky)
+
+struct IkArgs {
+    const float2 *T2;  // [10][NH][N][N]
+    float2 *G;         // [4][NH][N][N]
+    const DevScalars *sc;
+    LatticeConsts c;
+    int slot;
+    unsigned int *status;
+};
+
+template <int N, int T, int NB>
+__global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
+    using Rg = LineRing<N, kIkLines, NB>;
+    constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2, NH = N / 2 + 1, PL = Rg::PL;
+    constexpr long long M = (long long)NH * N * N;
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *bar = Rg::bars(sm);
+    float2 *tw = Rg::twid(sm);
+    const int tid = threadIdx.x;
+    constexpr long long ntasks = (long long)NH * N;  // task = kz N + ky
+    const KsCoef<float> kc = ks_coef<float>(a.c, a.sc->gw[a.slot]);
+    if (tid == 0) {
+        for (int b = 0; b < NB; b++) tma::mbar_init(&bar[b], 1);
+        tma::fence_barrier_init();
+    }
+    f3d::twiddles<N>(tw);
+    __syncthreads();
+    int fills[NB] = {};  // thread 0: fills issued per buffer
+    auto issue = [&](long long task, int b) {
+        fills[b]++;
+        float2 *dst = Rg::buf(sm, b);
+        tma::mbar_arrive_expect(&bar[b], kIkLines * N * (uint32_t)sizeof(float2));
+        for (int q = 0; q < 2 * kSrc; q++)
+            tma::load(dst + q * PL, a.T2 + q * M + task * N, N * (uint32_t)sizeof(float2), &bar[b]);
+        for (int p = 0; p < 4; p++)
+            tma::load(dst + (2 * kSrc + p) * PL, a.G + p * M + task * N, N * (uint32_t)sizeof(float2), &bar[b]);
+    };
+    if (tid == 0)
+        for (int q = 0; q < NB - 1; q++) {
+            const long long t = blockIdx.x + (long long)q * gridDim.x;
+            if (t < ntasks) issue(t, q);
+        }
+    int it = 0;
+    for (long long task = blockIdx.x; task < ntasks; task += gridDim.x, it++) {
+        const int b = it % NB;
+        if (tid == 0) {
+            const long long ahead = task + (long long)(NB - 1) * gridDim.x;
+            if (ahead < ntasks) {
+                tma::fence_proxy_async();
+                issue(ahead, (it + NB - 1) % NB);
+            }
+        }
+        const bool ok = tma::mbar_wait(&bar[b], (uint32_t)((it / NB) & 1), a.status);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) tma::drain(bar, fills, NB, a.status);
+            break;
+        }
+        float2 *buf = Rg::buf(sm, b);
+        lines_step_a<N, T>(buf, 2 * kSrc, tw);
+        __syncthreads();
+        // step B over the ten source lines (lanes over lines), results back in natural order
+        {
+            constexpr int NT = (2 * kSrc * L2 + T - 1) / T;
+            float2 y[NT][L1];
+#pragma unroll
+            for (int r = 0; r < NT; r++) {
+                const int t = r * T + tid;
+                if (t < 2 * kSrc * L2) lines_step_b<N>(buf, t % (2 * kSrc), t / (2 * kSrc), y[r]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < NT; r++) {
+                const int t = r * T + tid;
+                if (t < 2 * kSrc * L2) {
+                    float2 *ln = buf + (t % (2 * kSrc)) * PL;
+                    const int k2 = t / (2 * kSrc);
+#pragma unroll
+                    for (int k1 = 0; k1 < L1; k1++) ln[k2 + L2 * k1] = y[r][k1];
+                }
+            }
+        }
+        __syncthreads();
+        const int kz = (int)(task / N), ky = (int)(task % N);
+        const int py = ky <= N / 2 ? ky : ky - N;
+        float2 *gout = a.G + task * N;
+        for (int kx = tid; kx < N; kx += T) {
+            Cplx<float> s[10], g[4];
+#pragma unroll
+            for (int q = 0; q < 2 * kSrc; q++) {
+                const float2 v = buf[q * PL + kx];
+                s[q] = {v.x, v.y};
+            }
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const float2 v = buf[(2 * kSrc + p) * PL + kx];
+                g[p] = {v.x, v.y};
+            }
+            const int px = kx <= N / 2 ? kx : kx - N;
+            kspace_update_vals<float>(kc, px, py, kz, s, g);
+#pragma unroll
+            for (int p = 0; p < 4; p++) gout[p * M + kx] = make_float2(g[p].re, g[p].im);
+        }
+        __syncthreads();  // buffer b consumed
+    }
+}
+
+}  // namespace f3t
+}  // namespace gabe

@@ -123,14 +123,15 @@ cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l) {
     return cudaGetLastError();
 }
 
-cudaError_t gw_pack_f32(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
+cudaError_t gw_pack_f32(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms, int gt,
                       cudaStream_t s) {
-    gw_pack_kernel<float><<<4 * 148, 256, 0, s>>>(src, cnt, m0, N, M, static_cast<Cplx<float> *>(G), which, norms);
+    gw_pack_kernel<float><<<4 * 148, 256, 0, s>>>(src, cnt, m0, N, M, static_cast<Cplx<float> *>(G), which, norms, gt);
     return cudaGetLastError();
 }
 
-cudaError_t gw_unpack_f32(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s) {
-    gw_unpack_kernel<float><<<4 * 148, 256, 0, s>>>(static_cast<const Cplx<float> *>(G), cnt, m0, N, M, which, dst);
+cudaError_t gw_unpack_f32(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, int gt,
+                          cudaStream_t s) {
+    gw_unpack_kernel<float><<<4 * 148, 256, 0, s>>>(static_cast<const Cplx<float> *>(G), cnt, m0, N, M, which, dst, gt);
     return cudaGetLastError();
 }
 

@@ -60,12 +60,12 @@ cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l) {
 
 cudaError_t gw_pack_f64(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
                       cudaStream_t s) {
-    gw_pack_kernel<double><<<4 * 148, 256, 0, s>>>(src, cnt, m0, N, M, static_cast<Cplx<double> *>(G), which, norms);
+    gw_pack_kernel<double><<<4 * 148, 256, 0, s>>>(src, cnt, m0, N, M, static_cast<Cplx<double> *>(G), which, norms, 0);
     return cudaGetLastError();
 }
 
 cudaError_t gw_unpack_f64(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s) {
-    gw_unpack_kernel<double><<<4 * 148, 256, 0, s>>>(static_cast<const Cplx<double> *>(G), cnt, m0, N, M, which, dst);
+    gw_unpack_kernel<double><<<4 * 148, 256, 0, s>>>(static_cast<const Cplx<double> *>(G), cnt, m0, N, M, which, dst, 0);
     return cudaGetLastError();
 }
 

@@ -92,17 +92,13 @@ __device__ __forceinline__ KsCoef<T> ks_coef(const LatticeConsts &c, const doubl
     return k;
 }
 
-// Both RK2 stages of the amplitudes of the k-point with integer wave vector
-// (px, py, kzi) stored at element idx of arrays of M points: sources Sc
-// [10][M], amplitudes G [4][M].
+// Both RK2 stages of the amplitudes g[4] (h+, hx, l+, lx) of the k-point
+// with integer wave vector (px, py, kzi), driven by its transformed
+// sources s[10] (stage-0 11,12,13,22,23, then stage 1); g is updated in
+// place.  k = 0 has no TT part and is left as it is.
 template <typename T>
-__device__ __forceinline__ void kspace_update(const KsCoef<T> &kc, int px, int py, int kzi, size_t M,
-                                              const Cplx<T> *Sc, Cplx<T> *G, size_t idx) {
-    Cplx<T> s[10], g[4];
-#pragma unroll
-    for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
-#pragma unroll
-    for (int q = 0; q < 4; q++) g[q] = G[(size_t)q * M + idx];
+__device__ __forceinline__ void kspace_update_vals(const KsCoef<T> &kc, int px, int py, int kzi, const Cplx<T> (&s)[10],
+                                                   Cplx<T> (&g)[4]) {
     const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
     if (m2 == 0.0) return;  // no TT mode at k = 0; its amplitudes stay zero
     double ep[6], ex[6];
@@ -138,9 +134,25 @@ __device__ __forceinline__ void kspace_update(const KsCoef<T> &kc, int px, int p
             (ri ? hn.im : hn.re) = h0 + kc.dt * l1;
             (ri ? ln.im : ln.re) = l0 + kc.dt * ld1;
         }
-        G[(size_t)p * M + idx] = hn;
-        G[(size_t)(2 + p) * M + idx] = ln;
+        g[p] = hn;
+        g[2 + p] = ln;
     }
+}
+
+// The same for the k-point stored at element idx of arrays of M points:
+// sources Sc [10][M], amplitudes G [4][M].
+template <typename T>
+__device__ __forceinline__ void kspace_update(const KsCoef<T> &kc, int px, int py, int kzi, size_t M,
+                                              const Cplx<T> *Sc, Cplx<T> *G, size_t idx) {
+    Cplx<T> s[10], g[4];
+#pragma unroll
+    for (int q = 0; q < 10; q++) s[q] = Sc[(size_t)q * M + idx];
+#pragma unroll
+    for (int q = 0; q < 4; q++) g[q] = G[(size_t)q * M + idx];
+    if (px == 0 && py == 0 && kzi == 0) return;
+    kspace_update_vals<T>(kc, px, py, kzi, s, g);
+#pragma unroll
+    for (int q = 0; q < 4; q++) G[(size_t)q * M + idx] = g[q];
 }
 
 // k-point idx of the half spectrum [N][N][N/2+1] (M points).
@@ -167,6 +179,13 @@ __global__ void __launch_bounds__(256) kspace_kernel(KspaceArgs args) {
         kspace_point<T>(kc, N, M, Sc, G, idx);
 }
 
+// Element of the amplitude arrays that holds k-point (i, j, kz) of the half
+// spectrum: [i][j][kz] (the library r2c's order), or [kz][j][i] for the
+// transposed transform of fftt.cuh (gt = 1).
+__host__ __device__ inline size_t g_index(int i, int j, int kz, int N, int gt) {
+    return gt ? ((size_t)kz * N + j) * N + i : ((size_t)i * N + j) * (N / 2 + 1) + kz;
+}
+
 // ---------------------------------------------------------------------------
 // conversions between the reference's 12-component layout (FP64 host data,
 // staged in device memory as [12][cnt]) and the amplitudes, for k-points
@@ -174,7 +193,7 @@ __global__ void __launch_bounds__(256) kspace_kernel(KspaceArgs args) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void gw_pack_kernel(const double *src, size_t cnt, size_t m0, int N, size_t M, Cplx<T> *G, int which,
-                               double *norms /* [2]: |X|^2, |X - TT(X)|^2 */) {
+                               double *norms /* [2]: |X|^2, |X - TT(X)|^2 */, int gt) {
     const int nz = N / 2 + 1;
     double nrm = 0., res = 0.;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
@@ -218,8 +237,9 @@ __global__ void gw_pack_kernel(const double *src, size_t cnt, size_t m0, int N, 
                 nrm += w9[c6] * X[ri][c6] * X[ri][c6];
                 res += w9[c6] * r * r;
             }
-        G[(size_t)(2 * which) * M + idx] = ap;
-        G[(size_t)(2 * which + 1) * M + idx] = ax;
+        const size_t gi = g_index(i, j, kzi, N, gt);
+        G[(size_t)(2 * which) * M + gi] = ap;
+        G[(size_t)(2 * which + 1) * M + gi] = ax;
     }
     // block sums then one atomic pair per block (a check, order is irrelevant)
     __shared__ double sred[8 * 2];
@@ -232,7 +252,8 @@ __global__ void gw_pack_kernel(const double *src, size_t cnt, size_t m0, int N, 
 }
 
 template <typename T>
-__global__ void gw_unpack_kernel(const Cplx<T> *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst) {
+__global__ void gw_unpack_kernel(const Cplx<T> *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst,
+                                 int gt) {
     const int nz = N / 2 + 1;
     for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
         const size_t idx = m0 + q;
@@ -242,7 +263,8 @@ __global__ void gw_unpack_kernel(const Cplx<T> *G, size_t cnt, size_t m0, int N,
         const int px = i <= N / 2 ? i : i - N, py = j <= N / 2 ? j : j - N;
         double ep[6] = {0, 0, 0, 0, 0, 0}, ex[6] = {0, 0, 0, 0, 0, 0};
         if (px || py || kzi) pol_tensors(px, py, kzi, ep, ex);
-        const Cplx<T> ap = G[(size_t)(2 * which) * M + idx], ax = G[(size_t)(2 * which + 1) * M + idx];
+        const size_t gi = g_index(i, j, kzi, N, gt);
+        const Cplx<T> ap = G[(size_t)(2 * which) * M + gi], ax = G[(size_t)(2 * which + 1) * M + gi];
 #pragma unroll
         for (int c6 = 0; c6 < 6; c6++) {
             dst[(size_t)(2 * c6) * cnt + q] = ep[c6] * (double)ap.re + ex[c6] * (double)ax.re;

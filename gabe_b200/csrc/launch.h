@@ -65,7 +65,8 @@ inline LatticeConsts make_lattice_consts(const gabe_params &p) {
 
 // Stencil grid: tile shape (the requested one if it divides N, else the first
 // in kShapes that does) and planes per block, shrunk until the grid has at
-// least 8 blocks per SM of a 148-SM B200.
+// least 8 blocks per SM of a 148-SM B200.  shape = -1 (and an empty grid)
+// when no tile shape divides N.
 struct GridPlan {
     int shape, ci;
     dim3 grid;
@@ -78,6 +79,7 @@ inline GridPlan plan_grid(int N, int want_shape, int want_ci) {
     int shape = (want_shape >= 0 && want_shape < kNumShapes && fits(want_shape)) ? want_shape : -1;
     for (int q = 0; shape < 0 && q < kNumShapes; q++)
         if (fits(q)) shape = q;
+    if (shape < 0) return GridPlan{-1, 0, dim3(0, 0, 0)};  // no tile divides N (N % 4 != 0)
     const int TK = kShapes[shape][0], TJ = kShapes[shape][1];
     const int bxy = (N / TK) * (N / TJ);
     int ci = want_ci > 0 ? want_ci : N;
@@ -99,6 +101,7 @@ inline GridPlan plan_grid32(int N, int want_shape, int want_ci) {
     int shape = (want_shape >= 0 && want_shape < kNumShapes32 && fits(want_shape)) ? want_shape : -1;
     for (int q = 0; shape < 0 && q < kNumShapes32; q++)
         if (fits(q)) shape = q;
+    if (shape < 0) return GridPlan{-1, 0, dim3(0, 0, 0)};  // no tile divides N (N % 16 != 0)
     const int TK = kShapes32[shape][0], TJ = kShapes32[shape][1];
     const int bxy = (N / TK) * (N / TJ);
     int ci = want_ci > 0 ? want_ci : N;
@@ -106,6 +109,33 @@ inline GridPlan plan_grid32(int N, int want_shape, int want_ci) {
         while (ci > 4 && (long long)bxy * ((N + ci - 1) / ci) < 4 * 148) ci /= 2;
     if (ci > N) ci = N;
     return GridPlan{shape, ci, dim3(N / TK, N / TJ, (N + ci - 1) / ci)};
+}
+
+// Checks of gabe_params shared by gabe_create and gabe_energy_noalloc; false
+// with a message in msg when p is invalid.  The stencil tiling is checked
+// separately (plan_grid / plan_grid32 return shape -1).
+inline bool params_valid(const gabe_params &p, char *msg, size_t n) {
+    auto fail = [&](const char *m) {
+        if (msg && n) {
+            size_t i = 0;
+            for (; m[i] && i + 1 < n; i++) msg[i] = m[i];
+            msg[i] = 0;
+        }
+        return false;
+    };
+    if (p.struct_size != (int32_t)sizeof(gabe_params)) return fail("struct_size differs from sizeof(gabe_params)");
+    if (p.N < 4 || p.N > 1290 || (p.N & 1)) return fail("N must be even and in [4, 1290]");
+    if (p.nflds != 2) return fail("nflds must be 2");
+    if (p.expansion < 0 || p.expansion > 2) return fail("expansion_type must be 0, 1 or 2");
+    if (p.gws_on != 0 && p.gws_on != 1) return fail("calc_gws must be 0 or 1");
+    if (p.model != GABE_MODEL_QUADRATIC && p.model != GABE_MODEL_LPHI4) return fail("unknown model");
+    if (p.precision != GABE_FP64 && p.precision != GABE_FP32) return fail("unknown precision");
+    if (!(p.L > 0) || !(p.dt > 0) || !std::isfinite(p.L) || !std::isfinite(p.dt))
+        return fail("L and dt must be positive and finite");
+    if (!std::isfinite(p.model_c[0]) || !std::isfinite(p.model_c[1]) ||
+        (p.model == GABE_MODEL_QUADRATIC && p.model_c[0] == 0.0))
+        return fail("invalid model constants (non-finite, or mphi = 0 for the quadratic model)");
+    return true;
 }
 
 cudaError_t sweep_f64(int shape, int mode, const StencilArgs &a, dim3 grid, cudaStream_t s);
@@ -137,10 +167,12 @@ cudaError_t bins_f32(const BinArgs &a, const Launch &l);
 cudaError_t configure_bins(size_t max_smem);
 cudaError_t gw_pack_f64(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
                         cudaStream_t s);
+// gt = 1: G in the transposed order [..][kz][j][i] of the transposed transform (fftt.cuh)
 cudaError_t gw_pack_f32(const double *src, size_t cnt, size_t m0, int N, size_t M, void *G, int which, double *norms,
-                        cudaStream_t s);
+                        int gt, cudaStream_t s);
 cudaError_t gw_unpack_f64(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s);
-cudaError_t gw_unpack_f32(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, cudaStream_t s);
+cudaError_t gw_unpack_f32(const void *G, size_t cnt, size_t m0, int N, size_t M, int which, double *dst, int gt,
+                          cudaStream_t s);
 
 // meansvars() and outputfield() rows on the device (output.cuh)
 cudaError_t meansvars_f64(const OutArgs &a, int pass, int nblocks, cudaStream_t s);
@@ -172,6 +204,15 @@ cudaError_t fft_col_gather_f32(int N, const void *recv, void *T, int ncomp, int 
 cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int ranks, cudaStream_t s);
 // Its passes along j and i alone, for sources already transformed along k.
 cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s);
+
+// FP32 transposed three-pass transform (fftt.cuh): rows along k S -> T1, the pass
+// along j T1 -> T2, and the pass along i fused with the TT projection and h/l
+// update of the amplitudes G (kept in the transposed order [4][kz][ky][kx]).
+bool fftt_supported(int N);
+cudaError_t fftt_rows_f32(int N, const float *S, void *T1, int ncomp, cudaStream_t s);
+cudaError_t fftt_cols_f32(int N, const void *T1, void *T2, int ncomp, unsigned int *status, cudaStream_t s);
+cudaError_t fftt_ikspace_f32(int N, const void *T2, void *G, const DevScalars *sc, const LatticeConsts &c, int slot,
+                             unsigned int *status, cudaStream_t s);
 
 // FP32 k-space update with the FFT pass along i fused in (kspace_fused.cuh);
 // S holds the 2-D (j, k) transforms of the sources.

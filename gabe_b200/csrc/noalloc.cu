@@ -29,6 +29,11 @@
 //   * All calls on a device share the array: calls that overlap on the GPU
 //     (on different streams, or from several threads) race on it.  Each call
 //     resets what must start at zero (counter, status) before its sweep.
+//   * The looked-up address is kept for the life of the process.  After a
+//     cudaDeviceReset the device's context, and the array's address with it,
+//     are new, so the entry point must not be called again in that process.
+//   * A non-finite result (a state holding NaN or Inf) is returned as NaN or
+//     Inf in out4; the call has no status word, so check out4.
 #include <mutex>
 
 #include "launch.h"
@@ -90,10 +95,10 @@ using namespace gabe;
 extern "C" int gabe_energy_noalloc(const gabe_params *p, const double *field0, const double *dfield0, double a0,
                                    double *out4, void *stream) {
     if (!p || !field0 || !dfield0 || !out4) return GABE_ERR_PARAM;
-    if (p->struct_size != (int32_t)sizeof(gabe_params) || p->N < 4 || p->N > 1290 || (p->N & 1) || p->nflds != 2 ||
-        (p->model != GABE_MODEL_QUADRATIC && p->model != GABE_MODEL_LPHI4) || !(p->L > 0) || !(a0 > 0))
-        return GABE_ERR_PARAM;
+    // the same parameter checks as gabe_create, and the FP64 stencil tiling
+    if (!params_valid(*p, nullptr, 0) || !(a0 > 0) || !std::isfinite(a0)) return GABE_ERR_PARAM;
     const GridPlan g = plan_grid(p->N, p->tile_shape, p->tile_ci);
+    if (g.shape < 0) return GABE_ERR_PARAM;  // no tile divides N (N % 4 != 0)
     const long long nblocks = (long long)g.grid.x * g.grid.y * g.grid.z;
     if (nblocks > kNoAllocMaxBlocks) return GABE_ERR_PARAM;  // scratch too small for this grid
     int dev = 0;
@@ -127,7 +132,8 @@ extern "C" int gabe_energy_noalloc(const gabe_params *p, const double *field0, c
             case 2: e = launch_e0<32, 4>(a, g.grid, s); break;
             case 3: e = launch_e0<16, 8>(a, g.grid, s); break;
             case 4: e = launch_e0<8, 8>(a, g.grid, s); break;
-            default: e = launch_e0<4, 4>(a, g.grid, s); break;
+            case 5: e = launch_e0<4, 4>(a, g.grid, s); break;
+            default: e = cudaErrorInvalidValue; break;
         }
     }
     if (e == cudaSuccess) {

@@ -227,6 +227,10 @@ int gabe_slab_create(const gabe_params *p, const gabe_slab_params *sp, gabe_slab
     }
     // the whole lattice's tile and plane chunk, with the chunks cut from this slab's planes
     GridPlan g = s->f32 ? plan_grid32(N, p->tile_shape, p->tile_ci) : plan_grid(N, p->tile_shape, p->tile_ci);
+    if (g.shape < 0) {
+        serr(s, GABE_ERR_PARAM, "N = %d: no stencil tile divides N", N);
+        return bail(GABE_ERR_PARAM);
+    }
     s->shape = g.shape;
     s->ci = g.ci < s->nloc ? g.ci : s->nloc;
     s->grid = dim3(g.grid.x, g.grid.y, (s->nloc + s->ci - 1) / s->ci);

@@ -11,6 +11,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "kspace.cuh"
 
 namespace gabe {
 
@@ -24,6 +25,7 @@ struct BinArgs {
     int fix_zero;
     // a slab's k-points (slab.cu): F and G hold [..][N][m][N/2+1] with ky = y0 + y; m = 0: all of them
     int m, y0;
+    int gt;                 // G in the transposed order [4][kz][ky][kx] (fftt.cuh); whole lattices only
 };
 
 template <typename T>
@@ -56,7 +58,8 @@ __global__ void __launch_bounds__(256) bin_kernel(BinArgs a) {
         if (ns > 2) {
             // sum_ij |l_ij|^2 with the reference's weights (diagonal 1,
             // off-diagonal 2) = 2 (|l+|^2 + |lx|^2) for a TT tensor
-            const size_t src = (a.quirk && kz == 0) ? idx + (size_t)(N / 2) : idx;
+            const size_t src = a.gt ? g_index(i, j, (a.quirk && kz == 0) ? N / 2 : kz, N, 1)
+                                    : ((a.quirk && kz == 0) ? idx + (size_t)(N / 2) : idx);
             const double pr = (double)G[2 * (2 * M + src)], pi = (double)G[2 * (2 * M + src) + 1];
             const double xr = (double)G[2 * (3 * M + src)], xi = (double)G[2 * (3 * M + src) + 1];
             const double p = 2. * ((pr * pr + pi * pi) + (xr * xr + xi * xi));

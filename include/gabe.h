@@ -88,9 +88,15 @@ enum gabe_flags {
                                    transforms along j and i are the library's column passes (one HBM
                                    pass fewer, but about 8% slower per step at 512^3 on B200: one
                                    block per SM, whose transform phases leave most warps idle) */
-    GABE_FLAG_CUFFT_3D = 64     /* FP32 at N = 512: cuFFT's 3-D plan for the GW sources instead of the
+    GABE_FLAG_CUFFT_3D = 64,    /* FP32 at N = 512: cuFFT's 3-D plan for the GW sources instead of the
                                    library's three-pass r2c (cuFFT's plan is the default at every other
                                    size and precision) */
+    GABE_FLAG_TRANSPOSED_FFT = 128 /* FP32 with N in {64, 128, 256, 512}: the library's transposed three-pass
+                                   transform -- rows along k, then along j, each written transposed so
+                                   that every pass reads whole contiguous lines (bulk copies), and the
+                                   pass along i fused with the TT projection and h/l update, so the
+                                   transformed sources are never written back.  Needs the second source
+                                   buffer whatever GABE_FLAG_NO_OVERLAP says */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two
@@ -149,8 +155,11 @@ int gabe_profile_steps(gabe_handle *h, int nsteps, double ms_out[4]);
  * N = 512 by default, or GABE_FLAG_OWN_FFT): runs its three passes nreps
  * times on the source buffer (in place; the next step rewrites the
  * sources) with CUDA events between them and returns the mean milliseconds
- * of {rows along k, pass along j, pass along i}.  Measurement hook; no
- * reference counterpart. */
+ * of {rows along k, pass along j, pass along i}.  With
+ * GABE_FLAG_TRANSPOSED_FFT: runs nreps full steps (the state advances) with
+ * events around the transform's launches and returns {rows along k, pass
+ * along j, pass along i fused with the k-space update}.  Other handles:
+ * GABE_ERR_STATE.  Measurement hook; no reference counterpart. */
 int gabe_profile_fft_passes(gabe_handle *h, int nreps, double ms_out[3]);
 
 /* The handle's CUDA stream (a cudaStream_t), so callers can order their own
@@ -225,8 +234,13 @@ int gabe_field_slice(gabe_handle *h, int outdim, int skip, double *out, size_t o
  * 32768 blocks' partial sums (about 2 MiB), held by each device that loads
  * the library until exit; a lattice needing more blocks returns
  * GABE_ERR_PARAM.  The first call on a device looks up that array's device
- * address (make it before any stream capture); calls that overlap on the
- * GPU share the array and race.  No counterpart in the reference. */
+ * address (make it before any stream capture) and keeps it for the life of
+ * the process, so the entry point must not be called after a
+ * cudaDeviceReset in the same process; calls that overlap on the GPU share
+ * the array and race.  Parameters are checked as gabe_create checks them
+ * (GABE_ERR_PARAM, also for N % 4 != 0).  The call has no status word: a
+ * state holding NaN or Inf gives NaN or Inf in out4, so check out4.  No
+ * counterpart in the reference. */
 int gabe_energy_noalloc(const gabe_params *p, const double *field0, const double *dfield0, double a0,
                         double *out4, void *stream);
 

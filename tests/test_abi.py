@@ -59,8 +59,9 @@ def test_params_struct_matches_header():
     assert gb.numbins(256) == 222 and gb.numbins(512) == 444 and gb.numbins(1024) == 887
 
 
-@pytest.mark.parametrize("field,value", [("N", 63), ("N", 2), ("nflds", 3), ("expansion", 3), ("expansion", -1),
-                                         ("model", 7), ("precision", 5), ("dt", -1.0), ("gws_on", 2)])
+@pytest.mark.parametrize("field,value", [("N", 63), ("N", 2), ("N", 6), ("N", 1290), ("nflds", 3), ("expansion", 3),
+                                         ("expansion", -1), ("model", 7), ("precision", 5), ("dt", -1.0),
+                                         ("gws_on", 2)])
 def test_create_rejects_bad_params(field, value):
     lib = gb.library()
     p = gb.Params()
@@ -70,6 +71,37 @@ def test_create_rejects_bad_params(field, value):
     rc = lib.gabe_create(ctypes.byref(p), ctypes.byref(h))
     assert rc == 1 and not h.value
     assert lib.gabe_last_error(None)
+
+
+@pytest.mark.parametrize("N,precision", [(6, 0), (10, 0), (1290, 0), (24, 1), (40, 1)])
+def test_create_rejects_lattices_no_stencil_tile_divides(N, precision):
+    """Even N that no stencil tile divides (FP64 tiles need N % 4 == 0, FP32
+    tiles N % 16 == 0) are refused with a message, before any device work."""
+    lib = gb.library()
+    p = gb.Params()
+    lib.gabe_default_params(ctypes.byref(p), N)
+    p.precision = precision
+    h = ctypes.c_void_p()
+    assert lib.gabe_create(ctypes.byref(p), ctypes.byref(h)) == 1 and not h.value
+    assert b"no stencil tile divides N" in lib.gabe_last_error(None)
+
+
+@pytest.mark.parametrize("field,value", [("N", 6), ("N", 1290), ("model", 7), ("dt", float("nan")),
+                                         ("L", float("inf")), ("expansion", 5)])
+def test_energy_noalloc_rejects_bad_params_before_device_work(field, value):
+    """gabe_energy_noalloc checks its parameters as gabe_create does and
+    refuses untileable N; the refusal comes before any CUDA call (the device
+    pointers here are never touched)."""
+    lib = gb.library()
+    p = gb.Params()
+    lib.gabe_default_params(ctypes.byref(p), 32)
+    setattr(p, field, value)
+    dummy = ctypes.c_void_p(0x1000)
+    assert lib.gabe_energy_noalloc(ctypes.byref(p), dummy, dummy, 1.0, dummy, None) == 1
+    p2 = gb.Params()
+    lib.gabe_default_params(ctypes.byref(p2), 32)
+    p2.model, p2.model_c[0] = gb.MODEL_QUADRATIC, 0.0  # mphi = 0: the model constants divide by it
+    assert lib.gabe_energy_noalloc(ctypes.byref(p2), dummy, dummy, 1.0, dummy, None) == 1
 
 
 def test_null_handles_are_errors_not_crashes():
@@ -101,11 +133,16 @@ def test_bench_counts_each_fft_pass_and_the_step_once():
     b = bench.algorithmic_bytes(N, w, True)
     assert b["fft_rows"] == b["fft"] == 10 * (n3 + 2 * M) * w
     assert b["fft_j"] == b["fft_i"] == 10 * 4 * M * w
-    step = sum(v for k, v in b.items() if k not in ("fft_rows", "fft_j", "fft_i"))
+    assert b["fft_i_kspace"] == b["kspace"] == 36 * M * w
+    step = sum(v for k, v in b.items() if k in ("stage1", "fft", "kspace", "stage2"))
     assert step == (56 + 32) * n3 + 40 * (n3 + 2 * M) + 144 * M
     assert abs(step / n3 - 240.4) < 0.1
     assert bench.reference_formulation_bytes(w, True) == 336
     assert set(bench.algorithmic_bytes(N, w, False)) == {"stage1", "stage2"}
+    # the ensemble's step counts the transforms once (one pass), not once per pass on top
+    for n in (32, 48, 64, 96, 128):
+        n3e, Me = n ** 3, n * n * (n // 2 + 1)
+        assert bench.ensemble_step_bytes(n) == (56 + 32) * n3e + 40 * (n3e + 2 * Me) + 144 * Me
     t256 = bench.traffic_scaled("fft_i", "fp32", 256)
     t512 = bench.traffic_scaled("fft_i", "fp32", 512)
     assert t256 and abs(t512 / t256 - M / (256 * 256 * 129)) < 1e-12

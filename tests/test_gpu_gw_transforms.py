@@ -6,7 +6,10 @@ The reference form of the comparisons below keeps the reference's structure
 195, here cuFFT's 3-D plan: the default below N = 512, GABE_FLAG_CUFFT_3D at
 512) and a separate k-space pass (TT projection + both RK2 stages of h, l).
 With FP32 storage and N in {64, 128, 256, 512}: GABE_FLAG_OWN_FFT does the
-3-D r2c with the library's own three-pass FFT (the default at 512); GABE_FLAG_FUSED_ROWS has sweep A write the sources already
+3-D r2c with the library's own three-pass FFT (the default at 512);
+GABE_FLAG_TRANSPOSED_FFT runs the transposed three passes (fftt.cuh), the last
+one fused with the k-space update and the amplitudes kept transposed;
+GABE_FLAG_FUSED_ROWS has sweep A write the sources already
 transformed along k (whole rows per block) and runs the library's passes along
 j and i; GABE_FLAG_FUSED_KSPACE transforms the ten source arrays
 over each (j, k) plane only (cuFFT's batched 2-D plan, or with
@@ -27,9 +30,9 @@ pytestmark = pytest.mark.gpu
 
 FFT_TOL = 1e-5  # relative, FP32 transforms of ~1e5..1e8 terms
 FORMS = {"own": gb.FLAG_OWN_FFT, "fused": gb.FLAG_FUSED_KSPACE, "plane": gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT,
-         "rows": gb.FLAG_FUSED_ROWS}
+         "rows": gb.FLAG_FUSED_ROWS, "trans": gb.FLAG_TRANSPOSED_FFT}
 LAUNCHES = {gb.FLAG_OWN_FFT: 6, gb.FLAG_FUSED_KSPACE: 3, gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT: 4,
-            gb.FLAG_FUSED_ROWS: 5, gb.FLAG_CUFFT_3D: 3, 0: 3}
+            gb.FLAG_FUSED_ROWS: 5, gb.FLAG_TRANSPOSED_FFT: 5, gb.FLAG_CUFFT_3D: 3, 0: 3}
 
 
 def _norm_rel(got, want):
@@ -113,3 +116,29 @@ def test_gw_transforms_512_match_cufft_3d():
     for name in FORMS:
         assert np.all(np.isfinite(specs[name]))
         assert _gw_cols_close(specs[name], specs["3d"]) <= FFT_TOL, name
+
+
+def test_transposed_form_keeps_an_uploaded_gw_state():
+    """The transposed form stores the amplitudes as [4][kz][ky][kx]: an
+    uploaded TT state (the oracle's, after a few steps with GWs) must
+    download unchanged, and stepping it must match cuFFT's form."""
+    from oracle import pyoracle as po
+
+    cfg = po.Config(N=64, model=po.MODEL_LPHI4, gws=1)
+    st = po.init_state(cfg)
+    po.step(st, 4)
+    c0, c1, *_ = po.model_constants(cfg.model)
+    out = {}
+    for name, flags in (("trans", gb.FLAG_TRANSPOSED_FFT), ("3d", gb.FLAG_CUFFT_3D)):
+        with gb.Lattice(cfg.N, L=cfg.L, dt=cfg.dt, gws=True, model=cfg.model, model_c=(c0, c1),
+                        precision=gb.FP32, flags=flags) as lat:
+            lat.upload_state(st.field[0], st.dfield[0], st.h[0], st.l[0], a0=st.sc.a[0], adot0=st.sc.adot[0])
+            _, _, h, l = lat.download_state()
+            assert _norm_rel(h, st.h[0]) <= 1e-6 and _norm_rel(l, st.l[0]) <= 1e-6
+            lat.step(3)
+            out[name] = (lat.download_state(), lat.spec_out())
+    (f0, d0, h0, l0), s0 = out["trans"]
+    (f1, d1, h1, l1), s1 = out["3d"]
+    np.testing.assert_array_equal(f0, f1)
+    assert _norm_rel(h0, h1) <= FFT_TOL and _norm_rel(l0, l1) <= FFT_TOL
+    assert _gw_cols_close(s0, s1) <= FFT_TOL

@@ -23,7 +23,10 @@ def _tol(name, want, rho):
     return 1e-12 * (abs(rho) if name == "grad" else abs(want))
 
 
-def test_energy_noalloc_matches_handle_energies_twice():
+# the default tile plan, and 4x4 tiles with one plane per block (8 x 8 x 32 =
+# 2048 blocks): another arm of the entry point's tile dispatch, many planes
+@pytest.mark.parametrize("tile_shape,tile_ci", [(-1, 0), (5, 1)])
+def test_energy_noalloc_matches_handle_energies_twice(tile_shape, tile_ci):
     import torch
 
     lib = gb.library()
@@ -33,7 +36,8 @@ def test_energy_noalloc_matches_handle_energies_twice():
     po.step(st, 20)
     c0, c1, *_ = po.model_constants(cfg.model)
     for state in (first, st):  # two calls in a row, different states
-        with gb.Lattice(cfg.N, L=cfg.L, dt=cfg.dt, model=cfg.model, model_c=(c0, c1), device=0) as lat:
+        with gb.Lattice(cfg.N, L=cfg.L, dt=cfg.dt, model=cfg.model, model_c=(c0, c1), device=0,
+                        tile_shape=tile_shape, tile_ci=tile_ci) as lat:
             lat.upload_state(state.field[0], state.dfield[0], a0=state.sc.a[0], adot0=state.sc.adot[0])
             want = lat.calc_energy()
             params = lat.params
