@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-slab", action="store_true", help="skip the slab leg (one lattice split over the ranks)")
     ap.add_argument("--no-energy", action="store_true", help="skip the energy-conservation block (64^3, rank 0)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the FP32-vs-FP64 accuracy block on the headline lattice (rank 0)")
+    ap.add_argument("--acc-steps", type=int, default=1000, help="steps of the accuracy block")
+    ap.add_argument("--acc-dt-div", type=float, default=40.0, help="accuracy block's dt = dx / this (stable RK2)")
     ap.add_argument("--slab-N", type=int, default=512, help="lattice of the slab leg")
     ap.add_argument("--slab-steps", type=int, default=20)
     ap.add_argument("--ens-lattices", type=int, default=256)
@@ -414,6 +418,30 @@ def energy_conservation(N: int = 64, steps: int = 500, dt: float = 0.01, device:
             "spectra_max_rel_diff_fp32_vs_fp64": {"fields": max_rel([1, 2, 3, 4]), "gw": max_rel([5, 6])}}
 
 
+def accuracy_block(args, device: int) -> dict:
+    """FP32 storage against the FP64 path on the headline lattice with GWs,
+    from one initial state, at a dt inside RK2's stability region
+    (gabe_b200.accuracy): the largest relative differences of a, adot, kin,
+    pot, grad, rho over every step, the continuity residual eps(t) of both
+    runs, and the per-bin differences of every spectrum column at four
+    output times.  Outside the timed regions."""
+    import torch
+
+    from gabe_b200.accuracy import compare_precisions
+    from gabe_b200.ic import random_state
+
+    N, L = args.N, 20.0
+    f, d, a0, ad0 = random_state(N, seed=20261204, device="cuda")
+    f, d = f.cpu().numpy(), d.cpu().numpy()
+    torch.cuda.empty_cache()
+    K = args.acc_steps
+    rep = compare_precisions(f, d, a0, ad0, N=N, steps=K, dt=L / N / args.acc_dt_div, L=L, gws=True,
+                             spectra_every=max(1, K // 4), device=device, flags32=args.lattice_flags)
+    rep["workload"] = (f"{N}^3 lattice, GWs on, dt = dx/{args.acc_dt_div:g}, {K} steps, FP32 storage and FP64 "
+                       f"from one initial state, scalars compared every step, spectra every {max(1, K // 4)} steps")
+    return rep
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -595,6 +623,11 @@ def main():
             line["energy_conservation"] = energy_conservation(device=local)
         except Exception as e:  # noqa: BLE001 -- the headline line is still printed
             line["energy_conservation"] = {"error": f"{type(e).__name__}: {e}"[:300]}
+    if rank == 0 and not args.no_accuracy:
+        try:
+            line["accuracy"] = accuracy_block(args, local)
+        except Exception as e:  # noqa: BLE001 -- the headline line is still printed
+            line["accuracy"] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         v, info = cpu_reference_sample(args.ref_N or N, max(3, args.cpu_baseline_steps), warm=1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],

@@ -109,6 +109,8 @@ def library():
     L.gabe_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
     L.gabe_energy_noalloc.argtypes = [ctypes.POINTER(Params), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double,
                                       ctypes.c_void_p, ctypes.c_void_p]
+    L.gabe_save_state.argtypes = [H, ctypes.c_char_p]
+    L.gabe_load_state.argtypes = [H, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -282,6 +284,20 @@ class Lattice:
         self._check(library().gabe_scalars(self._h, out))
         names = ("a", "adot", "edkin", "edpot", "edgrad", "edrho")
         return {n: (out[2 * i], out[2 * i + 1]) for i, n in enumerate(names)}
+
+    # -- checkpoint / restart ---------------------------------------------
+    def save(self, path: str) -> None:
+        """Checkpoint to a gabe_dump.h file with the library's restart block
+        (gabe_save_state)."""
+        self._check(library().gabe_save_state(self._h, os.fsencode(path)))
+
+    def load(self, path: str) -> bool:
+        """Loads a gabe_dump.h file (gabe_load_state): True when its restart
+        block became the state (bit-exact continuation), False when its FP64
+        arrays were uploaded as an initial state."""
+        restored = ctypes.c_int(0)
+        self._check(library().gabe_load_state(self._h, os.fsencode(path), ctypes.byref(restored)))
+        return bool(restored.value)
 
     # -- analysis ---------------------------------------------------------
     def spec_out(self) -> np.ndarray:

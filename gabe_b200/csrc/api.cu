@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/gabe.h"
+#include "../../include/gabe_dump.h"
 #include "launch.h"
 
 using namespace gabe;
@@ -1007,6 +1008,174 @@ int gabe_spectra_from_sums(const gabe_params *p, double edrho0, const double *su
         }
     }
     return GABE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoint / restart (gabe_dump.h files with the restart block)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() {
+        if (f) fclose(f);
+    }
+};
+
+// Device bytes -> file through a pinned-free host bounce buffer of `chunk` bytes.
+int write_device(gabe_handle *h, FILE *f, const void *dev, size_t bytes, std::vector<char> &bounce) {
+    for (size_t o = 0; o < bytes; o += bounce.size()) {
+        const size_t n = bytes - o < bounce.size() ? bytes - o : bounce.size();
+        CK(h, cudaMemcpy(bounce.data(), static_cast<const char *>(dev) + o, n, cudaMemcpyDeviceToHost));
+        if (fwrite(bounce.data(), 1, n, f) != n) return set_err(h, GABE_ERR_PARAM, "checkpoint write failed");
+    }
+    return GABE_OK;
+}
+
+int read_device(gabe_handle *h, FILE *f, void *dev, size_t bytes, std::vector<char> &bounce) {
+    for (size_t o = 0; o < bytes; o += bounce.size()) {
+        const size_t n = bytes - o < bounce.size() ? bytes - o : bounce.size();
+        if (fread(bounce.data(), 1, n, f) != n) return set_err(h, GABE_ERR_PARAM, "checkpoint file is truncated");
+        CK(h, cudaMemcpy(static_cast<char *>(dev) + o, bounce.data(), n, cudaMemcpyHostToDevice));
+    }
+    return GABE_OK;
+}
+
+void fill_restart(const gabe_handle *h, gabe_restart_header *r) {
+    std::memset(r, 0, sizeof(*r));
+    std::memcpy(r->magic, GABE_RESTART_MAGIC, 8);
+    r->precision = h->p.precision;
+    r->gw_layout = h->fftt ? 1 : 0;
+    r->expansion = h->p.expansion;
+    r->tile_shape = h->shape;
+    r->tile_ci = h->ci;
+    r->e0_stale = h->e0_stale ? 1 : 0;
+    r->scalar_bytes = (int32_t)sizeof(DevScalars);
+    r->elem_bytes = (int32_t)h->esz;
+    r->field_bytes = (int64_t)(2 * h->n3 * h->esz);
+    r->gw_bytes = h->p.gws_on ? (int64_t)(8 * h->M * h->esz) : 0;
+}
+
+}  // namespace
+
+int gabe_save_state(gabe_handle *h, const char *path) {
+    if (!h) return GABE_ERR_PARAM;
+    if (!path) return set_err(h, GABE_ERR_PARAM, "path is NULL");
+    if (!h->uploaded) return set_err(h, GABE_ERR_STATE, "save before upload");
+    CK(h, cudaSetDevice(h->dev));
+    DevScalars sc;
+    int rc = read_scalars(h, &sc);  // synchronises; reduces the stage-0 energies if they are stale
+    if (rc) return rc;
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) return set_err(h, GABE_ERR_PARAM, "cannot open %s for writing", path);
+    gabe_dump_header hd;
+    gabe_dump_header_init(&hd, h->N, 2, h->p.gws_on, 8, h->p.model);
+    hd.step = sc.step;
+    hd.t = (double)sc.step * h->p.dt;
+    hd.L = h->p.L;
+    hd.dt = h->p.dt;
+    for (int s = 0; s < 2; s++) {
+        hd.a[s] = sc.a[s];
+        hd.adot[s] = sc.adot[s];
+        hd.edkin[s] = sc.edkin[s];
+        hd.edpot[s] = sc.edpot[s];
+        hd.edgrad[s] = sc.edgrad[s];
+        hd.edrho[s] = sc.edrho[s];
+    }
+    if (fwrite(&hd, sizeof(hd), 1, fc.f) != 1) return set_err(h, GABE_ERR_PARAM, "checkpoint write failed");
+    // the portable part: FP64 arrays in the reference's layout, one at a time
+    {
+        const size_t nf = 2 * h->n3, ng = gabe_dump_gw_count(h->N);
+        std::vector<double> buf(h->p.gws_on && ng > nf ? ng : nf);
+        for (int a = 0; a < (h->p.gws_on ? 4 : 2); a++) {
+            double *ptr[4] = {nullptr, nullptr, nullptr, nullptr};
+            ptr[a] = buf.data();
+            rc = gabe_download_state(h, ptr[0], ptr[1], ptr[2], ptr[3]);
+            if (rc) return rc;
+            const size_t n = a < 2 ? nf : ng;
+            if (fwrite(buf.data(), sizeof(double), n, fc.f) != n)
+                return set_err(h, GABE_ERR_PARAM, "checkpoint write failed");
+        }
+    }
+    // the restart block: the device state as it is
+    gabe_restart_header r;
+    fill_restart(h, &r);
+    if (fwrite(&r, sizeof(r), 1, fc.f) != 1 || fwrite(&sc, sizeof(sc), 1, fc.f) != 1)
+        return set_err(h, GABE_ERR_PARAM, "checkpoint write failed");
+    std::vector<char> bounce((size_t)64 << 20);
+    if ((rc = write_device(h, fc.f, h->X[h->cur], (size_t)r.field_bytes, bounce)) ||
+        (rc = write_device(h, fc.f, h->D[h->cur], (size_t)r.field_bytes, bounce)))
+        return rc;
+    if (r.gw_bytes && (rc = write_device(h, fc.f, h->G, (size_t)r.gw_bytes, bounce))) return rc;
+    FILE *f = fc.f;
+    fc.f = nullptr;
+    if (fclose(f) != 0) return set_err(h, GABE_ERR_PARAM, "checkpoint write failed");
+    return GABE_OK;
+}
+
+int gabe_load_state(gabe_handle *h, const char *path, int *restored) {
+    if (!h) return GABE_ERR_PARAM;
+    if (restored) *restored = 0;
+    if (!path) return set_err(h, GABE_ERR_PARAM, "path is NULL");
+    CK(h, cudaSetDevice(h->dev));
+    h->err.clear();
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return set_err(h, GABE_ERR_PARAM, "cannot open %s", path);
+    gabe_dump_header hd;
+    if (fread(&hd, sizeof(hd), 1, fc.f) != 1 || std::memcmp(hd.magic, GABE_DUMP_MAGIC, 8) != 0 ||
+        hd.version != GABE_DUMP_VERSION || hd.elem_bytes != 8)
+        return set_err(h, GABE_ERR_PARAM, "%s is not a gabe_dump.h state dump", path);
+    if (hd.N != h->N || hd.nflds != 2)
+        return set_err(h, GABE_ERR_PARAM, "dump holds an N = %d lattice with %d fields; the handle's N is %d", hd.N,
+                       hd.nflds, h->N);
+    if (hd.L != h->p.L || hd.dt != h->p.dt)
+        return set_err(h, GABE_ERR_PARAM, "dump was written with L = %g, dt = %g; the handle has L = %g, dt = %g",
+                       hd.L, hd.dt, h->p.L, h->p.dt);
+    if (hd.model != h->p.model) return set_err(h, GABE_ERR_PARAM, "dump model %d != handle model %d", hd.model, h->p.model);
+    const size_t nf = 2 * h->n3, ng = gabe_dump_gw_count(h->N);
+    const long long payload = (long long)(2 * nf + (hd.gws ? 2 * ng : 0)) * 8;
+    // the restart block, if the file has one that fits this handle
+    gabe_restart_header r;
+    gabe_restart_header want;
+    fill_restart(h, &want);
+    bool native = false;
+    if (fseeko(fc.f, (off_t)(sizeof(hd) + payload), SEEK_SET) == 0 && fread(&r, sizeof(r), 1, fc.f) == 1 &&
+        std::memcmp(r.magic, GABE_RESTART_MAGIC, 8) == 0) {
+        native = r.precision == want.precision && r.gw_layout == want.gw_layout && r.expansion == want.expansion &&
+                 r.scalar_bytes == want.scalar_bytes && r.elem_bytes == want.elem_bytes &&
+                 r.field_bytes == want.field_bytes && r.gw_bytes == want.gw_bytes && hd.gws == h->p.gws_on;
+    }
+    if (native) {
+        DevScalars sc;
+        if (fread(&sc, sizeof(sc), 1, fc.f) != 1) return set_err(h, GABE_ERR_PARAM, "checkpoint file is truncated");
+        sc.status = 0;
+        CK(h, cudaStreamSynchronize(h->stream));
+        std::vector<char> bounce((size_t)64 << 20);
+        int rc;
+        if ((rc = read_device(h, fc.f, h->X[0], (size_t)r.field_bytes, bounce)) ||
+            (rc = read_device(h, fc.f, h->D[0], (size_t)r.field_bytes, bounce)))
+            return rc;
+        if (r.gw_bytes && (rc = read_device(h, fc.f, h->G, (size_t)r.gw_bytes, bounce))) return rc;
+        CK(h, cudaMemcpy(h->sc, &sc, sizeof(sc), cudaMemcpyHostToDevice));
+        h->cur = 0;
+        h->e0_stale = r.e0_stale != 0;
+        h->uploaded = true;
+        if (restored) *restored = 1;
+        return GABE_OK;
+    }
+    // the portable part: upload as an initial state (the reference harness's dumps have no restart block)
+    if (fseeko(fc.f, (off_t)sizeof(hd), SEEK_SET) != 0) return set_err(h, GABE_ERR_PARAM, "seek failed in %s", path);
+    std::vector<double> f(nf), d(nf), hh, ll;
+    if (fread(f.data(), 8, nf, fc.f) != nf || fread(d.data(), 8, nf, fc.f) != nf)
+        return set_err(h, GABE_ERR_PARAM, "%s is truncated", path);
+    if (hd.gws && h->p.gws_on) {
+        hh.resize(ng);
+        ll.resize(ng);
+        if (fread(hh.data(), 8, ng, fc.f) != ng || fread(ll.data(), 8, ng, fc.f) != ng)
+            return set_err(h, GABE_ERR_PARAM, "%s is truncated", path);
+    }
+    return gabe_upload_state(h, f.data(), d.data(), hh.empty() ? nullptr : hh.data(), ll.empty() ? nullptr : ll.data(),
+                             hd.a[0], hd.adot[0]);
 }
 
 const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }

@@ -179,6 +179,24 @@ int gabe_scalars(gabe_handle *h, double out12[12]);
 /* Copies stage 0 back to the host; any pointer may be NULL. */
 int gabe_download_state(gabe_handle *h, double *field0, double *dfield0, double *h0, double *l0);
 
+/* Checkpoint of the current state to `path` (synchronises).  The file is a
+ * gabe_dump.h state dump -- the FP64 arrays in the reference's layout and
+ * the scalars, readable by anything that reads that format (the oracle,
+ * the reference harness's --ic) -- followed by a restart block holding the
+ * device state as the library keeps it.  The reference has no restartable
+ * output (its slices are sampled %e text, g2output.cpp:25-68); this
+ * replaces a restart from a reference initial-condition dump. */
+int gabe_save_state(gabe_handle *h, const char *path);
+
+/* Loads a gabe_dump.h file written for this handle's N, L, dt and model.
+ * If it carries a restart block of the same precision, amplitude layout and
+ * expansion type (a gabe_save_state file of an equal handle), that block
+ * becomes the state and the run continues bit for bit (with the same tile
+ * plan; *restored = 1).  Otherwise its FP64 arrays are uploaded as
+ * gabe_upload_state does (*restored = 0): e.g. the dumps of the reference
+ * harness.  restored may be NULL. */
+int gabe_load_state(gabe_handle *h, const char *path, int *restored);
+
 /* Number of native |k| bins, (int)(sqrt(3) N/2 + 1) (g2spectra.cpp:31). */
 int gabe_spectra_numbins(int N);
 

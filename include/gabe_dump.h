@@ -111,6 +111,33 @@ static inline int gabe_dump_read(const char *path, gabe_dump_header *hd, double 
     return bad;
 }
 
+/* Restart block.  A checkpoint written by the library (gabe_save_state)
+ * is a dump as above -- any reader of the format takes its FP64 arrays --
+ * followed by this header, the library's device scalar block
+ * (scalar_bytes bytes), and the device arrays as the library holds them:
+ * field and momenta of stage 0 (field_bytes each: FP64 values, or for
+ * FP32 storage the FP32 fluctuations about the homogeneous trajectory kept
+ * in the scalar block) and, with GWs, the four TT amplitudes h+, hx, l+,
+ * lx (gw_bytes; complex, [4][i][j][kz] for gw_layout 0 or [4][kz][j][i]
+ * for gw_layout 1).  Loading the block into a handle of the same precision,
+ * amplitude layout and tile plan continues the run bit for bit. */
+#define GABE_RESTART_MAGIC "GABERST1"
+
+typedef struct {
+    char magic[8];
+    int32_t precision;      /* enum gabe_precision of the writer */
+    int32_t gw_layout;      /* 0 [4][i][j][kz], 1 [4][kz][j][i] */
+    int32_t expansion;
+    int32_t tile_shape, tile_ci;
+    int32_t e0_stale;       /* the stage-0 energies of the scalar block were not yet reduced */
+    int32_t scalar_bytes;
+    int32_t elem_bytes;     /* 8 FP64, 4 FP32 storage */
+    int64_t field_bytes, gw_bytes;
+    char reserved[72];
+} gabe_restart_header;
+
+typedef char gabe_restart_header_is_128_bytes[(sizeof(gabe_restart_header) == 128) ? 1 : -1];
+
 #ifdef __cplusplus
 }
 #endif
