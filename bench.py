@@ -330,6 +330,7 @@ def ensemble_leg(args, rank: int, world: int, local: int, dist, barrier, max_ove
     logs, cnt, _ = ens.log_spectra()
     local_rows = np.concatenate([logs.reshape(len(mine), -1), sc], axis=1)
     launches = ens.launches_per_step
+    graph_active = ens.graph_active
     dev_bytes = ens.device_bytes
     ens.close()
     torch.cuda.empty_cache()
@@ -351,6 +352,7 @@ def ensemble_leg(args, rank: int, world: int, local: int, dist, barrier, max_ove
         "step_achieved_gbs": algo / (ms_steps / K / 1e3) / 1e9,
         "ms_init": ms_init,
         "gpu_launches_per_step": launches,
+        "graph_active": graph_active,
         "device_bytes_rank0": dev_bytes,
     }
     if full is not None:
@@ -544,6 +546,7 @@ def main():
         e1.synchronize()
         ms_e2e = max_over_ranks(e0.elapsed_time(e1))
         legs[name] = {"ms": ms, "ms_e2e": ms_e2e, "phases": phases, "energies": en, "finite": finite,
+                      "graph_active": lat.graph_active,
                       "nonfinite_e2e": nonfinite_e2e, "device_bytes": lat.device_bytes,
                       "launches_per_step": lat.launches_per_step,
                       "tile": [lat.params.tile_shape, lat.params.tile_ci]}
@@ -608,6 +611,7 @@ def main():
         "clocks": clocks,
         "finite": L32["finite"],
         "tile": {"fp32": L32["tile"], "fp64": legs.get("fp64", {}).get("tile")},
+        "graph_active": L32["graph_active"],
         "device_bytes": L32["device_bytes"],
     }
     line.update(extra)

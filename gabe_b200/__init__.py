@@ -104,6 +104,7 @@ def library():
     L.gabe_device_bytes.argtypes = [H]
     L.gabe_device_bytes.restype = ctypes.c_size_t
     L.gabe_launches_per_step.argtypes = [H]
+    L.gabe_graph_active.argtypes = [H]
     L.gabe_profile_steps.argtypes = [H, ctypes.c_int, _dp]
     L.gabe_profile_fft_passes.argtypes = [H, ctypes.c_int, _dp]
     L.gabe_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
@@ -202,6 +203,11 @@ class Lattice:
     @property
     def launches_per_step(self) -> int:
         return library().gabe_launches_per_step(self._h)
+
+    @property
+    def graph_active(self) -> int:
+        """1: steps replay the captured CUDA graphs; 0: direct launches; -1: before the first step."""
+        return library().gabe_graph_active(self._h)
 
     # -- state ------------------------------------------------------------
     def upload_state(self, field0, dfield0, h0=None, l0=None, *, a0: float = 1.0, adot0: float):
@@ -371,6 +377,7 @@ def _ens_lib():
         L.gabe_ensemble_stream.argtypes = [E]
         L.gabe_ensemble_stream.restype = ctypes.c_void_p
         L.gabe_ensemble_launches_per_step.argtypes = [E]
+        L.gabe_ensemble_graph_active.argtypes = [E]
         L._ens_ready = True
     return L
 
@@ -460,6 +467,11 @@ class Ensemble:
     @property
     def launches_per_step(self) -> int:
         return _ens_lib().gabe_ensemble_launches_per_step(self._h)
+
+    @property
+    def graph_active(self) -> int:
+        """1: steps replay the captured CUDA graph; 0: direct launches; -1: before the first step."""
+        return _ens_lib().gabe_ensemble_graph_active(self._h)
 
     def init(self):
         self._check(_ens_lib().gabe_ensemble_init(self._h))

@@ -1182,6 +1182,11 @@ const char *gabe_last_error(const gabe_handle *h) { return h ? h->err.c_str() : 
 
 size_t gabe_device_bytes(const gabe_handle *h) { return h ? h->dev_bytes : 0; }
 
+int gabe_graph_active(const gabe_handle *h) {
+    if (!h) return -GABE_ERR_PARAM;
+    return h->graph_tried ? (h->graph_ok ? 1 : 0) : -1;
+}
+
 int gabe_launches_per_step(const gabe_handle *h) {
     return h ? (h->evolve_gw ? (h->own_fft ? 6 : (h->rows_fused || h->fftt) ? 5 : h->plane_fft ? 4 : 3) : 2) : 0;
 }

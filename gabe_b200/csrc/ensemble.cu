@@ -631,4 +631,9 @@ void *gabe_ensemble_stream(const gabe_ensemble *e) { return e ? (void *)e->strea
 
 int gabe_ensemble_launches_per_step(const gabe_ensemble *e) { return e ? (e->gws ? 3 : 2) : 0; }
 
+int gabe_ensemble_graph_active(const gabe_ensemble *e) {
+    if (!e) return GABE_ERR_PARAM * -1;
+    return e->graph_tried ? (e->graph_ok ? 1 : 0) : -1;
+}
+
 }  // extern "C"

@@ -272,6 +272,12 @@ size_t gabe_device_bytes(const gabe_handle *h);
 /* Kernel launches one step enqueues (for launch accounting). */
 int gabe_launches_per_step(const gabe_handle *h);
 
+/* 1 when gabe_step replays the captured CUDA graphs of the step, 0 when it
+ * launches the kernels one by one (GABE_FLAG_NO_GRAPH, or the capture
+ * failed), -1 before the first gabe_step (the graphs are captured then),
+ * -GABE_ERR_PARAM for a NULL handle.  No reference counterpart. */
+int gabe_graph_active(const gabe_handle *h);
+
 /* ------------------------------------------------------------------------
  * Batched ensemble: many independent lattices of uneven size, coupling,
  * fluctuation amplitude and seed, evolved together in FP32 storage with FP64
@@ -355,6 +361,9 @@ size_t gabe_ensemble_device_bytes(const gabe_ensemble *e);
  * not counted). */
 void *gabe_ensemble_stream(const gabe_ensemble *e);
 int gabe_ensemble_launches_per_step(const gabe_ensemble *e);
+
+/* As gabe_graph_active, for the ensemble's step. */
+int gabe_ensemble_graph_active(const gabe_ensemble *e);
 
 /* ------------------------------------------------------------------------
  * One slab of a lattice split along i over several processes (one GPU each).

@@ -88,7 +88,10 @@ def test_ensemble_graph_and_direct_launches_agree():
     for flags in (0, gb.FLAG_NO_GRAPH):
         with gb.Ensemble(sizes, g, amp, seeds, nlog=16, tiles=None, flags=flags) as ens:
             ens.init()
+            assert ens.graph_active == -1  # captured at the first step
             ens.step(5)
+            # the graph path is reported, not silently lost
+            assert ens.graph_active == (0 if flags else 1)
             out.append((ens.scalars(), ens.download(0)))
     np.testing.assert_array_equal(out[0][0], out[1][0])
     for a, b in zip(out[0][1], out[1][1]):
