@@ -12,7 +12,10 @@
 // nothing but coalescing.  64x64 output tiles, 16-deep k slices in shared
 // memory, 4x4 outputs per thread, FP32 FMA accumulation.  Activations are
 // read as BF16 (or FP32) and widened on the way into shared memory; weights
-// are FP32.
+// are FP32.  With BF16 activations the forward of every layer after the
+// first runs on tensor cores instead (tc::gemm_tc_kernel, BF16 weight
+// copies); the first layer (a handful of inputs) and the backward products
+// stay on this kernel.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -163,6 +166,152 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core forward of the layers fed by BF16 activations (all but the
+// first): Z = H W + b with H [M][K] BF16 and the layer's weights as a BF16
+// copy kept transposed, Wt [N][K] (k contiguous), multiplied by
+// mma.sync.m16n8k16 (BF16 x BF16, FP32 accumulation).  128 x 128 output
+// tiles, 8 warps of 64 x 32, 32-deep k slices double-buffered in shared
+// memory by cp.async, fragments by ldmatrix; rows padded to 40 BF16 so
+// that the eight 16-byte rows of each ldmatrix hit distinct banks.
+// Epilogue as the SIMT kernel's: bias and SiLU into Z and H (BF16), or bias
+// into the FP32 output.
+// ---------------------------------------------------------------------------
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 32, LDS = BK + 8, T = 256;
+
+struct Args {
+    int M, N, K;
+    const bf16 *A;    // [M][K]
+    const bf16 *Wt;   // [N][K]
+    const float *bias;
+    bf16 *Z;          // EPI_HIDDEN: pre-activation (may be null)
+    void *C;          // EPI_HIDDEN: H (BF16); EPI_OUT: y (FP32), [M][N]
+};
+
+__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp16(void *s, const void *g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr(s)), "l"(g) : "memory");
+}
+
+__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], const void *p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(saddr(p)));
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+        "{%0, %1, %2, %3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(T) gemm_tc_kernel(Args g) {
+    __shared__ __align__(16) bf16 As[2][BM][LDS];
+    __shared__ __align__(16) bf16 Bs[2][BN][LDS];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps: 64 rows x 32 columns each
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nk = g.K / BK;
+    // one 16-byte piece (8 BF16) of a 128 x 32 tile per thread and round
+    auto load = [&](int st, int k0) {
+#pragma unroll
+        for (int r = 0; r < 2; r++) {
+            const int idx = tid + r * T, row = idx >> 2, c8 = (idx & 3) * 8;
+            const int gm = m0 + row, gn = n0 + row;
+            if (gm < g.M) cp16(&As[st][row][c8], g.A + (long long)gm * g.K + k0 + c8);
+            else *reinterpret_cast<uint4 *>(&As[st][row][c8]) = make_uint4(0, 0, 0, 0);
+            if (gn < g.N) cp16(&Bs[st][row][c8], g.Wt + (long long)gn * g.K + k0 + c8);
+            else *reinterpret_cast<uint4 *>(&Bs[st][row][c8]) = make_uint4(0, 0, 0, 0);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    float acc[4][4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
+    load(0, 0);
+    for (int kc = 0; kc < nk; kc++) {
+        const int st = kc & 1;
+        if (kc + 1 < nk) {
+            load(st ^ 1, (kc + 1) * BK);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < BK / 16; ks++) {
+            uint32_t a[4][4], b[2][4];
+#pragma unroll
+            for (int mf = 0; mf < 4; mf++)
+                ldsm4(a[mf], &As[st][wm * 64 + mf * 16 + (lane & 7) + ((lane >> 3) & 1) * 8][ks * 16 + (lane >> 4) * 8]);
+#pragma unroll
+            for (int nb = 0; nb < 2; nb++)
+                ldsm4(b[nb], &Bs[st][wn * 32 + nb * 16 + (lane & 7) + (lane >> 4) * 8][ks * 16 + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+            for (int mf = 0; mf < 4; mf++)
+#pragma unroll
+                for (int nf = 0; nf < 4; nf++)
+                    mma_bf16(acc[mf][nf], a[mf], b[nf >> 1][(nf & 1) * 2], b[nf >> 1][(nf & 1) * 2 + 1]);
+        }
+        __syncthreads();  // stage st is refilled by the next round's load
+    }
+    const int gr = lane >> 2, gc = (lane & 3) * 2;
+#pragma unroll
+    for (int mf = 0; mf < 4; mf++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int m = m0 + wm * 64 + mf * 16 + gr + 8 * h;
+            if (m >= g.M) continue;
+#pragma unroll
+            for (int nf = 0; nf < 4; nf++) {
+                const int n = n0 + wn * 32 + nf * 8 + gc;
+                if (n >= g.N) continue;
+                const float z0 = acc[mf][nf][2 * h] + g.bias[n], z1 = acc[mf][nf][2 * h + 1] + g.bias[n + 1];
+                const long long o = (long long)m * g.N + n;
+                if constexpr (EPI == EPI_HIDDEN) {
+                    if (g.Z) *reinterpret_cast<__nv_bfloat162 *>(g.Z + o) = __floats2bfloat162_rn(z0, z1);
+                    *reinterpret_cast<__nv_bfloat162 *>(static_cast<bf16 *>(g.C) + o) =
+                        __floats2bfloat162_rn(silu(z0), silu(z1));
+                } else {
+                    *reinterpret_cast<float2 *>(static_cast<float *>(g.C) + o) = make_float2(z0, z1);
+                }
+            }
+        }
+}
+
+// BF16 transposed copies Wt_l [N][K] of the weights W_l [K][N] of layers
+// 1 .. nl-1 (the layers the tensor-core forward runs).
+struct WtTable {
+    int nl;
+    long long offW[17], offWt[17];
+    int K[17], N[17];
+};
+
+__global__ void weights_bf16t_kernel(const float *params, bf16 *wt, WtTable t) {
+    for (int l = 1; l < t.nl; l++) {
+        const long long n = (long long)t.K[l] * t.N[l];
+        const float *W = params + t.offW[l];
+        bf16 *Wt = wt + t.offWt[l];
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+             i += (long long)gridDim.x * blockDim.x) {
+            const int nn = (int)(i / t.K[l]), k = (int)(i % t.K[l]);
+            Wt[i] = __float2bfloat16_rn(W[(long long)k * t.N[l] + nn]);
+        }
+    }
+}
+
+}  // namespace tc
+
 // dW = sum over splits of the partial products, db = sum of the partial
 // column sums; fixed order, so the result does not depend on scheduling.
 __global__ void __launch_bounds__(256) splitk_reduce_kernel(const float *ws, const float *dbp, int splits,
@@ -310,6 +459,8 @@ struct gabe_mlp {
     float *params = nullptr, *grads = nullptr, *mom = nullptr, *vel = nullptr;
     float *xb = nullptr, *tb = nullptr, *y = nullptr, *dy = nullptr, *d0 = nullptr, *d1 = nullptr;
     float *ws = nullptr, *dbp = nullptr;  // split-K partials of the weight gradient
+    bf16 *wt = nullptr;              // BF16 transposed weights of layers >= 1 (tensor-core forward)
+    tc::WtTable wtab{};
     void *Z = nullptr, *H = nullptr;  // [depth][max_rows][width] activation type
     double2 *part = nullptr;
     TrainScalars *ts = nullptr;
@@ -357,10 +508,44 @@ int launch_gemm(gabe_mlp *m, const GemmArgs &g, int splits = 1) {
     return GABE_OK;
 }
 
+// Refreshes the BF16 transposed weight copies after the FP32 weights changed.
+int refresh_wt(gabe_mlp *m) {
+    if (m->f32act) return GABE_OK;
+    tc::weights_bf16t_kernel<<<148, 256, 0, m->stream>>>(m->params, m->wt, m->wtab);
+    MCK(m, cudaGetLastError());
+    return GABE_OK;
+}
+
+template <int EPI>
+int launch_tc(gabe_mlp *m, const tc::Args &a) {
+    const dim3 grid((a.N + tc::BN - 1) / tc::BN, (a.M + tc::BM - 1) / tc::BM);
+    tc::gemm_tc_kernel<EPI><<<grid, tc::T, 0, m->stream>>>(a);
+    MCK(m, cudaGetLastError());
+    return GABE_OK;
+}
+
 // Input activations of layer l: x (FP32) for l = 0, H[l-1] otherwise.
+// With BF16 activations every layer after the first runs on tensor cores.
 template <typename TACT>
 int forward_rows(gabe_mlp *m, const float *x, int rows, float *y, bool keep_z) {
     for (int l = 0; l < m->nl; l++) {
+        if constexpr (sizeof(TACT) == 2) {
+            if (l > 0) {
+                tc::Args a{};
+                a.M = rows;
+                a.N = m->N[l];
+                a.K = m->K[l];
+                a.A = static_cast<const bf16 *>(act_at(m, m->H, l - 1));
+                a.Wt = m->wt + m->wtab.offWt[l];
+                a.bias = m->params + m->offb[l];
+                const bool last = l + 1 == m->nl;
+                a.Z = (!last && keep_z) ? static_cast<bf16 *>(act_at(m, m->Z, l)) : nullptr;
+                a.C = last ? static_cast<void *>(y) : act_at(m, m->H, l);
+                const int rc = last ? launch_tc<EPI_OUT>(m, a) : launch_tc<EPI_HIDDEN>(m, a);
+                if (rc) return rc;
+                continue;
+            }
+        }
         GemmArgs g{};
         g.M = rows;
         g.N = m->N[l];
@@ -464,7 +649,7 @@ int train_step(gabe_mlp *m, const float *x, const float *t, const int32_t *perm,
     AdamHyper h{m->p.lr, m->p.beta1, m->p.beta2, m->p.eps, m->p.weight_decay, m->p.lr_min, m->p.decay_steps};
     adam_kernel<<<148 * 4, 256, 0, m->stream>>>(m->params, m->grads, m->mom, m->vel, m->P, h, m->ts);
     MCK(m, cudaGetLastError());
-    return GABE_OK;
+    return refresh_wt(m);
 }
 
 uint64_t splitmix(uint64_t &s) {
@@ -478,7 +663,7 @@ void free_all(gabe_mlp *m) {
     if (m->gexec) cudaGraphExecDestroy(m->gexec);
     if (m->graph) cudaGraphDestroy(m->graph);
     void *bufs[] = {m->params, m->grads, m->mom, m->vel, m->xb, m->tb, m->y, m->dy, m->d0, m->d1, m->Z, m->H,
-                    m->part, m->ts, m->ws, m->dbp};
+                    m->part, m->ts, m->ws, m->dbp, m->wt};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -523,10 +708,17 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
     m->p = *p;
     m->f32act = (p->flags & GABE_MLP_FP32_ACT) != 0;
     m->nl = p->depth + 1;
+    long long nwt = 0;
+    m->wtab.nl = m->nl;
     for (int l = 0; l < m->nl; l++) {
         m->K.push_back(l == 0 ? p->n_in : p->width);
         m->N.push_back(l + 1 == m->nl ? p->n_out : p->width);
         m->offW.push_back(m->P);
+        m->wtab.offW[l] = m->P;
+        m->wtab.K[l] = m->K[l];
+        m->wtab.N[l] = m->N[l];
+        m->wtab.offWt[l] = nwt;
+        if (l > 0) nwt += (long long)m->K[l] * m->N[l];
         m->P += (long long)m->K[l] * m->N[l];
         m->offb.push_back(m->P);
         m->P += m->N[l];
@@ -559,6 +751,7 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         {(void **)&m->d1, R * wide * 4}, {&m->Z, (size_t)p->depth * R * W * A}, {&m->H, (size_t)p->depth * R * W * A},
         {(void **)&m->part, kLossBlocks * sizeof(double2)}, {(void **)&m->ts, sizeof(TrainScalars)},
         {(void **)&m->ws, (size_t)kMaxSplits * wide * wide * 4}, {(void **)&m->dbp, (size_t)kMaxSplits * wide * 4},
+        {(void **)&m->wt, (size_t)(nwt > 0 ? nwt : 1) * sizeof(bf16)},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.ptr, a.bytes) != cudaSuccess) {
@@ -582,7 +775,7 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         cudaMemsetAsync(m->mom, 0, m->P * 4, m->stream) != cudaSuccess ||
         cudaMemsetAsync(m->vel, 0, m->P * 4, m->stream) != cudaSuccess ||
         cudaMemcpyAsync(m->ts, &ts, sizeof(ts), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
-        cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        refresh_wt(m) != GABE_OK || cudaStreamSynchronize(m->stream) != cudaSuccess) {
         cudaGetLastError();
         mset(m, GABE_ERR_CUDA, "initialisation copies failed");
         return fail(GABE_ERR_CUDA);
@@ -606,6 +799,8 @@ int gabe_mlp_set_params(gabe_mlp *m, const float *h_params) {
     if (!m || !h_params) return GABE_ERR_PARAM;
     MCK(m, cudaSetDevice(m->dev));
     MCK(m, cudaMemcpyAsync(m->params, h_params, m->P * 4, cudaMemcpyHostToDevice, m->stream));
+    int rc = refresh_wt(m);
+    if (rc) return rc;
     MCK(m, cudaStreamSynchronize(m->stream));
     return GABE_OK;
 }
@@ -730,7 +925,9 @@ int gabe_mlp_sync(gabe_mlp *m) {
 
 void *gabe_mlp_stream(const gabe_mlp *m) { return m ? (void *)m->stream : nullptr; }
 
-int gabe_mlp_launches_per_train_step(const gabe_mlp *m) { return m ? 3 + 3 * m->nl + (m->nl - 1) : 0; }
+int gabe_mlp_launches_per_train_step(const gabe_mlp *m) {
+    return m ? 3 + 3 * m->nl + (m->nl - 1) + (m->f32act ? 0 : 1) : 0;
+}
 
 
 int gabe_mlp_launches_per_forward(const gabe_mlp *m) { return m ? m->nl : 0; }

@@ -4,10 +4,14 @@
 product in the library's own kernels.  `Emulator` adds what a parameter
 sweep needs around it:
 
-* inputs (log10 g^2/lambda, amplitude multiplier, tau) and targets (the
-  ensemble's 3 x nlog log10 spectra, NaN where a log bin is empty) are
+* inputs (log10 g^2/lambda, amplitude multiplier, tau, log2 N) and targets
+  (the ensemble's 3 x nlog log10 spectra, NaN where a log bin is empty) are
   standardised with statistics of the training set; NaN targets are
-  excluded from the loss;
+  excluded from the loss.  The lattice size is an input because the GW
+  source of the initial vacuum fluctuations is gradient (UV) dominated:
+  spectra of the same parameters differ by about a decade between 32^3 and
+  128^3, so an emulator trained on an uneven ensemble must know which size
+  it is asked for;
 * `members` networks from different seeds are trained on the same data; the
   spread of their predictions flags parameter points the emulator should not
   be trusted on, which the lattice then re-runs (`screen`).
@@ -223,13 +227,15 @@ class MLP:
 
 
 class Emulator:
-    """`members` MLPs on standardised (log10 g^2/lambda, amplitude, tau) ->
-    standardised log spectra."""
+    """`members` MLPs on standardised (log10 g^2/lambda, amplitude, tau,
+    log2 N) -> standardised log spectra."""
+
+    N_IN = 4
 
     def __init__(self, members: int = 4, *, n_out=192, width=256, depth=4, lr=1e-3, seed=1, fp32_act=False,
                  device=-1):
-        self.nets = [MLP(n_out=n_out, width=width, depth=depth, lr=lr, seed=seed + 7919 * k, fp32_act=fp32_act,
-                         device=device) for k in range(members)]
+        self.nets = [MLP(n_in=self.N_IN, n_out=n_out, width=width, depth=depth, lr=lr, seed=seed + 7919 * k,
+                         fp32_act=fp32_act, device=device) for k in range(members)]
         self.n_out = n_out
         self.stats = None
 
@@ -238,9 +244,10 @@ class Emulator:
             n.close()
 
     @staticmethod
-    def features(g2_over_lambda, amplitude, tau):
+    def features(g2_over_lambda, amplitude, tau, N):
         return np.stack([np.log10(np.asarray(g2_over_lambda, dtype=np.float64)),
-                         np.asarray(amplitude, dtype=np.float64), np.asarray(tau, dtype=np.float64)], axis=-1)
+                         np.asarray(amplitude, dtype=np.float64), np.asarray(tau, dtype=np.float64),
+                         np.log2(np.asarray(N, dtype=np.float64))], axis=-1)
 
     def fit(self, feats: np.ndarray, targets: np.ndarray, epochs: int, batch: int = 512, seed: int = 0,
             lr_min: float | None = 1e-5):
@@ -291,14 +298,16 @@ class Emulator:
 
 def nearest_neighbour(train_feats: np.ndarray, train_targets: np.ndarray, query_feats: np.ndarray):
     """The lookup a sweep without the emulator has: the target of the
-    training sample nearest in standardised (log g, amplitude) at the same
-    tau (nearest tau if none matches)."""
+    training sample nearest in standardised (log g, amplitude) among those
+    of the nearest lattice size and, within it, the nearest tau."""
     tf = np.asarray(train_feats, dtype=np.float64)
     qf = np.asarray(query_feats, dtype=np.float64)
     sd = tf.std(0) + 1e-12
     out = np.empty((len(qf), train_targets.shape[1]))
     for i, q in enumerate(qf):
-        dtau = np.abs(tf[:, 2] - q[2])
+        dn = np.abs(tf[:, 3] - q[3])
+        same = dn == dn.min()
+        dtau = np.where(same, np.abs(tf[:, 2] - q[2]), np.inf)
         cand = np.flatnonzero(dtau == dtau.min())
         d = (((tf[cand, :2] - q[:2]) / sd[:2]) ** 2).sum(1)
         out[i] = train_targets[cand[np.argmin(d)]]
@@ -308,11 +317,19 @@ def nearest_neighbour(train_feats: np.ndarray, train_targets: np.ndarray, query_
 def per_bin_error(pred: np.ndarray, truth: np.ndarray):
     """Mean absolute error in dex per output over rows where the truth is
     finite (NaN where no row is)."""
+    pred, truth = np.asarray(pred, dtype=np.float64), np.asarray(truth, dtype=np.float64)
     ok = np.isfinite(truth) & np.isfinite(pred)
-    err = np.where(ok, np.abs(pred - truth), 0.0)
+    err = np.zeros(truth.shape)
+    err[ok] = np.abs(pred[ok] - truth[ok])
     n = ok.sum(0)
-    with np.errstate(invalid="ignore"):
-        return np.where(n > 0, err.sum(0) / np.maximum(n, 1), np.nan)
+    return np.where(n > 0, err.sum(0) / np.maximum(n, 1), np.nan)
+
+
+def _nanmean(x) -> float:
+    """Mean of the finite entries (NaN when there are none, without a warning)."""
+    x = np.asarray(x, dtype=np.float64)
+    ok = np.isfinite(x)
+    return float(x[ok].mean()) if ok.any() else float("nan")
 
 
 def queries_per_second(net: MLP, n: int = 1 << 20, reps: int = 5):
@@ -344,7 +361,7 @@ __all__ = ["MLP", "Emulator", "nearest_neighbour", "per_bin_error", "queries_per
 # ---------------------------------------------------------------------------
 def ensemble_samples(N, g, amp, seeds, steps: int, every: int, nlog: int = 64, dt: float = 0.01, device: int = -1,
                      log_top_bin: int | None = None):
-    """Evolves one batched ensemble and returns (features [T*nlat, 3],
+    """Evolves one batched ensemble and returns (features [T*nlat, 4],
     targets [T*nlat, 3*nlog], lattice index per row, device ms).  The log
     bins end at native bin `log_top_bin` (default: that of the largest sweep
     size, 128^3), the same for every ensemble of a sweep."""
@@ -365,7 +382,7 @@ def ensemble_samples(N, g, amp, seeds, steps: int, every: int, nlog: int = 64, d
     ms = e0.elapsed_time(e1)
     ens.close()
     T, nlat = logs.shape[:2]
-    feats = Emulator.features(np.tile(g, T), np.tile(amp, T), np.repeat(taus, nlat))
+    feats = Emulator.features(np.tile(g, T), np.tile(amp, T), np.repeat(taus, nlat), np.tile(N, T))
     targets = logs.reshape(T * nlat, 3 * nlog)
     lat = np.tile(np.arange(nlat), T)
     return feats, targets, lat, ms
@@ -435,8 +452,10 @@ def run_sweep(*, nlat=256, ensembles=2, steps=2000, every=50, nlog=64, holdout=3
     nn = nearest_neighbour(F[~is_val], Y[~is_val], fh)
     report["mae_dex_by_tau"] = {
         "tau": [float(t) for t in np.unique(fh[:, 2])],
-        "emulator": [[float(np.nanmean(per_bin_error(mean[fh[:, 2] == t], yh[fh[:, 2] == t]).reshape(3, nlog)[s]))
+        "emulator": [[_nanmean(per_bin_error(mean[fh[:, 2] == t], yh[fh[:, 2] == t]).reshape(3, nlog)[s])
                       for s in range(3)] for t in np.unique(fh[:, 2])],
+        "nearest_neighbour": [[_nanmean(per_bin_error(nn[fh[:, 2] == t], yh[fh[:, 2] == t]).reshape(3, nlog)[s])
+                               for s in range(3)] for t in np.unique(fh[:, 2])],
     }
     err_em = per_bin_error(mean, yh)
     err_nn = per_bin_error(nn, yh)
@@ -445,8 +464,7 @@ def run_sweep(*, nlat=256, ensembles=2, steps=2000, every=50, nlog=64, holdout=3
 
     def summary(err):
         e = err.reshape(3, nlog)
-        return {"phi": float(np.nanmean(e[0])), "chi": float(np.nanmean(e[1])), "gw": float(np.nanmean(e[2])),
-                "all": float(np.nanmean(err))}
+        return {"phi": _nanmean(e[0]), "chi": _nanmean(e[1]), "gw": _nanmean(e[2]), "all": _nanmean(err)}
 
     report["per_bin_mae_dex"] = {"emulator": err_em.reshape(3, nlog).tolist(),
                                  "nearest_neighbour": err_nn.reshape(3, nlog).tolist()}

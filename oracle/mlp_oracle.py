@@ -13,7 +13,10 @@ Three arithmetic modes:
   "bf16"  float32 products; pre-activations Z and activations H rounded to
           bfloat16 (round to nearest even) where the device stores them; the
           SiLU is taken of the unrounded FP32 pre-activation, its derivative
-          of the stored (rounded) one.
+          of the stored (rounded) one.  The forward products of every layer
+          after the first take the weights rounded to bfloat16 (the device
+          runs them on tensor cores from BF16 weight copies); the first layer
+          and the backward products use the FP32 weights.
 """
 from __future__ import annotations
 
@@ -99,7 +102,8 @@ def forward(params, x, shape=(3, 256, 4, 192), mode="fp64"):
         h = np.asarray(x, dtype=dt)
         Zs, Hs = [], []
         for l in range(len(lay)):
-            z = (h @ Ws[l] + bs[l]).astype(dt)
+            W = bf16_round(Ws[l]) if (mode == "bf16" and l > 0) else Ws[l]
+            z = (h @ W + bs[l]).astype(dt)
             if l + 1 == len(lay):
                 return z, Zs, Hs
             a = _silu(z).astype(dt)

@@ -138,3 +138,14 @@ def test_cosine_schedule_matches_oracle():
             lr = lr1 + 0.5 * (lr0 - lr1) * (1 + np.cos(np.pi * f))
             ref, m, v = mo.adamw_step(ref, g, m, v, s, lr=lr)
             np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
+
+
+def test_tensor_core_forward_outruns_the_fp32_path():
+    """With BF16 activations the layers after the first run on tensor cores
+    (mma.sync BF16 x BF16 -> FP32); on a million queries that forward must
+    be several times faster than the FP32-activation path, which keeps
+    every product on the CUDA-core kernel."""
+    with em.MLP(seed=1, max_rows=1 << 20) as tcn, em.MLP(seed=1, fp32_act=True, max_rows=1 << 20) as simt:
+        q_tc, info_tc = em.queries_per_second(tcn, n=1 << 20, reps=3)
+        q_s, info_s = em.queries_per_second(simt, n=1 << 20, reps=3)
+    assert q_tc > 3 * q_s, (info_tc, info_s)
