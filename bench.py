@@ -51,10 +51,13 @@ def parse():
     ap.add_argument("--cpu-baseline-steps", type=int, default=3, help="timed steps of the in-line CPU baseline")
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--lattice-flags", type=int, default=0,
-                    help="gabe_params.flags of the lattices (e.g. 16: GABE_FLAG_OWN_FFT, 8: GABE_FLAG_FUSED_KSPACE)")
+                    help="gabe_params.flags of the lattices (e.g. 16: GABE_FLAG_OWN_FFT, 128: GABE_FLAG_TRANSPOSED_FFT)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the batched-ensemble leg")
     ap.add_argument("--no-slab", action="store_true", help="skip the slab leg (one lattice split over the ranks)")
     ap.add_argument("--no-energy", action="store_true", help="skip the energy-conservation block (64^3, rank 0)")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end leg and its pinned output buffers (for lattices whose FP64 host "
+                         "copies would not fit pinned memory, e.g. 1024^3)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the FP32-vs-FP64 accuracy block on the headline lattice (rank 0)")
     ap.add_argument("--acc-steps", type=int, default=1000, help="steps of the accuracy block")
@@ -487,8 +490,8 @@ def main():
     hd = torch.empty(d.shape, dtype=torch.float64, pin_memory=True)
     hf.copy_(f)
     hd.copy_(d)
-    of = torch.empty_like(hf, pin_memory=True)
-    od = torch.empty_like(hd, pin_memory=True)
+    of = None if args.no_e2e else torch.empty_like(hf, pin_memory=True)
+    od = None if args.no_e2e else torch.empty_like(hd, pin_memory=True)
     del f, d
     torch.cuda.empty_cache()
 
@@ -526,25 +529,26 @@ def main():
         except gb.GabeError:  # cuFFT's plan: one phase
             pass
         # ---- end-to-end leg through the C ABI with host buffers
-        barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        lat.upload_ptrs(hf.data_ptr(), hd.data_ptr(), None, None, a0, adot0)
-        nonfinite_e2e = False
-        for _ in range(K):
-            lat.step(1)
+        ms_e2e, nonfinite_e2e = None, False
+        if not args.no_e2e:
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            lat.upload_ptrs(hf.data_ptr(), hd.data_ptr(), None, None, a0, adot0)
+            for _ in range(K):
+                lat.step(1)
+                try:
+                    lat.calc_energy()
+                except gb.GabeError:
+                    nonfinite_e2e = True
             try:
-                lat.calc_energy()
+                lat.spec_out()
             except gb.GabeError:
                 nonfinite_e2e = True
-        try:
-            lat.spec_out()
-        except gb.GabeError:
-            nonfinite_e2e = True
-        lat.download_ptrs(of.data_ptr(), od.data_ptr())
-        e1.record(stream)
-        e1.synchronize()
-        ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+            lat.download_ptrs(of.data_ptr(), od.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            ms_e2e = max_over_ranks(e0.elapsed_time(e1))
         legs[name] = {"ms": ms, "ms_e2e": ms_e2e, "phases": phases, "energies": en, "finite": finite,
                       "graph_active": lat.graph_active,
                       "nonfinite_e2e": nonfinite_e2e, "device_bytes": lat.device_bytes,
@@ -556,7 +560,7 @@ def main():
     sites = N ** 3
     L32 = legs["fp32"]
     value = world * sites * K / (L32["ms"] / 1e3)
-    e2e = world * sites * K / (L32["ms_e2e"] / 1e3)
+    e2e = world * sites * K / (L32["ms_e2e"] / 1e3) if L32["ms_e2e"] else None
     w = 4
     algo = algorithmic_bytes(N, w, gws)
     kern = {}
@@ -586,7 +590,8 @@ def main():
     if "fp64" in legs:
         L64 = legs["fp64"]
         v64 = world * sites * K / (L64["ms"] / 1e3)
-        extra["fp64"] = {"value": v64, "ms_per_step": L64["ms"] / K, "e2e": world * sites * K / (L64["ms_e2e"] / 1e3),
+        extra["fp64"] = {"value": v64, "ms_per_step": L64["ms"] / K,
+                         "e2e": world * sites * K / (L64["ms_e2e"] / 1e3) if L64["ms_e2e"] else None,
                          "phases_ms": L64["phases"]}
         extra["fp32_over_fp64"] = value / v64
         if L32["energies"] and L64["energies"]:

@@ -35,10 +35,7 @@ FP64, FP32 = 0, 1
 MODEL_QUADRATIC, MODEL_LPHI4 = 0, 1
 FLAG_NO_GRAPH = 1
 FLAG_NO_OVERLAP = 2
-FLAG_PLANE_FFT = 4
-FLAG_FUSED_KSPACE = 8
 FLAG_OWN_FFT = 16
-FLAG_FUSED_ROWS = 32
 FLAG_CUFFT_3D = 64
 FLAG_TRANSPOSED_FFT = 128
 

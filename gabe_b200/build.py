@@ -25,7 +25,6 @@ UNITS = [
     ("api.cu", []),
     ("kernels_f64.cu", ["-fmad=false"]),
     ("kernels_f32.cu", []),
-    ("planefft.cu", []),
     ("fft3d.cu", []),
     ("fftt.cu", []),
     ("noalloc.cu", ["-fmad=false"]),

@@ -56,16 +56,10 @@ struct gabe_handle {
     int nbins = 0;
     cufftHandle plan_src = 0, plan_spec = 0;
     bool have_plan_src = false, have_plan_spec = false;
-    // FP32 sources: 2-D (j, k) transforms (cuFFT 2-D plan, or the plane kernel
-    // of planefft.cuh) and the k-space update with the pass along i fused in
     bool evolve_gw = false; // calc_gws with expansion_type 1: the step evolves h, l (types 0 and 2 do not)
     bool own_fft = false;   // the library's three-pass 3-D r2c (fft3d.cuh)
     bool fftt = false;      // the transposed three-pass transform with the pass along i fused into the
                             // k-space update (fftt.cuh); G is then kept as [4][kz][ky][kx]
-    bool rows_fused = false;  // sweep A writes the sources transformed along k (sweeprows.cuh)
-    bool ks_fused = false;
-    bool plane_fft = false;
-    int plane_grid = 0;
     void *fft_work = nullptr;
     size_t fft_work_bytes = 0;
     LatticeConsts lc{};
@@ -131,27 +125,12 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    h->ks_fused = h->evolve_gw && h->f32 && !h->fftt && kspace_fused_supported(h->N) &&
-                  (h->p.flags & GABE_FLAG_FUSED_KSPACE);
-    h->plane_fft = h->ks_fused && plane_r2c_supported(h->N) && (h->p.flags & GABE_FLAG_PLANE_FFT);
-    h->rows_fused = h->evolve_gw && h->f32 && !h->fftt && !h->ks_fused && sweep32_rows_supported(h->N) &&
-                    (h->p.flags & GABE_FLAG_FUSED_ROWS);
     // the library's 3-D r2c: on request, and by default at N = 512 (measured faster than cuFFT's plan there)
     const bool own_default = h->N == 512 && !(h->p.flags & GABE_FLAG_CUFFT_3D);
-    h->own_fft = h->evolve_gw && h->f32 && !h->ks_fused && !h->rows_fused && !h->fftt && fft3d_supported(h->N) &&
+    h->own_fft = h->evolve_gw && h->f32 && !h->fftt && fft3d_supported(h->N) &&
                  ((h->p.flags & GABE_FLAG_OWN_FFT) || own_default);
-    if (h->plane_fft) {
-        CK(h, plane_r2c_setup(h->N, &h->plane_grid));
-    } else if (h->own_fft || h->rows_fused || h->fftt) {
+    if (h->own_fft || h->fftt) {
         // no plan: fft3d.cuh / fftt.cuh
-    } else if (h->ks_fused) {
-        // 2-D r2c of every (source, i) plane: N x (N+2) reals in, N x nz complex out, in place
-        long long n2[2] = {N, N}, inem[2] = {N, 2 * nz}, onem[2] = {N, nz};
-        CF(h, cufftCreate(&h->plan_src));
-        h->have_plan_src = true;
-        CF(h, cufftSetAutoAllocation(h->plan_src, 0));
-        CF(h, cufftMakePlanMany64(h->plan_src, 2, n2, inem, 1, N * 2 * nz, onem, 1, N * nz, CUFFT_R2C,
-                                  2 * kSrc * N, &ws_src));
     } else if (h->evolve_gw) {
         long long inem[3] = {N, N, 2 * nz}, onem[3] = {N, N, nz};
         CF(h, cufftCreate(&h->plan_src));
@@ -192,16 +171,12 @@ bool overlapped(const gabe_handle *h) { return h->evolve_gw && h->S2 != nullptr 
 float *fft_scratch(const gabe_handle *h) { return h->own_fft ? static_cast<float *>(h->S2) : nullptr; }
 void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->S2 : h->S; }
 
-// In-place transforms of the 2*kSrc source arrays in source buffer `slot`
+// Transforms of the 2*kSrc source arrays in source buffer `slot`
 // (fft_stresstensor's transforms, g2evolutionpert.cpp:190-195): the full 3-D
-// r2c, or -- with the fused k-space update, which does the pass along i --
-// the 2-D r2c of every (j, k) plane.
+// r2c, or -- for the transposed form, whose k-space update does the pass
+// along i -- its passes along k and j.
 int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
     void *S = source_buffer(h, slot);
-    if (h->plane_fft) {
-        CK(h, plane_r2c_f32(h->N, static_cast<float *>(S), 2 * kSrc * h->N, h->plane_grid, s));
-        return GABE_OK;
-    }
     if (h->fftt) {  // rows S -> S2, pass along j S2 -> S; the pass along i runs inside the k-space update
         CK(h, fftt_rows_f32(h->N, static_cast<const float *>(S), h->S2, 2 * kSrc, s));
         CK(h, fftt_cols_f32(h->N, h->S2, S, 2 * kSrc, &h->sc->status, s));
@@ -211,15 +186,11 @@ int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
         CK(h, fft3d_r2c_f32(h->N, static_cast<float *>(S), fft_scratch(h), 2 * kSrc, s));
         return GABE_OK;
     }
-    if (h->rows_fused) {  // the pass along k was taken by sweep A
-        CK(h, fft3d_cols_f32(h->N, static_cast<float *>(S), 2 * kSrc, s));
-        return GABE_OK;
-    }
     CF(h, cufftSetStream(h->plan_src, s));
     return fft_r2c(h, h->plan_src, S, S);
 }
 
-// TT projection and both RK2 stages of h, l (kspace.cuh / kspace_fused.cuh).
+// TT projection and both RK2 stages of h, l (kspace.cuh, or fftt.cuh with the pass along i).
 int kspace(gabe_handle *h, int slot, cudaStream_t s) {
     KspaceArgs k{};
     k.S = source_buffer(h, slot);
@@ -229,10 +200,6 @@ int kspace(gabe_handle *h, int slot, cudaStream_t s) {
     k.slot = slot;
     if (h->fftt) {
         CK(h, fftt_ikspace_f32(h->N, k.S, h->G, h->sc, h->lc, slot, &h->sc->status, s));
-        return GABE_OK;
-    }
-    if (h->ks_fused) {
-        CK(h, kspace_fused_f32(h->N, k, s));
         return GABE_OK;
     }
     Launch lk{dim3(148 * 8), dim3(256), 0, s};
@@ -258,10 +225,6 @@ StencilArgs stencil_args(gabe_handle *h, int cur, int slot = 0) {
 int sweep(gabe_handle *h, int mode, int cur, int counter, int slot = 0) {
     StencilArgs a = stencil_args(h, cur, slot);
     a.counter = h->counters + counter;
-    if (mode == MODE_A_GW && h->rows_fused) {
-        CK(h, sweep32_rows_f32(a, h->stream));
-        return GABE_OK;
-    }
     CK(h, h->f32 ? sweep32_f32(h->shape, mode, a, h->grid, h->stream)
                  : sweep_f64(h->shape, mode, a, h->grid, h->stream));
     return GABE_OK;
@@ -469,6 +432,9 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
         return set_err(nullptr, GABE_ERR_PARAM, "struct_size %d != %zu", p->struct_size, sizeof(gabe_params));
     char msg[160];
     if (!params_valid(*p, msg, sizeof(msg))) return set_err(nullptr, GABE_ERR_PARAM, "%s (N = %d)", msg, p->N);
+    const int known = GABE_FLAG_NO_GRAPH | GABE_FLAG_NO_OVERLAP | GABE_FLAG_OWN_FFT | GABE_FLAG_CUFFT_3D |
+                      GABE_FLAG_TRANSPOSED_FFT;
+    if (p->flags & ~known) return set_err(nullptr, GABE_ERR_PARAM, "unknown flags 0x%x", p->flags & ~known);
     const bool f32 = p->precision == GABE_FP32;
     if ((f32 ? plan_grid32(p->N, p->tile_shape, p->tile_ci) : plan_grid(p->N, p->tile_shape, p->tile_ci)).shape < 0)
         return set_err(nullptr, GABE_ERR_PARAM, "N = %d: no stencil tile divides N (%s)", p->N,
@@ -1188,7 +1154,7 @@ int gabe_graph_active(const gabe_handle *h) {
 }
 
 int gabe_launches_per_step(const gabe_handle *h) {
-    return h ? (h->evolve_gw ? (h->own_fft ? 6 : (h->rows_fused || h->fftt) ? 5 : h->plane_fft ? 4 : 3) : 2) : 0;
+    return h ? (h->evolve_gw ? (h->own_fft ? 6 : h->fftt ? 5 : 3) : 2) : 0;
 }
 
 }  // extern "C"

@@ -20,22 +20,6 @@ cudaError_t persistent_grid(K kernel, int threads, size_t smem, int *grid) {
     return cudaSuccess;
 }
 
-// passes along j and i of ncomp arrays whose rows are already transformed along k
-template <int N>
-cudaError_t fft3d_cols_n(float *S, int ncomp, cudaStream_t s) {
-    constexpr long long nz = N / 2 + 1;
-    int g2 = 0;
-    cudaError_t e = persistent_grid(f3d::col_fft_kernel<N>, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, &g2);
-    if (e != cudaSuccess) return e;
-    float2 *X = reinterpret_cast<float2 *>(S);
-    f3d::ColArgs aj{X, (long long)N * nz, 0, nz, ncomp * N, 1, (int)nz};
-    f3d::col_fft_kernel<N><<<g2, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(aj);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    f3d::ColArgs ai{X, (long long)N * N * nz, nz, (long long)N * nz, ncomp, N, (int)nz};
-    f3d::col_fft_kernel<N><<<g2, f3d::kFftThreads, f3d::ColGeom<N>::SMEM_BYTES, s>>>(ai);
-    return cudaGetLastError();
-}
-
 template <int N>
 cudaError_t col_pass_n(const f3d::ColArgs &a, cudaStream_t s) {
     int g = 0;
@@ -123,16 +107,6 @@ cudaError_t plane_scatter_n(float *S, void *send, int nplanes, int ranks, cudaSt
 }  // namespace
 
 bool fft3d_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
-
-cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s) {
-    switch (N) {
-        case 64: return fft3d_cols_n<64>(S, ncomp, s);
-        case 128: return fft3d_cols_n<128>(S, ncomp, s);
-        case 256: return fft3d_cols_n<256>(S, ncomp, s);
-        case 512: return fft3d_cols_n<512>(S, ncomp, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
 
 cudaError_t fft_col_pass_f32(int N, void *X, long long s1, long long s2, long long sn, int n1, int n2, int ncol,
                              cudaStream_t s) {

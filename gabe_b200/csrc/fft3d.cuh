@@ -21,14 +21,14 @@
 // of the ranks' transpose (scatter along j, gather along i).
 #pragma once
 
-#include "planefft.cuh"
+#include "fftreg.cuh"
 #include "slabsplit.h"
 #include "sweep32.cuh"
 
 namespace gabe {
 namespace f3d {
 
-using pfft::PlaneCfg;
+using pfft::FourStep;
 
 constexpr int kFftThreads = 512;
 constexpr int kFftBufs = 2;  // tile buffers: copies run one tile ahead (a third buffer measured slower)
@@ -36,7 +36,7 @@ constexpr int kFftBufs = 2;  // tile buffers: copies run one tile ahead (a third
 // W_N^(n1 k2) for the four-step split N = L1 L2, stored [k2][n1].
 template <int N>
 __device__ __forceinline__ void twiddles(float2 *tw) {
-    constexpr int L1 = PlaneCfg<N>::L1;
+    constexpr int L1 = FourStep<N>::L1;
     for (int m = threadIdx.x; m < N; m += blockDim.x) {
         const int k2 = m / L1, n1 = m % L1;
         double sn, cs;
@@ -60,7 +60,7 @@ __device__ __forceinline__ void twiddles(float2 *tw) {
 // fall on distinct banks while every pair stays 8-byte aligned.
 template <int N, int R_ = 16, int NB_ = 2>
 struct RowGeom {
-    using C_ = PlaneCfg<N>;
+    using C_ = FourStep<N>;
     static constexpr int L1 = C_::L1, L2 = C_::L2;
     static constexpr int R = R_, P = R / 2, T = 128, NB = NB_;  // rows per tile, pairs, threads, buffers
     static constexpr int PITCH = N;                             // floats per shared row
@@ -214,7 +214,7 @@ constexpr int kColInPlace = 0, kColGather = 1, kColScatter = 2, kColOutOfPlace =
 
 template <int N, int T_ = kFftThreads>
 struct ColGeom {
-    static constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2;
+    static constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2;
     static constexpr int W = 16, T = T_;  // columns per tile, threads
     static constexpr int BUF = N * W;                // complex per tile buffer
     static constexpr int SMEM_C = kFftBufs * BUF + N;  // tile ring + twiddles (complex)

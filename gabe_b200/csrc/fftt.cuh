@@ -36,7 +36,7 @@
 namespace gabe {
 namespace f3t {
 
-using pfft::PlaneCfg;
+using pfft::FourStep;
 
 // ---------------------------------------------------------------------------
 // pass 1: rows along k -> T1[q][i][kz][j]
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(f3d::RowGeom<N>::T, 2) rowt_kernel(const float
 // (lanes over n1: consecutive words).
 template <int N, int T>
 __device__ __forceinline__ void lines_step_a(float2 *buf, int nlines, const float2 *tw) {
-    constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2, PL = N + 2;
+    constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, PL = N + 2;
     for (int t = threadIdx.x; t < nlines * L1; t += T) {
         const int w = t / L1, n1 = t % L1;
         float2 *ln = buf + w * PL;
@@ -193,8 +193,8 @@ __device__ __forceinline__ void lines_step_a(float2 *buf, int nlines, const floa
 // line w (16-byte loads), transformed in registers; y[k1] is output element
 // k2 + L2 k1.
 template <int N>
-__device__ __forceinline__ void lines_step_b(const float2 *buf, int w, int k2, float2 (&y)[PlaneCfg<N>::L1]) {
-    constexpr int L1 = PlaneCfg<N>::L1, PL = N + 2;
+__device__ __forceinline__ void lines_step_b(const float2 *buf, int w, int k2, float2 (&y)[FourStep<N>::L1]) {
+    constexpr int L1 = FourStep<N>::L1, PL = N + 2;
     const float4 *src = reinterpret_cast<const float4 *>(buf + w * PL + L1 * k2);
 #pragma unroll
     for (int h = 0; h < L1 / 2; h++) {
@@ -227,7 +227,7 @@ template <int N, int T, int NB>
 __global__ void __launch_bounds__(T, 1) colt_kernel(const float2 *__restrict__ T1, float2 *__restrict__ T2, int ncomp,
                                                     unsigned int *status) {
     using Rg = LineRing<N, kColW, NB>;
-    constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2, NH = N / 2 + 1, W = kColW;
+    constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, NH = N / 2 + 1, W = kColW;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t *bar = Rg::bars(sm);
     float2 *tw = Rg::twid(sm);
@@ -306,7 +306,7 @@ struct IkArgs {
 template <int N, int T, int NB>
 __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
     using Rg = LineRing<N, kIkLines, NB>;
-    constexpr int L1 = PlaneCfg<N>::L1, L2 = PlaneCfg<N>::L2, NH = N / 2 + 1, PL = Rg::PL;
+    constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, NH = N / 2 + 1, PL = Rg::PL;
     constexpr long long M = (long long)NH * N * N;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t *bar = Rg::bars(sm);

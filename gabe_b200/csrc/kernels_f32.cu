@@ -3,10 +3,8 @@
 
 #include "convert.cuh"
 #include "launch.h"
-#include "kspace_fused.cuh"
 #include "sweep32.cuh"
 #include "slabgw.cuh"
-#include "sweeprows.cuh"
 
 namespace gabe {
 
@@ -63,59 +61,6 @@ cudaError_t slab_kspace_f32(const void *T, void *G, const DevScalars *sc, const 
 cudaError_t slab_gw_amplitudes_f32(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
                                    cudaStream_t s) {
     return slab_gw_amplitudes<float>(G, cnt, m0, N, m, y0, which, dst, s);
-}
-
-template <int N>
-static cudaError_t sweep32_rows_n(StencilArgs a, int ci, cudaStream_t s) {
-    using G = s32::RowsGeom<N>;
-    auto k = s32::sweep32_rows_kernel<N>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    a.ci = ci;
-    k<<<dim3(N / 2, (N + ci - 1) / ci), G::T, G::SMEM_BYTES, s>>>(a);
-    return cudaGetLastError();
-}
-
-bool sweep32_rows_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
-
-int sweep32_rows_ci(int N) { return N >= 512 ? 64 : (N >= 256 ? 32 : (N >= 128 ? 16 : 8)); }
-
-cudaError_t sweep32_rows_f32(const StencilArgs &a, cudaStream_t s) {
-    const int ci = sweep32_rows_ci(a.c.N);
-    switch (a.c.N) {
-        case 64: return sweep32_rows_n<64>(a, ci, s);
-        case 128: return sweep32_rows_n<128>(a, ci, s);
-        case 256: return sweep32_rows_n<256>(a, ci, s);
-        case 512: return sweep32_rows_n<512>(a, ci, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
-
-template <int N>
-static cudaError_t kspace_fused_n(const KspaceArgs &a, cudaStream_t s) {
-    using G = ksf::KsGeom<N>;
-    auto k = ksf::kspace_fused_kernel<N>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    int dev = 0, nsm = 0, per_sm = 0;
-    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
-    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, G::T, G::SMEM_BYTES)) != cudaSuccess) return e;
-    if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    k<<<nsm * per_sm, G::T, G::SMEM_BYTES, s>>>(a);
-    return cudaGetLastError();
-}
-
-bool kspace_fused_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
-
-cudaError_t kspace_fused_f32(int N, const KspaceArgs &a, cudaStream_t s) {
-    switch (N) {
-        case 64: return kspace_fused_n<64>(a, s);
-        case 128: return kspace_fused_n<128>(a, s);
-        case 256: return kspace_fused_n<256>(a, s);
-        case 512: return kspace_fused_n<512>(a, s);
-        default: return cudaErrorInvalidValue;
-    }
 }
 
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l) {

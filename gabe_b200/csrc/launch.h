@@ -155,11 +155,6 @@ cudaError_t slab_kspace_f64(const void *T, void *G, const DevScalars *sc, const 
                             cudaStream_t s);
 cudaError_t slab_gw_amplitudes_f64(const void *G, size_t cnt, size_t m0, int N, int m, int y0, int which, double *dst,
                                    cudaStream_t s);
-// FP32 sweep A with sources that writes them transformed along k (sweeprows.cuh):
-// one block per pair of rows and chunk of sweep32_rows_ci(N) planes.
-bool sweep32_rows_supported(int N);
-int sweep32_rows_ci(int N);
-cudaError_t sweep32_rows_f32(const StencilArgs &a, cudaStream_t s);
 cudaError_t kspace_f64(const KspaceArgs &a, const Launch &l);
 cudaError_t kspace_f32(const KspaceArgs &a, const Launch &l);
 cudaError_t bins_f64(const BinArgs &a, const Launch &l);
@@ -202,8 +197,6 @@ cudaError_t fft_col_gather_f32(int N, const void *recv, void *T, int ncomp, int 
 // pass along j written to the transpose's send buffer (blocks by destination rank of
 // [nplanes][n(r)][N/2+1]), for N in {64, 128, 256, 512} (fft3d.cuh).
 cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int ranks, cudaStream_t s);
-// Its passes along j and i alone, for sources already transformed along k.
-cudaError_t fft3d_cols_f32(int N, float *S, int ncomp, cudaStream_t s);
 
 // FP32 transposed three-pass transform (fftt.cuh): rows along k S -> T1, the pass
 // along j T1 -> T2, and the pass along i fused with the TT projection and h/l
@@ -213,16 +206,6 @@ cudaError_t fftt_rows_f32(int N, const float *S, void *T1, int ncomp, cudaStream
 cudaError_t fftt_cols_f32(int N, const void *T1, void *T2, int ncomp, unsigned int *status, cudaStream_t s);
 cudaError_t fftt_ikspace_f32(int N, const void *T2, void *G, const DevScalars *sc, const LatticeConsts &c, int slot,
                              unsigned int *status, cudaStream_t s);
-
-// FP32 k-space update with the FFT pass along i fused in (kspace_fused.cuh);
-// S holds the 2-D (j, k) transforms of the sources.
-bool kspace_fused_supported(int N);
-cudaError_t kspace_fused_f32(int N, const KspaceArgs &a, cudaStream_t s);
-
-// FP32 2-D r2c over the (j, k) planes of the source array (planefft.cuh).
-bool plane_r2c_supported(int N);
-cudaError_t plane_r2c_setup(int N, int *grid);
-cudaError_t plane_r2c_f32(int N, float *S, int nplanes, int grid, cudaStream_t s);
 
 cudaError_t bin_reduce(const double *part_sum, const unsigned int *part_cnt, int nblocks, int nseries, int nbins,
                        double *sum, double *cnt, cudaStream_t s);

@@ -63,6 +63,8 @@ enum gabe_model {
                                  model_c = {lam_pr, gsq_pr} */
 };
 
+/* Flag values 4, 8 and 32 belonged to transform forms that measured slower
+ * on B200 and were removed; gabe_create refuses them, like any unknown bit. */
 enum gabe_flags {
     GABE_FLAG_NO_GRAPH = 1,  /* launch kernels one by one instead of replaying a CUDA graph */
     GABE_FLAG_NO_OVERLAP = 2, /* one source buffer: the GW transforms and k-space update run in line
@@ -70,24 +72,11 @@ enum gabe_flags {
                                  words of device memory).  With the library's 3-D FFT the chain runs
                                  in line anyway and the second buffer is the target of its column
                                  passes (out of place, faster); this flag makes them in place */
-    GABE_FLAG_FUSED_KSPACE = 8, /* FP32 with N in {64, 128, 256, 512}: transform the GW sources over each
-                                   (j, k) plane only and do the FFT along i inside the k-space update,
-                                   instead of a full 3-D transform followed by the k-space pass (the
-                                   default, and faster on B200: the fused form reads its columns in
-                                   32-byte pieces) */
-    GABE_FLAG_PLANE_FFT = 4,    /* with GABE_FLAG_FUSED_KSPACE: the 2-D (j, k) transforms by the
-                                   library's plane kernel (one thread-block cluster per plane) instead
-                                   of cuFFT's batched 2-D plan */
     GABE_FLAG_OWN_FFT = 16,     /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
                                    library's three-pass 3-D r2c instead of cuFFT's 3-D plan (no cuFFT
                                    call on the step path).  The default for FP32 at N = 512, where it
                                    is about 4% faster than cuFFT's plan on B200 (7.97 against 8.30 ms
                                    for the ten transforms of a step) */
-    GABE_FLAG_FUSED_ROWS = 32,  /* FP32 with N in {64, 128, 256, 512}: sweep A writes the GW sources already
-                                   transformed along k (one block per pair of whole rows), and the
-                                   transforms along j and i are the library's column passes (one HBM
-                                   pass fewer, but about 8% slower per step at 512^3 on B200: one
-                                   block per SM, whose transform phases leave most warps idle) */
     GABE_FLAG_CUFFT_3D = 64,    /* FP32 at N = 512: cuFFT's 3-D plan for the GW sources instead of the
                                    library's three-pass r2c (cuFFT's plan is the default at every other
                                    size and precision) */

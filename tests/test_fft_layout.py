@@ -1,6 +1,6 @@
 """Index arithmetic of the library's row pass along k (fft3d.cuh
 row_r2c_kernel), restated on the CPU for N in {64, 128, 256, 512} with the
-four-step splits N = L1 L2 of planefft.cuh PlaneCfg:
+four-step splits N = L1 L2 of fftreg.cuh FourStep:
 
 * RowGeom::phys, the position of real e of a row in shared memory, permutes
   the row, keeps each pair of reals (2m, 2m+1) together and 8-byte aligned

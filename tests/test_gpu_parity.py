@@ -260,15 +260,13 @@ def test_runs_are_deterministic():
 
 
 @pytest.mark.parametrize("N,gws,flags", [(32, 0, 0), (32, 1, 0), (64, 1, 0), (64, 1, gb.FLAG_OWN_FFT),
-                                         (64, 1, gb.FLAG_FUSED_KSPACE),
-                                         (64, 1, gb.FLAG_FUSED_KSPACE | gb.FLAG_PLANE_FFT)])
+                                         (64, 1, gb.FLAG_TRANSPOSED_FFT)])
 def test_fp32_against_fp64(N, gws, flags):
     """FP32 storage of fluctuations vs the FP64 path: energies <= 1e-4.  The
     FP32 GW sources go through cuFFT's 3-D plan, or the library's three-pass
-    3-D FFT (GABE_FLAG_OWN_FFT), and the separate k-space pass, or
-    (GABE_FLAG_FUSED_KSPACE) through 2-D plane transforms -- cuFFT's, or the
-    library's with GABE_FLAG_PLANE_FFT -- and the k-space update with the FFT
-    along i fused in."""
+    3-D FFT (GABE_FLAG_OWN_FFT), and the separate k-space pass, or through the
+    transposed passes with the pass along i fused into the k-space update
+    (GABE_FLAG_TRANSPOSED_FFT)."""
     steps = 200
     cfg = po.Config(N=N, model=po.MODEL_LPHI4, gws=gws)
     st = po.init_state(cfg)
