@@ -125,10 +125,8 @@ int make_plans(gabe_handle *h) {
     long long n[3] = {N, N, N};
     size_t ws_src = 0, ws_spec = 0;
     const cufftType t = h->f32 ? CUFFT_R2C : CUFFT_D2Z;
-    // the library's 3-D r2c: on request, and by default at N = 512 (measured faster than cuFFT's plan there)
-    const bool own_default = h->N == 512 && !(h->p.flags & GABE_FLAG_CUFFT_3D);
-    h->own_fft = h->evolve_gw && h->f32 && !h->fftt && fft3d_supported(h->N) &&
-                 ((h->p.flags & GABE_FLAG_OWN_FFT) || own_default);
+    // the library's in-layout three-pass r2c: on request
+    h->own_fft = h->evolve_gw && h->f32 && !h->fftt && fft3d_supported(h->N) && (h->p.flags & GABE_FLAG_OWN_FFT);
     if (h->own_fft || h->fftt) {
         // no plan: fft3d.cuh / fftt.cuh
     } else if (h->evolve_gw) {
@@ -503,7 +501,10 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     }
     // sources need 10 padded slots; spectra need 2; uploads stage one FP64 field array
     h->evolve_gw = p->gws_on && p->expansion == 1;
-    h->fftt = h->evolve_gw && h->f32 && fftt_supported(h->N) && (p->flags & GABE_FLAG_TRANSPOSED_FFT);
+    // the transposed form: on request, and by default for FP32 at N = 512 (measured fastest there)
+    h->fftt = h->evolve_gw && h->f32 && fftt_supported(h->N) &&
+              ((p->flags & GABE_FLAG_TRANSPOSED_FFT) ||
+               (h->N == 512 && !(p->flags & (GABE_FLAG_OWN_FFT | GABE_FLAG_CUFFT_3D))));
     h->nslots = h->evolve_gw ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);

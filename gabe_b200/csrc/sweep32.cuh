@@ -17,7 +17,6 @@
 // L2 by the neighbouring tiles).
 #pragma once
 
-#include "site2.cuh"
 #include "stencil.cuh"
 
 namespace gabe {
@@ -202,9 +201,8 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     };
     auto next_slot = [](int sl) { return sl + 1 == S ? 0 : sl + 1; };
 
-    s2::Mom mom;  // the two sites' FP32 moments, one lane each
-    s2::zero(mom);
-    const s2::K2 k2 = s2::k2_of(s);
+    Moments mom;
+    zero(mom);
     int ngroup = 0;  // planes in the current moment group
 
     // prologue: planes i0-1 .. i0+S-3 (one commit group each) into slots 0 .. S-2
@@ -238,7 +236,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
                     cu[a] = *reinterpret_cast<const float2 *>(sc + a * Rg::ARR + so_own);
                 }
             }
-            s2::Nb nb[4];  // both sites of each array, one lane each
+            Nb7<float> nb[4][2];  // [array][site]
             float2 nx[4];
 #pragma unroll
             for (int a = 0; a < 4; a++) {
@@ -248,35 +246,38 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
                 const float2 dn = *reinterpret_cast<const float2 *>(sc + ao - PK);
                 const float lm = sc[ao - 1], rp = sc[ao + 2];
                 // reference neighbour order: centre, i+1, i-1, j+1, j-1, k+1, k-1
-                nb[a] = s2::Nb{{s2::mk(cu[a]), s2::mk(nx[a]), s2::mk(pr[a]), s2::mk(up), s2::mk(dn),
-                                s2::mk(cu[a].y, rp), s2::mk(lm, cu[a].x)}};
+                nb[a][0] = Nb7<float>{{cu[a].x, nx[a].x, pr[a].x, up.x, dn.x, cu[a].y, lm}};
+                nb[a][1] = Nb7<float>{{cu[a].y, nx[a].y, pr[a].y, up.y, dn.y, rp, cu[a].x}};
             }
             if constexpr (MODE == MODE_B) {
-                s2::F2 xo[2], dout[2];  // [field], both sites
-                s2::site_b(c, s, k2, nb[0], nb[1], nb[2], nb[3], xo, dout);
-                const int gx = i * NN + o_own;
-                __stcs(reinterpret_cast<float2 *>(t.Xo + gx), xo[0].v);
-                __stcs(reinterpret_cast<float2 *>(t.Xo + n3 + gx), xo[1].v);
-                __stcs(reinterpret_cast<float2 *>(t.Do + gx), dout[0].v);
-                __stcs(reinterpret_cast<float2 *>(t.Do + n3 + gx), dout[1].v);
-            } else {
-                s2::F2 s0[kSrc], s1[kSrc];
+                float xo[2][2], dout[2][2];  // [site][field]
 #pragma unroll
-                for (int q = 0; q < kSrc; q++) s0[q] = s1[q] = s2::sp(0.f);
-                s2::site_a<MODE>(c, s, k2, nb[0], nb[1], nb[2], nb[3], mom, s0, s1);
+                for (int v = 0; v < 2; v++) {
+                    site_b32(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], xo[v], dout[v]);
+                }
+                const int gx = i * NN + o_own;
+                __stcs(reinterpret_cast<float2 *>(t.Xo + gx), make_float2(xo[0][0], xo[1][0]));
+                __stcs(reinterpret_cast<float2 *>(t.Xo + n3 + gx), make_float2(xo[0][1], xo[1][1]));
+                __stcs(reinterpret_cast<float2 *>(t.Do + gx), make_float2(dout[0][0], dout[1][0]));
+                __stcs(reinterpret_cast<float2 *>(t.Do + n3 + gx), make_float2(dout[0][1], dout[1][1]));
+            } else {
+                float s0[2][kSrc] = {}, s1[2][kSrc] = {};
+#pragma unroll
+                for (int v = 0; v < 2; v++) {
+                    site_a32<MODE>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], mom, s0[v], s1[v]);
+                }
                 if (++ngroup == kGroup || i == i1 - 1) {
-                    Moments m1;
-                    s2::collapse(mom, m1);
-                    fold<MODE>(s.mt, s.q3f, 2 * ngroup, m1, acc);
-                    s2::zero(mom);
+                    fold<MODE>(s.mt, s.q3f, 2 * ngroup, mom, acc);
                     ngroup = 0;
                 }
                 if constexpr (MODE == MODE_A_GW) {
                     float *g = t.S + ((i - sfirst) * (N * (N + 2)) + so_row);
 #pragma unroll
-                    for (int q = 0; q < kSrc; q++, g += sstride) __stcs(reinterpret_cast<float2 *>(g), s0[q].v);
+                    for (int q = 0; q < kSrc; q++, g += sstride)
+                        __stcs(reinterpret_cast<float2 *>(g), make_float2(s0[0][q], s0[1][q]));
 #pragma unroll
-                    for (int q = 0; q < kSrc; q++, g += sstride) __stcs(reinterpret_cast<float2 *>(g), s1[q].v);
+                    for (int q = 0; q < kSrc; q++, g += sstride)
+                        __stcs(reinterpret_cast<float2 *>(g), make_float2(s1[0][q], s1[1][q]));
                 }
             }
 #pragma unroll

@@ -73,19 +73,18 @@ enum gabe_flags {
                                  in line anyway and the second buffer is the target of its column
                                  passes (out of place, faster); this flag makes them in place */
     GABE_FLAG_OWN_FFT = 16,     /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
-                                   library's three-pass 3-D r2c instead of cuFFT's 3-D plan (no cuFFT
-                                   call on the step path).  The default for FP32 at N = 512, where it
-                                   is about 4% faster than cuFFT's plan on B200 (7.97 against 8.30 ms
-                                   for the ten transforms of a step) */
-    GABE_FLAG_CUFFT_3D = 64,    /* FP32 at N = 512: cuFFT's 3-D plan for the GW sources instead of the
-                                   library's three-pass r2c (cuFFT's plan is the default at every other
-                                   size and precision) */
+                                   library's in-layout three-pass 3-D r2c (the layout of a library r2c)
+                                   followed by the separate k-space pass, instead of the default */
+    GABE_FLAG_CUFFT_3D = 64,    /* FP32 at N = 512: cuFFT's 3-D plan and the separate k-space pass instead
+                                   of the default transposed transform (cuFFT's plan is the default at
+                                   every other size and for FP64) */
     GABE_FLAG_TRANSPOSED_FFT = 128 /* FP32 with N in {64, 128, 256, 512}: the library's transposed three-pass
                                    transform -- rows along k, then along j, each written transposed so
                                    that every pass reads whole contiguous lines (bulk copies), and the
                                    pass along i fused with the TT projection and h/l update, so the
-                                   transformed sources are never written back.  Needs the second source
-                                   buffer whatever GABE_FLAG_NO_OVERLAP says */
+                                   transformed sources are never written back.  The default for FP32 at
+                                   N = 512 (the fastest form measured there on B200); needs the second
+                                   source buffer whatever GABE_FLAG_NO_OVERLAP says */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two

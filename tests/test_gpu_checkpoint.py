@@ -2,8 +2,9 @@
 
 A run of K steps is saved, the file is loaded into a new handle with the
 same parameters, and both continue for M steps: the restarted run must equal
-the uninterrupted one bit for bit -- fields, momenta, h, l, all twelve
-scalars and the spectra -- in FP64 and in FP32 storage (cuFFT's plan, the
+the uninterrupted one bit for bit -- fields, momenta, h, l and all twelve
+scalars; the spectra to the last-bit noise of their binning -- in FP64 and
+in FP32 storage (cuFFT's plan, the
 library's three-pass FFT and the transposed form, whose amplitudes are kept
 in another order).  The file's portable part holds the FP64 state at step K
 in the reference's layout.  A dump without a restart block (as the
@@ -53,8 +54,16 @@ def test_restart_continues_bit_for_bit(tmp_path, precision, flags, N):
         assert b.load(path) is True
         b.step(M)
         got = _snapshot(b)
-    for x, y in zip(got, want):
+    _same(got, want)
+
+
+def _same(got, want):
+    """State and scalars bit for bit; the spectra to 1e-12, because the
+    binning adds FP64 histogram entries with shared-memory atomics whose
+    order (and so the last bit of a bin) varies from run to run."""
+    for x, y in zip(got[:5], want[:5]):
         np.testing.assert_array_equal(x, y)
+    np.testing.assert_allclose(got[5], want[5], rtol=1e-12, atol=0)
 
 
 def test_a_dump_without_restart_block_is_an_initial_state(tmp_path):
@@ -68,8 +77,7 @@ def test_a_dump_without_restart_block_is_an_initial_state(tmp_path):
         b.upload_state(st.field[0], st.dfield[0], st.h[0], st.l[0], a0=st.sc.a[0], adot0=st.sc.adot[0])
         a.step(4)
         b.step(4)
-        for x, y in zip(_snapshot(a), _snapshot(b)):
-            np.testing.assert_array_equal(x, y)
+        _same(_snapshot(a), _snapshot(b))
 
 
 def test_load_refuses_a_dump_of_another_lattice(tmp_path):

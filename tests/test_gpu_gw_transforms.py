@@ -88,13 +88,13 @@ def test_gw_transforms_512_match_cufft_3d():
     for name, flags in [*FORMS.items(), ("3d", gb.FLAG_CUFFT_3D), ("default", 0)]:
         with gb.Lattice(N, gws=True, precision=gb.FP32, flags=flags) as lat:
             if name == "default":
-                assert lat.launches_per_step == LAUNCHES[gb.FLAG_OWN_FFT]  # the library's FFT at 512
+                assert lat.launches_per_step == LAUNCHES[gb.FLAG_TRANSPOSED_FFT]  # the transposed form at 512
             lat.upload_state(f, d, a0=a0, adot0=ad0)
             lat.step(2)
             specs[name] = lat.spec_out()
     assert np.abs(specs["3d"][:, 5]).max() > 0
     # same kernels; the binning's FP64 shared-memory sums vary in the last bit
-    np.testing.assert_allclose(specs["default"], specs["own"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(specs["default"], specs["trans"], rtol=1e-12, atol=0)
     for name in FORMS:
         assert np.all(np.isfinite(specs[name]))
         assert _gw_cols_close(specs[name], specs["3d"]) <= FFT_TOL, name
