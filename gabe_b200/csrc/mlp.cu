@@ -171,9 +171,9 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
 // first): Z = H W + b with H [M][K] BF16 and the layer's weights as a BF16
 // copy kept transposed, Wt [N][K] (k contiguous), multiplied by
 // mma.sync.m16n8k16 (BF16 x BF16, FP32 accumulation).  128 x 128 output
-// tiles, 8 warps of 64 x 32, 32-deep k slices double-buffered in shared
-// memory by cp.async, fragments by ldmatrix; rows padded to 40 BF16 so
-// that the eight 16-byte rows of each ldmatrix hit distinct banks.
+// tiles, 8 warps of 64 x 32, 32-deep k slices in a 4-stage cp.async ring,
+// fragments by ldmatrix; rows padded to 40 BF16 so that the eight 16-byte
+// rows of each ldmatrix hit distinct banks.
 // Epilogue as the SIMT kernel's: bias and SiLU into Z and H (BF16), or bias
 // into the FP32 output.
 // ---------------------------------------------------------------------------
@@ -210,10 +210,17 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
+// Shared memory: STAGES ring slots of one 128 x 32 A tile and one 128 x 32
+// Wt tile; slices k0 + BK (STAGES - 1) ahead are in flight while slice k0
+// is multiplied, so global latency hides behind three slices of MMAs.
+constexpr int STAGES = 4;
+constexpr size_t SMEM_BYTES = (size_t)STAGES * 2 * BM * LDS * sizeof(bf16);
+
 template <int EPI>
-__global__ void __launch_bounds__(T) gemm_tc_kernel(Args g) {
-    __shared__ __align__(16) bf16 As[2][BM][LDS];
-    __shared__ __align__(16) bf16 Bs[2][BN][LDS];
+__global__ void __launch_bounds__(T, 2) gemm_tc_kernel(Args g) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    auto As = reinterpret_cast<bf16(*)[BM][LDS]>(smraw);                                   // [STAGES][BM][LDS]
+    auto Bs = reinterpret_cast<bf16(*)[BN][LDS]>(smraw + (size_t)STAGES * BM * LDS * sizeof(bf16));
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps: 64 rows x 32 columns each
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -229,7 +236,6 @@ __global__ void __launch_bounds__(T) gemm_tc_kernel(Args g) {
             if (gn < g.N) cp16(&Bs[st][row][c8], g.Wt + (long long)gn * g.K + k0 + c8);
             else *reinterpret_cast<uint4 *>(&Bs[st][row][c8]) = make_uint4(0, 0, 0, 0);
         }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
     float acc[4][4][4];
 #pragma unroll
@@ -238,16 +244,17 @@ __global__ void __launch_bounds__(T) gemm_tc_kernel(Args g) {
         for (int j = 0; j < 4; j++)
 #pragma unroll
             for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
-    load(0, 0);
+#pragma unroll
+    for (int q = 0; q < STAGES - 1; q++) {  // prologue: slices 0 .. STAGES-2, one commit group each
+        if (q < nk) load(q, q * BK);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
     for (int kc = 0; kc < nk; kc++) {
-        const int st = kc & 1;
-        if (kc + 1 < nk) {
-            load(st ^ 1, (kc + 1) * BK);
-            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        }
-        __syncthreads();
+        const int st = kc % STAGES;
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(STAGES - 2) : "memory");  // slice kc has landed
+        __syncthreads();  // ... for every thread; every warp is done with slice kc-1
+        if (kc + STAGES - 1 < nk) load((kc + STAGES - 1) % STAGES, (kc + STAGES - 1) * BK);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
 #pragma unroll
         for (int ks = 0; ks < BK / 16; ks++) {
             uint32_t a[4][4], b[2][4];
@@ -263,8 +270,8 @@ __global__ void __launch_bounds__(T) gemm_tc_kernel(Args g) {
                 for (int nf = 0; nf < 4; nf++)
                     mma_bf16(acc[mf][nf], a[mf], b[nf >> 1][(nf & 1) * 2], b[nf >> 1][(nf & 1) * 2 + 1]);
         }
-        __syncthreads();  // stage st is refilled by the next round's load
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     const int gr = lane >> 2, gc = (lane & 3) * 2;
 #pragma unroll
     for (int mf = 0; mf < 4; mf++)
@@ -519,7 +526,9 @@ int refresh_wt(gabe_mlp *m) {
 template <int EPI>
 int launch_tc(gabe_mlp *m, const tc::Args &a) {
     const dim3 grid((a.N + tc::BN - 1) / tc::BN, (a.M + tc::BM - 1) / tc::BM);
-    tc::gemm_tc_kernel<EPI><<<grid, tc::T, 0, m->stream>>>(a);
+    MCK(m, cudaFuncSetAttribute(tc::gemm_tc_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tc::SMEM_BYTES));
+    tc::gemm_tc_kernel<EPI><<<grid, tc::T, tc::SMEM_BYTES, m->stream>>>(a);
     MCK(m, cudaGetLastError());
     return GABE_OK;
 }
