@@ -303,7 +303,7 @@ struct IkArgs {
     unsigned int *status;
 };
 
-template <int N, int T, int NB>
+template <int N, int T, int NB, bool POL32 = false>
 __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
     using Rg = LineRing<N, kIkLines, NB>;
     constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, NH = N / 2 + 1, PL = Rg::PL;
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
                 g[p] = {v.x, v.y};
             }
             const int px = kx <= N / 2 ? kx : kx - N;
-            kspace_update_vals<float>(kc, px, py, kz, s, g);
+            kspace_update_vals<float, POL32>(kc, px, py, kz, s, g);
 #pragma unroll
             for (int p = 0; p < 4; p++) gout[p * M + kx] = make_float2(g[p].re, g[p].im);
         }

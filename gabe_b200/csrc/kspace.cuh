@@ -25,6 +25,8 @@
 // reference zeroes T there, :319-321) and stays zero.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace gabe {
@@ -62,6 +64,26 @@ __host__ __device__ inline void pol_tensors(int px, int py, int pz, double ep[6]
     ex[3] = 2. * e1y * e2y; ex[4] = e1y * e2z + e2y * e1z; ex[5] = 2. * e1z * e2z;
 }
 
+// The same in FP32 (for the FP32 path's k-space update): the reference axis
+// is chosen by comparing the integer components, which orders them exactly as
+// the FP64 form's |k_i| / |n| do, so both forms take the same basis; e1, e2
+// then carry FP32 rounding (~1e-7 relative).
+__device__ inline void pol_tensors32(int px, int py, int pz, float ep[6], float ex[6]) {
+    const float inv = rsqrtf((float)(px * px + py * py + pz * pz));
+    const float kx = px * inv, ky = py * inv, kz = pz * inv;
+    const int ax = abs(px), ay = abs(py), az = abs(pz);
+    const int r = (ax <= ay && ax <= az) ? 0 : (ay <= az ? 1 : 2);
+    const float kr = r == 0 ? kx : (r == 1 ? ky : kz);
+    float e1x = (r == 0 ? 1.f : 0.f) - kr * kx, e1y = (r == 1 ? 1.f : 0.f) - kr * ky, e1z = (r == 2 ? 1.f : 0.f) - kr * kz;
+    const float n1 = rsqrtf(e1x * e1x + e1y * e1y + e1z * e1z);
+    e1x *= n1; e1y *= n1; e1z *= n1;
+    const float e2x = ky * e1z - kz * e1y, e2y = kz * e1x - kx * e1z, e2z = kx * e1y - ky * e1x;
+    ep[0] = e1x * e1x - e2x * e2x; ep[1] = e1x * e1y - e2x * e2y; ep[2] = e1x * e1z - e2x * e2z;
+    ep[3] = e1y * e1y - e2y * e2y; ep[4] = e1y * e1z - e2y * e2z; ep[5] = e1z * e1z - e2z * e2z;
+    ex[0] = 2.f * e1x * e2x; ex[1] = e1x * e2y + e2x * e1y; ex[2] = e1x * e2z + e2x * e1z;
+    ex[3] = 2.f * e1y * e2y; ex[4] = e1y * e2z + e2y * e1z; ex[5] = 2.f * e1z * e2z;
+}
+
 // eps : S / 2 for a symmetric traceless S given by (S11, S12, S13, S22, S23).
 template <typename T>
 __device__ __forceinline__ T pol_contract(const T *w, const T *S) {
@@ -96,16 +118,20 @@ __device__ __forceinline__ KsCoef<T> ks_coef(const LatticeConsts &c, const doubl
 // with integer wave vector (px, py, kzi), driven by its transformed
 // sources s[10] (stage-0 11,12,13,22,23, then stage 1); g is updated in
 // place.  k = 0 has no TT part and is left as it is.
-template <typename T>
+// P: precision of the polarization tensors (double, or float for POL32).
+template <typename T, bool POL32 = false>
 __device__ __forceinline__ void kspace_update_vals(const KsCoef<T> &kc, int px, int py, int kzi, const Cplx<T> (&s)[10],
                                                    Cplx<T> (&g)[4]) {
     const double m2 = ((double)px * px + (double)py * py) + (double)kzi * kzi;
     if (m2 == 0.0) return;  // no TT mode at k = 0; its amplitudes stay zero
-    double ep[6], ex[6];
-    pol_tensors(px, py, kzi, ep, ex);
+    using P = typename std::conditional<POL32, float, double>::type;
+    P ep[6], ex[6];
+    if constexpr (POL32) pol_tensors32(px, py, kzi, ep, ex);
+    else pol_tensors(px, py, kzi, ep, ex);
     // weights of (S11, S12, S13, S22, S23) in eps:S/2 with S33 = -S11-S22
-    const T wp[5] = {(T)(0.5 * (ep[0] - ep[5])), (T)ep[1], (T)ep[2], (T)(0.5 * (ep[3] - ep[5])), (T)ep[4]};
-    const T wx[5] = {(T)(0.5 * (ex[0] - ex[5])), (T)ex[1], (T)ex[2], (T)(0.5 * (ex[3] - ex[5])), (T)ex[4]};
+    const P half = (P)0.5;
+    const T wp[5] = {(T)(half * (ep[0] - ep[5])), (T)ep[1], (T)ep[2], (T)(half * (ep[3] - ep[5])), (T)ep[4]};
+    const T wx[5] = {(T)(half * (ex[0] - ex[5])), (T)ex[1], (T)ex[2], (T)(half * (ex[3] - ex[5])), (T)ex[4]};
     const T kk0 = (T)(m2 * kc.norm0), kk1 = (T)(m2 * kc.norm1);
     T Tp[2][2][2];  // [stage][pol][re/im], already times 2 (8 pi/a^2) dx^3
 #pragma unroll
