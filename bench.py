@@ -192,7 +192,7 @@ def traffic_scaled(kernel: str, precision: str, N: int):
     if not e:
         return None
     # DRAM bytes grow with the sites (sweeps, row pass) or k-points (k-space, column passes) processed
-    kpts = kernel in ("kspace", "fft_j", "fft_i")
+    kpts = kernel in ("kspace", "fft_j", "fft_i", "fft_i_kspace")
     scale = (N / e["N"]) ** 3 if not kpts else (N * N * (N // 2 + 1)) / (e["N"] ** 2 * (e["N"] // 2 + 1))
     return e["bytes"] * scale
 

@@ -257,8 +257,7 @@ class Lattice:
         fft_i_kspace}, timed inside n full steps (the state advances n steps)."""
         out = (ctypes.c_double * 3)()
         self._check(library().gabe_profile_fft_passes(self._h, int(n), out))
-        last = "fft_i_kspace" if self.params.flags & FLAG_TRANSPOSED_FFT and self.gws and \
-            self.precision == FP32 and self.N in (64, 128, 256, 512) else "fft_i"
+        last = "fft_i_kspace" if self.launches_per_step == 5 else "fft_i"  # 5: the transposed form
         return {"fft_rows": out[0], "fft_j": out[1], last: out[2]}
 
     @property

@@ -143,8 +143,8 @@ def test_bench_counts_each_fft_pass_and_the_step_once():
     for n in (32, 48, 64, 96, 128):
         n3e, Me = n ** 3, n * n * (n // 2 + 1)
         assert bench.ensemble_step_bytes(n) == (56 + 32) * n3e + 40 * (n3e + 2 * Me) + 144 * Me
-    t256 = bench.traffic_scaled("fft_i", "fp32", 256)
-    t512 = bench.traffic_scaled("fft_i", "fp32", 512)
+    t256 = bench.traffic_scaled("fft_i_kspace", "fp32", 256)
+    t512 = bench.traffic_scaled("fft_i_kspace", "fp32", 512)
     assert t256 and abs(t512 / t256 - M / (256 * 256 * 129)) < 1e-12
 
 
