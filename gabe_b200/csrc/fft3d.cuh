@@ -58,12 +58,12 @@ __device__ __forceinline__ void twiddles(float2 *tw) {
 // (one four-step chunk) the pairs of reals are permuted by an XOR with the
 // chunk's index, so that the stride-L1 reads of the second four-step pass
 // fall on distinct banks while every pair stays 8-byte aligned.
-template <int N, int R_ = 16, int NB_ = 2>
+template <int N, int R_ = 16, int NB_ = 2, int T_ = 128, int PAD_ = 0>
 struct RowGeom {
     using C_ = FourStep<N>;
     static constexpr int L1 = C_::L1, L2 = C_::L2;
-    static constexpr int R = R_, P = R / 2, T = 128, NB = NB_;  // rows per tile, pairs, threads, buffers
-    static constexpr int PITCH = N;                             // floats per shared row
+    static constexpr int R = R_, P = R / 2, T = T_, NB = NB_;  // rows per tile, pairs, threads, buffers
+    static constexpr int PITCH = N + PAD_;                     // floats per shared row
     static constexpr int BUF = R * PITCH;                       // floats per tile buffer
     static constexpr int SMEM_FLOATS = NB * BUF + 2 * N;        // + twiddles
     static constexpr size_t SMEM_BYTES = (size_t)SMEM_FLOATS * sizeof(float);
