@@ -23,14 +23,13 @@ cudaError_t grid_of(K kernel, int threads, size_t smem, int *grid) {
 
 // Launch shapes: threads per CTA and ring depth of the passes with bulk copies.
 constexpr int kRowT = 128;
-constexpr bool kRowStaged = true;
 constexpr int kColT = 512, kColNB = 2;
 constexpr int kIkT = 512, kIkNB = 2;
 
 template <int N>
 cudaError_t rows_n(const float *S, float2 *T1, int ncomp, cudaStream_t s) {
-    constexpr size_t smem = f3t::RowTGeom<N, kRowT, kRowStaged>::SMEM_BYTES;
-    auto k = f3t::rowt_kernel<N, kRowT, kRowStaged>;
+    constexpr size_t smem = f3t::RowTGeom<N, kRowT>::SMEM_BYTES;
+    auto k = f3t::rowt_kernel<N, kRowT>;
     int g = 0;
     cudaError_t e = grid_of(k, kRowT, smem, &g);
     if (e != cudaSuccess) return e;

@@ -11,7 +11,7 @@
 //   pass 1 (rowt_kernel)   S[q][i][j][N+2] reals   -> T1[q][i][kz][j]
 //          rows along k, two real rows as one complex sequence (the row
 //          kernel of fft3d.cuh), each kz written as one 128-byte piece of
-//          16 consecutive j;
+//          16 consecutive j (eight 16-byte pair stores);
 //   pass 2 (colt_kernel)   T1 lines along j         -> T2[q][kz][ky][i]
 //          16 lines of consecutive i per tile, landed in shared memory by
 //          bulk copies (cp.async.bulk + mbarrier), each ky written as one
@@ -42,35 +42,30 @@ using pfft::FourStep;
 // pass 1: rows along k -> T1[q][i][kz][j]
 // ---------------------------------------------------------------------------
 // The row kernel of fft3d.cuh (cp.async ring, four-step FFT of row pairs in a
-// swizzled unpadded layout) with its output staged per tile in shared memory
-// as [kz][16 rows] (pitch 17 complex: the pair-wise writes of the separation,
-// lanes over kz, and the piece-wise reads, lanes over rows, both hit distinct
-// banks) and written as one 128-byte piece per kz.
-// Two output forms (STAGED): the separated pairs go through a staging tile
-// [kz][16 rows] in shared memory (pitch 17 complex) and leave as one 128-byte
-// piece of 16 rows per kz; or (direct) each thread separates one pair of rows
-// at one kz (lanes over the 8 pairs, 4 kz per warp) and stores the pair as
-// one 16-byte value, eight lanes making the 128-byte piece -- rows then sit
-// N + 2 floats apart in shared memory, so that the eight pairs' rows start
-// on different banks.
-template <int N, int T_ = 128, bool STAGED = true>
+// swizzled layout) with its output written transposed.  The separated pairs
+// go straight to HBM: each thread separates one pair of
+// rows at one kz (lanes over the 8 pairs, 4 kz per warp) and stores it as one
+// 16-byte value, eight lanes making the 128-byte piece of 16 rows.  Rows sit
+// N + 2 floats apart in shared memory, so that the eight pairs' rows start on
+// different banks.  (Staging the tile as [kz][16 rows] in shared memory and
+// writing it piece by piece gave the same bytes in 3.30 ms at 512^3 against
+// 2.28 ms: the extra barrier and shared-memory round trip held the 8 warps
+// per SM.)
+template <int N, int T_ = 128>
 struct RowTGeom {
-    using RG = f3d::RowGeom<N, 16, 2, T_, STAGED ? 0 : 2>;
-    static constexpr int NH = N / 2 + 1, SP = RG::R + 1;  // staging pitch (complex)
-    static constexpr size_t STAGE_BYTES = STAGED ? (size_t)NH * SP * sizeof(float2) : 0;
-    static constexpr size_t SMEM_BYTES = RG::SMEM_BYTES + STAGE_BYTES;
+    using RG = f3d::RowGeom<N, 16, 2, T_, 2>;
+    static constexpr size_t SMEM_BYTES = RG::SMEM_BYTES;
 };
 
-template <int N, int T_ = 128, bool STAGED = true>
+template <int N, int T_ = 128>
 __global__ void __launch_bounds__(T_, 2) rowt_kernel(const float *S, float2 *T1, long long nrows) {
-    using Gm = typename RowTGeom<N, T_, STAGED>::RG;
+    using Gm = typename RowTGeom<N, T_>::RG;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2,
                   NB = Gm::NB;
-    constexpr int RP = N + 2, NH = N / 2 + 1, SP = RowTGeom<N, T_, STAGED>::SP;
+    constexpr int RP = N + 2, NH = N / 2 + 1;
     static_assert(R == 16 && P == 8, "one 128-byte output piece per kz");
     extern __shared__ __align__(16) float smem[];
     float2 *tw = reinterpret_cast<float2 *>(smem + NB * Gm::BUF);
-    float2 *st = tw + N;  // staging [NH][SP]
     const int tid = threadIdx.x;
     f3d::twiddles<N>(tw);
     const long long ntiles = nrows / R;
@@ -92,7 +87,7 @@ __global__ void __launch_bounds__(T_, 2) rowt_kernel(const float *S, float2 *T1,
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
         float *rows = smem + (it % NB) * Gm::BUF;
         s32::cp_wait<NB - 2>();
-        __syncthreads();  // this tile landed; the buffer and the staging of tile it-1 are consumed
+        __syncthreads();  // this tile landed; the buffer of tile it-1 is consumed
         const long long ahead = tile + (long long)(NB - 1) * gridDim.x;
         if (ahead < ntiles) issue(ahead, (it + NB - 1) % NB);
         s32::cp_commit();
@@ -153,32 +148,14 @@ __global__ void __launch_bounds__(T_, 2) rowt_kernel(const float *S, float2 *T1,
         const long long qi = tile / (N / R);  // q N + i
         const int j0 = (int)(tile % (N / R)) * R;
         float2 *o = T1 + qi * NH * N + j0;
-        if constexpr (STAGED) {
-            // separate each pair into the staging tile [kz][row]
-            for (int t = tid; t < P * NH; t += T) {
-                const int p = t / NH, k = t % NH, km = (N - k) & (N - 1);
-                const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
-                const int ak = Gm::phys(k & (N - 1)), am = Gm::phys(km);
-                const float zr = re[ak], zi = im[ak], mr = re[am], mi = im[am];
-                st[k * SP + 2 * p] = make_float2(0.5f * (zr + mr), 0.5f * (zi - mi));
-                st[k * SP + 2 * p + 1] = make_float2(0.5f * (zi + mi), 0.5f * (mr - zr));
-            }
-            __syncthreads();
-            // one 128-byte piece of 16 rows per kz: T1[q][i][kz][j0 .. j0+15]
-            for (int t = tid; t < NH * R; t += T) {
-                const int kz = t / R, jj = t % R;
-                __stcs(o + (long long)kz * N + jj, st[kz * SP + jj]);
-            }
-        } else {
-            // pair p of kz k -> rows j0 + 2p, j0 + 2p + 1 of T1[q][i][k] as one 16-byte store
-            for (int t = tid; t < P * NH; t += T) {
-                const int p = t % P, k = t / P, km = (N - k) & (N - 1);
-                const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
-                const int ak = Gm::phys(k & (N - 1)), am = Gm::phys(km);
-                const float zr = re[ak], zi = im[ak], mr = re[am], mi = im[am];
-                __stcs(reinterpret_cast<float4 *>(o + (long long)k * N + 2 * p),
-                       make_float4(0.5f * (zr + mr), 0.5f * (zi - mi), 0.5f * (zi + mi), 0.5f * (mr - zr)));
-            }
+        // pair p of kz k -> rows j0 + 2p, j0 + 2p + 1 of T1[q][i][k] as one 16-byte store
+        for (int t = tid; t < P * NH; t += T) {
+            const int p = t % P, k = t / P, km = (N - k) & (N - 1);
+            const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
+            const int ak = Gm::phys(k & (N - 1)), am = Gm::phys(km);
+            const float zr = re[ak], zi = im[ak], mr = re[am], mi = im[am];
+            __stcs(reinterpret_cast<float4 *>(o + (long long)k * N + 2 * p),
+                   make_float4(0.5f * (zr + mr), 0.5f * (zi - mi), 0.5f * (zi + mi), 0.5f * (mr - zr)));
         }
     }
     s32::cp_wait<0>();

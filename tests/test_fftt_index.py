@@ -3,8 +3,9 @@
 the in-kernel ones.
 
 * pass 1 (rowt_kernel): tile t of 16 rows (q N + i = t / (N/16), rows
-  j0 = 16 (t % (N/16)) ..) of S[q][i][j][N+2]; kz of row j written to
-  T1 at ((q N + i) NH + kz) N + j;
+  j0 = 16 (t % (N/16)) ..) of S[q][i][j][N+2]; task (p = t % 8, kz = t / 8)
+  writes rows j0 + 2p, j0 + 2p + 1 at kz to T1 at ((q N + i) NH + kz) N +
+  j0 + 2p as one 16-byte pair;
 * pass 2 (colt_kernel): tile t = (q NH + kz) (N/16) + ib reads the 16 lines
   (q, i = 16 ib + w, kz) at ((q N + i) NH + kz) N, N values each, and writes
   output ky of line w to T2 at (q NH + kz) N N + ky N + 16 ib + w;
@@ -32,12 +33,12 @@ def _chain(N, ncomp, S):
         rows = flat[tile * R * RP:(tile + 1) * R * RP].reshape(R, RP)[:, :N]
         X = np.fft.rfft(rows, axis=1)  # [16][NH]
         qi, j0 = tile // (N // R), (tile % (N // R)) * R
-        kz = np.arange(NH)[:, None]
-        jj = np.arange(R)[None, :]
-        off = qi * NH * N + kz * N + j0 + jj
-        assert off.min() >= 0 and off.max() < ncomp * M
-        T1[off] = X.T
-        written[off] += 1
+        for t in range(8 * NH):  # the kernel's task order: p = t % 8, kz = t // 8
+            p, kz = t % 8, t // 8
+            off = qi * NH * N + kz * N + j0 + 2 * p
+            assert off % 2 == 0 and 0 <= off and off + 1 < ncomp * M  # 16-byte aligned pair
+            T1[off:off + 2] = X[2 * p:2 * p + 2, kz]
+            written[off:off + 2] += 1
     assert np.all(written == 1)
     # pass 2
     T2 = np.full(ncomp * M, np.nan + 0j, dtype=np.complex128)
