@@ -23,9 +23,23 @@
  *                        gsq from g2parameters.h), 1: lambda phi^4 in program
  *                        units with constants lam_pr, gsq_pr
  *   GABE_B200_PRECISION  0: FP64 (default), 1: FP32 fluctuation storage
+ *
+ * Checkpoint and restart (run-time, environment; the reference has neither):
+ *   GABE_B200_CHECKPOINT_EVERY=n and GABE_B200_CHECKPOINT=<file> write a
+ *   checkpoint (gabe_save_state) every n steps; a %d in <file> takes the
+ *   step count.
+ *   GABE_B200_RESTART=<file> starts from such a file -- or any gabe_dump.h
+ *   dump of this lattice -- instead of the state the reference's
+ *   initialisation made, and sets t to starttime + step * dt of the dump,
+ *   so the run continues the saved one (bit for bit from a checkpoint of
+ *   the same build and precision).
  */
 #include "gabe.h"
+#include "gabe_dump.h"
 #include "g2header.h"
+
+#include <cstdlib>
+#include <string>
 
 #ifndef GABE_B200_MODEL
 #define GABE_B200_MODEL 0
@@ -80,6 +94,25 @@ void ensure_device_state()
     if (rc != GABE_OK) {
         fprintf(stderr, "gabe_b200: gabe_create failed (status %d): %s\n", rc, gabe_last_error(nullptr));
         exit(1);
+    }
+    const char *restart = getenv("GABE_B200_RESTART");
+    if (restart && *restart) {
+        int restored = 0;
+        rc = gabe_load_state(g_gpu, restart, &restored);
+        if (rc != GABE_OK) gabe_die("gabe_load_state", rc);
+        gabe_dump_header hd;
+        FILE *f = fopen(restart, "rb");
+        if (!f || fread(&hd, sizeof(hd), 1, f) != 1) {
+            fprintf(stderr, "gabe_b200: cannot read the header of %s\n", restart);
+            exit(1);
+        }
+        fclose(f);
+        t = starttime + (gNum)hd.step * dt;
+        g_steps = (long)hd.step;
+        pull_scalars();
+        printf("gabe_b200: %s %s at step %lld, t = %e\n", restored ? "restarted from" : "initial state from", restart,
+               (long long)hd.step, (double)t);
+        return;
     }
     const double *h0 = nullptr, *l0 = nullptr;
 #if calc_gws == 1
@@ -173,6 +206,15 @@ void step()
     if (rc != GABE_OK) gabe_die("gabe_step", rc);
     g_steps++;
     pull_scalars();
+    static const char *every_s = getenv("GABE_B200_CHECKPOINT_EVERY"), *path = getenv("GABE_B200_CHECKPOINT");
+    static const long every = every_s ? atol(every_s) : 0;
+    if (every > 0 && path && *path && g_steps % every == 0) {
+        std::string name(path);
+        const size_t at = name.find("%d");
+        if (at != std::string::npos) name.replace(at, 2, std::to_string(g_steps));
+        rc = gabe_save_state(g_gpu, name.c_str());
+        if (rc != GABE_OK) gabe_die("gabe_save_state", rc);
+    }
 }
 
 // outputslice() (g2output.cpp:129-186): the same cadence, the same files in
@@ -183,6 +225,7 @@ void outputslice()
     static int first = 0;
     static int lastslice, lastspec;
     static int slicewaitm;
+    ensure_device_state();  // a restart sets t before the first row is written
     if (first == 0) {
         slicewaitm = slicewait == 0 ? slicewaitf() : slicewait;
         lastslice = slicewaitm;

@@ -68,3 +68,33 @@ def test_dropin_program_matches_reference_program(cfg, tmp_path):
             assert _close(got, want, 1e-5, floor_frac=1e-10), n
         else:
             assert _close(got, want, 2e-6), n
+
+
+def test_dropin_checkpoint_and_restart_continue_the_run(tmp_path):
+    """GABE_B200_CHECKPOINT(_EVERY) writes checkpoints from the drop-in
+    program; GABE_B200_RESTART starts a new run from one, at the saved
+    step's time.  The restarted run's slices_time.dat rows must equal the
+    uninterrupted run's rows at the same times, to every printed digit (the
+    restart block holds the device state bit for bit)."""
+    gpu_bin = os.path.join(po.REF_DIR, "dropin_m1_n32_g1_p0")
+    if not os.path.exists(gpu_bin):
+        pytest.skip("drop-in programs are built by `make -C oracle full dropin` where the reference is mounted")
+    a, b = tmp_path / "full", tmp_path / "restart"
+    for d in (a, b):
+        os.makedirs(d / "slices")
+    ck = str(tmp_path / "ck_%d.bin")
+    env = dict(os.environ, GABE_REF_THREADS="1", GABE_B200_CHECKPOINT=ck, GABE_B200_CHECKPOINT_EVERY="10")
+    r = subprocess.run([gpu_bin], cwd=str(a), capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert os.path.exists(str(tmp_path / "ck_10.bin"))
+    env = dict(os.environ, GABE_REF_THREADS="1", GABE_B200_RESTART=str(tmp_path / "ck_10.bin"))
+    r = subprocess.run([gpu_bin], cwd=str(b), capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "restarted from" in r.stdout
+    full = {row[0]: row for row in np.loadtxt(a / "slices" / "slices_time.dat", ndmin=2)}
+    rest = np.loadtxt(b / "slices" / "slices_time.dat", ndmin=2)
+    assert rest[0, 0] == pytest.approx(0.1) and len(rest) >= 2
+    common = [row for row in rest if row[0] in full]
+    assert len(common) >= 2
+    for row in common:
+        np.testing.assert_array_equal(row, full[row[0]])
