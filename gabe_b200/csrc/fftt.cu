@@ -52,7 +52,7 @@ cudaError_t cols_n(const float2 *T1, float2 *T2, int ncomp, unsigned int *status
 // divisions held its warps at the barriers.
 template <int N>
 cudaError_t ik_n(const f3t::IkArgs &a, cudaStream_t s) {
-    constexpr size_t smem = f3t::LineRing<N, f3t::kIkLines, kIkNB>::SMEM_BYTES;
+    constexpr size_t smem = f3t::LineRing<N, f3t::kIkLines, kIkNB, 2 * kSrc>::SMEM_BYTES;
     auto k = f3t::ikspace_kernel<N, kIkT, kIkNB, true>;
     int g = 0;
     cudaError_t e = grid_of(k, kIkT, smem, &g);

@@ -201,15 +201,18 @@ __device__ __forceinline__ void lines_step_b(const float2 *buf, int w, int k2, f
 
 // Shared-memory ring of NB tiles, each of nl lines of pitch N + 2, filled by
 // bulk copies; barrier b completes when tile buffer b has landed.
-template <int N, int NL, int NB>
+// EXTRA lines of pitch N + 2 follow the ring (a result area).
+template <int N, int NL, int NB, int EXTRA = 0>
 struct LineRing {
     static constexpr int PL = N + 2, BUF = NL * PL;
     static constexpr size_t HEAD = 128;  // NB mbarriers (8 bytes each)
-    static constexpr size_t SMEM_BYTES = HEAD + (size_t)N * sizeof(float2) + (size_t)NB * BUF * sizeof(float2);
+    static constexpr size_t SMEM_BYTES =
+        HEAD + (size_t)N * sizeof(float2) + ((size_t)NB * BUF + (size_t)EXTRA * PL) * sizeof(float2);
     static_assert(NB * 8 <= (int)HEAD, "barriers fit the head");
     __device__ static uint64_t *bars(unsigned char *sm) { return reinterpret_cast<uint64_t *>(sm); }
     __device__ static float2 *twid(unsigned char *sm) { return reinterpret_cast<float2 *>(sm + HEAD); }
     __device__ static float2 *buf(unsigned char *sm, int b) { return twid(sm) + N + b * BUF; }
+    __device__ static float2 *extra(unsigned char *sm) { return twid(sm) + N + NB * BUF; }
 };
 
 // ---------------------------------------------------------------------------
@@ -297,14 +300,20 @@ struct IkArgs {
     unsigned int *status;
 };
 
+// Three barriers per (kz, ky): after the bulk copies land, after step A, and
+// after step B, whose results go to a separate area (the transformed
+// source lines) so that it needs no barrier between its reads and writes;
+// the refill of a ring buffer is issued after the next task's first barrier,
+// by which every thread has finished reading it.
 template <int N, int T, int NB, bool POL32 = false>
 __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
-    using Rg = LineRing<N, kIkLines, NB>;
+    using Rg = LineRing<N, kIkLines, NB, 2 * kSrc>;
     constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, NH = N / 2 + 1, PL = Rg::PL;
     constexpr long long M = (long long)NH * N * N;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t *bar = Rg::bars(sm);
     float2 *tw = Rg::twid(sm);
+    float2 *xs = Rg::extra(sm);  // [10][PL]: the source lines transformed along i, natural order
     const int tid = threadIdx.x;
     constexpr long long ntasks = (long long)NH * N;  // task = kz N + ky
     const KsCoef<float> kc = ks_coef<float>(a.c, a.sc->gw[a.slot]);
@@ -332,41 +341,29 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
     int it = 0;
     for (long long task = blockIdx.x; task < ntasks; task += gridDim.x, it++) {
         const int b = it % NB;
+        const bool ok = tma::mbar_wait(&bar[b], (uint32_t)((it / NB) & 1), a.status);
+        if (__syncthreads_or(!ok)) {  // also: every thread is done with task it-1 (its buffer, xs)
+            if (tid == 0) tma::drain(bar, fills, NB, a.status);
+            break;
+        }
         if (tid == 0) {
             const long long ahead = task + (long long)(NB - 1) * gridDim.x;
             if (ahead < ntasks) {
-                tma::fence_proxy_async();
+                tma::fence_proxy_async();  // the buffer's last reads (task it-1) precede its refill
                 issue(ahead, (it + NB - 1) % NB);
             }
-        }
-        const bool ok = tma::mbar_wait(&bar[b], (uint32_t)((it / NB) & 1), a.status);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) tma::drain(bar, fills, NB, a.status);
-            break;
         }
         float2 *buf = Rg::buf(sm, b);
         lines_step_a<N, T>(buf, 2 * kSrc, tw);
         __syncthreads();
-        // step B over the ten source lines (lanes over lines), results back in natural order
-        {
-            constexpr int NT = (2 * kSrc * L2 + T - 1) / T;
-            float2 y[NT][L1];
+        // step B over the ten source lines (lanes over lines) into xs in natural order
+        for (int t = tid; t < 2 * kSrc * L2; t += T) {
+            const int w = t % (2 * kSrc), k2 = t / (2 * kSrc);
+            float2 y[L1];
+            lines_step_b<N>(buf, w, k2, y);
+            float2 *ln = xs + w * PL;
 #pragma unroll
-            for (int r = 0; r < NT; r++) {
-                const int t = r * T + tid;
-                if (t < 2 * kSrc * L2) lines_step_b<N>(buf, t % (2 * kSrc), t / (2 * kSrc), y[r]);
-            }
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < NT; r++) {
-                const int t = r * T + tid;
-                if (t < 2 * kSrc * L2) {
-                    float2 *ln = buf + (t % (2 * kSrc)) * PL;
-                    const int k2 = t / (2 * kSrc);
-#pragma unroll
-                    for (int k1 = 0; k1 < L1; k1++) ln[k2 + L2 * k1] = y[r][k1];
-                }
-            }
+            for (int k1 = 0; k1 < L1; k1++) ln[k2 + L2 * k1] = y[k1];
         }
         __syncthreads();
         const int kz = (int)(task / N), ky = (int)(task % N);
@@ -376,7 +373,7 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
             Cplx<float> s[10], g[4];
 #pragma unroll
             for (int q = 0; q < 2 * kSrc; q++) {
-                const float2 v = buf[q * PL + kx];
+                const float2 v = xs[q * PL + kx];
                 s[q] = {v.x, v.y};
             }
 #pragma unroll
@@ -389,7 +386,6 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
 #pragma unroll
             for (int p = 0; p < 4; p++) gout[p * M + kx] = make_float2(g[p].re, g[p].im);
         }
-        __syncthreads();  // buffer b consumed
     }
 }
 
