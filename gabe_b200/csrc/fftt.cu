@@ -24,7 +24,7 @@ cudaError_t grid_of(K kernel, int threads, size_t smem, int *grid) {
 // Launch shapes: threads per CTA and ring depth of the passes with bulk copies.
 constexpr int kRowT = 128;
 constexpr int kColT = 512, kColNB = 2;
-constexpr int kIkT = 512, kIkNB = 2;
+constexpr int kIkT = 192, kIkNB = 1, kIkMinB = 2;
 
 template <int N>
 cudaError_t rows_n(const float *S, float2 *T1, int ncomp, cudaStream_t s) {
@@ -52,8 +52,8 @@ cudaError_t cols_n(const float2 *T1, float2 *T2, int ncomp, unsigned int *status
 // divisions held its warps at the barriers.
 template <int N>
 cudaError_t ik_n(const f3t::IkArgs &a, cudaStream_t s) {
-    constexpr size_t smem = f3t::LineRing<N, f3t::kIkLines, kIkNB, 2 * kSrc>::SMEM_BYTES;
-    auto k = f3t::ikspace_kernel<N, kIkT, kIkNB, true>;
+    constexpr size_t smem = f3t::LineRing<N, 2 * kSrc, kIkNB, 2 * kSrc>::SMEM_BYTES;
+    auto k = f3t::ikspace_kernel<N, kIkT, kIkNB, kIkMinB>;
     int g = 0;
     cudaError_t e = grid_of(k, kIkT, smem, &g);
     if (e != cudaSuccess) return e;

@@ -57,8 +57,8 @@ struct RowTGeom {
     static constexpr size_t SMEM_BYTES = RG::SMEM_BYTES;
 };
 
-template <int N, int T_ = 128>
-__global__ void __launch_bounds__(T_, 2) rowt_kernel(const float *S, float2 *T1, long long nrows) {
+template <int N, int T_ = 128, int MINB = 2>
+__global__ void __launch_bounds__(T_, MINB) rowt_kernel(const float *S, float2 *T1, long long nrows) {
     using Gm = typename RowTGeom<N, T_>::RG;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2,
                   NB = Gm::NB;
@@ -92,24 +92,27 @@ __global__ void __launch_bounds__(T_, 2) rowt_kernel(const float *S, float2 *T1,
         if (ahead < ntiles) issue(ahead, (it + NB - 1) % NB);
         s32::cp_commit();
         // four-step pass 1: L2-point FFTs over n2 (stride L1), twiddle W_N^(n1 k2), in place
-#pragma unroll
-        for (int t0 = 0; t0 < P * L1; t0 += T) {
-            const int t = t0 + tid, p = t / L1, n1 = t % L1;
-            if (t >= P * L1) break;
+        // two adjacent n1 per thread: each pair of reals is one 8-byte access
+        for (int t = tid; t < P * (L1 / 2); t += T) {
+            const int p = t / (L1 / 2), n1 = 2 * (t % (L1 / 2));
             float *re = rows + 2 * p * PITCH, *im = re + PITCH;
-            float2 x[L2];
+            float2 xa[L2], xb[L2];
 #pragma unroll
             for (int n2 = 0; n2 < L2; n2++) {
                 const int a = Gm::phys(n1 + L1 * n2);
-                x[n2] = make_float2(re[a], im[a]);
+                const float2 r2 = *reinterpret_cast<const float2 *>(re + a), i2 = *reinterpret_cast<const float2 *>(im + a);
+                xa[n2] = make_float2(r2.x, i2.x);
+                xb[n2] = make_float2(r2.y, i2.y);
             }
-            pfft::fft_reg<L2>(x);
+            pfft::fft_reg<L2>(xa);
+            pfft::fft_reg<L2>(xb);
 #pragma unroll
             for (int k2 = 0; k2 < L2; k2++) {
-                const float2 y = k2 ? pfft::cmul(x[k2], tw[k2 * L1 + n1]) : x[k2];
+                const float2 ya = k2 ? pfft::cmul(xa[k2], tw[k2 * L1 + n1]) : xa[k2];
+                const float2 yb = k2 ? pfft::cmul(xb[k2], tw[k2 * L1 + n1 + 1]) : xb[k2];
                 const int a = Gm::phys(n1 + L1 * k2);
-                re[a] = y.x;
-                im[a] = y.y;
+                *reinterpret_cast<float2 *>(re + a) = make_float2(ya.x, yb.x);
+                *reinterpret_cast<float2 *>(im + a) = make_float2(ya.y, yb.y);
             }
         }
         __syncthreads();
@@ -122,9 +125,12 @@ __global__ void __launch_bounds__(T_, 2) rowt_kernel(const float *S, float2 *T1,
                 if (t < P * L2) {
                     const float *re = rows + 2 * p * PITCH, *im = re + PITCH;
 #pragma unroll
-                    for (int n1 = 0; n1 < L1; n1++) {
+                    for (int n1 = 0; n1 < L1; n1 += 2) {
                         const int a = Gm::phys(n1 + L1 * k2);
-                        y[q][n1] = make_float2(re[a], im[a]);
+                        const float2 r2 = *reinterpret_cast<const float2 *>(re + a);
+                        const float2 i2 = *reinterpret_cast<const float2 *>(im + a);
+                        y[q][n1] = make_float2(r2.x, i2.x);
+                        y[q][n1 + 1] = make_float2(r2.y, i2.y);
                     }
                     pfft::fft_reg<L1>(y[q]);
                 }
@@ -220,8 +226,8 @@ struct LineRing {
 // ---------------------------------------------------------------------------
 constexpr int kColW = 16;  // lines (consecutive i) per tile: one 128-byte output piece per ky
 
-template <int N, int T, int NB>
-__global__ void __launch_bounds__(T, 1) colt_kernel(const float2 *__restrict__ T1, float2 *__restrict__ T2, int ncomp,
+template <int N, int T, int NB, int MINB = 1>
+__global__ void __launch_bounds__(T, MINB) colt_kernel(const float2 *__restrict__ T1, float2 *__restrict__ T2, int ncomp,
                                                     unsigned int *status) {
     using Rg = LineRing<N, kColW, NB>;
     constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, NH = N / 2 + 1, W = kColW;
@@ -289,7 +295,6 @@ __global__ void __launch_bounds__(T, 1) colt_kernel(const float2 *__restrict__ T
 // ---------------------------------------------------------------------------
 // pass 3: along i, fused with the TT projection and both RK2 stages of h, l
 // ---------------------------------------------------------------------------
-constexpr int kIkLines = 14;  // 10 source lines + 4 amplitude lines per (kz, ky)
 
 struct IkArgs {
     const float2 *T2;  // [10][NH][N][N]
@@ -301,14 +306,22 @@ struct IkArgs {
 };
 
 // Three barriers per (kz, ky): after the bulk copies land, after step A, and
-// after step B, whose results go to a separate area (the transformed
-// source lines) so that it needs no barrier between its reads and writes;
-// the refill of a ring buffer is issued after the next task's first barrier,
-// by which every thread has finished reading it.
-template <int N, int T, int NB, bool POL32 = false>
-__global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
-    using Rg = LineRing<N, kIkLines, NB, 2 * kSrc>;
+// after step B, whose results go to a separate area (the transformed source
+// lines) so that it needs no barrier between its reads and writes.  The
+// amplitudes are read straight from global memory: each thread loads its
+// k-points' four amplitudes into registers when a task starts (the loads
+// overlap the wait for the source lines), so the ring holds only the ten
+// source lines and two CTAs fit on an SM -- one CTA's transforms fill the
+// other's barrier waits (1.69 ms at 512^3 for two CTAs of 192 threads,
+// 1.75 for 256, against 2.28 for one CTA of 512 threads with the amplitude
+// lines in its ring).  Buffer b is refilled as
+// soon as step B has read it (third barrier), while the k-space phase of
+// the same task runs.
+template <int N, int T, int NB, int MINB>
+__global__ void __launch_bounds__(T, MINB) ikspace_kernel(IkArgs a) {
+    using Rg = LineRing<N, 2 * kSrc, NB, 2 * kSrc>;
     constexpr int L1 = FourStep<N>::L1, L2 = FourStep<N>::L2, NH = N / 2 + 1, PL = Rg::PL;
+    constexpr int KPT = (N + T - 1) / T;  // k-points per thread
     constexpr long long M = (long long)NH * N * N;
     extern __shared__ __align__(128) unsigned char sm[];
     uint64_t *bar = Rg::bars(sm);
@@ -327,31 +340,30 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
     auto issue = [&](long long task, int b) {
         fills[b]++;
         float2 *dst = Rg::buf(sm, b);
-        tma::mbar_arrive_expect(&bar[b], kIkLines * N * (uint32_t)sizeof(float2));
+        tma::mbar_arrive_expect(&bar[b], 2 * kSrc * N * (uint32_t)sizeof(float2));
         for (int q = 0; q < 2 * kSrc; q++)
             tma::load(dst + q * PL, a.T2 + q * M + task * N, N * (uint32_t)sizeof(float2), &bar[b]);
-        for (int p = 0; p < 4; p++)
-            tma::load(dst + (2 * kSrc + p) * PL, a.G + p * M + task * N, N * (uint32_t)sizeof(float2), &bar[b]);
     };
     if (tid == 0)
-        for (int q = 0; q < NB - 1; q++) {
+        for (int q = 0; q < NB; q++) {
             const long long t = blockIdx.x + (long long)q * gridDim.x;
             if (t < ntasks) issue(t, q);
         }
     int it = 0;
     for (long long task = blockIdx.x; task < ntasks; task += gridDim.x, it++) {
         const int b = it % NB;
+        float2 *gl = a.G + task * N;
+        float2 gv[KPT][4];
+#pragma unroll
+        for (int r = 0; r < KPT; r++) {
+            const int kx = tid + r * T;
+#pragma unroll
+            for (int p = 0; p < 4; p++) gv[r][p] = kx < N ? __ldcs(gl + p * M + kx) : make_float2(0.f, 0.f);
+        }
         const bool ok = tma::mbar_wait(&bar[b], (uint32_t)((it / NB) & 1), a.status);
-        if (__syncthreads_or(!ok)) {  // also: every thread is done with task it-1 (its buffer, xs)
+        if (__syncthreads_or(!ok)) {  // also: every thread is done with task it-1's k-space phase (xs)
             if (tid == 0) tma::drain(bar, fills, NB, a.status);
             break;
-        }
-        if (tid == 0) {
-            const long long ahead = task + (long long)(NB - 1) * gridDim.x;
-            if (ahead < ntasks) {
-                tma::fence_proxy_async();  // the buffer's last reads (task it-1) precede its refill
-                issue(ahead, (it + NB - 1) % NB);
-            }
         }
         float2 *buf = Rg::buf(sm, b);
         lines_step_a<N, T>(buf, 2 * kSrc, tw);
@@ -366,10 +378,19 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
             for (int k1 = 0; k1 < L1; k1++) ln[k2 + L2 * k1] = y[k1];
         }
         __syncthreads();
+        if (tid == 0) {
+            const long long ahead = task + (long long)NB * gridDim.x;
+            if (ahead < ntasks) {
+                tma::fence_proxy_async();  // the buffer's reads by steps A and B precede its refill
+                issue(ahead, b);
+            }
+        }
         const int kz = (int)(task / N), ky = (int)(task % N);
         const int py = ky <= N / 2 ? ky : ky - N;
-        float2 *gout = a.G + task * N;
-        for (int kx = tid; kx < N; kx += T) {
+#pragma unroll
+        for (int r = 0; r < KPT; r++) {
+            const int kx = tid + r * T;
+            if (kx >= N) break;
             Cplx<float> s[10], g[4];
 #pragma unroll
             for (int q = 0; q < 2 * kSrc; q++) {
@@ -377,14 +398,11 @@ __global__ void __launch_bounds__(T, 1) ikspace_kernel(IkArgs a) {
                 s[q] = {v.x, v.y};
             }
 #pragma unroll
-            for (int p = 0; p < 4; p++) {
-                const float2 v = buf[(2 * kSrc + p) * PL + kx];
-                g[p] = {v.x, v.y};
-            }
+            for (int p = 0; p < 4; p++) g[p] = {gv[r][p].x, gv[r][p].y};
             const int px = kx <= N / 2 ? kx : kx - N;
-            kspace_update_vals<float, POL32>(kc, px, py, kz, s, g);
+            kspace_update_vals<float, true>(kc, px, py, kz, s, g);
 #pragma unroll
-            for (int p = 0; p < 4; p++) gout[p * M + kx] = make_float2(g[p].re, g[p].im);
+            for (int p = 0; p < 4; p++) __stcs(gl + p * M + kx, make_float2(g[p].re, g[p].im));
         }
     }
 }

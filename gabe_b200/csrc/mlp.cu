@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(T, 2) gemm_tc_kernel(Args g) {
 // 1 .. nl-1 (the layers the tensor-core forward runs).
 struct WtTable {
     int nl;
-    long long offW[17], offWt[17], offb[17];
+    long long offW[17], offWt[17];
     int K[17], N[17];
 };
 
@@ -315,123 +315,6 @@ __global__ void weights_bf16t_kernel(const float *params, bf16 *wt, WtTable t) {
             Wt[i] = __float2bfloat16_rn(W[(long long)k * t.N[l] + nn]);
         }
     }
-}
-
-// ---------------------------------------------------------------------------
-// Fused inference forward (gabe_mlp_forward with BF16 activations, hidden
-// width 256): one CTA carries a tile of 128 rows through every layer.  The
-// activations stay in shared memory (two BF16 buffers of 128 x 264, the
-// padding making every ldmatrix conflict-free); the first layer (a handful
-// of FP32 inputs) is taken on CUDA cores exactly as the layer-by-layer
-// forward takes it; each later layer multiplies the activations by its BF16
-// transposed weights, streamed from L2 in 32-deep slices through a 4-stage
-// cp.async ring that runs on across layer boundaries, with mma.sync BF16 x
-// BF16 -> FP32 (8 warps, 64 rows x 64 columns each); the epilogue adds the
-// bias, applies SiLU and writes the next layer's activations in BF16, or the
-// FP32 outputs.  The same operations in the same order as the layer-by-layer
-// path, without its four HBM round trips of the activations and its five
-// launches.
-// ---------------------------------------------------------------------------
-constexpr int FBM = 128, FW = 256, FHP = FW + 8;
-constexpr size_t F_H_BYTES = 2ull * FBM * FHP * sizeof(bf16);
-constexpr size_t F_B_BYTES = (size_t)STAGES * FW * LDS * sizeof(bf16);
-constexpr size_t F_SMEM_BYTES = F_H_BYTES + F_B_BYTES;
-
-template <int NF_OUT>
-__global__ void __launch_bounds__(T, 1) mlp_fused_kernel(const float *x, int rows, int n_in, const float *params,
-                                                          const bf16 *wt, WtTable tab, float *y) {
-    extern __shared__ __align__(16) unsigned char smraw[];
-    auto H = reinterpret_cast<bf16(*)[FBM][FHP]>(smraw);            // [2][FBM][FHP]
-    auto Bs = reinterpret_cast<bf16(*)[FW][LDS]>(smraw + F_H_BYTES);  // [STAGES][FW][LDS]
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps
-    const int m0 = blockIdx.x * FBM;
-    const int nl = tab.nl;
-    constexpr int SPL = FW / BK;        // slices per layer (K = 256)
-    const int S = (nl - 1) * SPL;       // slices of all tensor-core layers
-    auto load_slice = [&](int sl) {
-        const int l = 1 + sl / SPL, kc = sl % SPL, N = tab.N[l], st = sl % STAGES;
-        const bf16 *src = wt + tab.offWt[l] + kc * BK;
-        for (int idx = tid; idx < N * (BK / 8); idx += T) {
-            const int n = idx >> 2, c8 = (idx & 3) * 8;
-            cp16(&Bs[st][n][c8], src + (long long)n * FW + c8);
-        }
-    };
-#pragma unroll
-    for (int q = 0; q < STAGES - 1; q++) {
-        if (q < S) load_slice(q);
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
-    }
-    // layer 0 on CUDA cores: z = sum_k x_k W0[k][n] (k in order, FMA) + b_n
-    {
-        const float *W0 = params + tab.offW[0], *b0 = params + tab.offb[0];
-        for (int idx = tid; idx < FBM * FW; idx += T) {
-            const int r = idx / FW, n = idx % FW, gr = m0 + r;
-            float acc = 0.f;
-            if (gr < rows)
-                for (int k = 0; k < n_in; k++) acc = fmaf(x[(long long)gr * n_in + k], W0[k * FW + n], acc);
-            H[0][r][n] = __float2bfloat16_rn(silu(acc + b0[n]));
-        }
-    }
-    int cur = 0, sl = 0;
-    for (int l = 1; l < nl; l++) {
-        const bool last = l == nl - 1;
-        const int nfw = last ? NF_OUT : 8;  // 8-column fragments per warp
-        float acc[4][8][4];
-#pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 8; j++)
-#pragma unroll
-                for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
-        for (int kc = 0; kc < SPL; kc++, sl++) {
-            const int st = sl % STAGES;
-            asm volatile("cp.async.wait_group %0;\n" ::"n"(STAGES - 2) : "memory");
-            __syncthreads();  // slice sl (and the previous layer's activations) visible; slice sl-1 consumed
-            if (sl + STAGES - 1 < S) load_slice(sl + STAGES - 1);
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-#pragma unroll
-            for (int ks = 0; ks < BK / 16; ks++) {
-                const int k0 = kc * BK + ks * 16;
-                uint32_t a[4][4];
-#pragma unroll
-                for (int mf = 0; mf < 4; mf++)
-                    ldsm4(a[mf], &H[cur][wm * 64 + mf * 16 + (lane & 7) + ((lane >> 3) & 1) * 8][k0 + (lane >> 4) * 8]);
-#pragma unroll
-                for (int nb = 0; nb < 4; nb++) {
-                    if (2 * nb >= nfw) break;
-                    uint32_t b[4];
-                    ldsm4(b, &Bs[st][wn * nfw * 8 + nb * 16 + (lane & 7) + (lane >> 4) * 8][ks * 16 + ((lane >> 3) & 1) * 8]);
-#pragma unroll
-                    for (int mf = 0; mf < 4; mf++) {
-                        mma_bf16(acc[mf][2 * nb], a[mf], b[0], b[1]);
-                        mma_bf16(acc[mf][2 * nb + 1], a[mf], b[2], b[3]);
-                    }
-                }
-            }
-        }
-        const float *bias = params + tab.offb[l];
-        const int gr = lane >> 2, gc = (lane & 3) * 2;
-#pragma unroll
-        for (int mf = 0; mf < 4; mf++)
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int r = wm * 64 + mf * 16 + gr + 8 * h;
-#pragma unroll
-                for (int nf = 0; nf < 8; nf++) {
-                    if (nf >= nfw) break;
-                    const int n = wn * nfw * 8 + nf * 8 + gc;
-                    const float z0 = acc[mf][nf][2 * h] + bias[n], z1 = acc[mf][nf][2 * h + 1] + bias[n + 1];
-                    if (!last) {
-                        *reinterpret_cast<__nv_bfloat162 *>(&H[cur ^ 1][r][n]) = __floats2bfloat162_rn(silu(z0), silu(z1));
-                    } else if (m0 + r < rows) {
-                        *reinterpret_cast<float2 *>(y + (long long)(m0 + r) * tab.N[l] + n) = make_float2(z0, z1);
-                    }
-                }
-            }
-        cur ^= 1;  // the next layer's first barrier orders these writes before its reads
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 }  // namespace tc
@@ -755,34 +638,6 @@ int backward_rows(gabe_mlp *m, const float *x, int rows) {
     return GABE_OK;
 }
 
-// The fused inference forward takes BF16 activations, hidden width 256 and
-// n_out in {64, 128, 192, 256}; other shapes run layer by layer.
-bool fused_ok(const gabe_mlp *m) {
-    const int no = m->p.n_out;
-    return !m->f32act && m->p.width == tc::FW && (no == 64 || no == 128 || no == 192 || no == 256);
-}
-
-template <int NF>
-int launch_fused(gabe_mlp *m, const float *x, int rows, float *y) {
-    MCK(m, cudaFuncSetAttribute(tc::mlp_fused_kernel<NF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)tc::F_SMEM_BYTES));
-    const int grid = (rows + tc::FBM - 1) / tc::FBM;
-    tc::mlp_fused_kernel<NF><<<grid, tc::T, tc::F_SMEM_BYTES, m->stream>>>(x, rows, m->p.n_in, m->params, m->wt,
-                                                                           m->wtab, y);
-    MCK(m, cudaGetLastError());
-    return GABE_OK;
-}
-
-int fwd_fused(gabe_mlp *m, const float *x, int rows, float *y) {
-    if (rows <= 0) return GABE_OK;
-    switch (m->p.n_out) {
-        case 64: return launch_fused<2>(m, x, rows, y);
-        case 128: return launch_fused<4>(m, x, rows, y);
-        case 192: return launch_fused<6>(m, x, rows, y);
-        default: return launch_fused<8>(m, x, rows, y);
-    }
-}
-
 int fwd(gabe_mlp *m, const float *x, int rows, float *y, bool keep_z) {
     return m->f32act ? forward_rows<float>(m, x, rows, y, keep_z) : forward_rows<bf16>(m, x, rows, y, keep_z);
 }
@@ -874,7 +729,6 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         m->wtab.offWt[l] = nwt;
         if (l > 0) nwt += (long long)m->K[l] * m->N[l];
         m->P += (long long)m->K[l] * m->N[l];
-        m->wtab.offb[l] = m->P;
         m->offb.push_back(m->P);
         m->P += m->N[l];
     }
@@ -971,14 +825,6 @@ int gabe_mlp_get_params(gabe_mlp *m, float *h_params) {
 int gabe_mlp_forward(gabe_mlp *m, const float *x, int64_t n, float *y) {
     if (!m || n < 0 || (n > 0 && (!x || !y))) return GABE_ERR_PARAM;
     MCK(m, cudaSetDevice(m->dev));
-    if (fused_ok(m)) {
-        for (int64_t r0 = 0; r0 < n; r0 += (int64_t)1 << 28) {
-            const int rows = (int)((n - r0) < ((int64_t)1 << 28) ? (n - r0) : ((int64_t)1 << 28));
-            int rc = fwd_fused(m, x + r0 * m->p.n_in, rows, y + r0 * m->p.n_out);
-            if (rc) return rc;
-        }
-        return GABE_OK;
-    }
     for (int64_t r0 = 0; r0 < n; r0 += m->p.max_rows) {
         const int rows = (int)((n - r0) < m->p.max_rows ? (n - r0) : m->p.max_rows);
         int rc = fwd(m, x + r0 * m->p.n_in, rows, y + r0 * m->p.n_out, false);
@@ -1093,7 +939,7 @@ int gabe_mlp_launches_per_train_step(const gabe_mlp *m) {
 }
 
 
-int gabe_mlp_launches_per_forward(const gabe_mlp *m) { return m ? (fused_ok(m) ? 1 : m->nl) : 0; }
+int gabe_mlp_launches_per_forward(const gabe_mlp *m) { return m ? m->nl : 0; }
 
 const char *gabe_mlp_last_error(const gabe_mlp *m) { return m ? m->err.c_str() : g_mlp_create_error.c_str(); }
 

@@ -94,16 +94,26 @@ __device__ __forceinline__ void source_add64(const LatticeConsts &c, const Nb7<d
     s[3] += -c13 * d1 * d1 + c23 * d2 * d2 - c13 * d3 * d3;
     s[4] += (dn * d2 * d3);
 }
-__device__ __forceinline__ void source_add32(float dn, const Nb7<float> &f, float *s) {
-    const float d1 = 0.5f * (f.v[1] - f.v[2]);
-    const float d2 = 0.5f * (f.v[3] - f.v[4]);
-    const float d3 = 0.5f * (f.v[5] - f.v[6]);
-    const float t = (1.f / 3.f) * (d1 * d1 + d2 * d2 + d3 * d3);
-    s[0] += dn * (d1 * d1 - t);
-    s[1] += dn * d1 * d2;
-    s[2] += dn * d1 * d3;
-    s[3] += dn * (d2 * d2 - t);
-    s[4] += dn * d2 * d3;
+// FP32 form: the products of the undivided central differences e_i =
+// f(x + e_i) - f(x - e_i) are summed over both fields first (grad_prod_add),
+// then scaled once (source_from_prod): dn/4 (e_i e_j - delta_ij |e|^2 / 3),
+// the same tensor as source_add64 in fewer instructions.
+__device__ __forceinline__ void grad_prod_add(const Nb7<float> &f, float (&P)[6]) {
+    const float e1 = f.v[1] - f.v[2], e2 = f.v[3] - f.v[4], e3 = f.v[5] - f.v[6];
+    P[0] = fmaf(e1, e1, P[0]);
+    P[1] = fmaf(e2, e2, P[1]);
+    P[2] = fmaf(e3, e3, P[2]);
+    P[3] = fmaf(e1, e2, P[3]);
+    P[4] = fmaf(e1, e3, P[4]);
+    P[5] = fmaf(e2, e3, P[5]);
+}
+__device__ __forceinline__ void source_from_prod(float q /* dn / 4 */, const float (&P)[6], float *s) {
+    const float t = (1.f / 3.f) * ((P[0] + P[1]) + P[2]);
+    s[0] = q * (P[0] - t);
+    s[1] = q * P[3];
+    s[2] = q * P[4];
+    s[3] = q * (P[1] - t);
+    s[4] = q * P[5];
 }
 
 // Homogeneous-trajectory values of the FP32 path (start and midpoint of a

@@ -50,7 +50,7 @@ struct Ring {
 struct Site32 {
     MeanTraj mt;
     MeanF m0, m1;
-    float ia02f, ia12f, c3H0f, c3H1f, hf, dtf, inv_dx2f, dnf, q3f;
+    float ia02f, ia12f, c3H0f, c3H1f, hf, dtf, inv_dx2f, qsf, q3f;  // qsf = dn / 4
 };
 
 template <int MODE>
@@ -64,7 +64,7 @@ __device__ __forceinline__ Site32 site32_consts(const LatticeConsts &c, const De
     s.hf = (float)h;
     s.dtf = (float)c.dt;
     s.inv_dx2f = (float)(1.0 / c.inv_dx2_div);
-    s.dnf = (float)c.dn;
+    s.qsf = (float)(0.25 * c.dn);
     s.q3f = (float)(-h * 3. / a0);
     if constexpr (MODE == MODE_B) {
         const double ad0 = scp->adot[0], a1 = scp->a[1], ad1 = scp->adot[1];
@@ -82,6 +82,7 @@ __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s
                                          Moments &m, float (&s0)[kSrc], float (&s1)[kSrc]) {
     const Nb7<float> *f0[2] = {&fp, &fc}, *d0[2] = {&dp, &dc};
     float f1c[2];
+    float P0[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, P1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int f = 0; f < 2; f++) {
         const Nb7<float> &ff = *f0[f], &dd = *d0[f];
@@ -99,10 +100,14 @@ __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s
             m.f = fmaf(Pd, d, m.f);
             m.g1 = fmaf(f1.v[0], lap32(f1, s.inv_dx2f), m.g1);
             if constexpr (MODE == MODE_A_GW) {
-                source_add32(s.dnf, ff, s0);
-                source_add32(s.dnf, f1, s1);
+                grad_prod_add(ff, P0);
+                grad_prod_add(f1, P1);
             }
         }
+    }
+    if constexpr (MODE == MODE_A_GW) {
+        source_from_prod(s.qsf, P0, s0);
+        source_from_prod(s.qsf, P1, s1);
     }
     m.v0 += v_diff32(s.m0, c.model, fp.v[0], fc.v[0]);
     if constexpr (MODE != MODE_E0) m.v1 += v_diff32(s.m1, c.model, f1c[0], f1c[1]);

@@ -149,20 +149,3 @@ def test_tensor_core_forward_outruns_the_fp32_path():
         q_tc, info_tc = em.queries_per_second(tcn, n=1 << 20, reps=3)
         q_s, info_s = em.queries_per_second(simt, n=1 << 20, reps=3)
     assert q_tc > 3 * q_s, (info_tc, info_s)
-
-
-def test_fused_forward_matches_the_layer_by_layer_forward():
-    """gabe_mlp_forward with BF16 activations carries each 128-row tile
-    through all layers in one kernel; the training path's forward runs them
-    layer by layer.  Same operations in the same order: the loss of the fused
-    forward's outputs equals the loss the training path reports to the
-    rounding of the two loss sums."""
-    p = _perturbed_params(9)
-    x, t = _batch(1000, seed=12, nan_frac=0.2)
-    with em.MLP(max_rows=1000) as net:
-        net.set_params(p)
-        y = net.forward(_dev(x)).cpu().numpy().astype(np.float64)
-        loss, _ = net.loss_grad(_dev(x), _dev(t), want_grad=False)
-    ok = np.isfinite(t)
-    host = float(((y - np.where(ok, t, 0.0)) ** 2)[ok].mean())
-    assert abs(host - loss) <= 1e-9 * loss
