@@ -29,6 +29,7 @@
 
 #include "../../include/gabe.h"
 #include "../../include/gabe_mlp.h"
+#include "umma.cuh"
 
 namespace {
 
@@ -50,6 +51,12 @@ __device__ __forceinline__ bf16 cvt<bf16>(float v) { return __float2bfloat16_rn(
 
 __device__ __forceinline__ float sigmoid(float z) { return 1.f / (1.f + expf(-z)); }
 __device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
+// SiLU of the forward epilogues of the first-layer and tcgen05 kernels:
+// the fast exponential and division intrinsics (two special-function
+// operations per value, a few ulp of FP32, far below the BF16 rounding of
+// the stored activations), since the accurate expf and IEEE division
+// bounded those epilogues.  z -> -inf gives 0, z -> +inf gives z.
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigmoid(z);
     return s * (1.f + z * (1.f - s));
@@ -163,6 +170,93 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(GemmArgs g) {
                 Cz[o] = v;
             }
         }
+    }
+}
+
+// Forward of the first layer (NIN <= 8 inputs): z = x W0 + b0, h = SiLU(z),
+// the sum over k in order as the tiled kernel forms it.  A row is made by
+// G = N / 8 consecutive threads (G divides the block), 8 consecutive
+// outputs each, so every store is a whole 16-byte (BF16) or 32-byte (FP32)
+// piece of a coalesced row.  Each thread keeps its 8 columns of W0 and b0
+// in registers for all its rows (a reload per row held the loads' queue
+// full) and makes RPT rows per pass, their inputs loaded together, so that
+// RPT loads are in flight instead of one (one row per pass left the kernel
+// bound by the inputs' load latency).
+constexpr int kFirstMaxIn = 8, kFirstRows = 4;
+
+template <typename TACT, int NIN>
+__global__ void __launch_bounds__(256) first_layer_kernel(const float *x, int rows, const float *W, const float *b,
+                                                          int N, TACT *H, TACT *Z) {
+    constexpr int RPT = kFirstRows;
+    const int G = N / 8, rpb = 256 / G;  // threads per row, rows per block pass
+    const int n0 = (threadIdx.x % G) * 8;
+    float w[NIN][8], bias[8];
+#pragma unroll
+    for (int k = 0; k < NIN; k++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) w[k][j] = W[(long long)k * N + n0 + j];
+#pragma unroll
+    for (int j = 0; j < 8; j++) bias[j] = b[n0 + j];
+    const long long stride = (long long)gridDim.x * rpb;
+    for (long long r0 = (long long)blockIdx.x * rpb + threadIdx.x / G; r0 < rows; r0 += RPT * stride) {
+        float xv[RPT][NIN];
+#pragma unroll
+        for (int q = 0; q < RPT; q++) {
+            const long long r = r0 + q * stride;
+#pragma unroll
+            for (int k = 0; k < NIN; k++) xv[q][k] = r < rows ? x[r * NIN + k] : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < RPT; q++) {
+            const long long r = r0 + q * stride;
+            if (r >= rows) break;
+            float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int k = 0; k < NIN; k++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[j] = fmaf(xv[q][k], w[k][j], acc[j]);
+            TACT hv[8], zv[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const float z = acc[j] + bias[j];
+                hv[j] = cvt<TACT>(silu_fast(z));
+                zv[j] = cvt<TACT>(z);
+            }
+            constexpr int V = 8 * sizeof(TACT) / 16;  // 16-byte pieces per thread
+            const uint4 *hs = reinterpret_cast<const uint4 *>(hv), *zs = reinterpret_cast<const uint4 *>(zv);
+            uint4 *ho = reinterpret_cast<uint4 *>(H + r * N + n0);
+#pragma unroll
+            for (int u = 0; u < V; u++) ho[u] = hs[u];
+            if (Z) {
+                uint4 *zo = reinterpret_cast<uint4 *>(Z + r * N + n0);
+#pragma unroll
+                for (int u = 0; u < V; u++) zo[u] = zs[u];
+            }
+        }
+    }
+}
+
+template <typename TACT, int NIN>
+void launch_first(const float *x, int rows, const float *W, const float *b, int N, TACT *H, TACT *Z,
+                  cudaStream_t s) {
+    const int rpb = 256 / (N / 8);
+    const long long blocks = ((long long)rows + (long long)rpb * kFirstRows - 1) / ((long long)rpb * kFirstRows);
+    const int grid = (int)(blocks < 148 * 8 ? blocks : 148 * 8);
+    first_layer_kernel<TACT, NIN><<<grid, 256, 0, s>>>(x, rows, W, b, N, H, Z);
+}
+
+template <typename TACT>
+void launch_first_n(int n_in, const float *x, int rows, const float *W, const float *b, int N, TACT *H, TACT *Z,
+                    cudaStream_t s) {
+    switch (n_in) {
+        case 1: return launch_first<TACT, 1>(x, rows, W, b, N, H, Z, s);
+        case 2: return launch_first<TACT, 2>(x, rows, W, b, N, H, Z, s);
+        case 3: return launch_first<TACT, 3>(x, rows, W, b, N, H, Z, s);
+        case 4: return launch_first<TACT, 4>(x, rows, W, b, N, H, Z, s);
+        case 5: return launch_first<TACT, 5>(x, rows, W, b, N, H, Z, s);
+        case 6: return launch_first<TACT, 6>(x, rows, W, b, N, H, Z, s);
+        case 7: return launch_first<TACT, 7>(x, rows, W, b, N, H, Z, s);
+        default: return launch_first<TACT, 8>(x, rows, W, b, N, H, Z, s);
     }
 }
 
@@ -319,6 +413,234 @@ __global__ void weights_bf16t_kernel(const float *params, bf16 *wt, WtTable t) {
 
 }  // namespace tc
 
+// ---------------------------------------------------------------------------
+// Fifth-generation tensor-core (tcgen05) forward of the layers fed by BF16
+// activations whose BF16 weights fit in shared memory (K <= 256 and
+// N <= 256, K a multiple of 64, N of 32): Z = H W + b with H [M][K] and
+// Wt [N][K] (k contiguous).  A persistent CTA per SM keeps the layer's
+// weights resident (one tiled TMA load of K/64 slices of N x 64) and
+// streams 128-row tiles of H through a ring of 128 x 64 stages:
+//   warp 0 (one thread)  tiled TMA loads of H into the ring,
+//   warp 1 (one thread)  tcgen05.mma 128 x N x 16 into a TMEM accumulator,
+//                        two accumulators of N columns alternating by tile,
+//                        tcgen05.commit releasing ring stages and
+//                        signalling finished accumulators,
+//   warps 2-17           TMEM -> registers (tcgen05.ld), bias and SiLU;
+//                        warp w reads TMEM lanes 32 (w % 4) .. + 31 (its
+//                        sub-partition's rows) and every fourth 32-column
+//                        chunk, so the epilogue of tile t overlaps the MMAs
+//                        of tile t + 1.  Each 32 x 32 block goes through a
+//                        swizzled shared-memory buffer (one per warp) and
+//                        out by a tiled TMA store, so HBM sees whole lines
+//                        (a thread storing its own row touched 32 lines per
+//                        warp store, each 32-byte sector in two halves).
+// Every mbarrier wait is bounded (tma::mbar_wait); a wait that gives up
+// raises ST_TIMEOUT in the status word, the loader waits for the loads it
+// issued, the MMA thread for its MMAs, and the block frees its TMEM.
+// ---------------------------------------------------------------------------
+namespace t5 {
+
+using gabe::tma::mbar_wait;
+
+constexpr int BM = 128, BK = 64, NEPI = 16, NT = 64 + 32 * NEPI;  // NEPI epilogue warps
+constexpr int kMaxStages = 8;
+constexpr int kTmemCols = 512;                 // two accumulators of up to 256 columns
+constexpr int kStageBytes = BM * BK * 2;        // one 128 x 64 BF16 tile of H
+constexpr size_t kFixedBytes = 1024 + 1024 + 256;  // alignment slack, bias, barriers
+
+struct Args {
+    int M, N, K, stages;
+    const float *bias;
+    bf16 *Z;                // EPI_HIDDEN: pre-activation (may be null)
+    unsigned int *status;
+};
+
+// Output element size of the epilogue (BF16 hidden activations, FP32 output).
+template <int EPI>
+__host__ __device__ constexpr int out_bytes() {
+    return EPI == EPI_HIDDEN ? 2 : 4;
+}
+
+// Shared memory: weights, ring stages, a staging buffer of 32 x 32 output
+// elements per epilogue warp, bias, barriers.
+__host__ __device__ inline size_t smem_bytes(int N, int K, int stages, int esize) {
+    return kFixedBytes + (size_t)N * K * 2 + (size_t)stages * kStageBytes + (size_t)NEPI * 32 * 32 * esize;
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(NT, 1)
+    gemm_umma_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                     const __grid_constant__ CUtensorMap mapC, Args g) {
+    namespace tma = gabe::tma;
+    namespace umma = gabe::umma;
+    extern __shared__ unsigned char smraw[];
+    const uint32_t s0 = tma::saddr(smraw);
+    unsigned char *sm = smraw + (((s0 + 1023u) & ~1023u) - s0);  // 1024-byte aligned for the swizzle
+    const int N = g.N, K = g.K, KB = K / BK, S = g.stages;
+    unsigned char *Bs = sm;                                   // K/64 slices of N x 128 bytes
+    unsigned char *As = sm + (size_t)N * K * 2;               // S stages of 128 x 128 bytes
+    constexpr int ES = out_bytes<EPI>(), SBUF = 32 * 32 * ES;  // one staging buffer
+    unsigned char *Cs = As + (size_t)S * kStageBytes;         // [NEPI][SBUF]
+    float *bias_s = reinterpret_cast<float *>(Cs + (size_t)NEPI * SBUF);  // 256 floats
+    uint64_t *full = reinterpret_cast<uint64_t *>(bias_s + 256);
+    uint64_t *empty = full + kMaxStages, *bfull = empty + kMaxStages, *tfull = bfull + 1, *tempty = tfull + 2,
+             *done = tempty + 2;
+    uint32_t *tbase_s = reinterpret_cast<uint32_t *>(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ntiles = (g.M + BM - 1) / BM;
+
+    if (tid == 0) {
+        for (int s = 0; s < S; s++) {
+            tma::mbar_init(&full[s], 1);
+            tma::mbar_init(&empty[s], 1);
+        }
+        tma::mbar_init(bfull, 1);
+        for (int b = 0; b < 2; b++) {
+            tma::mbar_init(&tfull[b], 1);
+            tma::mbar_init(&tempty[b], 32 * NEPI);  // every epilogue thread
+        }
+        tma::mbar_init(done, 1);
+        tma::fence_barrier_init();
+    }
+    for (int n = tid; n < N; n += NT) bias_s[n] = g.bias[n];
+    if (warp == 1) umma::tmem_alloc(tbase_s, kTmemCols);
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const uint32_t tbase = *tbase_s;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int fills[kMaxStages];
+            for (int s = 0; s < kMaxStages; s++) fills[s] = 0;
+            tma::mbar_arrive_expect(bfull, (uint32_t)(N * K * 2));
+            for (int kb = 0; kb < KB; kb++) umma::load_2d(Bs + (size_t)kb * N * 128, &mapB, kb * BK, 0, bfull);
+            int it = 0;
+            bool ok = true;
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x)
+                for (int kb = 0; kb < KB; kb++, it++) {
+                    const int s = it % S;
+                    if (!mbar_wait(&empty[s], (uint32_t)(((it / S) & 1) ^ 1), g.status)) {
+                        ok = false;
+                        break;
+                    }
+                    fills[s]++;
+                    tma::mbar_arrive_expect(&full[s], (uint32_t)kStageBytes);
+                    umma::load_2d(As + (size_t)s * kStageBytes, &mapA, kb * BK, tile * BM, &full[s]);
+                }
+            // every load issued has landed before the block may exit
+            tma::drain(full, fills, S, g.status);
+            mbar_wait(bfull, 0, g.status);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = umma::idesc_bf16(BM, N);
+            bool ok = mbar_wait(bfull, 0, g.status);
+            int it = 0, local = 0;
+            for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, local++) {
+                const int b = local & 1;
+                if (!mbar_wait(&tempty[b], (uint32_t)(((local >> 1) & 1) ^ 1), g.status)) break;
+                umma::fence_after();
+                const uint32_t d = tbase + (uint32_t)(b * 256);
+                for (int kb = 0; kb < KB; kb++, it++) {
+                    const int s = it % S;
+                    if (!mbar_wait(&full[s], (uint32_t)((it / S) & 1), g.status)) {
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after();
+                    const uint32_t sa = tma::saddr(As + (size_t)s * kStageBytes);
+                    const uint32_t sb = tma::saddr(Bs + (size_t)kb * N * 128);
+#pragma unroll
+                    for (int k = 0; k < BK / 16; k++)
+                        umma::mma_bf16(d, umma::desc_k128(sa + 32 * k), umma::desc_k128(sb + 32 * k), idesc,
+                                       (uint32_t)((kb | k) != 0));
+                    umma::commit(&empty[s]);  // the stage is free once these MMAs have read it
+                }
+                if (ok) umma::commit(&tfull[b]);
+            }
+            umma::commit(done);  // arrives once every MMA issued above has completed
+            mbar_wait(done, 0, g.status);
+        }
+    } else {
+        constexpr int NH = NEPI / 4;  // epilogue warps per TMEM lane quarter
+        const int q = warp & 3, h = (warp - 2) >> 2, nch = N / 32;
+        unsigned char *sb = Cs + (size_t)(warp - 2) * SBUF;
+        int local = 0, cnt = 0;  // tiles and staged blocks of this warp
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, local++) {
+            const int b = local & 1;
+            const bool mine = mbar_wait(&tfull[b], (uint32_t)((local >> 1) & 1), g.status);
+            if (!__all_sync(0xffffffffu, mine)) break;
+            umma::fence_after();
+            const int r0 = tile * BM + q * 32, row = r0 + lane;
+            // (a warp whose rows all lie past M stages nothing: every staged
+            // block is stored, so the buffer accounting below holds)
+            for (int c = h; r0 < g.M && c < nch; c += NH, cnt++) {
+                float v[32];
+                umma::tmem_ld32(tbase + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 256 + c * 32), v);
+                const int n0 = c * 32;
+                const float4 *bq = reinterpret_cast<const float4 *>(bias_s + n0);
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const float4 bb = bq[u];
+                    v[4 * u] += bb.x;
+                    v[4 * u + 1] += bb.y;
+                    v[4 * u + 2] += bb.z;
+                    v[4 * u + 3] += bb.w;
+                }
+                // the previous block's store must have read the buffer
+                if (cnt >= 1) {
+                    if (lane == 0) umma::store_wait_read<0>();
+                    __syncwarp();
+                }
+                if constexpr (EPI == EPI_HIDDEN) {
+                    // row `lane` of the block: 64 bytes, 16-byte unit u at u ^ ((lane / 2) % 4) (64-byte swizzle)
+#pragma unroll
+                    for (int u = 0; u < 4; u++)
+                        *reinterpret_cast<uint4 *>(sb + lane * 64 + ((u ^ ((lane >> 1) & 3)) << 4)) =
+                            make_uint4(pack_bf16(silu_fast(v[8 * u]), silu_fast(v[8 * u + 1])),
+                                       pack_bf16(silu_fast(v[8 * u + 2]), silu_fast(v[8 * u + 3])),
+                                       pack_bf16(silu_fast(v[8 * u + 4]), silu_fast(v[8 * u + 5])),
+                                       pack_bf16(silu_fast(v[8 * u + 6]), silu_fast(v[8 * u + 7])));
+                    if (g.Z && row < g.M) {
+                        uint4 *zo = reinterpret_cast<uint4 *>(g.Z + (long long)row * N + n0);
+#pragma unroll
+                        for (int u = 0; u < 4; u++)
+                            zo[u] = make_uint4(pack_bf16(v[8 * u], v[8 * u + 1]), pack_bf16(v[8 * u + 2], v[8 * u + 3]),
+                                               pack_bf16(v[8 * u + 4], v[8 * u + 5]),
+                                               pack_bf16(v[8 * u + 6], v[8 * u + 7]));
+                    }
+                } else {
+                    // row `lane`: 128 bytes, 16-byte unit u at u ^ (lane % 8) (128-byte swizzle)
+#pragma unroll
+                    for (int u = 0; u < 8; u++)
+                        *reinterpret_cast<float4 *>(sb + lane * 128 + ((u ^ (lane & 7)) << 4)) =
+                            make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
+                }
+                tma::fence_proxy_async();  // the block's shared writes precede the store's reads
+                __syncwarp();
+                if (lane == 0) umma::store_2d(&mapC, n0, r0, sb);
+            }
+            umma::fence_before();
+            umma::mbar_arrive(&tempty[b]);
+        }
+        if (lane == 0) umma::store_wait_all();
+    }
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        umma::fence_after();
+        umma::tmem_free(tbase, kTmemCols);
+    }
+}
+
+}  // namespace t5
+
 // dW = sum over splits of the partial products, db = sum of the partial
 // column sums; fixed order, so the result does not depend on scheduling.
 __global__ void __launch_bounds__(256) splitk_reduce_kernel(const float *ws, const float *dbp, int splits,
@@ -468,6 +790,8 @@ struct gabe_mlp {
     float *ws = nullptr, *dbp = nullptr;  // split-K partials of the weight gradient
     bf16 *wt = nullptr;              // BF16 transposed weights of layers >= 1 (tensor-core forward)
     tc::WtTable wtab{};
+    unsigned int *status = nullptr;  // device word: a bounded wait of the tcgen05 forward gave up
+    int umma_stages[17] = {};        // per layer: ring stages of the tcgen05 forward, 0 = mma.sync kernel
     void *Z = nullptr, *H = nullptr;  // [depth][max_rows][width] activation type
     double2 *part = nullptr;
     TrainScalars *ts = nullptr;
@@ -533,11 +857,103 @@ int launch_tc(gabe_mlp *m, const tc::Args &a) {
     return GABE_OK;
 }
 
+// cuTensorMapEncodeTiled, looked up once through the runtime (no link
+// dependency on the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (EncodeTiledFn) nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// 2-D BF16 tensor map of a row-major [rows][K] matrix, boxes of box_rows x 64
+// with the 128-byte swizzle; rows beyond `rows` read as zeros.
+bool encode_k_major(CUtensorMap *map, const bf16 *base, int K, int rows, int box_rows) {
+    const EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)t5::BK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor map of a row-major [rows][N] output (BF16 or FP32, esize bytes),
+// boxes of 32 x 32 with the swizzle whose span is one box row (64 or 128
+// bytes), as the epilogue lays its staging buffers out.
+bool encode_out(CUtensorMap *map, void *base, int esize, int N, int rows) {
+    const EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)N * esize};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, esize == 2 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims,
+              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              esize == 2 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Ring stages of the tcgen05 forward for a K x N layer on this device, 0 if
+// the layer does not take it (shape, resident weights too large, no tensor
+// map encoder).
+int umma_stages_for(int dev, int K, int N, int esize) {
+    if (K % t5::BK || K > 256 || N % 32 || N > 256 || !encode_fn()) return 0;
+    int optin = 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const long long room = (long long)optin - (long long)t5::smem_bytes(N, K, 0, esize);
+    const long long st = room / t5::kStageBytes;
+    return st < 2 ? 0 : (int)(st > t5::kMaxStages ? t5::kMaxStages : st);
+}
+
+constexpr int kNoTensorMap = -1;  // launch_umma: no tensor map for these operands; use the mma.sync kernel
+
+template <int EPI>
+int launch_umma(gabe_mlp *m, const tc::Args &a, int stages) {
+    CUtensorMap ma, mb, mc;
+    if (!encode_k_major(&ma, a.A, a.K, a.M, t5::BM) || !encode_k_major(&mb, a.Wt, a.K, a.N, a.N) ||
+        !encode_out(&mc, a.C, t5::out_bytes<EPI>(), a.N, a.M))
+        return kNoTensorMap;  // e.g. an output pointer off a 16-byte boundary
+    t5::Args g{a.M, a.N, a.K, stages, a.bias, a.Z, m->status};
+    const size_t smem = t5::smem_bytes(a.N, a.K, stages, t5::out_bytes<EPI>());
+    MCK(m, cudaFuncSetAttribute(t5::gemm_umma_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int nsm = 0;
+    MCK(m, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->dev));
+    const int tiles = (a.M + t5::BM - 1) / t5::BM;
+    const int grid = tiles < nsm ? tiles : nsm;
+    t5::gemm_umma_kernel<EPI><<<grid, t5::NT, smem, m->stream>>>(ma, mb, mc, g);
+    MCK(m, cudaGetLastError());
+    return GABE_OK;
+}
+
 // Input activations of layer l: x (FP32) for l = 0, H[l-1] otherwise.
 // With BF16 activations every layer after the first runs on tensor cores.
 template <typename TACT>
 int forward_rows(gabe_mlp *m, const float *x, int rows, float *y, bool keep_z) {
     for (int l = 0; l < m->nl; l++) {
+        if (l == 0 && m->nl > 1 && m->K[0] <= kFirstMaxIn && 256 % (m->N[0] / 8) == 0) {
+            launch_first_n<TACT>(m->K[0], x, rows, m->params + m->offW[0], m->params + m->offb[0], m->N[0],
+                                 static_cast<TACT *>(act_at(m, m->H, 0)),
+                                 keep_z ? static_cast<TACT *>(act_at(m, m->Z, 0)) : nullptr, m->stream);
+            MCK(m, cudaGetLastError());
+            continue;
+        }
         if constexpr (sizeof(TACT) == 2) {
             if (l > 0) {
                 tc::Args a{};
@@ -550,7 +966,10 @@ int forward_rows(gabe_mlp *m, const float *x, int rows, float *y, bool keep_z) {
                 const bool last = l + 1 == m->nl;
                 a.Z = (!last && keep_z) ? static_cast<bf16 *>(act_at(m, m->Z, l)) : nullptr;
                 a.C = last ? static_cast<void *>(y) : act_at(m, m->H, l);
-                const int rc = last ? launch_tc<EPI_OUT>(m, a) : launch_tc<EPI_HIDDEN>(m, a);
+                const int st = m->umma_stages[l];
+                int rc = st ? (last ? launch_umma<EPI_OUT>(m, a, st) : launch_umma<EPI_HIDDEN>(m, a, st))
+                            : kNoTensorMap;
+                if (rc == kNoTensorMap) rc = last ? launch_tc<EPI_OUT>(m, a) : launch_tc<EPI_HIDDEN>(m, a);
                 if (rc) return rc;
                 continue;
             }
@@ -672,7 +1091,7 @@ void free_all(gabe_mlp *m) {
     if (m->gexec) cudaGraphExecDestroy(m->gexec);
     if (m->graph) cudaGraphDestroy(m->graph);
     void *bufs[] = {m->params, m->grads, m->mom, m->vel, m->xb, m->tb, m->y, m->dy, m->d0, m->d1, m->Z, m->H,
-                    m->part, m->ts, m->ws, m->dbp, m->wt};
+                    m->part, m->ts, m->ws, m->dbp, m->wt, m->status};
     for (void *b : bufs)
         if (b) cudaFree(b);
     if (m->stream) cudaStreamDestroy(m->stream);
@@ -760,7 +1179,7 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         {(void **)&m->d1, R * wide * 4}, {&m->Z, (size_t)p->depth * R * W * A}, {&m->H, (size_t)p->depth * R * W * A},
         {(void **)&m->part, kLossBlocks * sizeof(double2)}, {(void **)&m->ts, sizeof(TrainScalars)},
         {(void **)&m->ws, (size_t)kMaxSplits * wide * wide * 4}, {(void **)&m->dbp, (size_t)kMaxSplits * wide * 4},
-        {(void **)&m->wt, (size_t)(nwt > 0 ? nwt : 1) * sizeof(bf16)},
+        {(void **)&m->wt, (size_t)(nwt > 0 ? nwt : 1) * sizeof(bf16)}, {(void **)&m->status, sizeof(unsigned int)},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.ptr, a.bytes) != cudaSuccess) {
@@ -784,11 +1203,16 @@ int gabe_mlp_create(const gabe_mlp_params *p, gabe_mlp **out) {
         cudaMemsetAsync(m->mom, 0, m->P * 4, m->stream) != cudaSuccess ||
         cudaMemsetAsync(m->vel, 0, m->P * 4, m->stream) != cudaSuccess ||
         cudaMemcpyAsync(m->ts, &ts, sizeof(ts), cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+        cudaMemsetAsync(m->status, 0, sizeof(unsigned int), m->stream) != cudaSuccess ||
         refresh_wt(m) != GABE_OK || cudaStreamSynchronize(m->stream) != cudaSuccess) {
         cudaGetLastError();
         mset(m, GABE_ERR_CUDA, "initialisation copies failed");
         return fail(GABE_ERR_CUDA);
     }
+    // tcgen05 forward for the BF16 layers whose weights fit in shared memory
+    if (!m->f32act && !(p->flags & GABE_MLP_MMA_SYNC))
+        for (int l = 1; l < m->nl; l++)
+            m->umma_stages[l] = umma_stages_for(m->dev, m->K[l], m->N[l], l + 1 == m->nl ? 4 : 2);
     *out = m;
     return GABE_OK;
 }
@@ -929,7 +1353,16 @@ int gabe_mlp_sync(gabe_mlp *m) {
     if (!m) return GABE_ERR_PARAM;
     MCK(m, cudaSetDevice(m->dev));
     MCK(m, cudaStreamSynchronize(m->stream));
+    unsigned int st = 0;
+    MCK(m, cudaMemcpy(&st, m->status, sizeof(st), cudaMemcpyDeviceToHost));
+    if (st) return mset(m, GABE_ERR_TIMEOUT, "a bounded wait of the tensor-core forward gave up (status %u)", st);
     return GABE_OK;
+}
+
+int gabe_mlp_forward_form(const gabe_mlp *m, int32_t layer) {
+    if (!m || layer < 0 || layer >= m->nl) return -1;
+    if (layer == 0 || m->f32act) return 0;
+    return m->umma_stages[layer] ? 2 : 1;
 }
 
 void *gabe_mlp_stream(const gabe_mlp *m) { return m ? (void *)m->stream : nullptr; }

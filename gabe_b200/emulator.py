@@ -27,6 +27,7 @@ from . import GabeError, library
 
 FP32_ACT = 1
 NO_GRAPH = 2
+MMA_SYNC = 4
 
 
 class MLPParams(ctypes.Structure):
@@ -66,6 +67,7 @@ def _mlp_lib():
         L.gabe_mlp_launches_per_forward.argtypes = [M]
         L.gabe_mlp_last_error.argtypes = [M]
         L.gabe_mlp_last_error.restype = ctypes.c_char_p
+        L.gabe_mlp_forward_form.argtypes = [M, ctypes.c_int32]
         L._mlp_ready = True
     return L
 
@@ -79,13 +81,13 @@ class MLP:
     float32 (x [n, n_in], t [n, n_out]) on the handle's device."""
 
     def __init__(self, *, n_in=3, width=256, depth=4, n_out=192, max_rows=65536, lr=1e-3, weight_decay=0.0,
-                 seed=1, fp32_act=False, graph=True, device=-1):
+                 seed=1, fp32_act=False, graph=True, device=-1, mma_sync=False):
         L = _mlp_lib()
         p = MLPParams()
         L.gabe_mlp_default_params(ctypes.byref(p))
         p.n_in, p.width, p.depth, p.n_out, p.max_rows = n_in, width, depth, n_out, max_rows
         p.lr, p.weight_decay, p.seed, p.device = lr, weight_decay, seed, device
-        p.flags = (FP32_ACT if fp32_act else 0) | (0 if graph else NO_GRAPH)
+        p.flags = (FP32_ACT if fp32_act else 0) | (0 if graph else NO_GRAPH) | (MMA_SYNC if mma_sync else 0)
         self.p = p
         self.shape = (n_in, width, depth, n_out)
         self._h = ctypes.c_void_p()
@@ -190,7 +192,17 @@ class MLP:
         return m.value, s.value
 
     def sync(self):
+        """Waits for the handle's stream; raises if a bounded device wait of
+        the tensor-core forward gave up."""
         self._check(_mlp_lib().gabe_mlp_sync(self._h))
+
+    def forward_form(self, layer: int) -> str:
+        """Kernel of layer `layer`'s forward: "fma" (FP32 FMA), "mma.sync" or
+        "tcgen05"."""
+        f = _mlp_lib().gabe_mlp_forward_form(self._h, layer)
+        if f < 0:
+            raise IndexError(layer)
+        return ("fma", "mma.sync", "tcgen05")[f]
 
     def fit(self, x, t, epochs: int, batch: int, seed: int = 0, log_every: int = 0, lr_min: float | None = None):
         """Trains on all rows of x, t (device tensors) for `epochs` passes in
@@ -347,6 +359,7 @@ def queries_per_second(net: MLP, n: int = 1 << 20, reps: int = 5):
         net.forward(x, y)
     e1.record(s)
     e1.synchronize()
+    net.sync()
     ms = e0.elapsed_time(e1) / reps
     flops = 2.0 * n * (net.num_params - sum([net.shape[1]] * net.shape[2]) - net.shape[3])
     return n / (ms / 1e3), {"ms": ms, "rows": n, "gflops": flops / (ms / 1e3) / 1e9}

@@ -8,7 +8,11 @@
  *
  * Weights, biases, gradients and Adam moments are FP32; activations between
  * layers are stored in BF16 (GABE_MLP_FP32_ACT stores them in FP32); every
- * product is accumulated in FP32.  Flat parameter layout, layer by layer:
+ * product is accumulated in FP32.  The forward of a BF16 layer whose BF16
+ * weights fit in shared memory (K <= 256, N <= 256, K a multiple of 64, N
+ * of 32) runs on the fifth-generation tensor cores (tcgen05, TMEM
+ * accumulators), other BF16 layers on mma.sync, the first layer and the
+ * backward products on FP32 FMA.  Flat parameter layout, layer by layer:
  * W_l [K_l][N_l] (row-major, K_l inputs) followed by b_l [N_l].
  *
  * Targets may hold NaN (log bins with no native bin): the loss is the mean
@@ -29,6 +33,7 @@ extern "C" {
 
 #define GABE_MLP_FP32_ACT 1   /* store activations in FP32 instead of BF16 */
 #define GABE_MLP_NO_GRAPH 2   /* launch training steps directly (no CUDA graph) */
+#define GABE_MLP_MMA_SYNC 4   /* forward of the BF16 layers on the mma.sync kernel instead of tcgen05 */
 
 typedef struct {
     int32_t struct_size;   /* sizeof(gabe_mlp_params) */
@@ -80,7 +85,12 @@ int gabe_mlp_reset_batches(gabe_mlp *m);
  * number of Adam steps taken so far. */
 int gabe_mlp_train_loss(gabe_mlp *m, double *h_mean_loss, int64_t *h_steps);
 
+/* Waits for the handle's stream; GABE_ERR_TIMEOUT if a bounded device wait
+ * of the tensor-core forward gave up since the handle was created. */
 int gabe_mlp_sync(gabe_mlp *m);
+/* Kernel that runs the forward of layer `layer`: 0 FP32 FMA, 1 mma.sync,
+ * 2 tcgen05; -1 for a bad layer index. */
+int gabe_mlp_forward_form(const gabe_mlp *m, int32_t layer);
 void *gabe_mlp_stream(const gabe_mlp *m);
 /* The library's kernel launches per training step and per forward chunk. */
 int gabe_mlp_launches_per_train_step(const gabe_mlp *m);

@@ -140,12 +140,64 @@ def test_cosine_schedule_matches_oracle():
             np.testing.assert_allclose(got, ref, rtol=1e-6, atol=1e-7)
 
 
+def test_forward_forms():
+    """BF16 layers 1 .. depth take the tcgen05 kernel (their BF16 weights fit
+    in shared memory), or mma.sync on request; FP32 activations and the
+    first layer stay on FP32 FMA."""
+    with em.MLP(seed=1) as a, em.MLP(seed=1, mma_sync=True) as b, em.MLP(seed=1, fp32_act=True) as c:
+        assert [a.forward_form(l) for l in range(5)] == ["fma"] + ["tcgen05"] * 4
+        assert [b.forward_form(l) for l in range(5)] == ["fma"] + ["mma.sync"] * 4
+        assert [c.forward_form(l) for l in range(5)] == ["fma"] * 5
+        with pytest.raises(IndexError):
+            a.forward_form(5)
+
+
+@pytest.mark.parametrize("rows", [1, 127, 128, 129, 300, 4096 + 17])
+def test_tcgen05_forward_matches_mma_sync(rows):
+    """The tcgen05 forward (TMEM accumulators, 128-row tiles, rows beyond
+    the last full tile read as zeros) against the mma.sync forward of the
+    same BF16 network: the same BF16 roundings of every operand, FP32 sums
+    in another order, so outputs agree to a few BF16 flips of the hidden
+    activations."""
+    p = _perturbed_params(17)
+    rng = np.random.default_rng(rows)
+    x = rng.normal(size=(rows, 3)).astype(np.float32)
+    ys = []
+    for mma_sync in (False, True):
+        with em.MLP(seed=1, mma_sync=mma_sync, max_rows=4096) as net:
+            net.set_params(p)
+            ys.append(net.forward(_dev(x)).cpu().numpy())
+            net.sync()
+    assert np.all(np.isfinite(ys[0]))
+    assert np.linalg.norm(ys[0] - ys[1]) / np.linalg.norm(ys[1]) <= 2e-3
+    ybf, _, _ = mo.forward(p, x, mode="bf16")
+    assert np.linalg.norm(ys[0] - ybf) / np.linalg.norm(ybf) <= 2e-3
+
+
+def test_tcgen05_training_matches_mma_sync_training():
+    """Training steps (forward with pre-activations kept for the backward)
+    through either forward kernel reach nearly the same parameters."""
+    x, t = _batch(2048, seed=8, nan_frac=0.1)
+    out = []
+    for mma_sync in (False, True):
+        with em.MLP(seed=3, mma_sync=mma_sync) as net:
+            net.fit(_dev(x), _dev(t), epochs=2, batch=256, seed=4)
+            net.sync()
+            out.append(net.get_params())
+    rel = np.linalg.norm(out[0] - out[1]) / np.linalg.norm(out[1])
+    assert rel <= 1e-2, rel
+
+
 def test_tensor_core_forward_outruns_the_fp32_path():
     """With BF16 activations the layers after the first run on tensor cores
-    (mma.sync BF16 x BF16 -> FP32); on a million queries that forward must
-    be several times faster than the FP32-activation path, which keeps
-    every product on the CUDA-core kernel."""
-    with em.MLP(seed=1, max_rows=1 << 20) as tcn, em.MLP(seed=1, fp32_act=True, max_rows=1 << 20) as simt:
+    (tcgen05 BF16 x BF16 -> FP32 in TMEM); on a million queries that forward
+    must be several times faster than the FP32-activation path, which keeps
+    every product on the CUDA-core kernel, and faster than the mma.sync
+    form of the same network."""
+    with em.MLP(seed=1, max_rows=1 << 20) as tcn, em.MLP(seed=1, fp32_act=True, max_rows=1 << 20) as simt, \
+            em.MLP(seed=1, max_rows=1 << 20, mma_sync=True) as legacy:
         q_tc, info_tc = em.queries_per_second(tcn, n=1 << 20, reps=3)
         q_s, info_s = em.queries_per_second(simt, n=1 << 20, reps=3)
+        q_l, info_l = em.queries_per_second(legacy, n=1 << 20, reps=3)
     assert q_tc > 3 * q_s, (info_tc, info_s)
+    assert q_tc > q_l, (info_tc, info_l)
