@@ -55,7 +55,11 @@ __device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 // the fast exponential and division intrinsics (two special-function
 // operations per value, a few ulp of FP32, far below the BF16 rounding of
 // the stored activations), since the accurate expf and IEEE division
-// bounded those epilogues.  z -> -inf gives 0, z -> +inf gives z.
+// bounded those epilogues (608 against 185 us per 1M-row hidden layer).
+// A reciprocal by Newton-Raphson steps on the FMA pipe instead of the
+// second special-function operation measured slower (225 us): the
+// epilogue is bound by issue as much as by that pipe.  z -> -inf gives 0,
+// z -> +inf gives z.
 __device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
     const float s = sigmoid(z);
