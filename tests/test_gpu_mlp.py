@@ -174,6 +174,28 @@ def test_tcgen05_forward_matches_mma_sync(rows):
     assert np.linalg.norm(ys[0] - ybf) / np.linalg.norm(ybf) <= 2e-3
 
 
+@pytest.mark.parametrize("shape", [(4, 128, 2, 64), (2, 64, 3, 64), (5, 512, 2, 128)])
+def test_forward_forms_agree_on_other_shapes(shape):
+    """Other widths and depths: layers whose BF16 weights fit in shared
+    memory (K, N <= 256) take tcgen05 (K = 64 and 128, N = 64 .. 128 here),
+    wider ones the mma.sync kernel; both forms of the same network agree."""
+    n_in, width, depth, n_out = shape
+    rng = np.random.default_rng(n_in)
+    x = rng.normal(size=(1000, n_in)).astype(np.float32)
+    ys, forms = [], []
+    for mma_sync in (False, True):
+        with em.MLP(n_in=n_in, width=width, depth=depth, n_out=n_out, seed=2, mma_sync=mma_sync,
+                    max_rows=512) as net:
+            forms.append([net.forward_form(l) for l in range(depth + 1)])
+            ys.append(net.forward(_dev(x)).cpu().numpy())
+            net.sync()
+    want = "tcgen05" if width <= 256 else "mma.sync"
+    assert forms[0] == ["fma"] + [want] * depth
+    assert forms[1] == ["fma"] + ["mma.sync"] * depth
+    assert np.all(np.isfinite(ys[0]))
+    assert np.linalg.norm(ys[0] - ys[1]) / np.linalg.norm(ys[1]) <= 2e-3
+
+
 def test_tcgen05_training_matches_mma_sync_training():
     """Training steps (forward with pre-activations kept for the backward)
     through either forward kernel reach nearly the same parameters."""
