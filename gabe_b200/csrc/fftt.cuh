@@ -47,10 +47,12 @@ using pfft::FourStep;
 // rows at one kz (lanes over the 8 pairs, 4 kz per warp) and stores it as one
 // 16-byte value, eight lanes making the 128-byte piece of 16 rows.  Rows sit
 // N + 2 floats apart in shared memory, so that the eight pairs' rows start on
-// different banks.  (Staging the tile as [kz][16 rows] in shared memory and
-// writing it piece by piece gave the same bytes in 3.30 ms at 512^3 against
-// 2.28 ms: the extra barrier and shared-memory round trip held the 8 warps
-// per SM.)
+// different banks.  Measured at 512^3, same bytes: staging the tile as
+// [kz][16 rows] in shared memory and writing it piece by piece took 3.30 ms
+// against 2.28 ms (the extra barrier and shared-memory round trip held the 8
+// warps per SM); separating the pairs from the pass-2 registers through warp
+// shuffles, with no write-back, took 2.68 ms against 2.13 (each warp store
+// then spans 16 lines instead of 4).
 template <int N, int T_ = 128>
 struct RowTGeom {
     using RG = f3d::RowGeom<N, 16, 2, T_, 2>;
