@@ -176,7 +176,7 @@ void *source_buffer(const gabe_handle *h, int slot) { return slot && h->S2 ? h->
 int source_fft(gabe_handle *h, int slot, cudaStream_t s) {
     void *S = source_buffer(h, slot);
     if (h->fftt) {  // rows S -> S2, pass along j S2 -> S; the pass along i runs inside the k-space update
-        CK(h, fftt_rows_f32(h->N, static_cast<const float *>(S), h->S2, 2 * kSrc, s));
+        CK(h, fftt_rows_f32(h->N, static_cast<const float *>(S), h->S2, 2 * kSrc, &h->sc->status, s));
         CK(h, fftt_cols_f32(h->N, h->S2, S, 2 * kSrc, &h->sc->status, s));
         return GABE_OK;
     }
@@ -679,7 +679,8 @@ static int profile_fftt_passes(gabe_handle *h, int nreps, double ms_out[3]) {
         rc = sweep(h, MODE_A_GW, c, 0, 0);
         if (rc) break;
         cudaError_t ce = cudaEventRecord(e[0], h->stream);
-        if (ce == cudaSuccess) ce = fftt_rows_f32(h->N, static_cast<const float *>(h->S), h->S2, 2 * kSrc, h->stream);
+        if (ce == cudaSuccess) ce = fftt_rows_f32(h->N, static_cast<const float *>(h->S), h->S2, 2 * kSrc, &h->sc->status,
+                                                         h->stream);
         if (ce == cudaSuccess) ce = cudaEventRecord(e[1], h->stream);
         if (ce == cudaSuccess) ce = fftt_cols_f32(h->N, h->S2, h->S, 2 * kSrc, &h->sc->status, h->stream);
         if (ce == cudaSuccess) ce = cudaEventRecord(e[2], h->stream);

@@ -27,13 +27,13 @@ constexpr int kColT = 512, kColNB = 2;
 constexpr int kIkT = 192, kIkNB = 1, kIkMinB = 2;
 
 template <int N>
-cudaError_t rows_n(const float *S, float2 *T1, int ncomp, cudaStream_t s) {
+cudaError_t rows_n(const float *S, float2 *T1, int ncomp, unsigned int *status, cudaStream_t s) {
     constexpr size_t smem = f3t::RowTGeom<N, kRowT>::SMEM_BYTES;
     auto k = f3t::rowt_kernel<N, kRowT>;
     int g = 0;
     cudaError_t e = grid_of(k, kRowT, smem, &g);
     if (e != cudaSuccess) return e;
-    k<<<g, kRowT, smem, s>>>(S, T1, (long long)ncomp * N * N);
+    k<<<g, kRowT, smem, s>>>(S, T1, (long long)ncomp * N * N, status);
     return cudaGetLastError();
 }
 
@@ -65,13 +65,13 @@ cudaError_t ik_n(const f3t::IkArgs &a, cudaStream_t s) {
 
 bool fftt_supported(int N) { return N == 64 || N == 128 || N == 256 || N == 512; }
 
-cudaError_t fftt_rows_f32(int N, const float *S, void *T1, int ncomp, cudaStream_t s) {
+cudaError_t fftt_rows_f32(int N, const float *S, void *T1, int ncomp, unsigned int *status, cudaStream_t s) {
     float2 *o = static_cast<float2 *>(T1);
     switch (N) {
-        case 64: return rows_n<64>(S, o, ncomp, s);
-        case 128: return rows_n<128>(S, o, ncomp, s);
-        case 256: return rows_n<256>(S, o, ncomp, s);
-        case 512: return rows_n<512>(S, o, ncomp, s);
+        case 64: return rows_n<64>(S, o, ncomp, status, s);
+        case 128: return rows_n<128>(S, o, ncomp, status, s);
+        case 256: return rows_n<256>(S, o, ncomp, status, s);
+        case 512: return rows_n<512>(S, o, ncomp, status, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -9,18 +9,19 @@
 // so that the next pass's lines are contiguous again:
 //
 //   pass 1 (rowt_kernel)   S[q][i][j][N+2] reals   -> T1[q][i][kz][j]
-//          rows along k, two real rows as one complex sequence (the row
-//          kernel of fft3d.cuh), each kz written as one 128-byte piece of
-//          16 consecutive j (eight 16-byte pair stores);
+//          rows along k, two real rows as one complex sequence, 16-row
+//          tiles landed by one bulk copy each, each kz written as one
+//          128-byte piece of 16 consecutive j (eight 16-byte pair stores);
 //   pass 2 (colt_kernel)   T1 lines along j         -> T2[q][kz][ky][i]
 //          16 lines of consecutive i per tile, landed in shared memory by
 //          bulk copies (cp.async.bulk + mbarrier), each ky written as one
 //          128-byte piece of 16 consecutive i;
 //   pass 3 (ikspace_kernel) T2 lines along i + amplitudes G[p][kz][ky][kx]
-//          the ten source lines and four amplitude lines of one (kz, ky)
-//          land by bulk copies, the ten lines are transformed along i in
-//          shared memory, and the k-space update (kspace_update_vals) runs
-//          on each kx; only the amplitudes go back to HBM.
+//          the ten source lines of one (kz, ky) land by bulk copies and are
+//          transformed along i in shared memory, each thread reads its
+//          k-points' amplitudes into registers, and the k-space update
+//          (kspace_update_vals) runs on each kx; only the amplitudes go back
+//          to HBM.
 //
 // The transformed sources never return to HBM after pass 2, and the
 // amplitudes are kept in the transposed order [p][kz][ky][kx]
@@ -41,68 +42,90 @@ using pfft::FourStep;
 // ---------------------------------------------------------------------------
 // pass 1: rows along k -> T1[q][i][kz][j]
 // ---------------------------------------------------------------------------
-// The row kernel of fft3d.cuh (cp.async ring, four-step FFT of row pairs in a
-// swizzled layout) with its output written transposed.  The separated pairs
-// go straight to HBM: each thread separates one pair of
-// rows at one kz (lanes over the 8 pairs, 4 kz per warp) and stores it as one
-// 16-byte value, eight lanes making the 128-byte piece of 16 rows.  Rows sit
-// N + 2 floats apart in shared memory, so that the eight pairs' rows start on
-// different banks.  Measured at 512^3, same bytes: staging the tile as
-// [kz][16 rows] in shared memory and writing it piece by piece took 3.30 ms
-// against 2.28 ms (the extra barrier and shared-memory round trip held the 8
-// warps per SM); separating the pairs from the pass-2 registers through warp
-// shuffles, with no write-back, took 2.68 ms against 2.13 (each warp store
-// then spans 16 lines instead of 4).
+// A tile of 16 rows (8 pairs, each two real rows taken as one complex
+// sequence) is one contiguous run of 16 (N + 2) floats in S and lands in
+// shared memory by one bulk copy (cp.async.bulk + mbarrier) into a ring of
+// two linear buffers.  The four-step FFT's first pass reads the pairs from
+// the linear buffer (lanes over consecutive elements: conflict-free) and
+// writes its output into a work buffer in the pair-preserving XOR swizzle of
+// fft3d.cuh, so that the second pass's stride-L1 reads fall on distinct
+// banks; the linear buffer is refilled as soon as the first pass has read
+// it.  The separated pairs go straight to HBM: each thread separates one
+// pair of rows at one kz (lanes over the 8 pairs, 4 kz per warp) and stores
+// it as one 16-byte value, eight lanes making the 128-byte piece of 16 rows.
+// Work rows sit N + 2 floats apart, so that the eight pairs' rows start on
+// different banks.  Measured at 512^3, same bytes: loading the tile by 8-byte
+// cp.async copies straight into the swizzled layout took 2.13 ms against
+// 2.09 (bit-identical output; the loads were not what bounded the pass, its
+// two CTAs of 4 warps per SM are); staging the output as [kz][16 rows] in
+// shared memory and writing it
+// piece by piece 3.30 ms against 2.28 (the extra barrier and shared-memory
+// round trip held the 8 warps per SM); separating the pairs from the
+// pass-2 registers through warp shuffles, with no write-back, 2.68 ms
+// against 2.13 (each warp store then spans 16 lines instead of 4).
 template <int N, int T_ = 128>
 struct RowTGeom {
-    using RG = f3d::RowGeom<N, 16, 2, T_, 2>;
-    static constexpr size_t SMEM_BYTES = RG::SMEM_BYTES;
+    using RG = f3d::RowGeom<N, 16, 1, T_, 2>;  // the work buffer (swizzled, pitch N + 2)
+    static constexpr int R = 16, RP = N + 2, NB = 2;
+    static constexpr size_t HEAD = 128;                          // NB mbarriers
+    static constexpr size_t TW_BYTES = (size_t)N * sizeof(float2);  // twiddles of the four-step
+    static constexpr size_t LIN_BYTES = (size_t)R * RP * sizeof(float);
+    static constexpr size_t SMEM_BYTES = HEAD + TW_BYTES + NB * LIN_BYTES + (size_t)RG::BUF * sizeof(float);
+    static_assert(LIN_BYTES % 16 == 0 && (HEAD + TW_BYTES) % 16 == 0, "bulk copies of 16-byte multiples");
 };
 
 template <int N, int T_ = 128, int MINB = 2>
-__global__ void __launch_bounds__(T_, MINB) rowt_kernel(const float *S, float2 *T1, long long nrows) {
-    using Gm = typename RowTGeom<N, T_>::RG;
-    constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2,
-                  NB = Gm::NB;
-    constexpr int RP = N + 2, NH = N / 2 + 1;
+__global__ void __launch_bounds__(T_, MINB)
+    rowt_kernel(const float *S, float2 *T1, long long nrows, unsigned int *status) {
+    using G = RowTGeom<N, T_>;
+    using Gm = typename G::RG;
+    constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2;
+    constexpr int RP = G::RP, NB = G::NB, NH = N / 2 + 1;
     static_assert(R == 16 && P == 8, "one 128-byte output piece per kz");
-    extern __shared__ __align__(16) float smem[];
-    float2 *tw = reinterpret_cast<float2 *>(smem + NB * Gm::BUF);
+    extern __shared__ __align__(128) unsigned char sm[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm);
+    float2 *tw = reinterpret_cast<float2 *>(sm + G::HEAD);
+    float *lin0 = reinterpret_cast<float *>(sm + G::HEAD + G::TW_BYTES);  // [NB][R][RP]
+    float *rows = lin0 + NB * R * RP;                                     // work buffer [R][PITCH], swizzled
     const int tid = threadIdx.x;
-    f3d::twiddles<N>(tw);
     const long long ntiles = nrows / R;
-    auto issue = [&](long long tile, int b) {
-        const float *g = S + tile * R * RP;
-        float *rows = smem + b * Gm::BUF;
-#pragma unroll 4
-        for (int t = tid; t < R * (N / 2); t += T) {
-            const int jj = t / (N / 2), m = t % (N / 2);
-            s32::cp_async8(rows + jj * PITCH + Gm::phys(2 * m), g + jj * RP + 2 * m);
-        }
-    };
-#pragma unroll
-    for (int q = 0; q < NB - 1; q++) {
-        if (blockIdx.x + q * (long long)gridDim.x < ntiles) issue(blockIdx.x + q * (long long)gridDim.x, q);
-        s32::cp_commit();
+    if (tid == 0) {
+        for (int b = 0; b < NB; b++) tma::mbar_init(&bar[b], 1);
+        tma::fence_barrier_init();
     }
+    f3d::twiddles<N>(tw);
+    __syncthreads();
+    int fills[NB] = {};  // thread 0: fills issued per buffer
+    auto issue = [&](long long tile, int b) {
+        fills[b]++;
+        tma::mbar_arrive_expect(&bar[b], (uint32_t)G::LIN_BYTES);
+        tma::load(lin0 + b * R * RP, S + tile * R * RP, (uint32_t)G::LIN_BYTES, &bar[b]);
+    };
+    if (tid == 0)
+        for (int q = 0; q < NB; q++) {
+            const long long t = blockIdx.x + (long long)q * gridDim.x;
+            if (t < ntiles) issue(t, q);
+        }
     int it = 0;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
-        float *rows = smem + (it % NB) * Gm::BUF;
-        s32::cp_wait<NB - 2>();
-        __syncthreads();  // this tile landed; the buffer of tile it-1 is consumed
-        const long long ahead = tile + (long long)(NB - 1) * gridDim.x;
-        if (ahead < ntiles) issue(ahead, (it + NB - 1) % NB);
-        s32::cp_commit();
+        const int b = it % NB;
+        const bool ok = tma::mbar_wait(&bar[b], (uint32_t)((it / NB) & 1), status);
+        if (__syncthreads_or(!ok)) {  // also: every thread is done with tile it-1's work buffer
+            if (tid == 0) tma::drain(bar, fills, NB, status);
+            break;
+        }
+        const float *lin = lin0 + b * R * RP;
         // four-step pass 1: L2-point FFTs over n2 (stride L1), twiddle W_N^(n1 k2), in place
         // two adjacent n1 per thread: each pair of reals is one 8-byte access
         for (int t = tid; t < P * (L1 / 2); t += T) {
             const int p = t / (L1 / 2), n1 = 2 * (t % (L1 / 2));
+            const float *lre = lin + 2 * p * RP, *lim = lre + RP;
             float *re = rows + 2 * p * PITCH, *im = re + PITCH;
             float2 xa[L2], xb[L2];
 #pragma unroll
             for (int n2 = 0; n2 < L2; n2++) {
-                const int a = Gm::phys(n1 + L1 * n2);
-                const float2 r2 = *reinterpret_cast<const float2 *>(re + a), i2 = *reinterpret_cast<const float2 *>(im + a);
+                const float2 r2 = *reinterpret_cast<const float2 *>(lre + n1 + L1 * n2);
+                const float2 i2 = *reinterpret_cast<const float2 *>(lim + n1 + L1 * n2);
                 xa[n2] = make_float2(r2.x, i2.x);
                 xb[n2] = make_float2(r2.y, i2.y);
             }
@@ -117,7 +140,14 @@ __global__ void __launch_bounds__(T_, MINB) rowt_kernel(const float *S, float2 *
                 *reinterpret_cast<float2 *>(im + a) = make_float2(ya.y, yb.y);
             }
         }
-        __syncthreads();
+        __syncthreads();  // pass 1 done: the linear buffer may be refilled
+        if (tid == 0) {
+            const long long ahead = tile + (long long)NB * gridDim.x;
+            if (ahead < ntiles) {
+                tma::fence_proxy_async();  // the buffer's reads by pass 1 precede its refill
+                issue(ahead, b);
+            }
+        }
         // pass 2: L1-point FFTs over n1, written back in natural order k = k2 + L2 k1
         {
             float2 y[NT2][L1];
@@ -166,7 +196,6 @@ __global__ void __launch_bounds__(T_, MINB) rowt_kernel(const float *S, float2 *
                    make_float4(0.5f * (zr + mr), 0.5f * (zi - mi), 0.5f * (zi + mi), 0.5f * (mr - zr)));
         }
     }
-    s32::cp_wait<0>();
 }
 
 // ---------------------------------------------------------------------------

@@ -202,7 +202,7 @@ cudaError_t fft_plane_scatter_f32(int N, float *S, void *send, int nplanes, int 
 // along j T1 -> T2, and the pass along i fused with the TT projection and h/l
 // update of the amplitudes G (kept in the transposed order [4][kz][ky][kx]).
 bool fftt_supported(int N);
-cudaError_t fftt_rows_f32(int N, const float *S, void *T1, int ncomp, cudaStream_t s);
+cudaError_t fftt_rows_f32(int N, const float *S, void *T1, int ncomp, unsigned int *status, cudaStream_t s);
 cudaError_t fftt_cols_f32(int N, const void *T1, void *T2, int ncomp, unsigned int *status, cudaStream_t s);
 cudaError_t fftt_ikspace_f32(int N, const void *T2, void *G, const DevScalars *sc, const LatticeConsts &c, int slot,
                              unsigned int *status, cudaStream_t s);
