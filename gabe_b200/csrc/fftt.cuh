@@ -44,8 +44,8 @@ using pfft::FourStep;
 // ---------------------------------------------------------------------------
 // A tile of 16 rows (8 pairs, each two real rows taken as one complex
 // sequence) is one contiguous run of 16 (N + 2) floats in S and lands in
-// shared memory by one bulk copy (cp.async.bulk + mbarrier) into a ring of
-// two linear buffers.  The four-step FFT's first pass reads the pairs from
+// shared memory by one bulk copy (cp.async.bulk + mbarrier) into a linear
+// buffer.  The four-step FFT's first pass reads the pairs from
 // the linear buffer (lanes over consecutive elements: conflict-free) and
 // writes its output into a work buffer in the pair-preserving XOR swizzle of
 // fft3d.cuh, so that the second pass's stride-L1 reads fall on distinct
@@ -54,19 +54,22 @@ using pfft::FourStep;
 // pair of rows at one kz (lanes over the 8 pairs, 4 kz per warp) and stores
 // it as one 16-byte value, eight lanes making the 128-byte piece of 16 rows.
 // Work rows sit N + 2 floats apart, so that the eight pairs' rows start on
-// different banks.  Measured at 512^3, same bytes: loading the tile by 8-byte
-// cp.async copies straight into the swizzled layout took 2.13 ms against
-// 2.09 (bit-identical output; the loads were not what bounded the pass, its
-// two CTAs of 4 warps per SM are); staging the output as [kz][16 rows] in
-// shared memory and writing it
+// different banks.  One linear buffer per CTA (70 KB of shared memory with
+// the work buffer and twiddles), refilled after the first pass while the
+// second pass and the output run, and two CTAs per SM.  Measured at 512^3,
+// same bytes, bit-identical output: 1.80 ms, against 2.08 with two linear
+// buffers (103 KB per CTA), 2.00 and 1.97 with three CTAs per SM under
+// 168- and 128-register caps, 2.13 for tiles landed by 8-byte cp.async
+// copies straight into the swizzled layout; staging the output as
+// [kz][16 rows] in shared memory and writing it
 // piece by piece 3.30 ms against 2.28 (the extra barrier and shared-memory
 // round trip held the 8 warps per SM); separating the pairs from the
 // pass-2 registers through warp shuffles, with no write-back, 2.68 ms
 // against 2.13 (each warp store then spans 16 lines instead of 4).
-template <int N, int T_ = 128>
+template <int N, int T_ = 128, int NB_ = 1>
 struct RowTGeom {
     using RG = f3d::RowGeom<N, 16, 1, T_, 2>;  // the work buffer (swizzled, pitch N + 2)
-    static constexpr int R = 16, RP = N + 2, NB = 2;
+    static constexpr int R = 16, RP = N + 2, NB = NB_;
     static constexpr size_t HEAD = 128;                          // NB mbarriers
     static constexpr size_t TW_BYTES = (size_t)N * sizeof(float2);  // twiddles of the four-step
     static constexpr size_t LIN_BYTES = (size_t)R * RP * sizeof(float);
@@ -74,10 +77,10 @@ struct RowTGeom {
     static_assert(LIN_BYTES % 16 == 0 && (HEAD + TW_BYTES) % 16 == 0, "bulk copies of 16-byte multiples");
 };
 
-template <int N, int T_ = 128, int MINB = 2>
+template <int N, int T_ = 128, int MINB = 2, int NB_ = 1>
 __global__ void __launch_bounds__(T_, MINB)
     rowt_kernel(const float *S, float2 *T1, long long nrows, unsigned int *status) {
-    using G = RowTGeom<N, T_>;
+    using G = RowTGeom<N, T_, NB_>;
     using Gm = typename G::RG;
     constexpr int L1 = Gm::L1, L2 = Gm::L2, PITCH = Gm::PITCH, R = Gm::R, P = Gm::P, T = Gm::T, NT2 = Gm::NT2;
     constexpr int RP = G::RP, NB = G::NB, NH = N / 2 + 1;

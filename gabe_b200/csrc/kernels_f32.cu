@@ -8,12 +8,18 @@
 
 namespace gabe {
 
-constexpr int kRingSlots = 6;
+// Plane slots of a sweep's ring (three planes being read, the rest in
+// flight).  The energies-only sweep keeps four: at 512^3 it ran 0.5-0.6 ms
+// with four against 0.75 with six (less shared memory per SM leaves more
+// L1); sweeps A and B ran best with six (A 1.83 ms against 2.10 with four
+// and 2.18 with ten; B 0.87 against 1.00 with four).
+constexpr int kRingSlots = 6, kRingSlotsE0 = 4;
 
 template <int TK2, int TJ, int MODE>
 static cudaError_t launch32(const StencilArgs &a, dim3 grid, cudaStream_t s) {
-    auto k = s32::sweep32_kernel<TK2, TJ, MODE, kRingSlots>;
-    const size_t smem = (size_t)kRingSlots * s32::Ring<TK2, TJ>::SLOT * sizeof(float);
+    constexpr int S = MODE == MODE_E0 ? kRingSlotsE0 : kRingSlots;
+    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S>;
+    const size_t smem = (size_t)S * s32::Ring<TK2, TJ>::SLOT * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, TK2 * TJ, smem, s>>>(a);
