@@ -15,15 +15,22 @@ namespace gabe {
 // and 2.18 with ten; B 0.87 against 1.00 with four).
 constexpr int kRingSlots = 6, kRingSlotsE0 = 4;
 
-template <int TK2, int TJ, int MODE>
-static cudaError_t launch32(const StencilArgs &a, dim3 grid, cudaStream_t s) {
+template <int TK2, int TJ, int MODE, int MODEL>
+static cudaError_t launch32m(const StencilArgs &a, dim3 grid, cudaStream_t s) {
     constexpr int S = MODE == MODE_E0 ? kRingSlotsE0 : kRingSlots;
-    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S>;
+    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S, MODEL>;
     const size_t smem = (size_t)S * s32::Ring<TK2, TJ>::SLOT * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, TK2 * TJ, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+// One instantiation per potential, so that no site branches on the model.
+template <int TK2, int TJ, int MODE>
+static cudaError_t launch32(const StencilArgs &a, dim3 grid, cudaStream_t s) {
+    return a.c.model == MODEL_QUADRATIC ? launch32m<TK2, TJ, MODE, MODEL_QUADRATIC>(a, grid, s)
+                                        : launch32m<TK2, TJ, MODE, MODEL_LPHI4>(a, grid, s);
 }
 
 template <int TK2, int TJ>

@@ -75,11 +75,20 @@ __device__ __forceinline__ Site32 site32_consts(const LatticeConsts &c, const De
     return s;
 }
 
+// Potential of the site functions: MODEL >= 0 fixes it at compile time (the
+// single-lattice sweeps, one instantiation per model, no branch per site),
+// -1 reads it from the lattice constants (the ensemble's mixed batches).
+template <int MODEL>
+__device__ __forceinline__ int site_model(const LatticeConsts &c) {
+    return MODEL >= 0 ? MODEL : c.model;
+}
+
 // One site of sweep A / E0: adds to the moments, fills the sources.
-template <int MODE>
+template <int MODE, int MODEL = -1>
 __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s, const Nb7<float> &fp,
                                          const Nb7<float> &fc, const Nb7<float> &dp, const Nb7<float> &dc,
                                          Moments &m, float (&s0)[kSrc], float (&s1)[kSrc]) {
+    const int model = site_model<MODEL>(c);
     const Nb7<float> *f0[2] = {&fp, &fc}, *d0[2] = {&dp, &dc};
     float f1c[2];
     float P0[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, P1[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -94,7 +103,7 @@ __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s
         if constexpr (MODE != MODE_E0) {
             const Nb7<float> f1 = axpy7(ff, s.hf, dd);
             f1c[f] = f1.v[0];
-            const float Pd = d + s.hf * (lap0 * s.ia02f - dv_diff32(s.m0, c.model, f, fp.v[0], fc.v[0]));
+            const float Pd = d + s.hf * (lap0 * s.ia02f - dv_diff32(s.m0, model, f, fp.v[0], fc.v[0]));
             m.c[f] += Pd;
             m.e = fmaf(Pd, Pd, m.e);
             m.f = fmaf(Pd, d, m.f);
@@ -109,24 +118,26 @@ __device__ __forceinline__ void site_a32(const LatticeConsts &c, const Site32 &s
         source_from_prod(s.qsf, P0, s0);
         source_from_prod(s.qsf, P1, s1);
     }
-    m.v0 += v_diff32(s.m0, c.model, fp.v[0], fc.v[0]);
-    if constexpr (MODE != MODE_E0) m.v1 += v_diff32(s.m1, c.model, f1c[0], f1c[1]);
+    m.v0 += v_diff32(s.m0, model, fp.v[0], fc.v[0]);
+    if constexpr (MODE != MODE_E0) m.v1 += v_diff32(s.m1, model, f1c[0], f1c[1]);
 }
 
 // One site of sweep B: the new field and momentum of both fields.
+template <int MODEL = -1>
 __device__ __forceinline__ void site_b32(const LatticeConsts &c, const Site32 &s, const Nb7<float> &fp,
                                          const Nb7<float> &fc, const Nb7<float> &dp, const Nb7<float> &dc,
                                          float (&xo)[2], float (&dout)[2]) {
+    const int model = site_model<MODEL>(c);
     const Nb7<float> *f0[2] = {&fp, &fc}, *d0[2] = {&dp, &dc};
     const Nb7<float> f1[2] = {axpy7(fp, s.hf, dp), axpy7(fc, s.hf, dc)};
 #pragma unroll
     for (int f = 0; f < 2; f++) {
         const Nb7<float> &ff = *f0[f], &dd = *d0[f];
         const float lap0 = lap32(ff, s.inv_dx2f);
-        const float dd0 = lap0 * s.ia02f - dv_diff32(s.m0, c.model, f, fp.v[0], fc.v[0]) - s.c3H0f * dd.v[0];
+        const float dd0 = lap0 * s.ia02f - dv_diff32(s.m0, model, f, fp.v[0], fc.v[0]) - s.c3H0f * dd.v[0];
         const float d1c = dd.v[0] + s.hf * dd0;
         const float lap1 = lap32(f1[f], s.inv_dx2f);
-        const float dd1 = lap1 * s.ia12f - dv_diff32(s.m1, c.model, f, f1[0].v[0], f1[1].v[0]) - s.c3H1f * d1c;
+        const float dd1 = lap1 * s.ia12f - dv_diff32(s.m1, model, f, f1[0].v[0], f1[1].v[0]) - s.c3H1f * d1c;
         xo[f] = ff.v[0] + s.dtf * d1c;
         dout[f] = dd.v[0] + s.dtf * dd1;
     }
@@ -153,7 +164,7 @@ struct Tile32 {
 // threads (NT >= TK2 TJ; threads beyond TK2 TJ only take part in the
 // barriers).  Sweep A / E0 add the tile's folded sums to acc (per-thread
 // partials, zero on idle threads); sweep B writes the new state.
-template <int TK2, int TJ, int MODE, int S, int NT>
+template <int TK2, int TJ, int MODE, int S, int NT, int MODEL = -1>
 __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s, const Tile32 &t, float *ring,
                                         double (&acc)[kNV]) {
     using Rg = Ring<TK2, TJ>;
@@ -258,7 +269,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
                 float xo[2][2], dout[2][2];  // [site][field]
 #pragma unroll
                 for (int v = 0; v < 2; v++) {
-                    site_b32(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], xo[v], dout[v]);
+                    site_b32<MODEL>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], xo[v], dout[v]);
                 }
                 const int gx = i * NN + o_own;
                 __stcs(reinterpret_cast<float2 *>(t.Xo + gx), make_float2(xo[0][0], xo[1][0]));
@@ -269,7 +280,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
                 float s0[2][kSrc] = {}, s1[2][kSrc] = {};
 #pragma unroll
                 for (int v = 0; v < 2; v++) {
-                    site_a32<MODE>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], mom, s0[v], s1[v]);
+                    site_a32<MODE, MODEL>(c, s, nb[0][v], nb[1][v], nb[2][v], nb[3][v], mom, s0[v], s1[v]);
                 }
                 if (++ngroup == kGroup || i == i1 - 1) {
                     fold<MODE>(s.mt, s.q3f, 2 * ngroup, mom, acc);
@@ -300,7 +311,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     __syncthreads();  // the ring may be refilled by the block's next tile
 }
 
-template <int TK2, int TJ, int MODE, int S>
+template <int TK2, int TJ, int MODE, int S, int MODEL = -1>
 __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2 * TJ - 1) / (TK2 * TJ))
     sweep32_kernel(StencilArgs args) {
     extern __shared__ __align__(16) float ring[];  // S slots
@@ -327,7 +338,7 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
     double acc[kNV];
 #pragma unroll
     for (int q = 0; q < kNV; q++) acc[q] = 0.;
-    march32<TK2, TJ, MODE, S, TK2 * TJ>(c, s, t, ring, acc);
+    march32<TK2, TJ, MODE, S, TK2 * TJ, MODEL>(c, s, t, ring, acc);
 
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if constexpr (MODE != MODE_B) {
