@@ -18,8 +18,9 @@ constexpr int kRingSlots = 6, kRingSlotsE0 = 4;
 template <int TK2, int TJ, int MODE, int MODEL>
 static cudaError_t launch32m(const StencilArgs &a, dim3 grid, cudaStream_t s) {
     constexpr int S = MODE == MODE_E0 ? kRingSlotsE0 : kRingSlots;
-    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S, MODEL>;
-    const size_t smem = (size_t)S * s32::Ring<TK2, TJ>::SLOT * sizeof(float);
+    constexpr bool W16 = MODE != MODE_B;  // wide slots except for sweep B (sweep32.cuh, Ring)
+    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S, MODEL, W16>;
+    const size_t smem = (size_t)S * s32::Ring<TK2, TJ, W16>::SLOT * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, TK2 * TJ, smem, s>>>(a);

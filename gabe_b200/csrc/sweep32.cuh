@@ -26,6 +26,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+// 16 bytes, cached in L2 only.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -36,12 +41,18 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory");
 }
 
-// Shared-memory plane slot: [4 arrays][TJ + 2 rows][PK columns]; column 1 is
-// the k0-1 halo, columns 2 .. TK+1 the tile, column TK+2 the k0+TK halo, so
-// that every thread's pair starts on an 8-byte boundary.
-template <int TK2, int TJ>
+// Shared-memory plane slot: [4 arrays][TJ + 2 rows][PK columns]; column C0-1
+// is the k0-1 halo, columns C0 .. C0+TK-1 the tile, column C0+TK the k0+TK
+// halo.  Narrow (W16 false): C0 = 2, PK = TK + 4, every thread's pair on an
+// 8-byte boundary, one 8-byte copy per thread.  Wide (W16): C0 = 4,
+// PK = TK + 8, rows 16-byte multiples, so the pairs of threads 2m and 2m+1
+// land as one 16-byte copy (L2 only).  Measured at 512^3: sweep A 1.81 ms
+// wide against 1.83 narrow, the energies-only sweep 0.44 against ~0.55,
+// sweep B 0.94 against 0.85 (three CTAs per SM: the wider slots leave less
+// L1), so B takes the narrow slots.
+template <int TK2, int TJ, bool W16 = false>
 struct Ring {
-    static constexpr int TK = 2 * TK2, PK = TK + 4, ROWS = TJ + 2;
+    static constexpr int TK = 2 * TK2, PK = TK + (W16 ? 8 : 4), ROWS = TJ + 2, C0 = W16 ? 4 : 2;
     static constexpr int ARR = ROWS * PK, SLOT = 4 * ARR;
 };
 
@@ -164,11 +175,11 @@ struct Tile32 {
 // threads (NT >= TK2 TJ; threads beyond TK2 TJ only take part in the
 // barriers).  Sweep A / E0 add the tile's folded sums to acc (per-thread
 // partials, zero on idle threads); sweep B writes the new state.
-template <int TK2, int TJ, int MODE, int S, int NT, int MODEL = -1>
+template <int TK2, int TJ, int MODE, int S, int NT, int MODEL = -1, bool W16 = false>
 __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s, const Tile32 &t, float *ring,
                                         double (&acc)[kNV]) {
-    using Rg = Ring<TK2, TJ>;
-    constexpr int TK = Rg::TK, PK = Rg::PK;
+    using Rg = Ring<TK2, TJ, W16>;
+    constexpr int TK = Rg::TK, PK = Rg::PK, C0 = Rg::C0;
     static_assert(S >= 4, "ring needs planes i-1, i, i+1 and one in flight");
     static_assert(TK2 * TJ >= 2 * TK2 + 2 * TJ, "enough threads for the halo copies");
     static_assert(NT >= TK2 * TJ, "block smaller than the tile");
@@ -186,7 +197,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     const int NN = N * N;
     const int jm = wrapi(j0 - 1, N), jp = wrapi(j0 + TJ, N), km = wrapi(k0 - 1, N), kp = wrapi(k0 + TK, N);
     const int o_own = j * N + k;
-    const int so_own = (ty + 1) * PK + 2 + 2 * tx;  // shared offset of the own pair within an array
+    const int so_own = (ty + 1) * PK + C0 + 2 * tx;  // shared offset of the own pair within an array
     // halo duty, one copy per array: threads 0 .. 2 TK2 - 1 copy pairs of the
     // j0-1 and j0+TJ rows, the next 2 TJ threads single points of the k0-1 and
     // k0+TK columns
@@ -194,12 +205,12 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     if (tid < 2 * TK2) {
         const int r = tid / TK2, q = tid % TK2;
         h_kind = 8;
-        h_so = (r ? (TJ + 1) * PK : 0) + 2 + 2 * q;
+        h_so = (r ? (TJ + 1) * PK : 0) + C0 + 2 * q;
         h_go = (r ? jp : jm) * N + k0 + 2 * q;
     } else if (tid < 2 * TK2 + 2 * TJ) {
         const int r = (tid - 2 * TK2) / TJ, q = (tid - 2 * TK2) % TJ;
         h_kind = 4;
-        h_so = (q + 1) * PK + (r ? TK + 2 : 1);
+        h_so = (q + 1) * PK + (r ? TK + C0 : C0 - 1);
         h_go = (j0 + q) * N + (r ? kp : km);
     }
     auto issue = [&](int p, int sl) {  // plane p (wrapped) into slot sl
@@ -210,7 +221,12 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
         for (int a = 0; a < 4; a++) {
             float *sa = slot + a * Rg::ARR;
             const float *g = src[a] + pb;
-            cp_async8(sa + so_own, g + o_own);
+            if constexpr (W16) {
+                // the pairs of threads 2m and 2m+1 as one 16-byte copy (k0 + 4m is 16-byte aligned)
+                if ((tx & 1) == 0) cp_async16(sa + so_own, g + o_own);
+            } else {
+                cp_async8(sa + so_own, g + o_own);
+            }
             if (h_kind == 8) cp_async8(sa + h_so, g + h_go);
             else if (h_kind == 4) cp_async4(sa + h_so, g + h_go);
         }
@@ -311,7 +327,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     __syncthreads();  // the ring may be refilled by the block's next tile
 }
 
-template <int TK2, int TJ, int MODE, int S, int MODEL = -1>
+template <int TK2, int TJ, int MODE, int S, int MODEL = -1, bool W16 = false>
 __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2 * TJ - 1) / (TK2 * TJ))
     sweep32_kernel(StencilArgs args) {
     extern __shared__ __align__(16) float ring[];  // S slots
@@ -338,7 +354,7 @@ __global__ void __launch_bounds__(TK2 *TJ, (sweep32_threads_per_sm<MODE>() + TK2
     double acc[kNV];
 #pragma unroll
     for (int q = 0; q < kNV; q++) acc[q] = 0.;
-    march32<TK2, TJ, MODE, S, TK2 * TJ, MODEL>(c, s, t, ring, acc);
+    march32<TK2, TJ, MODE, S, TK2 * TJ, MODEL, W16>(c, s, t, ring, acc);
 
     const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     if constexpr (MODE != MODE_B) {
