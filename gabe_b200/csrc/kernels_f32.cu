@@ -9,18 +9,21 @@
 namespace gabe {
 
 // Plane slots of a sweep's ring (three planes being read, the rest in
-// flight).  The energies-only sweep keeps four: at 512^3 it ran 0.5-0.6 ms
-// with four against 0.75 with six (less shared memory per SM leaves more
-// L1); sweeps A and B ran best with six (A 1.83 ms against 2.10 with four
-// and 2.18 with ten; B 0.87 against 1.00 with four).
-constexpr int kRingSlots = 6, kRingSlotsE0 = 4;
+// flight), all in the wide layout (sweep32.cuh, Ring).  Measured at 512^3:
+// sweep A 1.81 ms with six slots (2.10 with four, 2.18 with ten); sweep B
+// 0.835 with five (0.87 with six narrow ones, 1.02 with four); the
+// energies-only sweep 0.2-0.4 with four against ~0.75 with six narrow ones.
+// Fewer slots leave more of the SM's shared memory to L1.
+template <int MODE>
+constexpr int ring_slots() {
+    return MODE == MODE_E0 ? 4 : (MODE == MODE_B ? 5 : 6);
+}
 
 template <int TK2, int TJ, int MODE, int MODEL>
 static cudaError_t launch32m(const StencilArgs &a, dim3 grid, cudaStream_t s) {
-    constexpr int S = MODE == MODE_E0 ? kRingSlotsE0 : kRingSlots;
-    constexpr bool W16 = MODE != MODE_B;  // wide slots except for sweep B (sweep32.cuh, Ring)
-    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S, MODEL, W16>;
-    const size_t smem = (size_t)S * s32::Ring<TK2, TJ, W16>::SLOT * sizeof(float);
+    constexpr int S = ring_slots<MODE>();
+    auto k = s32::sweep32_kernel<TK2, TJ, MODE, S, MODEL, true>;
+    const size_t smem = (size_t)S * s32::Ring<TK2, TJ, true>::SLOT * sizeof(float);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     k<<<grid, TK2 * TJ, smem, s>>>(a);
