@@ -25,7 +25,7 @@ import numpy as np
 
 __all__ = [
     "GabeError", "Params", "Lattice", "library", "lib_path", "lphi4_constants",
-    "FP64", "FP32", "MODEL_QUADRATIC", "MODEL_LPHI4", "numbins",
+    "FP64", "FP32", "MODEL_QUADRATIC", "MODEL_LPHI4", "numbins", "wait_probe",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -115,6 +115,20 @@ def library():
 
 def numbins(N: int) -> int:
     return int(math.sqrt(3.0) * N / 2 + 1)
+
+
+def wait_probe(limit_ns: int) -> tuple[int, int, int]:
+    """gabe_wait_probe: the library's bounded device wait run on a barrier
+    nothing arrives at.  Returns (return code, device status word, GPU ns
+    waited); the code is 6 (GABE_ERR_TIMEOUT) when the wait gave up as
+    designed."""
+    L = library()
+    if not getattr(L, "_probe_ready", False):
+        L.gabe_wait_probe.argtypes = [ctypes.c_int64, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_int64)]
+        L._probe_ready = True
+    st, w = ctypes.c_uint32(), ctypes.c_int64()
+    rc = L.gabe_wait_probe(int(limit_ns), ctypes.byref(st), ctypes.byref(w))
+    return rc, st.value, w.value
 
 
 def lphi4_constants(g2_over_lambda: float = 100.0, phi0: float = 0.342) -> tuple[float, float]:

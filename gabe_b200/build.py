@@ -31,6 +31,7 @@ UNITS = [
     ("ensemble.cu", []),
     ("slab.cu", []),
     ("mlp.cu", []),
+    ("probe.cu", []),
 ]
 
 

@@ -67,17 +67,21 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
 }
 
 // Waits until the barrier's phase with parity `parity` has completed.
-// false (and ST_TIMEOUT in *status) if it did not within kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned int *status) {
+// false (and ST_TIMEOUT in *status) if it did not within limit_ns.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t *bar, uint32_t parity, unsigned int *status,
+                                              unsigned long long limit_ns) {
     if (mbar_test(bar, parity)) return true;
     const unsigned long long t0 = now_ns();
     while (!mbar_test(bar, parity)) {
-        if (now_ns() - t0 > kWaitNs) {
+        if (now_ns() - t0 > limit_ns) {
             atomicOr(status, ST_TIMEOUT);
             return false;
         }
     }
     return true;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned int *status) {
+    return mbar_wait_for(bar, parity, status, kWaitNs);
 }
 
 // After a wait gave up: waits (bounded again) for the last fill of each of

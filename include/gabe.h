@@ -157,6 +157,16 @@ int gabe_stream(gabe_handle *h, void **stream);
 /* Waits for queued work; returns the first error seen on the device. */
 int gabe_sync(gabe_handle *h);
 
+/* Diagnostic of the bounded device waits, no handle needed: runs the
+ * library's bounded mbarrier wait (the one every bulk copy, TMA load and
+ * tcgen05 MMA wait of its kernels uses) on a barrier that nothing arrives
+ * at, with a limit of limit_ns of GPU time (0 < limit_ns <= 1e10).  The
+ * wait gives up, raises the timeout bit (2) in a device status word and
+ * the kernel returns; *status_out receives that word, *waited_ns_out the
+ * GPU time waited (either may be NULL).  Returns GABE_ERR_TIMEOUT when the
+ * wait gave up, as designed; the context stays usable. */
+int gabe_wait_probe(int64_t limit_ns, uint32_t *status_out, int64_t *waited_ns_out);
+
 /* Stage-0 energies {kin, pot, grad, rho} and a, adot (synchronises). */
 int gabe_energies(gabe_handle *h, double out4[4], double *a, double *adot);
 

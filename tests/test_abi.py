@@ -171,3 +171,12 @@ def test_bench_reference_arm_line():
     env = dict(os.environ, RANK="1", WORLD_SIZE="2")
     other = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
     assert other.returncode == 0 and not other.stdout.strip()
+
+
+def test_wait_probe_refuses_bad_limits_before_any_device_call():
+    """gabe_wait_probe checks its limit on the host (no GPU needed here)."""
+    import gabe_b200 as gb
+
+    assert gb.wait_probe(0)[0] == 1
+    assert gb.wait_probe(-5)[0] == 1
+    assert gb.wait_probe(20_000_000_000)[0] == 1
