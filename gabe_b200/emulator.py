@@ -370,7 +370,7 @@ __all__ = ["MLP", "Emulator", "nearest_neighbour", "per_bin_error", "queries_per
 
 # ---------------------------------------------------------------------------
 # The parameter-sweep workflow: ensembles -> training set -> emulator ->
-# held-out lattice re-runs as judge.
+# held-out lattice re-runs as the check.
 # ---------------------------------------------------------------------------
 def ensemble_samples(N, g, amp, seeds, steps: int, every: int, nlog: int = 64, dt: float = 0.01, device: int = -1,
                      log_top_bin: int | None = None):
@@ -404,7 +404,7 @@ def ensemble_samples(N, g, amp, seeds, steps: int, every: int, nlog: int = 64, d
 def run_sweep(*, nlat=256, ensembles=2, steps=2000, every=50, nlog=64, holdout=32, holdout_N=64, members=4,
               epochs=1000, batch=512, lr=1e-3, master_seed=20261203, flag_quantile=0.9, sizes=None, log=print):
     """Trains the emulator on `ensembles` uneven ensembles of `nlat`
-    lattices and judges it on `holdout` new parameter points evolved at
+    lattices and checks it on `holdout` new parameter points evolved at
     holdout_N^3.  Returns the report dict."""
     import time
 
@@ -452,7 +452,7 @@ def run_sweep(*, nlat=256, ensembles=2, steps=2000, every=50, nlog=64, holdout=3
     per_point = np.array([vpt[vlat == l].max() for l in np.unique(vlat)])
     thr = float(np.quantile(per_point, flag_quantile))
     report["flag_threshold_dex"] = thr
-    # held-out parameter points, re-run on the lattice as judge
+    # held-out parameter points, re-run on the lattice as the check
     _, gh, ah, sh = sample_parameters(holdout, master_seed + 1000)
     Nh = np.full(holdout, holdout_N, dtype=np.int32)
     fh, yh, lath, ms_h = ensemble_samples(Nh, gh, ah, sh, steps, every, nlog)
@@ -499,7 +499,7 @@ def main():
     import argparse
     import json
 
-    ap = argparse.ArgumentParser(description="emulator sweep: ensembles -> training -> held-out lattice judge")
+    ap = argparse.ArgumentParser(description="emulator sweep: ensembles -> training -> held-out lattice check")
     ap.add_argument("--lattices", type=int, default=256)
     ap.add_argument("--ensembles", type=int, default=2)
     ap.add_argument("--steps", type=int, default=2000)

@@ -1,5 +1,5 @@
 """What the trained emulator gains over the sweep without it, on a small
-sweep (uniform 32^3 lattices so that the judge runs at the training size):
+sweep (uniform 32^3 lattices so that the held-out check runs at the training size):
 
 * accuracy: on held-out parameter points evolved on the lattice, the
   emulator's phi, chi and GW log spectra are closer to the lattice than the
@@ -32,8 +32,8 @@ def test_emulator_beats_nearest_neighbour_and_is_cheaper_than_the_lattice():
     assert np.isfinite(rep["flag_threshold_dex"])
 
 
-def test_emulator_trained_on_uneven_sizes_beats_nearest_neighbour_at_the_judge_size():
-    """Training lattices of two sizes, judge at the larger: the lattice size is
+def test_emulator_trained_on_uneven_sizes_beats_nearest_neighbour_at_the_checked_size():
+    """Training lattices of two sizes, checked at the larger: the lattice size is
     an input, so the GW spectra -- which differ strongly between sizes -- are
     emulated for the size asked for, and every column beats the lookup of the
     nearest training lattice of that size."""
