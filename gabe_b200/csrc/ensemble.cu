@@ -182,7 +182,7 @@ EnsArgs ens_args(gabe_ensemble *e, int cur) {
 
 template <int MODE>
 cudaError_t launch_sweep(const EnsArgs &a, cudaStream_t s) {
-    constexpr size_t smem = ens_ring_bytes();
+    constexpr size_t smem = ens_ring_bytes<MODE>();
     cudaError_t r = cudaFuncSetAttribute(ens_sweep_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (r != cudaSuccess) return r;
     ens_sweep_kernel<MODE><<<a.nitems, kEnsThreads, smem, s>>>(a);

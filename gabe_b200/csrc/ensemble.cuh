@@ -59,15 +59,22 @@ struct EnsArgs {
 // block, the FP32 plane march of the single-lattice sweeps (sweep32.cuh)
 // ---------------------------------------------------------------------------
 constexpr int kEnsThreads = 256;
-constexpr int kEnsRing = 6;  // plane slots of the cp.async ring
+// Plane slots of the cp.async ring per sweep (the wide slots of sweep32.cuh,
+// as the single-lattice sweeps: six for sweep A, five for sweep B, four for
+// the energies-only sweep).
+template <int MODE>
+__host__ __device__ constexpr int ens_ring() {
+    return MODE == MODE_E0 ? 4 : (MODE == MODE_B ? 5 : 6);
+}
 
 // Tile shapes of the work items, sites along k x j: 0 = 64 x 8, 1 = 32 x 16,
 // 2 = 16 x 16 (128 of the 256 threads march; for N = 16 (mod 32)).
 __host__ __device__ constexpr int ens_tile_k(int shape) { return shape == 0 ? 64 : (shape == 1 ? 32 : 16); }
 __host__ __device__ constexpr int ens_tile_j(int shape) { return shape == 0 ? 8 : 16; }
+template <int MODE>
 constexpr size_t ens_ring_bytes() {
-    constexpr int a = s32::Ring<32, 8>::SLOT, b = s32::Ring<16, 16>::SLOT, c = s32::Ring<8, 16>::SLOT;
-    return sizeof(float) * kEnsRing * (a > b ? (a > c ? a : c) : (b > c ? b : c));
+    constexpr int a = s32::Ring<32, 8, true>::SLOT, b = s32::Ring<16, 16, true>::SLOT, c = s32::Ring<8, 16, true>::SLOT;
+    return sizeof(float) * ens_ring<MODE>() * (a > b ? (a > c ? a : c) : (b > c ? b : c));
 }
 
 template <int MODE>
@@ -95,9 +102,10 @@ __global__ void __launch_bounds__(kEnsThreads, s32::sweep32_threads_per_sm<MODE>
     double acc[kNV];
 #pragma unroll
     for (int q = 0; q < kNV; q++) acc[q] = 0.;
-    if (item.shape == 0) s32::march32<32, 8, MODE, kEnsRing, kEnsThreads>(c, s, t, ring, acc);
-    else if (item.shape == 1) s32::march32<16, 16, MODE, kEnsRing, kEnsThreads>(c, s, t, ring, acc);
-    else s32::march32<8, 16, MODE, kEnsRing, kEnsThreads>(c, s, t, ring, acc);
+    constexpr int S = ens_ring<MODE>();
+    if (item.shape == 0) s32::march32<32, 8, MODE, S, kEnsThreads, -1, true>(c, s, t, ring, acc);
+    else if (item.shape == 1) s32::march32<16, 16, MODE, S, kEnsThreads, -1, true>(c, s, t, ring, acc);
+    else s32::march32<8, 16, MODE, S, kEnsThreads, -1, true>(c, s, t, ring, acc);
     if constexpr (MODE != MODE_B) {
         block_reduce<kNV>(acc, sred);
         if (tid == 0)

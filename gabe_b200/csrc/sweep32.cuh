@@ -46,10 +46,9 @@ __device__ __forceinline__ void cp_wait() {
 // halo.  Narrow (W16 false): C0 = 2, PK = TK + 4, every thread's pair on an
 // 8-byte boundary, one 8-byte copy per thread.  Wide (W16): C0 = 4,
 // PK = TK + 8, rows 16-byte multiples, so the pairs of threads 2m and 2m+1
-// land as one 16-byte copy (L2 only).  The single-lattice sweeps use the
-// wide slots (at 512^3 sweep A 1.81 ms against 1.83 narrow, sweep B 0.835
-// with five wide slots against 0.87 with six narrow ones); the ensemble's
-// mixed tiles keep the narrow ones.
+// land as one 16-byte copy (L2 only).  The single-lattice and ensemble
+// sweeps use the wide slots (at 512^3 sweep A 1.81 ms against 1.83 narrow,
+// sweep B 0.835 with five wide slots against 0.87 with six narrow ones).
 template <int TK2, int TJ, bool W16 = false>
 struct Ring {
     static constexpr int TK = 2 * TK2, PK = TK + (W16 ? 8 : 4), ROWS = TJ + 2, C0 = W16 ? 4 : 2;
