@@ -226,6 +226,8 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
             } else {
                 cp_async8(sa + so_own, g + o_own);
             }
+            // the energies-only sweep reads the momenta at the own sites only
+            if (MODE == MODE_E0 && a >= 2) continue;
             if (h_kind == 8) cp_async8(sa + h_so, g + h_go);
             else if (h_kind == 4) cp_async4(sa + h_so, g + h_go);
         }
