@@ -501,10 +501,12 @@ int gabe_create(const gabe_params *p, gabe_handle **out) {
     }
     // sources need 10 padded slots; spectra need 2; uploads stage one FP64 field array
     h->evolve_gw = p->gws_on && p->expansion == 1;
-    // the transposed form: on request, and by default for FP32 at N = 512 (measured fastest there)
+    // the transposed form: on request, and by default for FP32 at N >= 128 (measured fastest there:
+    // per step 8.1 against ~11 ms at 512^3, 1.21 against 1.41 at 256^3, 0.170 against 0.192 at 128^3
+    // with cuFFT's plan and the overlapped k-space chain; a tie at 64^3)
     h->fftt = h->evolve_gw && h->f32 && fftt_supported(h->N) &&
               ((p->flags & GABE_FLAG_TRANSPOSED_FFT) ||
-               (h->N == 512 && !(p->flags & (GABE_FLAG_OWN_FFT | GABE_FLAG_CUFFT_3D))));
+               (h->N >= 128 && !(p->flags & (GABE_FLAG_OWN_FFT | GABE_FLAG_CUFFT_3D))));
     h->nslots = h->evolve_gw ? 2 * kSrc : 2;
     h->S_bytes = (size_t)h->nslots * p->N * p->N * (p->N + 2) * h->esz;
     if ((rc = dalloc(h, &h->S, h->S_bytes))) return bail(rc);

@@ -75,16 +75,17 @@ enum gabe_flags {
     GABE_FLAG_OWN_FFT = 16,     /* FP32 with N in {64, 128, 256, 512}: transform the GW sources with the
                                    library's in-layout three-pass 3-D r2c (the layout of a library r2c)
                                    followed by the separate k-space pass, instead of the default */
-    GABE_FLAG_CUFFT_3D = 64,    /* FP32 at N = 512: cuFFT's 3-D plan and the separate k-space pass instead
-                                   of the default transposed transform (cuFFT's plan is the default at
-                                   every other size and for FP64) */
+    GABE_FLAG_CUFFT_3D = 64,    /* FP32 at N in {128, 256, 512}: cuFFT's 3-D plan and the separate k-space
+                                   pass instead of the default transposed transform (cuFFT's plan is the
+                                   default at every other size and for FP64) */
     GABE_FLAG_TRANSPOSED_FFT = 128 /* FP32 with N in {64, 128, 256, 512}: the library's transposed three-pass
                                    transform -- rows along k, then along j, each written transposed so
                                    that every pass reads whole contiguous lines (bulk copies), and the
                                    pass along i fused with the TT projection and h/l update, so the
                                    transformed sources are never written back.  The default for FP32 at
-                                   N = 512 (the fastest form measured there on B200); needs the second
-                                   source buffer whatever GABE_FLAG_NO_OVERLAP says */
+                                   N in {128, 256, 512} (the fastest form measured there on B200; a tie
+                                   with cuFFT's plan at 64); needs the second source buffer whatever
+                                   GABE_FLAG_NO_OVERLAP says */
 };
 
 /* Run-time form of the g2parameters.h knobs that the hot path reads.  Two

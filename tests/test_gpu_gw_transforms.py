@@ -81,6 +81,18 @@ def test_gw_transform_launch_forms_agree(form, flags):
         np.testing.assert_array_equal(x, y)
 
 
+@pytest.mark.parametrize("N,form", [(64, 0), (128, gb.FLAG_TRANSPOSED_FFT), (256, gb.FLAG_TRANSPOSED_FFT),
+                                    (512, gb.FLAG_TRANSPOSED_FFT)])
+def test_default_gw_transform_form(N, form):
+    """FP32 with GWs defaults to the transposed form at N >= 128 (measured
+    fastest there) and to cuFFT's plan at 64; GABE_FLAG_CUFFT_3D forces
+    cuFFT's plan."""
+    with gb.Lattice(N, gws=True, precision=gb.FP32) as lat:
+        assert lat.launches_per_step == LAUNCHES[form]
+    with gb.Lattice(N, gws=True, precision=gb.FP32, flags=gb.FLAG_CUFFT_3D) as lat:
+        assert lat.launches_per_step == LAUNCHES[gb.FLAG_CUFFT_3D]
+
+
 def test_gw_transforms_512_match_cufft_3d():
     N = 512
     f, d, a0, ad0 = _state(N, seed=3)
