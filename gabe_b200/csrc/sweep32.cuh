@@ -180,6 +180,7 @@ __device__ __forceinline__ void march32(const LatticeConsts &c, const Site32 &s,
     using Rg = Ring<TK2, TJ, W16>;
     constexpr int TK = Rg::TK, PK = Rg::PK, C0 = Rg::C0;
     static_assert(S >= 4, "ring needs planes i-1, i, i+1 and one in flight");
+    static_assert(!W16 || TK2 % 2 == 0, "wide slots copy the pairs of threads 2m and 2m+1 of one row together");
     static_assert(TK2 * TJ >= 2 * TK2 + 2 * TJ, "enough threads for the halo copies");
     static_assert(NT >= TK2 * TJ, "block smaller than the tile");
     const int N = c.N;
