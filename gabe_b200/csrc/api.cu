@@ -580,6 +580,7 @@ int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield
         return set_err(h, GABE_ERR_PARAM, "a0 must be positive and finite");
     CK(h, cudaSetDevice(h->dev));
     h->err.clear();
+    h->uploaded = false;  // until the whole state is in place: a refused upload leaves no half-new state to step
     DevScalars s{};
     s.a[0] = a0;
     s.adot[0] = adot0;
@@ -1120,6 +1121,7 @@ int gabe_load_state(gabe_handle *h, const char *path, int *restored) {
         if (fread(&sc, sizeof(sc), 1, fc.f) != 1) return set_err(h, GABE_ERR_PARAM, "checkpoint file is truncated");
         sc.status = 0;
         CK(h, cudaStreamSynchronize(h->stream));
+        h->uploaded = false;  // a read that fails below leaves a partly overwritten state: no steps on it
         std::vector<char> bounce((size_t)64 << 20);
         int rc;
         if ((rc = read_device(h, fc.f, h->X[0], (size_t)r.field_bytes, bounce)) ||

@@ -127,7 +127,9 @@ int gabe_destroy(gabe_handle *h);
  * h0/l0 [12][N][N][N/2+1] (NULL = zero; ignored without GWs).  a0/adot0 are
  * taken as given -- after the reference's initialisation adot[0] belongs to
  * the homogeneous state (g2init.cpp:29) -- and the stage-0 energies are
- * recomputed on the device as calcEnergy(0) would. */
+ * recomputed on the device as calcEnergy(0) would.  An upload that fails
+ * (e.g. non-TT h/l, a non-finite state) leaves the handle without a state:
+ * calls that need one return GABE_ERR_STATE until an upload succeeds. */
 int gabe_upload_state(gabe_handle *h, const double *field0, const double *dfield0,
                       const double *h0, const double *l0, double a0, double adot0);
 
@@ -193,7 +195,9 @@ int gabe_save_state(gabe_handle *h, const char *path);
  * becomes the state and the run continues bit for bit (with the same tile
  * plan; *restored = 1).  Otherwise its FP64 arrays are uploaded as
  * gabe_upload_state does (*restored = 0): e.g. the dumps of the reference
- * harness.  restored may be NULL. */
+ * harness.  restored may be NULL.  A load that fails after it began to
+ * overwrite the device state leaves the handle without a state, as a failed
+ * gabe_upload_state does. */
 int gabe_load_state(gabe_handle *h, const char *path, int *restored);
 
 /* Number of native |k| bins, (int)(sqrt(3) N/2 + 1) (g2spectra.cpp:31). */
