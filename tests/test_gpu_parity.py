@@ -326,6 +326,34 @@ def test_upload_download_roundtrip():
         assert ei.value.code == 1
 
 
+def test_refused_upload_leaves_the_handle_without_a_state():
+    """A re-upload that is refused after it began to overwrite the device
+    state (non-TT l: the fields are already in place when the amplitudes are
+    checked) must not leave a half-new state to step on: steps report
+    GABE_ERR_STATE until an upload succeeds, and the handle then runs as a
+    fresh one does."""
+    cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=1)
+    st = po.init_state(cfg)
+    po.step(st, 6)
+    bad = st.copy()
+    bad.l[0] = np.random.default_rng(1).standard_normal(bad.l[0].shape) * 1e-9
+    with _lattice(cfg) as lat, _lattice(cfg) as ref:
+        _upload(lat, st)
+        lat.step(2)
+        with pytest.raises(gb.GabeError) as ei:
+            _upload(lat, bad)
+        assert ei.value.code == 1
+        with pytest.raises(gb.GabeError) as ei:
+            lat.step(1)
+        assert ei.value.code == 7
+        _upload(lat, st)
+        _upload(ref, st)
+        lat.step(3)
+        ref.step(3)
+        for got, want in zip(lat.download_state(), ref.download_state()):
+            np.testing.assert_array_equal(got, want)
+
+
 def test_nonfinite_state_is_reported():
     cfg = po.Config(N=16, model=po.MODEL_LPHI4, gws=0)
     st = po.init_state(cfg)
