@@ -487,6 +487,8 @@ class Ensemble:
         self._check(_ens_lib().gabe_ensemble_init(self._h))
 
     def upload(self, lat: int, field0, dfield0, *, a0: float = 1.0, adot0: float):
+        """Replaces lattice `lat`'s state (gabe_ensemble_upload); init() must
+        have drawn every lattice's state first (GabeError GABE_ERR_STATE)."""
         n = int(self.N[lat])
         f = np.ascontiguousarray(field0, dtype=np.float64).reshape(2, n, n, n)
         d = np.ascontiguousarray(dfield0, dtype=np.float64).reshape(2, n, n, n)

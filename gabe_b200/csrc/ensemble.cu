@@ -463,7 +463,12 @@ int gabe_ensemble_init(gabe_ensemble *e) {
 
 int gabe_ensemble_upload(gabe_ensemble *e, int lat, const double *field0, const double *dfield0, double a0,
                          double adot0) {
-    if (!e || lat < 0 || lat >= e->nlat || !field0 || !dfield0 || !(a0 > 0)) return GABE_ERR_PARAM;
+    if (!e || lat < 0 || lat >= e->nlat || !field0 || !dfield0 || !(a0 > 0) || !std::isfinite(a0) ||
+        !std::isfinite(adot0))
+        return GABE_ERR_PARAM;
+    // an upload replaces one lattice's state; the others must hold one already, or the ensemble would step
+    // uninitialised lattices beside it
+    if (!e->ready) return eset(e, GABE_ERR_STATE, "upload before gabe_ensemble_init (it draws every lattice's state)");
     ECK(e, cudaSetDevice(e->dev));
     const EnsLat &Lt = e->h_lat[lat];
     const size_t n3 = (size_t)Lt.N * Lt.N * Lt.N;

@@ -352,6 +352,7 @@ int gabe_slab_upload(gabe_slab *s, const double *field0, const double *dfield0, 
     if (s->f32 && !mean) return serr(s, GABE_ERR_PARAM, "FP32 storage needs the whole lattice's means");
     if (!(a0 > 0) || !std::isfinite(a0) || !std::isfinite(adot0)) return serr(s, GABE_ERR_PARAM, "bad a0/adot0");
     SCK(s, cudaSetDevice(s->dev));
+    s->uploaded = false;  // until the whole slab is in place
     DevScalars d{};
     d.a[0] = a0;
     d.adot[0] = adot0;

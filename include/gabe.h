@@ -331,7 +331,8 @@ int gabe_ensemble_destroy(gabe_ensemble *e);
 int gabe_ensemble_init(gabe_ensemble *e);
 
 /* Replaces lattice `lat`'s state (FP64 host arrays in the reference
- * layout; h = l = 0). */
+ * layout; h = l = 0).  The ensemble must hold a state already
+ * (gabe_ensemble_init): GABE_ERR_STATE before it. */
 int gabe_ensemble_upload(gabe_ensemble *e, int lat, const double *field0, const double *dfield0, double a0,
                          double adot0);
 
