@@ -8,6 +8,7 @@ default contraction.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -62,16 +63,24 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     if not force and up_to_date():
         return LIB
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
     nv = nvcc()
-    for src, extra in UNITS:
+
+    def compile_unit(unit):
+        src, extra = unit
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         cmd = [nv, *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_v:
             cmd += ["-Xptxas", "-v"]
+        return obj, cmd, subprocess.run(cmd, capture_output=True, text=True)
+
+    # the units are independent: compile them side by side, report in order
+    workers = max(1, min(len(UNITS), os.cpu_count() or 1))
+    with concurrent.futures.ThreadPoolExecutor(max_workers=workers) as pool:
+        results = list(pool.map(compile_unit, UNITS))
+    objs = []
+    for (src, _), (obj, cmd, r) in zip(UNITS, results):
         if verbose:
             print(" ".join(cmd), flush=True)
-        r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed on {src}:\n{r.stdout}\n{r.stderr}")
         if ptxas_v or verbose:
