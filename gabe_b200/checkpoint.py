@@ -46,17 +46,18 @@ def read_state(path: str) -> dict:
     [nflds][N][N][N] and, with GWs, h, l [12][N][N][N/2+1]."""
     hd = read_header(path)
     N, nfl = hd["N"], hd["nflds"]
-    nf, ng = nfl * N ** 3, 12 * N * N * (N // 2 + 1)
     out = dict(hd)
+    shapes = [("field", (nfl, N, N, N)), ("dfield", (nfl, N, N, N))]
+    if hd["gws"]:
+        shapes += [("h", (12, N, N, N // 2 + 1)), ("l", (12, N, N, N // 2 + 1))]
     with open(path, "rb") as fh:
         fh.seek(_HDR.size)
-        out["field"] = np.fromfile(fh, np.float64, nf).reshape(nfl, N, N, N)
-        out["dfield"] = np.fromfile(fh, np.float64, nf).reshape(nfl, N, N, N)
-        if hd["gws"]:
-            out["h"] = np.fromfile(fh, np.float64, ng).reshape(12, N, N, N // 2 + 1)
-            out["l"] = np.fromfile(fh, np.float64, ng).reshape(12, N, N, N // 2 + 1)
-    if out["field"].size != nf or out["dfield"].size != nf:
-        raise ValueError(f"{path} is truncated")
+        for name, shape in shapes:
+            want = int(np.prod(shape))
+            arr = np.fromfile(fh, np.float64, want)
+            if arr.size != want:
+                raise ValueError(f"{path} is truncated: {name} holds {arr.size} of {want} values")
+            out[name] = arr.reshape(shape)
     return out
 
 

@@ -54,3 +54,17 @@ def test_rejects_files_that_are_not_dumps(tmp_path):
     p.write_bytes(b"\0" * 300)
     with pytest.raises(ValueError):
         ck.read_header(str(p))
+
+
+@pytest.mark.parametrize("cut", [8, 8 * 8 ** 3 * 2 + 8, 8 * 8 ** 3 * 4 + 8 * 12 * 8 * 8 * 5 + 8])
+def test_truncated_dumps_name_the_short_array(tmp_path, cut):
+    """A dump cut short anywhere in its payload (in field, in dfield, in l)
+    is refused with the array that ran out, not read as a shorter state."""
+    cfg = po.Config(N=8, model=po.MODEL_LPHI4, gws=1)
+    path = str(tmp_path / "d.bin")
+    po.write_dump(path, po.init_state(cfg))
+    with open(path, "r+b") as fh:
+        fh.truncate(256 + cut)
+    which = "field" if cut < 8 * 8 ** 3 * 2 else "dfield" if cut < 8 * 8 ** 3 * 4 else "l"
+    with pytest.raises(ValueError, match=f"truncated: {which} holds"):
+        ck.read_state(path)
