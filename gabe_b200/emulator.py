@@ -14,7 +14,8 @@ sweep needs around it:
   it is asked for;
 * `members` networks from different seeds are trained on the same data; the
   spread of their predictions flags parameter points the emulator should not
-  be trusted on, which the lattice then re-runs (`screen`).
+  be trusted on, which the lattice then re-runs (`screen`; `screened_sweep`
+  answers a whole sweep that way, the flagged points from the lattice).
 """
 from __future__ import annotations
 
@@ -399,6 +400,49 @@ def ensemble_samples(N, g, amp, seeds, steps: int, every: int, nlog: int = 64, d
     targets = logs.reshape(T * nlat, 3 * nlog)
     lat = np.tile(np.arange(nlat), T)
     return feats, targets, lat, ms
+
+
+def output_times(steps: int, every: int, dt: float = 0.01) -> np.ndarray:
+    """The times at which evolve_and_record reads the spectra: step 0 and
+    every `every` steps up to `steps`."""
+    return np.arange(0, steps + 1, every) * dt
+
+
+def screened_sweep(emu, threshold: float, N, g, amp, seeds, steps: int, every: int, nlog: int = 64,
+                   dt: float = 0.01, valid_mask=None, runner=None):
+    """Answers a parameter sweep with the emulator as screen and the lattice
+    as fallback: every (point, output time) is predicted by the emulator,
+    and every point whose largest member spread over its output times and
+    (valid) bins exceeds `threshold` dex is evolved on the lattice instead
+    and answered by it.
+
+    N, g, amp, seeds: per point (lattice size, g^2/lambda, amplitude
+    multiplier, seed).  valid_mask: None, [3 nlog] or [points, 3 nlog] bins
+    that count for the spread.  runner(N, g, amp, seeds, steps, every, nlog,
+    dt=dt) -> (features, targets, lattice, ms) in ensemble_samples' row order
+    (time-major, point-minor); by default one batched ensemble of the flagged
+    points.  Returns (answers [T * points, 3 nlog] in the same row order, NaN
+    where a flagged point's log bin holds no modes; flagged [points]; spread
+    [points])."""
+    N, g, amp, seeds = (np.asarray(v) for v in (N, g, amp, seeds))
+    P = len(g)
+    taus = output_times(steps, every, dt)
+    T = len(taus)
+    feats = Emulator.features(np.tile(g, T), np.tile(amp, T), np.repeat(taus, P), np.tile(N, T))
+    mean, spread = emu.predict(feats)
+    spread = spread.reshape(T, P, -1)
+    if valid_mask is not None:
+        vm = np.asarray(valid_mask, dtype=bool)
+        spread = np.where(vm if vm.ndim == 1 else vm[None, :, :], spread, 0.0)
+    pt_spread = spread.max(axis=(0, 2))
+    flagged = pt_spread > threshold
+    answers = np.array(mean, dtype=np.float64).reshape(T, P, -1)
+    idx = np.flatnonzero(flagged)
+    if len(idx):
+        run = runner if runner is not None else ensemble_samples
+        _, y, _, _ = run(N[idx], g[idx], amp[idx], seeds[idx], steps, every, nlog, dt=dt)
+        answers[:, idx, :] = np.asarray(y, dtype=np.float64).reshape(T, len(idx), -1)
+    return answers.reshape(T * P, -1), flagged, pt_spread
 
 
 def run_sweep(*, nlat=256, ensembles=2, steps=2000, every=50, nlog=64, holdout=32, holdout_N=64, members=4,
