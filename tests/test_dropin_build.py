@@ -1,0 +1,26 @@
+"""The drop-in translation unit (gabe_b200/host/gabe_dropin.cpp) compiles
+against the reference's headers for every combination of its compile-time
+knobs: GABE_B200_MODEL (0: the shipped m^2 phi^2 + g^2 phi^2 chi^2 model,
+1: lambda phi^4), GABE_B200_PRECISION (0 FP64, 1 FP32 storage) and
+calc_gws.  The GPU tests build and run two of these programs; this check
+covers the combinations they do not run.  Compile only (`make -C oracle
+dropin-knobs`); skipped where the reference tree is not mounted."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_dropin_compiles_for_every_knob_combination():
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "dropin-knobs"], capture_output=True, text=True,
+                       timeout=600)
+    if "reference tree not found" in r.stdout + r.stderr:
+        pytest.skip("the reference tree is not mounted here")
+    assert r.returncode == 0, (r.stdout + r.stderr)[-3000:]
+    out = os.path.join(ROOT, "oracle", "_ref", "dropin_knobs")
+    for m in (0, 1):
+        for p in (0, 1):
+            for g in (0, 1):
+                assert os.path.getsize(os.path.join(out, f"m{m}_p{p}_g{g}.o")) > 0
