@@ -23,6 +23,10 @@
  *                        gsq from g2parameters.h), 1: lambda phi^4 in program
  *                        units with constants lam_pr, gsq_pr
  *   GABE_B200_PRECISION  0: FP64 (default), 1: FP32 fluctuation storage
+ *   fftw_flag (the tree's g2parameters.h) 1: long double host arrays; the
+ *                        state crosses the boundary as doubles, the device
+ *                        computes in FP64, and the files are printed with
+ *                        %Le as the reference prints them
  *
  * Checkpoint and restart (run-time, environment; the reference has neither):
  *   GABE_B200_CHECKPOINT_EVERY=n and GABE_B200_CHECKPOINT=<file> write a
@@ -34,12 +38,13 @@
  *   so the run continues the saved one (bit for bit from a checkpoint of
  *   the same build and precision).
  */
+#include <cstdlib>
+#include <string>
+#include <vector>
+
 #include "gabe.h"
 #include "gabe_dump.h"
 #include "g2header.h"
-
-#include <cstdlib>
-#include <string>
 
 #ifndef GABE_B200_MODEL
 #define GABE_B200_MODEL 0
@@ -114,12 +119,36 @@ void ensure_device_state()
                (long long)hd.step, (double)t);
         return;
     }
+#if fftw_flag == 1
+    // long double host arrays: the library computes in FP64, so the state
+    // crosses the boundary as doubles
+    const size_t nf = (size_t)nflds * N * N * N;
+    std::vector<double> f0(nf), d0(nf), hv, lv;
+    const gNum *fs = &field[0][0][0][0][0], *ds = &dfield[0][0][0][0][0];
+    for (size_t q = 0; q < nf; q++) {
+        f0[q] = (double)fs[q];
+        d0[q] = (double)ds[q];
+    }
+#if calc_gws == 1
+    const size_t ng = (size_t)12 * N * N * (N / 2 + 1);
+    hv.resize(ng);
+    lv.resize(ng);
+    const gNum *hs = &h[0][0][0][0][0], *ls = &l[0][0][0][0][0];
+    for (size_t q = 0; q < ng; q++) {
+        hv[q] = (double)hs[q];
+        lv[q] = (double)ls[q];
+    }
+#endif
+    rc = gabe_upload_state(g_gpu, f0.data(), d0.data(), hv.empty() ? nullptr : hv.data(),
+                           lv.empty() ? nullptr : lv.data(), (double)a[0], (double)adot[0]);
+#else
     const double *h0 = nullptr, *l0 = nullptr;
 #if calc_gws == 1
     h0 = &h[0][0][0][0][0];
     l0 = &l[0][0][0][0][0];
 #endif
     rc = gabe_upload_state(g_gpu, &field[0][0][0][0][0], &dfield[0][0][0][0][0], h0, l0, a[0], adot[0]);
+#endif
     if (rc != GABE_OK) gabe_die("gabe_upload_state", rc);
 }
 
@@ -276,8 +305,13 @@ void specOut(int first)
         exit(1);
     }
     for (int b = 0; b < nb; b++) {
+#if fftw_flag == 1
+        fprintf(f, "%Le", (long double)tab[b * nc]);
+        for (int c = 1; c < nc; c++) fprintf(f, " %Le", (long double)tab[b * nc + c]);
+#else
         fprintf(f, "%e", tab[b * nc]);
         for (int c = 1; c < nc; c++) fprintf(f, " %e", tab[b * nc + c]);
+#endif
         fprintf(f, "\n");
     }
     fclose(f);

@@ -21,6 +21,7 @@
  *   GABE_EXPANSION expansion_type                     (reference :62)
  *   GABE_FULL_RAND field_full_rand                    (reference :72)
  *   GABE_SPEC_CUT, GABE_SPEC_SMOOTH  spec_cut_off, spec_smooth (reference :73-74)
+ *   GABE_FFTW_FLAG fftw_flag, 1 = long double         (reference :19-38)
  *                 run length and output knobs (reference :60,80,84,86) for
  *                 builds that use the reference's own g2main.cpp/g2output.cpp
  *
@@ -29,8 +30,21 @@
  */
 #include <math.h>
 
-#define fftw_flag 0
+#ifndef GABE_FFTW_FLAG
+#define GABE_FFTW_FLAG 0
+#endif
+#define fftw_flag GABE_FFTW_FLAG
+#if fftw_flag == 1
+/* long double state (reference :19-38); only the compile check of the
+ * drop-in translation unit builds this form: the FFT shim is double only */
+#define gNum long double
+#define exp expl
+#define sqrt sqrtl
+#define cbrt cbrtl
+#define log logl
+#else
 #define gNum double
+#endif
 
 #ifndef GABE_N
 #define GABE_N 64

@@ -2,9 +2,11 @@
 against the reference's headers for every combination of its compile-time
 knobs: GABE_B200_MODEL (0: the shipped m^2 phi^2 + g^2 phi^2 chi^2 model,
 1: lambda phi^4), GABE_B200_PRECISION (0 FP64, 1 FP32 storage) and
-calc_gws.  The GPU tests build and run two of these programs; this check
-covers the combinations they do not run.  Compile only (`make -C oracle
-dropin-knobs`); skipped where the reference tree is not mounted."""
+calc_gws, and with the reference's long double state (fftw_flag 1, whose
+arrays cross the boundary as doubles).  The GPU tests build and run two of
+these programs; this check covers the combinations they do not run.
+Compile only (`make -C oracle dropin-knobs`); skipped where the reference
+tree is not mounted."""
 import os
 import subprocess
 
@@ -24,3 +26,5 @@ def test_dropin_compiles_for_every_knob_combination():
         for p in (0, 1):
             for g in (0, 1):
                 assert os.path.getsize(os.path.join(out, f"m{m}_p{p}_g{g}.o")) > 0
+    for name in ("m1_p0_g1_ld", "m0_p1_g0_ld"):
+        assert os.path.getsize(os.path.join(out, name + ".o")) > 0
