@@ -44,3 +44,25 @@ def residual_from_rows(rows) -> np.ndarray:
         raise ValueError(f"rows need the {len(TIME_COLUMNS)} columns {TIME_COLUMNS}")
     t, a, adot, _, kin, pot, grad, rho = r.T
     return continuity_residual(t, a, adot, kin, pot, grad, rho)
+
+
+def main(argv=None) -> dict:
+    """python -m gabe_b200.energy <slices_time.dat>: prints, as one JSON
+    line, the number of rows, the last time, eps at the last time and the
+    largest eps of the run."""
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="energy-conservation error of a run from its slices_time.dat")
+    ap.add_argument("path", help="slices_time.dat written by the reference or by the drop-in")
+    args = ap.parse_args(argv)
+    rows = np.loadtxt(args.path, ndmin=2)
+    eps = residual_from_rows(rows)
+    out = {"rows": int(rows.shape[0]), "t_end": float(rows[-1, 0]), "eps_end": float(eps[-1]),
+           "eps_max": float(eps.max())}
+    print(json.dumps(out))
+    return out
+
+
+if __name__ == "__main__":
+    main()

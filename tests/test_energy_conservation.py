@@ -53,3 +53,25 @@ def test_bad_series_are_rejected():
                                    [1.0, 1.0])
     with pytest.raises(ValueError):
         energy.residual_from_rows(np.zeros((3, 7)))
+
+
+def test_command_line_check_on_the_reference_programs_own_file(tmp_path, capsys):
+    """`python -m gabe_b200.energy slices_time.dat` on the file the whole
+    reference program writes (g2main.cpp and g2output.cpp, built by
+    `make -C oracle full`): one row per output slice, eps(t0) = 0, and the
+    same eps as the library function on the same rows."""
+    import json
+    import os
+
+    binary = os.path.join(po.REF_DIR, "reffull_m1_n32_g0_p0")
+    if not os.path.exists(binary):
+        pytest.skip("built by `make -C oracle full` where the reference is mounted")
+    po.run_ref(binary, [], str(tmp_path), threads=1)
+    path = str(tmp_path / "slices" / "slices_time.dat")
+    out = energy.main([path])
+    assert json.loads(capsys.readouterr().out.strip().splitlines()[-1]) == out
+    rows = np.loadtxt(path, ndmin=2)
+    eps = energy.residual_from_rows(rows)
+    assert out["rows"] == rows.shape[0] >= 2 and eps[0] == 0.0
+    assert out["eps_end"] == eps[-1] and out["eps_max"] == eps.max()
+    assert 0.0 < out["eps_max"] < 1e-2
